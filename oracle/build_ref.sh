@@ -1,0 +1,30 @@
+#!/bin/sh
+# Builds the reference's own CPU implementation (trotter-suzuki-mpi 1.6.2,
+# read in place from its source tree, never copied) together with
+# oracle/ref_driver.cpp into oracle/_ref/.  Test infrastructure only.
+#
+#   libtsref.so       -O2 -fopenmp               parity oracle (no FMA contraction
+#                                                 without -march, as in a plain build)
+#   libtsref_fast.so  -Ofast -march=x86-64-v3     the reference's own optimisation
+#                     -fopenmp                    flags (configure.ac:37 uses -Ofast
+#                                                 -march=native; x86-64-v3 keeps the
+#                                                 binary runnable on another host CPU)
+#
+# Usage: oracle/build_ref.sh [reference_root]   (default /root/reference)
+set -eu
+REF=${1:-/root/reference}
+HERE=$(cd "$(dirname "$0")" && pwd)
+OUT="$HERE/_ref"
+SRC="$REF/src"
+if [ ! -f "$SRC/cpukernel.cpp" ]; then
+    echo "reference sources not found under $SRC" >&2
+    exit 1
+fi
+mkdir -p "$OUT"
+FILES="$SRC/common.cpp $SRC/cpukernel.cpp $SRC/cpucartesian.cpp $SRC/cpucylindrical.cpp $SRC/model.cpp $SRC/solver.cpp $HERE/ref_driver.cpp"
+CXX=${TSREF_CXX:-g++}
+$CXX -O2 -fopenmp -fPIC -shared -w -I"$SRC" $FILES -o "$OUT/libtsref.so.tmp"
+mv "$OUT/libtsref.so.tmp" "$OUT/libtsref.so"
+$CXX -Ofast -march=x86-64-v3 -fopenmp -fPIC -shared -w -I"$SRC" $FILES -o "$OUT/libtsref_fast.so.tmp"
+mv "$OUT/libtsref_fast.so.tmp" "$OUT/libtsref_fast.so"
+echo "built $OUT/libtsref.so $OUT/libtsref_fast.so"

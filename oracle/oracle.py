@@ -1,0 +1,262 @@
+"""ctypes binding of the C restatement in oracle/ts_oracle.c (test infrastructure).
+
+The restatement is the checker for the B200 kernels: tests/ and
+__graft_entry__.smoke() call it on the same seeded inputs as the CUDA path,
+bench.py times it as the CPU baseline when the compiled reference is absent.
+Nothing in the product imports this module.
+
+Geometry and set-up helpers below restate, in numpy with the same operation
+order, the reference's lattice geometry (src/common.cpp:83-102,
+src/model.cpp:103-158), coordinates (src/common.cpp:45-65), GaussianState
+(src/model.cpp:692-714) and HarmonicPotential (src/model.cpp:920-926).
+"""
+import ctypes as C
+import math
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libts_oracle.so")
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("W", C.c_int), ("H", C.c_int),
+        ("ix0", C.c_int), ("ix1", C.c_int), ("iy0", C.c_int), ("iy1", C.c_int),
+        ("periodic_x", C.c_int), ("periodic_y", C.c_int),
+        ("halo_x", C.c_int), ("halo_y", C.c_int),
+        ("imag_time", C.c_int),
+        ("aH", C.c_double), ("bH", C.c_double), ("aV", C.c_double), ("bV", C.c_double),
+        ("coupling", C.c_double), ("lhy_coupling", C.c_double),
+        ("alpha_x", C.c_double), ("alpha_y", C.c_double),
+        ("rot_off_x", C.c_int), ("rot_off_y", C.c_int),
+        ("delta_x", C.c_double), ("delta_y", C.c_double),
+        ("norm0", C.c_double),
+    ]
+
+
+class Geometry(C.Structure):
+    _fields_ = [
+        ("W", C.c_int), ("H", C.c_int), ("ix0", C.c_int), ("ix1", C.c_int),
+        ("iy0", C.c_int), ("iy1", C.c_int),
+        ("start_x", C.c_int), ("start_y", C.c_int),
+        ("global_no_halo_dim_x", C.c_int), ("global_no_halo_dim_y", C.c_int),
+        ("delta_x", C.c_double), ("delta_y", C.c_double),
+        ("length_x", C.c_double), ("length_y", C.c_double),
+    ]
+
+
+class Energies(C.Structure):
+    _fields_ = [(n, C.c_double) for n in
+                ("total", "kinetic", "potential", "rotational", "intra", "lhy", "norm2")]
+
+
+class Expectations(C.Structure):
+    _fields_ = [(n, C.c_double) for n in
+                ("norm2", "mean_x", "mean_xx", "mean_y", "mean_yy", "mean_px", "mean_pxpx",
+                 "mean_py", "mean_pypy", "mean_lz")]
+
+
+def build():
+    """Compile the restatement (gcc, no FMA contraction)."""
+    src = os.path.join(HERE, "ts_oracle.c")
+    tmp = LIB_PATH + ".tmp"
+    subprocess.check_call(["gcc", "-O2", "-ffp-contract=off", "-fPIC", "-shared", "-std=c99",
+                           src, "-o", tmp, "-lm"])
+    os.replace(tmp, LIB_PATH)
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        dp = C.c_void_p
+        L.tso_init_constants.argtypes = [C.POINTER(Params)] + [C.c_double] * 7
+        L.tso_exp_table.argtypes = [C.c_int, C.c_double, dp, C.c_size_t, dp, dp]
+        L.tso_full_step.argtypes = [C.POINTER(Params), dp, dp, dp, dp]
+        L.tso_halo_exchange.argtypes = [C.POINTER(Params), dp, dp]
+        L.tso_squared_norm.argtypes = [C.POINTER(Params), dp, dp]
+        L.tso_squared_norm.restype = C.c_double
+        L.tso_evolve.argtypes = [C.POINTER(Params), dp, dp, dp, dp, C.c_int]
+        L.tso_energies.argtypes = [C.POINTER(Geometry), dp, dp, dp, C.c_double, C.c_double,
+                                   C.c_double, C.c_double, C.POINTER(Energies)]
+        L.tso_expectations.argtypes = [C.POINTER(Geometry), dp, dp, C.POINTER(Expectations)]
+        _lib = L
+    return _lib
+
+
+# --------------------------------------------------------------------------
+# Reference geometry, restated (single process).
+# --------------------------------------------------------------------------
+def calculate_borders(length, halo, periodic):
+    """src/common.cpp:83-102 with one process (coord 0, dim 1)."""
+    inner = int(math.ceil(float(length) / 1.0))
+    inner_start = 0
+    start = inner_start - halo if periodic else 0
+    end = inner_start + (inner + halo)
+    if end > length:
+        end = length + halo if periodic else length
+    inner_end = end - halo if periodic else (end if end == length else end - halo)
+    return start, end, inner_start, inner_end
+
+
+class Lattice:
+    """Geometry of a reference Lattice2D / Lattice1D tile (src/model.cpp:32-158)."""
+
+    def __init__(self, dim_x, length_x, dim_y=None, length_y=None, periodic_x=False,
+                 periodic_y=False, angular_velocity=0.0, one_d=False):
+        if one_d:
+            dim_y, length_y = 1, 0.0
+            self.delta_x = length_x / float(dim_x)
+            self.delta_y = 1.0
+            self.halo_x, self.halo_y = 4, 0
+            periodic_y = False
+        else:
+            dim_y = dim_x if dim_y is None else dim_y
+            length_y = length_x if length_y is None else length_y
+            self.delta_x = length_x / float(dim_x)
+            self.delta_y = length_y / float(dim_y)
+            self.halo_x = self.halo_y = 4 if angular_velocity == 0.0 else 8
+        self.one_d = one_d
+        self.length_x, self.length_y = length_x, length_y
+        self.periodic_x, self.periodic_y = bool(periodic_x), bool(periodic_y)
+        self.global_no_halo_dim_x, self.global_no_halo_dim_y = dim_x, dim_y
+        self.start_x, self.end_x, self.inner_start_x, self.inner_end_x = calculate_borders(
+            dim_x, self.halo_x, periodic_x)
+        if one_d:
+            self.start_y, self.end_y, self.inner_start_y, self.inner_end_y = 0, 1, 0, 1
+        else:
+            self.start_y, self.end_y, self.inner_start_y, self.inner_end_y = calculate_borders(
+                dim_y, self.halo_y, periodic_y)
+        self.dim_x = self.end_x - self.start_x
+        self.dim_y = self.end_y - self.start_y
+
+    @property
+    def shape(self):
+        return (self.dim_y, self.dim_x)
+
+    def inner(self):
+        return (self.inner_start_x - self.start_x, self.inner_end_x - self.start_x,
+                self.inner_start_y - self.start_y, self.inner_end_y - self.start_y)
+
+    def geometry(self):
+        g = Geometry()
+        g.W, g.H = self.dim_x, self.dim_y
+        g.ix0, g.ix1, g.iy0, g.iy1 = self.inner()
+        g.start_x, g.start_y = self.start_x, self.start_y
+        g.global_no_halo_dim_x = self.global_no_halo_dim_x
+        g.global_no_halo_dim_y = self.global_no_halo_dim_y
+        g.delta_x, g.delta_y = self.delta_x, self.delta_y
+        g.length_x, g.length_y = self.length_x, self.length_y
+        return g
+
+    def coordinates(self):
+        """(x, y) arrays of shape (dim_y, dim_x), src/common.cpp:45-65."""
+        xi = np.arange(self.dim_x, dtype=np.float64)
+        yi = np.arange(self.dim_y, dtype=np.float64)
+        idx = self.start_x * self.delta_x + 0.5 * self.delta_x + xi * self.delta_x
+        idy = self.start_y * self.delta_y + 0.5 * self.delta_y + yi * self.delta_y
+        x_c = self.global_no_halo_dim_x * self.delta_x * 0.5
+        y_c = self.global_no_halo_dim_y * self.delta_y * 0.5
+        idx = np.where(idx - x_c < -self.length_x * 0.5, idx + self.length_x, idx)
+        idx = np.where(idx - x_c > self.length_x * 0.5, idx - self.length_x, idx)
+        idy = np.where(idy - y_c < -self.length_y * 0.5, idy + self.length_y, idy)
+        idy = np.where(idy - y_c > self.length_y * 0.5, idy - self.length_y, idy)
+        X = np.broadcast_to((idx - x_c)[None, :], self.shape)
+        Y = np.broadcast_to((idy - y_c)[:, None], self.shape)
+        return np.ascontiguousarray(X), np.ascontiguousarray(Y)
+
+    def harmonic(self, omega_x, omega_y, mass=1.0, mean_x=0.0, mean_y=0.0):
+        """HarmonicPotential::get_value over the tile (src/model.cpp:920-926)."""
+        X, Y = self.coordinates()
+        xr = X - mean_x
+        yr = Y - mean_y
+        return 0.5 * mass * (omega_x * omega_x * xr * xr + omega_y * omega_y * yr * yr)
+
+    def params(self, delta_t, imag_time=False, mass=1.0, coupling=0.0, lhy=0.0,
+               angular_velocity=0.0, rot_coord=(0.0, 0.0), norm0=0.0):
+        p = Params()
+        p.W, p.H = self.dim_x, self.dim_y
+        p.ix0, p.ix1, p.iy0, p.iy1 = self.inner()
+        p.periodic_x, p.periodic_y = int(self.periodic_x), int(self.periodic_y)
+        p.halo_x, p.halo_y = self.halo_x, self.halo_y
+        p.imag_time = int(imag_time)
+        lib().tso_init_constants(C.byref(p), delta_t, mass, coupling, lhy, angular_velocity,
+                                 self.delta_x, self.delta_y)
+        # Hamiltonian rotation centre in lattice units (src/model.cpp:950-956)
+        rcx = (self.global_no_halo_dim_x) * 0.5 + rot_coord[0] / self.delta_x
+        rcy = (self.global_no_halo_dim_y) * 0.5 + rot_coord[1] / self.delta_y
+        p.rot_off_x = int(self.start_x - rcx)
+        p.rot_off_y = int(self.start_y - rcy)
+        p.norm0 = norm0
+        return p
+
+
+def _ptr(a):
+    return a.ctypes.data
+
+
+def exp_table(V, delta_t, imag_time):
+    V = np.ascontiguousarray(V, np.float64)
+    re = np.empty_like(V)
+    im = np.empty_like(V)
+    lib().tso_exp_table(int(imag_time), delta_t, _ptr(V), V.size, _ptr(re), _ptr(im))
+    return re, im
+
+
+def evolve(params, psi, pot_re, pot_im, iterations):
+    """Evolve a tile in place semantics; returns the new complex tile."""
+    re = np.ascontiguousarray(np.real(psi), np.float64).copy()
+    im = np.ascontiguousarray(np.imag(psi), np.float64).copy()
+    pr = np.ascontiguousarray(pot_re, np.float64)
+    pi = np.ascontiguousarray(pot_im, np.float64)
+    lib().tso_evolve(C.byref(params), _ptr(re), _ptr(im), _ptr(pr), _ptr(pi), int(iterations))
+    return re + 1j * im
+
+
+def squared_norm(params, psi):
+    re = np.ascontiguousarray(np.real(psi), np.float64)
+    im = np.ascontiguousarray(np.imag(psi), np.float64)
+    return lib().tso_squared_norm(C.byref(params), _ptr(re), _ptr(im))
+
+
+def energies(lattice, psi, V, mass=1.0, coupling=0.0, lhy=0.0, omega=0.0):
+    re = np.ascontiguousarray(np.real(psi), np.float64)
+    im = np.ascontiguousarray(np.imag(psi), np.float64)
+    V = np.ascontiguousarray(V, np.float64)
+    out = Energies()
+    g = lattice.geometry()
+    lib().tso_energies(C.byref(g), _ptr(re), _ptr(im), _ptr(V), mass, coupling, lhy, omega,
+                       C.byref(out))
+    return {n: getattr(out, n) for n, _ in Energies._fields_}
+
+
+def expectations(lattice, psi):
+    re = np.ascontiguousarray(np.real(psi), np.float64)
+    im = np.ascontiguousarray(np.imag(psi), np.float64)
+    out = Expectations()
+    g = lattice.geometry()
+    lib().tso_expectations(C.byref(g), _ptr(re), _ptr(im), C.byref(out))
+    return {n: getattr(out, n) for n, _ in Expectations._fields_}
+
+
+def gaussian(lattice, omega_x, omega_y=-1.0, mean_x=0.0, mean_y=0.0, norm=1.0, phase=0.0):
+    """GaussianState values over the tile (src/model.cpp:692-714).
+
+    std::pow(v, 2.0) is evaluated as v*v by glibc for an exact exponent of 2.
+    """
+    if omega_y == -1.0:
+        omega_y = omega_x
+    X, Y = lattice.coordinates()
+    amp = math.sqrt(norm * math.sqrt(omega_x * omega_y) / math.pi)
+    dx = X - mean_x
+    dy = Y - mean_y
+    val = amp * np.exp(-(omega_x * (dx * dx) + omega_y * (dy * dy)) * 0.5)
+    return val * complex(math.cos(phase), math.sin(phase))

@@ -1,0 +1,426 @@
+/*
+ * ts_oracle.c -- CPU restatement of the reference's Trotter-Suzuki evolution
+ * path.  TEST INFRASTRUCTURE ONLY: tests/, __graft_entry__.smoke() and the
+ * CPU-baseline leg of bench.py load it as a checker.  No product code path
+ * links or calls it.
+ *
+ * It restates, in plain C99 double arithmetic with the same operation order
+ * per cell, the single-component path of trotter-suzuki-mpi 1.6.2:
+ *   - pair sweeps            src/cpucartesian.cpp:4-70
+ *   - potential / GPE / LHY   src/cpucartesian.cpp:73-138
+ *   - rotating frame          src/cpucartesian.cpp:141-262
+ *   - the Strang sequence     src/cpukernel.cpp:22-92
+ *   - step constants          src/cpukernel.cpp:185-217
+ *   - periodic halo exchange  src/cpukernel.cpp:691-747 (single process)
+ *   - imaginary-time renorm   src/cpukernel.cpp:526-570
+ *   - evolve loop             src/solver.cpp:150-242
+ *   - energies                src/solver.cpp:244-564 (single component)
+ *   - expectation values      src/model.cpp:385-536
+ *
+ * The reference evolves the tile in 128x128 cache blocks with a 4 (8 with
+ * rotation) cell overlap; every written cell lies at least that far from an
+ * interior block edge, so the blocked result equals one sweep over the whole
+ * tile.  This restatement sweeps the whole tile at once.  Two places where
+ * the reference's blocking itself is defective are not restated (see the
+ * project design notes): tile widths 128+120q (112q with rotation) leave a
+ * band of columns unwritten, and the periodic x-halo copy can read columns
+ * that the current step has not written yet.
+ *
+ * Compile with -ffp-contract=off so that no multiply-add is fused (the
+ * reference's plain -O2 x86-64 build has no FMA instructions either).
+ */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "ts_oracle.h"
+
+/* ---- pair sweeps (src/cpucartesian.cpp:4-70) ------------------------- */
+
+/* Pair (i, j): real time uses [[a, ib], [ib, a]], imaginary time [[a, b], [b, a]]. */
+static inline void pair_real(double a, double b, double *re, double *im, size_t i, size_t j) {
+    double tr = re[i], ti = im[i];
+    re[i] = a * tr - b * im[j];
+    im[i] = a * ti + b * re[j];
+    re[j] = a * re[j] - b * ti;
+    im[j] = a * im[j] + b * tr;
+}
+
+static inline void pair_imag(double a, double b, double *re, double *im, size_t i, size_t j) {
+    double tr = re[i], ti = im[i];
+    re[i] = a * tr + b * re[j];
+    im[i] = a * ti + b * im[j];
+    re[j] = a * re[j] + b * tr;
+    im[j] = a * im[j] + b * ti;
+}
+
+/* Vertical sweep s: pairs (x,y)-(x,y+1) with (x+y)%2 == s and y+1 < H. */
+static void sweep_vertical(const tso_params *p, int s, double a, double b, double *re, double *im) {
+    const size_t W = (size_t)p->W;
+    for (int y = 0; y + 1 < p->H; ++y)
+        for (int x = (s + y) & 1; x < p->W; x += 2) {
+            size_t i = (size_t)y * W + x;
+            if (p->imag_time) pair_imag(a, b, re, im, i, i + W);
+            else pair_real(a, b, re, im, i, i + W);
+        }
+}
+
+/* Horizontal sweep s: pairs (x,y)-(x+1,y) with (x+y)%2 == s and x+1 < W. */
+static void sweep_horizontal(const tso_params *p, int s, double a, double b, double *re, double *im) {
+    const size_t W = (size_t)p->W;
+    for (int y = 0; y < p->H; ++y)
+        for (int x = (s + y) & 1; x + 1 < p->W; x += 2) {
+            size_t i = (size_t)y * W + x;
+            if (p->imag_time) pair_imag(a, b, re, im, i, i + 1);
+            else pair_real(a, b, re, im, i, i + 1);
+        }
+}
+
+/* ---- potential, GPE and LHY phase (src/cpucartesian.cpp:94-108,128-136) */
+static void potential_step(const tso_params *p, const double *pot_re, const double *pot_im,
+                           double *re, double *im) {
+    const size_t n = (size_t)p->W * p->H;
+    for (size_t k = 0; k < n; ++k) {
+        double n2 = re[k] * re[k] + im[k] * im[k];
+        double n3 = n2 * sqrt(n2);
+        if (p->imag_time) {
+            double t = exp(-1. * (p->coupling * n2 + p->lhy_coupling * n3));
+            re[k] = t * pot_re[k] * re[k];
+            im[k] = t * pot_re[k] * im[k];
+        } else {
+            double c = cos(p->coupling * n2 + p->lhy_coupling * n3);
+            double s = sin(p->coupling * n2 + p->lhy_coupling * n3);
+            double t = re[k];
+            re[k] = pot_re[k] * t - pot_im[k] * im[k];
+            im[k] = pot_re[k] * im[k] + pot_im[k] * t;
+            t = re[k];
+            re[k] = c * t + s * im[k];
+            im[k] = c * im[k] - s * t;
+        }
+    }
+}
+
+/* ---- rotating frame (src/cpucartesian.cpp:141-262) ---------------------- */
+static inline void rot_pair(int imag_time, double a, double b, double *re, double *im,
+                            size_t i, size_t j) {
+    double tr = re[i], ti = im[i];
+    if (imag_time) {
+        re[i] = a * re[i] + b * im[j];
+        im[i] = a * im[i] - b * re[j];
+        re[j] = -b * ti + a * re[j];
+        im[j] = b * tr + a * im[j];
+    } else {
+        re[i] = a * re[i] + b * re[j];
+        im[i] = a * im[i] + b * im[j];
+        re[j] = a * re[j] - b * tr;
+        im[j] = a * im[j] - b * ti;
+    }
+}
+
+static void rotation_rows(const tso_params *p, double *re, double *im) {
+    const size_t W = (size_t)p->W;
+    for (int y = 0; y < p->H; ++y) {
+        double ang = -0.5 * p->alpha_y * (y + p->rot_off_y);
+        double a = p->imag_time ? cosh(ang) : cos(ang);
+        double b = p->imag_time ? sinh(ang) : sin(ang);
+        for (int par = 0; par < 2; ++par)
+            for (int x = par; x + 1 < p->W; x += 2)
+                rot_pair(p->imag_time, a, b, re, im, (size_t)y * W + x, (size_t)y * W + x + 1);
+    }
+}
+
+static void rotation_cols(const tso_params *p, double *re, double *im) {
+    const size_t W = (size_t)p->W;
+    for (int x = 0; x < p->W; ++x) {
+        double ang = p->alpha_x * (x + p->rot_off_x);
+        double a = p->imag_time ? cosh(ang) : cos(ang);
+        double b = p->imag_time ? sinh(ang) : sin(ang);
+        for (int par = 0; par < 2; ++par)
+            for (int y = par; y + 1 < p->H; y += 2)
+                rot_pair(p->imag_time, a, b, re, im, (size_t)y * W + x, (size_t)(y + 1) * W + x);
+    }
+}
+
+/* ---- one full step (src/cpukernel.cpp:22-92) ----------------------------- */
+void tso_full_step(const tso_params *p, double *re, double *im, const double *pot_re,
+                   const double *pot_im) {
+    const int vert = p->H > 1;
+    if (vert) sweep_vertical(p, 0, p->aV, p->bV, re, im);
+    sweep_horizontal(p, 0, p->aH, p->bH, re, im);
+    if (vert) sweep_vertical(p, 1, p->aV, p->bV, re, im);
+    sweep_horizontal(p, 1, p->aH, p->bH, re, im);
+    potential_step(p, pot_re, pot_im, re, im);
+    if (p->alpha_x != 0. && p->alpha_y != 0.) {
+        rotation_rows(p, re, im);
+        rotation_cols(p, re, im);
+        rotation_rows(p, re, im);
+    }
+    sweep_horizontal(p, 1, p->aH, p->bH, re, im);
+    if (vert) sweep_vertical(p, 1, p->aV, p->bV, re, im);
+    sweep_horizontal(p, 0, p->aH, p->bH, re, im);
+    if (vert) sweep_vertical(p, 0, p->aV, p->bV, re, im);
+}
+
+/* ---- periodic halo refresh (src/cpukernel.cpp:706-716,738-746) ----------- */
+void tso_halo_exchange(const tso_params *p, double *re, double *im) {
+    const size_t W = (size_t)p->W;
+    if (p->periodic_x) {
+        /* rows [iy0, iy0 + H - 2*halo_y), as the reference copies them */
+        int nrows = p->H - 2 * p->halo_y;
+        int n_in = p->W - 2 * p->halo_x;
+        for (int r = 0; r < nrows; ++r) {
+            size_t row = (size_t)(p->iy0 + r) * W;
+            for (int c = 0; c < p->halo_x; ++c) {
+                re[row + c] = re[row + c + n_in];
+                im[row + c] = im[row + c + n_in];
+                re[row + p->W - p->halo_x + c] = re[row + p->halo_x + c];
+                im[row + p->W - p->halo_x + c] = im[row + p->halo_x + c];
+            }
+        }
+    }
+    if (p->periodic_y) {
+        int n_in = p->H - 2 * p->halo_y;
+        for (int r = 0; r < p->halo_y; ++r) {
+            memcpy(re + (size_t)r * W, re + (size_t)(r + n_in) * W, W * sizeof(double));
+            memcpy(im + (size_t)r * W, im + (size_t)(r + n_in) * W, W * sizeof(double));
+            memcpy(re + (size_t)(p->H - p->halo_y + r) * W, re + (size_t)(p->halo_y + r) * W,
+                   W * sizeof(double));
+            memcpy(im + (size_t)(p->H - p->halo_y + r) * W, im + (size_t)(p->halo_y + r) * W,
+                   W * sizeof(double));
+        }
+    }
+}
+
+/* ---- norm and renormalisation (src/cpukernel.cpp:526-562) ---------------- */
+double tso_squared_norm(const tso_params *p, const double *re, const double *im) {
+    double s = 0.;
+    for (int y = p->iy0; y < p->iy1; ++y)
+        for (int x = p->ix0; x < p->ix1; ++x) {
+            size_t k = (size_t)y * p->W + x;
+            s += re[k] * re[k] + im[k] * im[k];
+        }
+    return s * p->delta_x * p->delta_y;
+}
+
+static void renormalise(const tso_params *p, double *re, double *im) {
+    if (!p->imag_time || p->norm0 == 0) return;
+    double f = sqrt(tso_squared_norm(p, re, im) / p->norm0);
+    const size_t n = (size_t)p->W * p->H;
+    for (size_t k = 0; k < n; ++k) {
+        re[k] /= f;
+        im[k] /= f;
+    }
+}
+
+/* ---- evolve loop (src/solver.cpp:186-230, single component) -------------- */
+void tso_evolve(const tso_params *p, double *re, double *im, const double *pot_re,
+                const double *pot_im, int iterations) {
+    for (int i = 0; i < iterations; ++i) {
+        tso_full_step(p, re, im, pot_re, pot_im);
+        if (i != iterations - 1) tso_halo_exchange(p, re, im);
+        renormalise(p, re, im);
+    }
+}
+
+/* ---- step constants (src/cpukernel.cpp:185-217) and table (src/solver.cpp:74-109) */
+void tso_init_constants(tso_params *p, double delta_t, double mass, double g, double g_lhy,
+                        double omega, double delta_x, double delta_y) {
+    double kx = delta_t / (4. * mass * delta_x * delta_x);
+    double ky = delta_t / (4. * mass * delta_y * delta_y);
+    if (p->imag_time) {
+        p->aH = cosh(kx); p->bH = sinh(kx);
+        p->aV = cosh(ky); p->bV = sinh(ky);
+    } else {
+        p->aH = cos(kx); p->bH = sin(kx);
+        p->aV = cos(ky); p->bV = sin(ky);
+    }
+    p->alpha_x = omega * delta_t * delta_x / (2 * delta_y);
+    p->alpha_y = omega * delta_t * delta_y / (2 * delta_x);
+    p->coupling = g * delta_t;
+    p->lhy_coupling = g_lhy * delta_t;
+    p->delta_x = delta_x;
+    p->delta_y = delta_y;
+}
+
+/* exp(-i dt V) in real time, exp(-dt V) in imaginary time: the real and
+ * imaginary parts of std::exp(complex) for a purely imaginary / purely real
+ * argument are (cos, sin) / (exp, 0) of the component. */
+void tso_exp_table(int imag_time, double delta_t, const double *V, size_t n, double *out_re,
+                   double *out_im) {
+    for (size_t k = 0; k < n; ++k) {
+        if (imag_time) {
+            out_re[k] = exp(-delta_t * V[k]);
+            out_im[k] = 0.;
+        } else {
+            double ang = -delta_t * V[k];
+            out_re[k] = cos(ang);
+            out_im[k] = sin(ang);
+        }
+    }
+}
+
+/* ---- coordinates (src/common.cpp:45-65, cartesian) ----------------------- */
+static void coords(const tso_geometry *g, int x_in, int y_in, double *x_out, double *y_out) {
+    double idy = g->start_y * g->delta_y + 0.5 * g->delta_y + y_in * g->delta_y;
+    double idx = g->start_x * g->delta_x + 0.5 * g->delta_x + x_in * g->delta_x;
+    double x_c = g->global_no_halo_dim_x * g->delta_x * 0.5;
+    double y_c = g->global_no_halo_dim_y * g->delta_y * 0.5;
+    if (idx - x_c < -g->length_x * 0.5) idx += g->length_x;
+    if (idx - x_c > g->length_x * 0.5) idx -= g->length_x;
+    if (idy - y_c < -g->length_y * 0.5) idy += g->length_y;
+    if (idy - y_c > g->length_y * 0.5) idy -= g->length_y;
+    *x_out = idx - x_c;
+    *y_out = idy - y_c;
+}
+
+void tso_coordinates(const tso_geometry *g, int x_in, int y_in, double *x_out, double *y_out) {
+    coords(g, x_in, y_in, x_out, y_out);
+}
+
+/* ---- energies (src/solver.cpp:244-564, single component, cartesian) ------- */
+typedef struct { double re, im; } cplx;
+
+static inline cplx cload(const double *re, const double *im, size_t k) {
+    cplx c = {re[k], im[k]};
+    return c;
+}
+
+/* complex<double>(c, 0) * z, as std::complex evaluates it for finite values */
+static inline cplx rscale(double c, cplx z) {
+    cplx r = {c * z.re - 0. * z.im, c * z.im + 0. * z.re};
+    return r;
+}
+static inline cplx cadd(cplx a, cplx b) {
+    cplx r = {a.re + b.re, a.im + b.im};
+    return r;
+}
+static inline cplx cmul(cplx a, cplx b) {
+    cplx r = {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+    return r;
+}
+static inline cplx conjc(cplx a) {
+    cplx r = {a.re, -a.im};
+    return r;
+}
+
+void tso_energies(const tso_geometry *g, const double *re, const double *im, const double *V,
+                  double mass, double g_coupling, double g_lhy, double omega,
+                  tso_energy_result *out) {
+    const int W = g->W;
+    double s_n2 = 0, s_n2k = 0, s_kin = 0, s_pot = 0, s_rot = 0, s_intra = 0, s_lhy = 0;
+    const int ihx = g->ix0, ihy = g->iy0;           /* inner_start - start */
+    const int ehx = W - g->ix1, ehy = g->H - g->iy1; /* end - inner_end */
+    const double dx = g->delta_x, dy = g->delta_y;
+    const double cost_E = -1. / (2. * mass);
+    const double c1 = -1. / 12., c2 = 4. / 3., c3 = -2.5;
+    const double d1 = 1. / 6., d2 = -1., d3 = 0.5, d4 = 1. / 3.;
+    for (int i = g->iy0; i < g->iy1; ++i) {
+        for (int j = g->ix0; j < g->ix1; ++j) {
+            size_t k = (size_t)i * W + j;
+            cplx c = cload(re, im, k);
+            double x, y;
+            coords(g, j, i, &x, &y);
+            double n2 = cmul(conjc(c), c).re;
+            s_n2 += n2;
+            s_pot += n2 * V[k];
+            s_intra += n2 * n2 * 0.5 * g_coupling;
+            s_lhy += pow(n2, 2.5) * 0.4 * g_lhy;
+            if (((i - g->iy0 >= (ihy == 0) * 2 && i < g->iy1 - (ehy == 0) * 2) || g->H == 1) &&
+                (j - g->ix0 >= (ihx == 0) * 2 && j < g->ix1 - (ehx == 0) * 2)) {
+                cplx r = cload(re, im, k + 1), l = cload(re, im, k - 1);
+                cplx rr = cload(re, im, k + 2), ll = cload(re, im, k - 2);
+                s_n2k += cmul(conjc(c), c).re;
+                /* cost_E * conj(c) * (lap) / (dx*dx): the division applies to the product */
+                cplx lap = cadd(cadd(cadd(cadd(rscale(c1, rr), rscale(c2, r)), rscale(c2, l)),
+                                     rscale(c1, ll)), rscale(c3, c));
+                cplx t = {cost_E * c.re, cost_E * (-c.im)};
+                s_kin += cmul(t, lap).re / (dx * dx);
+                if (g->H > 1) {
+                    cplx up = cload(re, im, k - W), dn = cload(re, im, k + W);
+                    cplx uu = cload(re, im, k - 2 * (size_t)W), dd = cload(re, im, k + 2 * (size_t)W);
+                    cplx lapy = cadd(cadd(cadd(cadd(rscale(c1, dd), rscale(c2, dn)), rscale(c2, up)),
+                                          rscale(c1, uu)), rscale(c3, c));
+                    s_kin += cmul(t, lapy).re / (dy * dy);
+                    /* rot_x = (complex(y) * omega / dx) * i, rot_y likewise with x, dy */
+                    cplx yo = {y * omega / dx, 0. * omega / dx};
+                    cplx xo = {x * omega / dy, 0. * omega / dy};
+                    cplx iu = {0., 1.};
+                    cplx rot_x = cmul(yo, iu), rot_y = cmul(xo, iu);
+                    cplx dyv = cadd(cadd(cadd(rscale(d4, up), rscale(d3, c)), rscale(d2, dn)),
+                                    rscale(d1, dd));
+                    cplx dxv = cadd(cadd(cadd(rscale(d4, r), rscale(d3, c)), rscale(d2, l)),
+                                    rscale(d1, ll));
+                    s_rot += cmul(conjc(c), cadd(cmul(rot_y, dyv), cmul(rot_x, dxv))).re;
+                }
+            }
+        }
+    }
+    out->kinetic = s_kin / s_n2k;
+    out->rotational = s_rot / s_n2k;
+    out->potential = s_pot / s_n2;
+    out->intra = s_intra / s_n2;
+    out->lhy = s_lhy / s_n2;
+    out->total = out->kinetic + out->potential + out->intra + out->rotational + out->lhy;
+    out->norm2 = s_n2 * (dy * g->length_x / g->global_no_halo_dim_x);
+}
+
+/* ---- expectation values (src/model.cpp:385-536, cartesian 2D) ------------- */
+void tso_expectations(const tso_geometry *g, const double *re, const double *im,
+                      tso_expectation_result *out) {
+    const int W = g->W;
+    const int ihx = g->ix0, ihy = g->iy0;
+    const int ehx = W - g->ix1, ehy = g->H - g->iy1;
+    double s_n2 = 0, sx = 0, sxx = 0, sy = 0, syy = 0, spx = 0, spxpx = 0, spy = 0, spypy = 0,
+           slz = 0;
+    const double param_px = -1. / g->delta_x, param_py = 1. / g->delta_y;
+    const double c1 = -1. / 12., c2 = 4. / 3., c3 = -2.5;
+    const double d1 = 1. / 6., d2 = -1., d3 = 0.5, d4 = 1. / 3.;
+    for (int i = ihy; i < g->iy1; ++i) {
+        for (int j = ihx; j < g->ix1; ++j) {
+            size_t k = (size_t)i * W + j;
+            cplx c = cload(re, im, k);
+            double x, y;
+            coords(g, j, i, &x, &y);
+            cplx cc = cmul(conjc(c), c);
+            cplx xr = {x, 0.}, yr = {y, 0.};
+            s_n2 += cc.re;
+            sx += cmul(cc, xr).re;
+            sy += cmul(cc, yr).re;
+            sxx += cmul(cmul(cc, xr), xr).re;
+            syy += cmul(cmul(cc, yr), yr).re;
+            if (i - ihy >= (ihy == 0) * 2 && i < g->iy1 - (ehy == 0) * 2 &&
+                j - ihx >= (ihx == 0) * 2 && j < g->ix1 - (ehx == 0) * 2) {
+                cplx up = cload(re, im, k - W), dn = cload(re, im, k + W);
+                cplx r = cload(re, im, k + 1), l = cload(re, im, k - 1);
+                cplx uu = cload(re, im, k - 2 * (size_t)W), dd = cload(re, im, k + 2 * (size_t)W);
+                cplx rr = cload(re, im, k + 2), ll = cload(re, im, k - 2);
+                cplx dxv = cadd(cadd(cadd(rscale(d4, r), rscale(d3, c)), rscale(d2, l)),
+                                rscale(d1, ll));
+                cplx dyv = cadd(cadd(cadd(rscale(d4, up), rscale(d3, c)), rscale(d2, dn)),
+                                rscale(d1, dd));
+                spx += cmul(conjc(c), dxv).im;
+                spy += cmul(conjc(c), dyv).im;
+                spxpx += cmul(conjc(c), cadd(cadd(cadd(cadd(rscale(c1, rr), rscale(c2, r)),
+                                                      rscale(c2, l)), rscale(c1, ll)),
+                                             rscale(c3, c))).re;
+                spypy += cmul(conjc(c), cadd(cadd(cadd(cadd(rscale(c1, dd), rscale(c2, dn)),
+                                                      rscale(c2, up)), rscale(c1, uu)),
+                                             rscale(c3, c))).re;
+                /* y_r / delta_x * (...) + x_r / delta_y * (...) */
+                cplx ydx = {y / g->delta_x, 0. / g->delta_x};
+                cplx xdy = {x / g->delta_y, 0. / g->delta_y};
+                slz += cmul(conjc(c), cadd(cmul(ydx, dxv), cmul(xdy, dyv))).im;
+            }
+        }
+    }
+    out->mean_x = sx / s_n2;
+    out->mean_y = sy / s_n2;
+    out->mean_xx = sxx / s_n2;
+    out->mean_yy = syy / s_n2;
+    out->mean_px = -spx * param_px / s_n2;
+    out->mean_py = -spy * param_py / s_n2;
+    out->mean_pxpx = -spxpx * param_px * param_px / s_n2;
+    out->mean_pypy = -spypy * param_py * param_py / s_n2;
+    out->mean_lz = slz / s_n2;
+    out->norm2 = s_n2 * (g->delta_x * g->delta_y);
+}
