@@ -1,0 +1,195 @@
+/*
+ * ts_b200.h -- C ABI of the B200 Trotter-Suzuki evolution kernel.
+ *
+ * This is the boundary behind which the checkerboard Trotter-Suzuki step of
+ * trotter-suzuki-mpi 1.6.2 runs on one NVIDIA B200 (sm_100a).  It replaces
+ * the reference's kernel plug-in interface ITrotterKernel
+ * (src/trottersuzuki.h:502-520) and its CUDA implementation CC2Kernel
+ * (src/kernel.h:173-269, src/gpukernel.cu:122-728).  The C++ host layer
+ * (class B200Kernel, an ITrotterKernel) and the Python binding both call only
+ * these functions.
+ *
+ * Conventions
+ *  - Plain pointers and sizes; no C++ types, no exceptions cross this ABI.
+ *  - Every function returns a ts_b200_status; TS_B200_OK is 0.  The message
+ *    of the last failure on a handle is returned by ts_b200_last_error().
+ *    (The reference turns CUDA failures into my_abort() ->
+ *    std::runtime_error, src/gpukernel.cu:24-36, src/common.cpp:104-115; the
+ *    C++ host layer does the same with these codes.)
+ *  - A "tile" is the reference's per-process lattice tile: dim_x * dim_y
+ *    cells, row-major, including the periodic halo (src/model.cpp:103-158).
+ *    Host arrays are the reference's SoA layout (p_real, p_imag,
+ *    src/trottersuzuki.h:125-126); on the device the tile is stored as
+ *    interleaved complex numbers (AoS) with a row pitch of a multiple of 4
+ *    cells.
+ *  - All work is queued on the handle's CUDA stream; calls that return data
+ *    to the host synchronise that stream.
+ */
+#ifndef TS_B200_H
+#define TS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    TS_B200_OK = 0,
+    TS_B200_INVALID_ARGUMENT = 1,
+    TS_B200_CUDA_ERROR = 2,
+    TS_B200_OUT_OF_MEMORY = 3,
+    TS_B200_UNSUPPORTED = 4,
+    TS_B200_DEVICE_TIMEOUT = 5,
+    TS_B200_NO_DEVICE = 6
+} ts_b200_status;
+
+typedef enum {
+    TS_B200_FP64 = 0,      /* psi and the exponential table stored and updated in double */
+    TS_B200_FP32 = 1       /* psi and the table stored in float, pair updates in float;
+                              norm, energies and the renormalisation factor in double */
+} ts_b200_precision;
+
+/* Everything a step needs.  Field meanings follow the reference's CPUBlock
+ * constructor (src/cpukernel.cpp:172-272) and Lattice (src/trottersuzuki.h:34-56). */
+typedef struct {
+    int32_t dim_x, dim_y;            /* tile size, halo included (Lattice::dim_x/dim_y) */
+    int32_t inner_x0, inner_x1;      /* inner (non-halo) columns, tile coordinates */
+    int32_t inner_y0, inner_y1;      /* inner rows, tile coordinates */
+    int32_t halo_x, halo_y;          /* Lattice::halo_x/halo_y (4, or 8 with rotation) */
+    int32_t periodic_x, periodic_y;  /* Lattice::periods[1] / periods[0] */
+    int32_t imag_time;               /* imaginary-time evolution */
+    int32_t precision;               /* ts_b200_precision */
+    double a_h, b_h, a_v, b_v;       /* cos/sin (cosh/sinh) of dt/(4 m dx^2), dt/(4 m dy^2) */
+    double coupling;                 /* g * dt            (coupling_const[0]) */
+    double lhy_coupling;             /* g_LHY * dt        (LeeHuangYang_coupling[0]) */
+    double alpha_x, alpha_y;         /* rotating-frame constants; both non-zero enable it */
+    double rot_offset_x;             /* start_x - rot_coord_x (truncated to int per column) */
+    double rot_offset_y;             /* start_y - rot_coord_y */
+    double delta_x, delta_y;
+    double norm0;                    /* imaginary time: squared norm kept after each step;
+                                        0 disables the renormalisation (as the reference) */
+} ts_b200_desc;
+
+typedef struct ts_b200_kernel ts_b200_kernel;
+
+/* Create a kernel on the current CUDA device.  Allocates the two tile
+ * buffers, the exponential table and the reduction scratch.
+ * Replaces: CC2Kernel::CC2Kernel (src/gpukernel.cu:122-238),
+ *           CPUBlock::CPUBlock (src/cpukernel.cpp:172-272). */
+int ts_b200_create(const ts_b200_desc *desc, ts_b200_kernel **out);
+
+/* Free everything.  Replaces: CC2Kernel::~CC2Kernel (src/gpukernel.cu:240-273). */
+int ts_b200_destroy(ts_b200_kernel *k);
+
+/* Upload the tile from host SoA arrays with row stride `stride` (cells).
+ * Replaces: the state upload in CC2Kernel::CC2Kernel (src/gpukernel.cu:196-206). */
+int ts_b200_set_state(ts_b200_kernel *k, const double *p_real, const double *p_imag,
+                      size_t stride);
+
+/* Upload exp(-i dt V) (real time) or exp(-dt V) (imaginary time; only the
+ * real part is read) for the tile, host SoA with row stride `stride`.
+ * Replaces: ITrotterKernel::update_potential (src/trottersuzuki.h:514,
+ *           src/gpukernel.cu:378-387). */
+int ts_b200_set_exp_potential(ts_b200_kernel *k, const double *pot_real, const double *pot_imag,
+                              size_t stride);
+
+/* One Trotter step of the whole tile: the 8 checkerboard pair sweeps, the
+ * potential/GPE/LHY phase and (if enabled) the rotating-frame sweeps, fused
+ * in one pass.  When `exchange` is non-zero the periodic halo is refreshed
+ * afterwards; in imaginary time the step's squared norm is computed and the
+ * renormalisation is applied when the tile is next read.
+ * Replaces: ITrotterKernel::run_kernel_on_halo + run_kernel +
+ *           start/finish_halo_exchange + wait_for_completion
+ *           (src/trottersuzuki.h:505-507,517-518; src/gpukernel.cu:439-521). */
+int ts_b200_step(ts_b200_kernel *k, int exchange);
+
+/* `iterations` steps with the reference's evolve() semantics: the halo is
+ * refreshed after every step but the last (src/solver.cpp:186-230).  Steps
+ * are replayed from a CUDA graph; nothing synchronises the host. */
+int ts_b200_evolve(ts_b200_kernel *k, int iterations);
+
+/* Copy a width x height window at (x, y) of the tile to host SoA arrays with
+ * row stride dest_stride (cells), applying any pending renormalisation.
+ * Replaces: ITrotterKernel::get_sample (src/trottersuzuki.h:508,
+ *           src/gpukernel.cu:547-561). */
+int ts_b200_get_sample(ts_b200_kernel *k, size_t dest_stride, size_t x, size_t y, size_t width,
+                       size_t height, double *dest_real, double *dest_imag);
+
+/* Squared norm of the inner region times delta_x * delta_y, in double.
+ * Replaces: ITrotterKernel::calculate_squared_norm (src/trottersuzuki.h:511,
+ *           src/gpukernel.cu:479-500). */
+int ts_b200_squared_norm(ts_b200_kernel *k, double *out);
+
+/* Energy functional of src/solver.cpp:244-564 (single component) on the
+ * device, FP64 accumulation.  `potential` is the tile of V values (host,
+ * row stride dim_x) or NULL to reuse the last one uploaded. */
+typedef struct {
+    double mass, coupling, lhy_coupling, angular_velocity;
+    int32_t start_x, start_y;                    /* Lattice::start_x/start_y */
+    int32_t global_no_halo_dim_x, global_no_halo_dim_y;
+    double length_x, length_y;
+} ts_b200_energy_params;
+
+typedef struct {
+    double total, kinetic, potential, rotational, intra, lhy, norm2;
+} ts_b200_energy_result;
+
+int ts_b200_energies(ts_b200_kernel *k, const double *potential,
+                     const ts_b200_energy_params *params, ts_b200_energy_result *out);
+
+/* Expectation values of src/model.cpp:385-536 (2D, cartesian) on the device. */
+typedef struct {
+    double norm2, mean_x, mean_xx, mean_y, mean_yy, mean_px, mean_pxpx, mean_py, mean_pypy,
+        mean_lz;
+} ts_b200_expectation_result;
+
+int ts_b200_expectations(ts_b200_kernel *k, const ts_b200_energy_params *params,
+                         ts_b200_expectation_result *out);
+
+/* Device-resident access (for callers that already hold device memory, such
+ * as a torch binding or a benchmark).  `aos` is a device array of dim_y rows
+ * of dim_x interleaved complex numbers in the kernel's precision with row
+ * pitch `pitch` cells. */
+int ts_b200_set_state_device(ts_b200_kernel *k, const void *aos, size_t pitch);
+int ts_b200_get_state_device(ts_b200_kernel *k, void *aos, size_t pitch);
+int ts_b200_set_exp_potential_device(ts_b200_kernel *k, const void *table, size_t pitch);
+
+/* Queue all work of this handle on `stream` (a cudaStream_t); NULL restores
+ * the handle's own stream. */
+int ts_b200_set_stream(ts_b200_kernel *k, void *stream);
+int ts_b200_synchronize(ts_b200_kernel *k);
+
+/* Geometry of the fused step launch chosen for this tile (for reporting):
+ * cells per lane, rows per segment, warps per block, ring depth, tasks. */
+typedef struct {
+    int32_t cells_per_lane, segment_rows, warps_per_block, ring_depth;
+    int32_t strips, segments, blocks, threads;
+    int64_t smem_bytes;
+} ts_b200_launch_shape;
+
+int ts_b200_launch_info(const ts_b200_kernel *k, ts_b200_launch_shape *out);
+
+/* Override the launch shape (autotuner / tests).  Zero fields keep the
+ * current choice.  Only shapes this build instantiates are accepted. */
+int ts_b200_set_launch(ts_b200_kernel *k, int cells_per_lane, int segment_rows, int warps_per_block,
+                       int ring_depth);
+
+/* Pinned host memory for the state arrays (page-locked so that host<->device
+ * copies run at full PCIe/C2C rate). */
+int ts_b200_host_alloc(void **ptr, size_t bytes);
+int ts_b200_host_free(void *ptr);
+
+const char *ts_b200_last_error(const ts_b200_kernel *k);
+const char *ts_b200_status_string(int status);
+
+/* Library version string and the number of kernel launches made by this
+ * process so far (used to report how many launches a measurement made). */
+const char *ts_b200_version(void);
+uint64_t ts_b200_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TS_B200_H */

@@ -1,0 +1,666 @@
+// Fused Trotter-Suzuki step for sm_100a.
+//
+// One launch advances the whole tile by one full step: the checkerboard pair
+// sweeps V0 H0 V1 H1 P [R] H1 V1 H0 V0 of src/cpukernel.cpp:22-92 with the
+// pair updates of src/cpucartesian.cpp:4-70, the potential / GPE / LHY phase
+// of src/cpucartesian.cpp:94-108,128-136 and the rotating-frame sweeps of
+// src/cpucartesian.cpp:141-262, each tile cell read once and written once.
+//
+// Work decomposition ("streaming strips"):
+//   * The tile is cut into column strips.  A warp owns one strip of
+//     32 lanes x C cells (C consecutive columns per lane) and walks down a
+//     segment of rows.  The outer HX columns on each side are recomputed
+//     halo (4 for the 4 horizontal sweeps, 8 when the 4 rotation row sweeps
+//     are added); the strip writes only its middle 32*C - 2*HX columns.
+//   * Walking down the rows, each lane keeps a window of NWIN rows of its C
+//     cells in registers.  A vertical sweep pairs a row with the one below,
+//     so every vertical stage of the sequence runs one row behind the
+//     previous one: with rows r (just loaded) ... r-NWIN+1 in the window,
+//     stage k works on the row pair that has become complete for it.  Row
+//     r-NWIN+1 leaves the window finished and is stored.  A segment reads HY
+//     rows above and below the rows it writes (4 vertical sweeps, 6 with the
+//     two rotation column sweeps).
+//   * Horizontal pairs inside a lane's C cells are register operations;
+//     pairs that straddle two lanes exchange the neighbour cell with a warp
+//     shuffle.  Pairs that would cross the tile edge are skipped, which is
+//     the reference's closed boundary (and its tile edge in periodic mode).
+//   * Rows reach shared memory through cp.async.bulk (the TMA bulk-copy
+//     engine) into a per-warp ring of D slots completed by mbarriers; a
+//     slot holds one row of psi and one row of the exponential table.  The
+//     table row is consumed two iterations after the psi row, then the slot
+//     is refilled D rows ahead.  Every mbarrier wait is bounded; a wait that
+//     gives up sets the error word and abandons the segment.
+//
+// Imaginary time (IMAG): the pair matrix is [[a, b], [b, a]], the table is
+// real, and the squared norm of the written inner cells is reduced in FP64
+// (per-warp partials, then the last block to finish sums them in a fixed
+// order).  The renormalisation of src/cpukernel.cpp:551-562 is deferred: the
+// next launch multiplies every cell it reads by 1/sqrt(norm/norm0).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <type_traits>
+
+namespace tsb {
+
+template <typename T>
+struct Cx {
+    T re, im;
+};
+
+struct Scalars {
+    double pending_inv;  // factor applied to the tile when it is next read
+    double last_norm;    // squared norm * dx * dy of the unnormalised tile of the last step
+    unsigned int ticket; // blocks finished in the current launch
+    int error;           // non-zero: a bounded wait gave up
+    int renorm;          // imaginary-time renormalisation enabled (norm0 != 0)
+    int pad;
+};
+
+template <typename T>
+struct StepArgs {
+    const void *psi_in;
+    void *psi_out;
+    const void *pot;     // Cx<T> per cell in real time, T per cell in imaginary time
+    const void *row_ab;  // Cx<T> per tile row: (a, b) of the rotation row sweeps
+    const void *col_ab;  // Cx<T> per tile column: (a, b) of the rotation column sweeps
+    int W, H, P;         // tile width, height, row pitch (cells, multiple of 4)
+    int ix0, ix1, iy0, iy1;
+    int n_strips, n_segs, seg_h, ring;
+    T aH, bH, aV, bV;
+    T ca, caa;           // g*dt and g_LHY*dt
+    double *partials;    // one per task (imaginary time)
+    Scalars *scal;
+    double dxdy, norm0;
+};
+
+// ---------------------------------------------------------------- PTX helpers
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+                 : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+// Bulk copy global -> shared (16-byte aligned addresses, size a multiple of 16).
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes,
+                                         uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+            "r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait: gives up after `limit_ns` nanoseconds of polling.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity,
+                                                  uint64_t limit_ns = 1000000000ull) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    while (true) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (global_ns() - t0 > limit_ns) return false;
+    }
+}
+
+// ------------------------------------------------------------- pair algebra
+// Multiply-adds are written as explicit fused operations so that every
+// kernel variant (cells per lane, rotation on/off) performs the same
+// rounding for a given cell: the result does not depend on the launch shape.
+__device__ __forceinline__ double fma_t(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float fma_t(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double mul_t(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul_t(float a, float b) { return __fmul_rn(a, b); }
+
+// Kinetic pair (src/cpucartesian.cpp:8-11 real time, :29-32 imaginary time);
+// the update is symmetric, so each cell is updated from (self, partner).
+template <bool IMAG, typename T>
+__device__ __forceinline__ Cx<T> kin(Cx<T> s, Cx<T> p, T a, T b) {
+    Cx<T> r;
+    if (IMAG) {
+        r.re = fma_t(a, s.re, mul_t(b, p.re));
+        r.im = fma_t(a, s.im, mul_t(b, p.im));
+    } else {
+        r.re = fma_t(a, s.re, -mul_t(b, p.im));
+        r.im = fma_t(a, s.im, mul_t(b, p.re));
+    }
+    return r;
+}
+
+// Rotation pair (src/cpucartesian.cpp:149-153 real, :210-214 imaginary):
+// `first` is the lower-index cell of the pair, `second` the higher one.
+template <bool IMAG, typename T>
+__device__ __forceinline__ Cx<T> rot_first(Cx<T> f, Cx<T> s, T a, T b) {
+    Cx<T> r;
+    if (IMAG) {
+        r.re = fma_t(a, f.re, mul_t(b, s.im));
+        r.im = fma_t(a, f.im, -mul_t(b, s.re));
+    } else {
+        r.re = fma_t(a, f.re, mul_t(b, s.re));
+        r.im = fma_t(a, f.im, mul_t(b, s.im));
+    }
+    return r;
+}
+
+template <bool IMAG, typename T>
+__device__ __forceinline__ Cx<T> rot_second(Cx<T> s, Cx<T> f, T a, T b) {
+    Cx<T> r;
+    if (IMAG) {
+        r.re = fma_t(a, s.re, -mul_t(b, f.im));
+        r.im = fma_t(a, s.im, mul_t(b, f.re));
+    } else {
+        r.re = fma_t(a, s.re, -mul_t(b, f.re));
+        r.im = fma_t(a, s.im, -mul_t(b, f.im));
+    }
+    return r;
+}
+
+template <typename T>
+__device__ __forceinline__ Cx<T> shfl_down1(Cx<T> v) {
+    Cx<T> r;
+    r.re = __shfl_down_sync(0xffffffffu, v.re, 1);
+    r.im = __shfl_down_sync(0xffffffffu, v.im, 1);
+    return r;
+}
+
+template <typename T>
+__device__ __forceinline__ Cx<T> shfl_up1(Cx<T> v) {
+    Cx<T> r;
+    r.re = __shfl_up_sync(0xffffffffu, v.re, 1);
+    r.im = __shfl_up_sync(0xffffffffu, v.im, 1);
+    return r;
+}
+
+// Per-lane masks of a strip (which cells exist, which horizontal pairs are live).
+template <int C>
+struct LaneMask {
+    bool pair_int[C];  // pair (i, i+1) inside the lane, both cells in the tile
+    bool pair_left;    // pair (lane-1 cell C-1, cell 0) exists
+    bool pair_right;   // pair (cell C-1, lane+1 cell 0) exists
+};
+
+// Vertical kinetic sweep on rows (u, u+1): cells with (x + u) % 2 == s pair,
+// i.e. lane cells with (i & 1) == PAR where PAR = (u + s) & 1 (strips start
+// on an even column).
+template <bool IMAG, int C, int PAR, typename T>
+__device__ __forceinline__ void vsweep(Cx<T> (&up)[C], Cx<T> (&lo)[C], T a, T b) {
+#pragma unroll
+    for (int i = PAR; i < C; i += 2) {
+        Cx<T> u = up[i], l = lo[i];
+        up[i] = kin<IMAG>(u, l, a, b);
+        lo[i] = kin<IMAG>(l, u, a, b);
+    }
+}
+
+// Horizontal kinetic sweep on one row: pairs (x, x+1) with (x + u) % 2 == s
+// start at lane cells with (i & 1) == PAR, PAR = (u + s) & 1.
+template <bool IMAG, int C, int PAR, typename T>
+__device__ __forceinline__ void hsweep(Cx<T> (&w)[C], T a, T b, const LaneMask<C> &m) {
+    if (PAR == 0) {
+#pragma unroll
+        for (int i = 0; i + 1 < C; i += 2) {
+            Cx<T> p = w[i], q = w[i + 1];
+            Cx<T> np = kin<IMAG>(p, q, a, b), nq = kin<IMAG>(q, p, a, b);
+            w[i] = m.pair_int[i] ? np : p;
+            w[i + 1] = m.pair_int[i] ? nq : q;
+        }
+    } else {
+        Cx<T> right = shfl_down1(w[0]);
+        Cx<T> left = shfl_up1(w[C - 1]);
+#pragma unroll
+        for (int i = 1; i + 1 < C; i += 2) {
+            Cx<T> p = w[i], q = w[i + 1];
+            Cx<T> np = kin<IMAG>(p, q, a, b), nq = kin<IMAG>(q, p, a, b);
+            w[i] = m.pair_int[i] ? np : p;
+            w[i + 1] = m.pair_int[i] ? nq : q;
+        }
+        Cx<T> n0 = kin<IMAG>(w[0], left, a, b);
+        Cx<T> nl = kin<IMAG>(w[C - 1], right, a, b);
+        if (m.pair_left) w[0] = n0;
+        if (m.pair_right) w[C - 1] = nl;
+    }
+}
+
+// Rotation row sweep on one row: pairs (x, x+1) with x % 2 == PAR.
+template <bool IMAG, int C, int PAR, typename T>
+__device__ __forceinline__ void rrow(Cx<T> (&w)[C], T a, T b, const LaneMask<C> &m) {
+    if (PAR == 0) {
+#pragma unroll
+        for (int i = 0; i + 1 < C; i += 2) {
+            Cx<T> f = w[i], s = w[i + 1];
+            Cx<T> nf = rot_first<IMAG>(f, s, a, b), ns = rot_second<IMAG>(s, f, a, b);
+            w[i] = m.pair_int[i] ? nf : f;
+            w[i + 1] = m.pair_int[i] ? ns : s;
+        }
+    } else {
+        Cx<T> right = shfl_down1(w[0]);
+        Cx<T> left = shfl_up1(w[C - 1]);
+#pragma unroll
+        for (int i = 1; i + 1 < C; i += 2) {
+            Cx<T> f = w[i], s = w[i + 1];
+            Cx<T> nf = rot_first<IMAG>(f, s, a, b), ns = rot_second<IMAG>(s, f, a, b);
+            w[i] = m.pair_int[i] ? nf : f;
+            w[i + 1] = m.pair_int[i] ? ns : s;
+        }
+        Cx<T> n0 = rot_second<IMAG>(w[0], left, a, b);
+        Cx<T> nl = rot_first<IMAG>(w[C - 1], right, a, b);
+        if (m.pair_left) w[0] = n0;
+        if (m.pair_right) w[C - 1] = nl;
+    }
+}
+
+// Rotation column sweep on rows (u, u+1) (every column pairs; u has the sweep's parity).
+template <bool IMAG, int C, typename T>
+__device__ __forceinline__ void rcol(Cx<T> (&up)[C], Cx<T> (&lo)[C], const Cx<T> (&ab)[C]) {
+#pragma unroll
+    for (int i = 0; i < C; ++i) {
+        Cx<T> f = up[i], s = lo[i];
+        up[i] = rot_first<IMAG>(f, s, ab[i].re, ab[i].im);
+        lo[i] = rot_second<IMAG>(s, f, ab[i].re, ab[i].im);
+    }
+}
+
+__device__ __forceinline__ void sincos_t(double x, double *s, double *c) { sincos(x, s, c); }
+__device__ __forceinline__ void sincos_t(float x, float *s, float *c) { sincosf(x, s, c); }
+__device__ __forceinline__ double exp_t(double x) { return exp(x); }
+__device__ __forceinline__ float exp_t(float x) { return expf(x); }
+__device__ __forceinline__ double sqrt_t(double x) { return sqrt(x); }
+__device__ __forceinline__ float sqrt_t(float x) { return sqrtf(x); }
+
+// Potential, GPE and LHY phase on one row (src/cpucartesian.cpp:96-106,130-134).
+// |psi|^2 is taken before the table multiply, as the reference does.
+template <bool IMAG, bool PHASE, int C, typename T, typename TabT>
+__device__ __forceinline__ void potential_row(Cx<T> (&w)[C], const TabT *tab, T ca, T caa) {
+#pragma unroll
+    for (int i = 0; i < C; ++i) {
+        Cx<T> v = w[i];
+        if (IMAG) {
+            const T pr = reinterpret_cast<const T *>(tab)[i];
+            if (PHASE) {
+                const T n2 = fma_t(v.re, v.re, mul_t(v.im, v.im));
+                T th = mul_t(ca, n2);
+                if (caa != T(0)) th = fma_t(caa, mul_t(n2, sqrt_t(n2)), th);
+                const T t = mul_t(exp_t(-th), pr);
+                v.re = mul_t(t, v.re);
+                v.im = mul_t(t, v.im);
+            } else {
+                v.re = mul_t(pr, v.re);
+                v.im = mul_t(pr, v.im);
+            }
+        } else {
+            const Cx<T> e = reinterpret_cast<const Cx<T> *>(tab)[i];
+            T c = T(1), s = T(0);
+            if (PHASE) {
+                const T n2 = fma_t(v.re, v.re, mul_t(v.im, v.im));
+                T th = mul_t(ca, n2);
+                if (caa != T(0)) th = fma_t(caa, mul_t(n2, sqrt_t(n2)), th);
+                sincos_t(th, &s, &c);
+            }
+            T t = v.re;
+            v.re = fma_t(e.re, t, -mul_t(e.im, v.im));
+            v.im = fma_t(e.re, v.im, mul_t(e.im, t));
+            if (PHASE) {
+                t = v.re;
+                v.re = fma_t(c, t, mul_t(s, v.im));
+                v.im = fma_t(c, v.im, -mul_t(s, t));
+            }
+        }
+        w[i] = v;
+    }
+}
+
+template <typename T>
+struct Vec2T;
+template <>
+struct Vec2T<double> {
+    using type = double2;
+};
+template <>
+struct Vec2T<float> {
+    using type = float2;
+};
+
+template <typename T>
+__device__ __forceinline__ Cx<T> ld_cx_shared(const Cx<T> *p) {
+    typename Vec2T<T>::type v = *reinterpret_cast<const typename Vec2T<T>::type *>(p);
+    Cx<T> r;
+    r.re = v.x;
+    r.im = v.y;
+    return r;
+}
+
+template <typename T>
+__device__ __forceinline__ void st_cx_global(Cx<T> *p, Cx<T> v) {
+    typename Vec2T<T>::type o;
+    o.x = v.re;
+    o.y = v.im;
+    *reinterpret_cast<typename Vec2T<T>::type *>(p) = o;
+}
+
+// Compile-time description of a kernel variant.
+template <typename T_, int C_, bool IMAG_, bool ROT_, bool PHASE_>
+struct Variant {
+    using T = T_;
+    static constexpr int C = C_;
+    static constexpr bool IMAG = IMAG_;
+    static constexpr bool ROT = ROT_;
+    static constexpr bool PHASE = PHASE_;
+    static constexpr int HX = ROT_ ? 8 : 4;
+    static constexpr int HY = ROT_ ? 6 : 4;
+    static constexpr int NWIN = ROT_ ? 7 : 5;
+    static constexpr int SW = 32 * C_;
+    static constexpr int WO = SW - 2 * HX;
+    using TabT = typename std::conditional<IMAG_, T_, Cx<T_>>::type;
+    static constexpr int PSI_BYTES = SW * (int)sizeof(Cx<T_>);
+    static constexpr int TAB_BYTES = SW * (int)sizeof(TabT);
+    static constexpr int SLOT = PSI_BYTES + TAB_BYTES;
+};
+
+
+// Per-warp state of one segment walk.  Every member is indexed with
+// compile-time constants after inlining, so the whole struct lives in
+// registers.
+template <class V>
+struct Walk {
+    using T = typename V::T;
+    using TabT = typename V::TabT;
+    static constexpr int C = V::C, NWIN = V::NWIN;
+
+    Cx<T> win[NWIN][C];
+    Cx<T> colab[C];
+    LaneMask<C> m;
+    bool present[C], out_col[C], norm_col[C];
+    int ra, rb, oy0, oy1, xl, lane, D;
+    int cs;
+    uint32_t psi_off, psi_bytes, tab_off, tab_bytes;
+    int next_issue;  // next row whose copy has not been issued
+    int consumed;    // rows [ra, consumed) have been waited for
+    unsigned char *ring;
+    uint64_t *bars;
+    double nacc;
+    bool failed;
+    T inv;
+
+    __device__ __forceinline__ void issue(const StepArgs<T> &a, int row) {
+        const int slot = (row - ra) % D;
+        unsigned char *sb = ring + (size_t)slot * V::SLOT;
+        mbar_expect_tx(&bars[slot], psi_bytes + tab_bytes);
+        const unsigned char *gp = reinterpret_cast<const unsigned char *>(a.psi_in) +
+                                  ((size_t)row * a.P + cs) * sizeof(Cx<T>);
+        bulk_g2s(sb + psi_off, gp, psi_bytes, &bars[slot]);
+        const unsigned char *gt = reinterpret_cast<const unsigned char *>(a.pot) +
+                                  ((size_t)row * a.P + cs) * sizeof(TabT);
+        bulk_g2s(sb + V::PSI_BYTES + tab_off, gt, tab_bytes, &bars[slot]);
+    }
+};
+
+// One iteration of the walk for row r = base + K (base even, so the parity
+// of every row index below is known at compile time).
+template <class V, int K>
+__device__ __forceinline__ void walk_row(Walk<V> &w, const StepArgs<typename V::T> &a, int r) {
+    using T = typename V::T;
+    using TabT = typename V::TabT;
+    constexpr int C = V::C, NWIN = V::NWIN;
+    constexpr bool IMAG = V::IMAG, ROT = V::ROT, PHASE = V::PHASE;
+    // row r - j lives in win[(K - j) mod NWIN]
+#define WS(j) w.win[((K) - (j) + 2 * NWIN) % NWIN]
+    const int ra = w.ra, rb = w.rb;
+    const T aH = a.aH, bH = a.bH, aV = a.aV, bV = a.bV;
+
+    // ---- load row r
+    if (r >= ra && r < rb) {
+        const int slot = (r - ra) % w.D;
+        const uint32_t par = (uint32_t)(((r - ra) / w.D) & 1);
+        if (!mbar_wait_bounded(&w.bars[slot], par)) {
+            w.failed = true;
+            return;
+        }
+        w.consumed = r + 1;
+        const Cx<T> *sp = reinterpret_cast<const Cx<T> *>(w.ring + (size_t)slot * V::SLOT);
+#pragma unroll
+        for (int i = 0; i < C; ++i) {
+            Cx<T> v = ld_cx_shared(sp + C * w.lane + i);
+            if (IMAG) {
+                v.re = v.re * w.inv;
+                v.im = v.im * w.inv;
+            }
+            WS(0)[i] = w.present[i] ? v : Cx<T>{T(0), T(0)};
+        }
+    }
+    // ---- S1: V0 on rows (r-1, r)
+    if (r - 1 >= ra && r < rb) vsweep<IMAG, C, ((K + 1) & 1)>(WS(1), WS(0), aV, bV);
+    // ---- S2: H0 on row r-1
+    if (r - 1 >= ra && r - 1 < rb) hsweep<IMAG, C, ((K + 1) & 1)>(WS(1), aH, bH, w.m);
+    // ---- S3: V1 on rows (r-2, r-1)
+    if (r - 2 >= ra && r - 1 < rb) vsweep<IMAG, C, ((K + 1) & 1)>(WS(2), WS(1), aV, bV);
+    // ---- S4: H1, P, then H1 (or the rotation row sweeps) on row r-2; free its slot
+    if (r - 2 >= ra && r - 2 < rb) {
+        const int u = r - 2;
+        hsweep<IMAG, C, ((K + 1) & 1)>(WS(2), aH, bH, w.m);
+        const int slot = (u - ra) % w.D;
+        const TabT *tp =
+            reinterpret_cast<const TabT *>(w.ring + (size_t)slot * V::SLOT + V::PSI_BYTES) +
+            C * w.lane;
+        potential_row<IMAG, PHASE, C>(WS(2), tp, a.ca, a.caa);
+        if constexpr (ROT) {
+            const Cx<T> ab = reinterpret_cast<const Cx<T> *>(a.row_ab)[u];
+            rrow<IMAG, C, 0>(WS(2), ab.re, ab.im, w.m);
+            rrow<IMAG, C, 1>(WS(2), ab.re, ab.im, w.m);
+        } else {
+            hsweep<IMAG, C, ((K + 1) & 1)>(WS(2), aH, bH, w.m);
+        }
+        __syncwarp();
+        if (u + w.D < rb) {
+            if (w.lane == 0) {
+                // the slot's last generic-proxy reads happen-before the bulk copy refills it
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                w.issue(a, u + w.D);
+            }
+            w.next_issue = u + w.D + 1;
+        }
+    }
+    if constexpr (!ROT) {
+        // ---- S5: V1 on rows (r-3, r-2)
+        if (r - 3 >= ra && r - 2 < rb) vsweep<IMAG, C, ((K) & 1)>(WS(3), WS(2), aV, bV);
+        // ---- S6: H0 on row r-3
+        if (r - 3 >= ra && r - 3 < rb) hsweep<IMAG, C, ((K + 1) & 1)>(WS(3), aH, bH, w.m);
+        // ---- S7: V0 on rows (r-4, r-3)
+        if (r - 4 >= ra && r - 3 < rb) vsweep<IMAG, C, ((K) & 1)>(WS(4), WS(3), aV, bV);
+    } else {
+        // ---- S5: rotation columns, even rows: pair (r-3, r-2) when r-3 is even
+        if (((K + 1) & 1) == 0 && r - 3 >= ra && r - 2 < rb) rcol<IMAG, C>(WS(3), WS(2), w.colab);
+        // ---- S6: rotation columns, odd rows: pair (r-4, r-3) when r-4 is odd
+        if (((K) & 1) == 1 && r - 4 >= ra && r - 3 < rb) rcol<IMAG, C>(WS(4), WS(3), w.colab);
+        // ---- S7: rotation rows again, then H1, on row r-4
+        if (r - 4 >= ra && r - 4 < rb) {
+            const Cx<T> ab = reinterpret_cast<const Cx<T> *>(a.row_ab)[r - 4];
+            rrow<IMAG, C, 0>(WS(4), ab.re, ab.im, w.m);
+            rrow<IMAG, C, 1>(WS(4), ab.re, ab.im, w.m);
+            hsweep<IMAG, C, ((K + 1) & 1)>(WS(4), aH, bH, w.m);
+        }
+        // ---- S8: V1 on rows (r-5, r-4)
+        if (r - 5 >= ra && r - 4 < rb) vsweep<IMAG, C, ((K) & 1)>(WS(5), WS(4), aV, bV);
+        // ---- S9: H0 on row r-5
+        if (r - 5 >= ra && r - 5 < rb) hsweep<IMAG, C, ((K + 1) & 1)>(WS(5), aH, bH, w.m);
+        // ---- S10: V0 on rows (r-6, r-5)
+        if (r - 6 >= ra && r - 5 < rb) vsweep<IMAG, C, ((K) & 1)>(WS(6), WS(5), aV, bV);
+    }
+    // ---- store the finished row r - (NWIN-1)
+    {
+        const int u = r - (NWIN - 1);
+        if (u >= w.oy0 && u < w.oy1) {
+            Cx<T> *out = reinterpret_cast<Cx<T> *>(a.psi_out);
+            const bool norm_row = IMAG && u >= a.iy0 && u < a.iy1;
+#pragma unroll
+            for (int i = 0; i < C; ++i) {
+                const Cx<T> v = WS(NWIN - 1)[i];
+                if (w.out_col[i]) st_cx_global(out + (size_t)u * a.P + (w.xl + i), v);
+                if (norm_row && w.norm_col[i])
+                    w.nacc += (double)v.re * (double)v.re + (double)v.im * (double)v.im;
+            }
+        }
+    }
+#undef WS
+}
+
+template <class V, int K>
+__device__ __forceinline__ void walk_rows(Walk<V> &w, const StepArgs<typename V::T> &a, int base,
+                                          int rlast) {
+    if constexpr (K < 2 * V::NWIN) {
+        const int r = base + K;
+        if (r > rlast || w.failed) return;
+        walk_row<V, K>(w, a, r);
+        walk_rows<V, K + 1>(w, a, base, rlast);
+    }
+}
+
+template <class V>
+__global__ void __launch_bounds__(128) step_kernel(StepArgs<typename V::T> a) {
+    using T = typename V::T;
+    using TabT = typename V::TabT;
+    constexpr int C = V::C, NWIN = V::NWIN, HX = V::HX, HY = V::HY, SW = V::SW, WO = V::WO;
+    constexpr bool IMAG = V::IMAG, ROT = V::ROT;
+
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int warps = blockDim.x >> 5;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int D = a.ring;
+    const int n_tasks = a.n_strips * a.n_segs;
+    const int task = blockIdx.x * warps + warp;
+
+    Walk<V> w;
+    w.nacc = 0.0;
+    w.failed = false;
+    w.inv = IMAG ? (T)a.scal->pending_inv : T(1);
+
+    if (task < n_tasks) {
+        w.D = D;
+        w.lane = lane;
+        w.ring = smem + (size_t)warp * D * V::SLOT;
+        w.bars = reinterpret_cast<uint64_t *>(smem + (size_t)warps * D * V::SLOT) + warp * D;
+        const int strip = task % a.n_strips, seg = task / a.n_strips;
+        const int ox0 = strip * WO, ox1 = min(ox0 + WO, a.W);
+        const int c0 = ox0 - HX;
+        w.oy0 = seg * a.seg_h;
+        w.oy1 = min(w.oy0 + a.seg_h, a.H);
+        w.ra = max(w.oy0 - HY, 0);
+        w.rb = min(w.oy1 + HY, a.H);
+        w.cs = max(c0, 0);
+        const int ce = min(c0 + SW, a.P);
+        w.psi_off = (uint32_t)(w.cs - c0) * sizeof(Cx<T>);
+        w.psi_bytes = (uint32_t)(ce - w.cs) * sizeof(Cx<T>);
+        w.tab_off = (uint32_t)(w.cs - c0) * sizeof(TabT);
+        w.tab_bytes = (uint32_t)(ce - w.cs) * sizeof(TabT);
+        w.xl = c0 + C * lane;
+#pragma unroll
+        for (int i = 0; i < C; ++i) {
+            const int x = w.xl + i;
+            w.present[i] = x >= 0 && x < a.W;
+            w.out_col[i] = x >= ox0 && x < ox1;
+            w.norm_col[i] = w.out_col[i] && x >= a.ix0 && x < a.ix1;
+        }
+#pragma unroll
+        for (int i = 0; i + 1 < C; ++i) w.m.pair_int[i] = w.present[i] && w.present[i + 1];
+        w.m.pair_int[C - 1] = false;
+        w.m.pair_left = lane > 0 && w.present[0] && w.xl - 1 >= 0;
+        w.m.pair_right = lane < 31 && w.present[C - 1] && w.xl + C < a.W;
+        if constexpr (ROT) {
+#pragma unroll
+            for (int i = 0; i < C; ++i)
+                w.colab[i] = reinterpret_cast<const Cx<T> *>(a.col_ab)[w.present[i] ? w.xl + i : 0];
+        }
+#pragma unroll
+        for (int j = 0; j < NWIN; ++j)
+#pragma unroll
+            for (int i = 0; i < C; ++i) w.win[j][i] = Cx<T>{T(0), T(0)};
+
+        if (lane == 0) {
+            for (int q = 0; q < D; ++q) mbar_init(&w.bars[q], 1);
+            fence_mbar_init();
+        }
+        __syncwarp();
+        w.next_issue = min(w.ra + D, w.rb);
+        w.consumed = w.ra;
+        if (lane == 0)
+            for (int row = w.ra; row < w.next_issue; ++row) w.issue(a, row);
+
+        const int rlast = w.rb - 1 + (NWIN - 1);
+        for (int base = w.ra & ~1; base <= rlast && !w.failed; base += 2 * NWIN)
+            walk_rows<V, 0>(w, a, base, rlast);
+
+        if (w.failed) {
+            if (lane == 0) atomicExch(&a.scal->error, 1);
+            // let copies already issued land before the block can exit
+            for (int row = w.consumed; row < w.next_issue; ++row)
+                (void)mbar_wait_bounded(&w.bars[(row - w.ra) % D], (uint32_t)(((row - w.ra) / D) & 1),
+                                        100000000ull);
+        }
+    }
+
+    if constexpr (IMAG) {
+        double nacc = w.nacc;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) nacc += __shfl_xor_sync(0xffffffffu, nacc, off);
+        if (lane == 0 && task < n_tasks) a.partials[task] = nacc;
+        __shared__ unsigned int s_last;
+        __shared__ double red[128];
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            const unsigned int t = atomicAdd(&a.scal->ticket, 1u);
+            s_last = (t == gridDim.x - 1) ? 1u : 0u;
+        }
+        __syncthreads();
+        if (s_last) {
+            __threadfence();
+            // fixed order: thread t sums tasks t, t + blockDim, ..., then a fixed tree
+            double s = 0.0;
+            for (int t = threadIdx.x; t < n_tasks; t += blockDim.x) s += __ldcg(&a.partials[t]);
+            red[threadIdx.x] = s;
+            __syncthreads();
+            for (int h = blockDim.x >> 1; h > 0; h >>= 1) {
+                if ((int)threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+                __syncthreads();
+            }
+            if (threadIdx.x == 0) {
+                const double tot = red[0] * a.dxdy;
+                a.scal->last_norm = tot;
+                if (a.scal->renorm) a.scal->pending_inv = 1.0 / sqrt(tot / a.norm0);
+                a.scal->ticket = 0u;
+            }
+        }
+    }
+}
+
+}  // namespace tsb

@@ -1,0 +1,1048 @@
+// C ABI of the B200 Trotter-Suzuki kernel (include/ts_b200.h).
+//
+// Host side: one handle per tile.  It owns two device tiles (the step reads
+// one and writes the other, as the reference's double buffer
+// p_real[.][sense], src/cpukernel.cpp:244-247), the exponential table, the
+// rotation coefficient tables, reduction scratch and a CUDA stream.  Work is
+// only queued; nothing synchronises the host except the calls that return
+// data.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <type_traits>
+
+#include "step_kernel.cuh"
+#include "step_launch.h"
+#include "ts_b200.h"
+
+using tsb::Cx;
+using tsb::Scalars;
+using tsb::StepArgs;
+
+namespace {
+
+std::atomic<uint64_t> g_launches{0};
+
+// ------------------------------------------------------------------ kernels
+
+// Interleave host-order SoA doubles (row stride `sstride`) into the device
+// AoS tile of type T (row pitch P); padding columns [W, P) are zeroed.
+template <typename T>
+__global__ void pack_state_kernel(Cx<T> *dst, int W, int H, int P, const double *re,
+                                  const double *im, size_t sstride) {
+    const size_t n = (size_t)P * H;
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
+         k += (size_t)gridDim.x * blockDim.x) {
+        const int y = (int)(k / P), x = (int)(k % P);
+        Cx<T> v{T(0), T(0)};
+        if (x < W) {
+            v.re = (T)re[(size_t)y * sstride + x];
+            v.im = (T)im[(size_t)y * sstride + x];
+        }
+        dst[k] = v;
+    }
+}
+
+// Table: Cx<T> per cell in real time, T (real part only) in imaginary time.
+template <typename T>
+__global__ void pack_table_kernel(void *dst, int imag, int W, int H, int P, const double *re,
+                                  const double *im, size_t sstride) {
+    const size_t n = (size_t)P * H;
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
+         k += (size_t)gridDim.x * blockDim.x) {
+        const int y = (int)(k / P), x = (int)(k % P);
+        const double vr = x < W ? re[(size_t)y * sstride + x] : 0.0;
+        const double vi = x < W ? im[(size_t)y * sstride + x] : 0.0;
+        if (imag) {
+            reinterpret_cast<T *>(dst)[k] = (T)vr;
+        } else {
+            reinterpret_cast<Cx<T> *>(dst)[k] = Cx<T>{(T)vr, (T)vi};
+        }
+    }
+}
+
+// De-interleave a w x h window at (x0, y0) into SoA doubles with stride w,
+// multiplying by `scale` (the pending imaginary-time renormalisation).
+template <typename T>
+__global__ void unpack_state_kernel(const Cx<T> *src, int P, int x0, int y0, int w, int h,
+                                    const Scalars *scal, int use_scale, double *re, double *im) {
+    const double s = use_scale ? scal->pending_inv : 1.0;
+    const size_t n = (size_t)w * h;
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
+         k += (size_t)gridDim.x * blockDim.x) {
+        const int y = (int)(k / w), x = (int)(k % w);
+        const Cx<T> v = src[(size_t)(y0 + y) * P + (x0 + x)];
+        re[k] = (double)v.re * s;
+        im[k] = (double)v.im * s;
+    }
+}
+
+// Copy the tile with a pitch change, optionally folding in the pending scale.
+template <typename T>
+__global__ void copy_tile_kernel(Cx<T> *dst, size_t dpitch, const Cx<T> *src, size_t spitch,
+                                 int W, int H, const Scalars *scal, int use_scale) {
+    const T s = use_scale ? (T)scal->pending_inv : T(1);
+    const size_t n = (size_t)W * H;
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
+         k += (size_t)gridDim.x * blockDim.x) {
+        const int y = (int)(k / W), x = (int)(k % W);
+        Cx<T> v = src[(size_t)y * spitch + x];
+        if (use_scale) {
+            v.re *= s;
+            v.im *= s;
+        }
+        dst[(size_t)y * dpitch + x] = v;
+    }
+}
+
+// Periodic halo refresh (src/cpukernel.cpp:706-716,738-746, one process):
+// x-halo columns of rows [iy0, iy0 + H - 2*hy) take the opposite inner
+// columns, then y-halo rows take the opposite inner rows (all columns).  Each
+// destination cell is written from the cell its value ends up coming from;
+// those source cells are never destinations, so one pass suffices.
+template <typename T>
+__global__ void halo_kernel(Cx<T> *psi, int W, int H, int P, int hx, int hy, int px, int py,
+                            int iy0) {
+    const int nx_dest = px ? 2 * hx * H : 0;
+    const int ncols_b = px ? W - 2 * hx : W;  // y-halo cells outside the x-halo columns
+    const int ny_dest = py ? 2 * hy * ncols_b : 0;
+    const int n = nx_dest + ny_dest;
+    const int Nx = W - 2 * hx, Ny = H - 2 * hy;
+    const int xr0 = iy0, xr1 = iy0 + H - 2 * hy;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        int x, y;
+        if (k < nx_dest) {
+            y = k / (2 * hx);
+            const int c = k % (2 * hx);
+            x = c < hx ? c : W - 2 * hx + c;
+        } else {
+            const int kk = k - nx_dest;
+            const int rr = kk / ncols_b, c = kk % ncols_b;
+            y = rr < hy ? rr : H - 2 * hy + rr;
+            x = px ? hx + c : c;
+        }
+        int ys = y;
+        if (py) {
+            if (y < hy) ys = y + Ny;
+            else if (y >= H - hy) ys = y - Ny;
+        }
+        int xs = x;
+        if (px && ys >= xr0 && ys < xr1) {
+            if (x < hx) xs = x + Nx;
+            else if (x >= W - hx) xs = x - Nx;
+        }
+        if (xs == x && ys == y) continue;
+        psi[(size_t)y * P + x] = psi[(size_t)ys * P + xs];
+    }
+}
+
+// -------------------------------------------------------------- reductions
+// Deterministic FP64 reductions over the inner region: a fixed grid, each
+// thread walks a fixed set of cells, a fixed block tree, then the last block
+// to finish sums the block partials in order.
+constexpr int RED_THREADS = 256;
+constexpr int RED_MAX_BLOCKS = 1184;  // 8 per SM on a 148-SM B200
+constexpr int RED_MAX_TERMS = 10;
+
+struct RedArgs {
+    const void *psi;
+    int W, H, P;
+    int ix0, ix1, iy0, iy1;
+    const Scalars *scal;
+    int use_scale;
+    const double *V;
+    double dx, dy;
+    int start_x, start_y, gnx, gny;
+    double Lx, Ly;
+    double mass, g, glhy, omega;
+    double *partials;  // gridDim.x * RED_MAX_TERMS
+    double *out;       // RED_MAX_TERMS
+    unsigned int *ticket;
+};
+
+// Cartesian cell-centre coordinates (src/common.cpp:45-65).
+__device__ __forceinline__ void cell_coords(const RedArgs &a, int xi, int yi, double *xo,
+                                            double *yo) {
+    double idy = __dadd_rn(__dadd_rn(__dmul_rn(a.start_y, a.dy), __dmul_rn(0.5, a.dy)),
+                           __dmul_rn(yi, a.dy));
+    double idx = __dadd_rn(__dadd_rn(__dmul_rn(a.start_x, a.dx), __dmul_rn(0.5, a.dx)),
+                           __dmul_rn(xi, a.dx));
+    const double x_c = __dmul_rn(__dmul_rn(a.gnx, a.dx), 0.5);
+    const double y_c = __dmul_rn(__dmul_rn(a.gny, a.dy), 0.5);
+    if (idx - x_c < -a.Lx * 0.5) idx = __dadd_rn(idx, a.Lx);
+    if (idx - x_c > a.Lx * 0.5) idx = __dsub_rn(idx, a.Lx);
+    if (idy - y_c < -a.Ly * 0.5) idy = __dadd_rn(idy, a.Ly);
+    if (idy - y_c > a.Ly * 0.5) idy = __dsub_rn(idy, a.Ly);
+    *xo = __dsub_rn(idx, x_c);
+    *yo = __dsub_rn(idy, y_c);
+}
+
+template <typename T>
+__device__ __forceinline__ Cx<double> ldc(const RedArgs &a, double s, int x, int y) {
+    const Cx<T> v = reinterpret_cast<const Cx<T> *>(a.psi)[(size_t)y * a.P + x];
+    return Cx<double>{(double)v.re * s, (double)v.im * s};
+}
+
+template <int NT>
+__device__ void block_reduce_and_finish(const RedArgs &a, double (&acc)[NT]) {
+    __shared__ double sh[RED_THREADS];
+    __shared__ unsigned int s_last;
+    for (int t = 0; t < NT; ++t) {
+        sh[threadIdx.x] = acc[t];
+        __syncthreads();
+        for (int h = RED_THREADS / 2; h > 0; h >>= 1) {
+            if ((int)threadIdx.x < h) sh[threadIdx.x] += sh[threadIdx.x + h];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) a.partials[blockIdx.x * RED_MAX_TERMS + t] = sh[0];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned int k = atomicAdd(a.ticket, 1u);
+        s_last = (k == gridDim.x - 1) ? 1u : 0u;
+    }
+    __syncthreads();
+    if (s_last && threadIdx.x < NT) {
+        __threadfence();
+        double s = 0.0;
+        for (unsigned int b = 0; b < gridDim.x; ++b)
+            s += __ldcg(&a.partials[b * RED_MAX_TERMS + threadIdx.x]);
+        a.out[threadIdx.x] = s;
+    }
+    if (s_last && threadIdx.x == 0) *a.ticket = 0u;
+}
+
+// Squared norm of the inner region (src/cpukernel.cpp:526-549).
+template <typename T>
+__global__ void __launch_bounds__(RED_THREADS) norm_kernel(RedArgs a) {
+    const double s = a.use_scale ? a.scal->pending_inv : 1.0;
+    const int w = a.ix1 - a.ix0;
+    const size_t n = (size_t)w * (a.iy1 - a.iy0);
+    double acc[1] = {0.0};
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
+         k += (size_t)gridDim.x * blockDim.x) {
+        const int y = a.iy0 + (int)(k / w), x = a.ix0 + (int)(k % w);
+        const Cx<double> c = ldc<T>(a, s, x, y);
+        acc[0] += c.re * c.re + c.im * c.im;
+    }
+    block_reduce_and_finish<1>(a, acc);
+}
+
+// Energy sums of src/solver.cpp:320-420 (single component, cartesian):
+// [0] norm2, [1] norm2 over the kinetic region, [2] kinetic, [3] potential,
+// [4] rotational, [5] intra-species, [6] Lee-Huang-Yang.
+template <typename T>
+__global__ void __launch_bounds__(RED_THREADS) energy_kernel(RedArgs a) {
+    const double s = a.use_scale ? a.scal->pending_inv : 1.0;
+    const int w = a.ix1 - a.ix0;
+    const size_t n = (size_t)w * (a.iy1 - a.iy0);
+    const int ihx = a.ix0, ihy = a.iy0, ehx = a.W - a.ix1, ehy = a.H - a.iy1;
+    const double cost_E = -1. / (2. * a.mass);
+    const double c1 = -1. / 12., c2 = 4. / 3., c3 = -2.5;
+    const double d1 = 1. / 6., d2 = -1., d3 = 0.5, d4 = 1. / 3.;
+    const double idx2 = 1.0 / (a.dx * a.dx), idy2 = 1.0 / (a.dy * a.dy);
+    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
+         k += (size_t)gridDim.x * blockDim.x) {
+        const int i = a.iy0 + (int)(k / w), j = a.ix0 + (int)(k % w);
+        const Cx<double> c = ldc<T>(a, s, j, i);
+        const double n2 = c.re * c.re + c.im * c.im;
+        acc[0] += n2;
+        acc[3] += n2 * a.V[(size_t)i * a.W + j];
+        acc[5] += n2 * n2 * 0.5 * a.g;
+        if (a.glhy != 0.0) acc[6] += pow(n2, 2.5) * 0.4 * a.glhy;
+        if (((i - a.iy0 >= (ihy == 0) * 2 && i < a.iy1 - (ehy == 0) * 2) || a.H == 1) &&
+            (j - a.ix0 >= (ihx == 0) * 2 && j < a.ix1 - (ehx == 0) * 2)) {
+            const Cx<double> r = ldc<T>(a, s, j + 1, i), l = ldc<T>(a, s, j - 1, i);
+            const Cx<double> rr = ldc<T>(a, s, j + 2, i), ll = ldc<T>(a, s, j - 2, i);
+            acc[1] += n2;
+            // Re(conj(c) * lap) with lap the 4th-order 5-point Laplacian
+            const double lre = c1 * rr.re + c2 * r.re + c2 * l.re + c1 * ll.re + c3 * c.re;
+            const double lim = c1 * rr.im + c2 * r.im + c2 * l.im + c1 * ll.im + c3 * c.im;
+            acc[2] += cost_E * (c.re * lre + c.im * lim) * idx2;
+            if (a.H > 1) {
+                const Cx<double> up = ldc<T>(a, s, j, i - 1), dn = ldc<T>(a, s, j, i + 1);
+                const Cx<double> uu = ldc<T>(a, s, j, i - 2), dd = ldc<T>(a, s, j, i + 2);
+                const double yre = c1 * dd.re + c2 * dn.re + c2 * up.re + c1 * uu.re + c3 * c.re;
+                const double yim = c1 * dd.im + c2 * dn.im + c2 * up.im + c1 * uu.im + c3 * c.im;
+                acc[2] += cost_E * (c.re * yre + c.im * yim) * idy2;
+                if (a.omega != 0.0) {
+                    double x, y;
+                    cell_coords(a, j, i, &x, &y);
+                    // rot_x = i*y*omega/dx, rot_y = i*x*omega/dy (src/solver.cpp:384-387)
+                    const double ry = x * a.omega / a.dy, rx = y * a.omega / a.dx;
+                    const double dyre = d4 * up.re + d3 * c.re + d2 * dn.re + d1 * dd.re;
+                    const double dyim = d4 * up.im + d3 * c.im + d2 * dn.im + d1 * dd.im;
+                    const double dxre = d4 * r.re + d3 * c.re + d2 * l.re + d1 * ll.re;
+                    const double dxim = d4 * r.im + d3 * c.im + d2 * l.im + d1 * ll.im;
+                    // inner = i*ry*dy_ + i*rx*dx_ ; Re(conj(c) * inner)
+                    const double inre = -(ry * dyim + rx * dxim);
+                    const double inim = ry * dyre + rx * dxre;
+                    acc[4] += c.re * inre + c.im * inim;
+                }
+            }
+        }
+    }
+    block_reduce_and_finish<7>(a, acc);
+}
+
+// Expectation-value sums of src/model.cpp:405-455 (2D cartesian):
+// [0] norm2 [1] x [2] y [3] xx [4] yy [5] px [6] py [7] pxpx [8] pypy [9] lz
+template <typename T>
+__global__ void __launch_bounds__(RED_THREADS) expect_kernel(RedArgs a) {
+    const double s = a.use_scale ? a.scal->pending_inv : 1.0;
+    const int w = a.ix1 - a.ix0;
+    const size_t n = (size_t)w * (a.iy1 - a.iy0);
+    const int ihx = a.ix0, ihy = a.iy0, ehx = a.W - a.ix1, ehy = a.H - a.iy1;
+    const double c1 = -1. / 12., c2 = 4. / 3., c3 = -2.5;
+    const double d1 = 1. / 6., d2 = -1., d3 = 0.5, d4 = 1. / 3.;
+    double acc[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
+         k += (size_t)gridDim.x * blockDim.x) {
+        const int i = a.iy0 + (int)(k / w), j = a.ix0 + (int)(k % w);
+        const Cx<double> c = ldc<T>(a, s, j, i);
+        double x, y;
+        cell_coords(a, j, i, &x, &y);
+        const double n2 = c.re * c.re + c.im * c.im;
+        acc[0] += n2;
+        acc[1] += n2 * x;
+        acc[2] += n2 * y;
+        acc[3] += n2 * x * x;
+        acc[4] += n2 * y * y;
+        if (i - ihy >= (ihy == 0) * 2 && i < a.iy1 - (ehy == 0) * 2 && j - ihx >= (ihx == 0) * 2 &&
+            j < a.ix1 - (ehx == 0) * 2) {
+            const Cx<double> up = ldc<T>(a, s, j, i - 1), dn = ldc<T>(a, s, j, i + 1);
+            const Cx<double> r = ldc<T>(a, s, j + 1, i), l = ldc<T>(a, s, j - 1, i);
+            const Cx<double> uu = ldc<T>(a, s, j, i - 2), dd = ldc<T>(a, s, j, i + 2);
+            const Cx<double> rr = ldc<T>(a, s, j + 2, i), ll = ldc<T>(a, s, j - 2, i);
+            const double dxre = d4 * r.re + d3 * c.re + d2 * l.re + d1 * ll.re;
+            const double dxim = d4 * r.im + d3 * c.im + d2 * l.im + d1 * ll.im;
+            const double dyre = d4 * up.re + d3 * c.re + d2 * dn.re + d1 * dd.re;
+            const double dyim = d4 * up.im + d3 * c.im + d2 * dn.im + d1 * dd.im;
+            // Im(conj(c) * z) = c.re*z.im - c.im*z.re ; Re(conj(c)*z) = c.re*z.re + c.im*z.im
+            acc[5] += c.re * dxim - c.im * dxre;
+            acc[6] += c.re * dyim - c.im * dyre;
+            const double lxre = c1 * rr.re + c2 * r.re + c2 * l.re + c1 * ll.re + c3 * c.re;
+            const double lxim = c1 * rr.im + c2 * r.im + c2 * l.im + c1 * ll.im + c3 * c.im;
+            const double lyre = c1 * dd.re + c2 * dn.re + c2 * up.re + c1 * uu.re + c3 * c.re;
+            const double lyim = c1 * dd.im + c2 * dn.im + c2 * up.im + c1 * uu.im + c3 * c.im;
+            acc[7] += c.re * lxre + c.im * lxim;
+            acc[8] += c.re * lyre + c.im * lyim;
+            const double zre = y / a.dx * dxre + x / a.dy * dyre;
+            const double zim = y / a.dx * dxim + x / a.dy * dyim;
+            acc[9] += c.re * zim - c.im * zre;
+        }
+    }
+    block_reduce_and_finish<10>(a, acc);
+}
+
+// --------------------------------------------------------- step dispatch
+// The step variants are instantiated in step_f64_real.cu, step_f64_imag.cu,
+// step_f32_real.cu and step_f32_imag.cu (compiled in parallel).
+template <typename T>
+cudaError_t dispatch_step(int C, bool imag, bool rot, bool phase, const StepArgs<T> &a, int warps,
+                          size_t smem, int blocks, cudaStream_t st);
+
+template <>
+cudaError_t dispatch_step<double>(int C, bool imag, bool rot, bool phase,
+                                  const StepArgs<double> &a, int warps, size_t smem, int blocks,
+                                  cudaStream_t st) {
+    return imag ? tsb::launch_step_f64_imag(C, rot, phase, a, warps, smem, blocks, st)
+                : tsb::launch_step_f64_real(C, rot, phase, a, warps, smem, blocks, st);
+}
+
+template <>
+cudaError_t dispatch_step<float>(int C, bool imag, bool rot, bool phase, const StepArgs<float> &a,
+                                 int warps, size_t smem, int blocks, cudaStream_t st) {
+    return imag ? tsb::launch_step_f32_imag(C, rot, phase, a, warps, smem, blocks, st)
+                : tsb::launch_step_f32_real(C, rot, phase, a, warps, smem, blocks, st);
+}
+
+int slot_bytes(int C, bool fp32, bool imag) {
+    const int cell = fp32 ? 8 : 16;
+    const int tab = imag ? cell / 2 : cell;
+    return 32 * C * (cell + tab);
+}
+
+int div_up(long a, long b) { return (int)((a + b - 1) / b); }
+
+}  // namespace
+
+// =================================================================== handle
+struct ts_b200_kernel {
+    ts_b200_desc d{};
+    int W = 0, H = 0, P = 0;
+    bool fp32 = false, imag = false, rot = false, phase = false;
+    size_t cell = 0, tab_cell = 0;
+    void *psi[2] = {nullptr, nullptr};
+    int cur = 0;
+    void *tab = nullptr;
+    void *row_ab = nullptr, *col_ab = nullptr;
+    double *partials = nullptr;
+    size_t partials_cap = 0;
+    Scalars *scal = nullptr;
+    double *staging = nullptr;  // 2 * W * H doubles
+    double *vtab = nullptr;     // V for energies (W * H)
+    bool have_v = false;
+    double *red_partials = nullptr;
+    double *red_out = nullptr;
+    unsigned int *red_ticket = nullptr;
+    cudaStream_t own_stream = nullptr, stream = nullptr;
+    int C = 2, seg_h = 64, warps = 4, ring = 4;
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = 0;
+    int num_sms = 148;
+    std::string err;
+};
+
+namespace {
+
+int fail(ts_b200_kernel *k, int status, const std::string &msg) {
+    if (k) k->err = msg;
+    return status;
+}
+
+int cuda_fail(ts_b200_kernel *k, cudaError_t e, const char *what) {
+    std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+    if (k) k->err = m;
+    return e == cudaErrorMemoryAllocation ? TS_B200_OUT_OF_MEMORY : TS_B200_CUDA_ERROR;
+}
+
+#define TSB_CHECK(k, call)                                   \
+    do {                                                     \
+        cudaError_t e_ = (call);                             \
+        if (e_ != cudaSuccess) return cuda_fail(k, e_, #call); \
+    } while (0)
+
+void drop_graph(ts_b200_kernel *k) {
+    if (k->graph) {
+        cudaGraphExecDestroy(k->graph);
+        k->graph = nullptr;
+        k->graph_steps = 0;
+    }
+}
+
+void choose_launch(ts_b200_kernel *k) {
+    // Column strips of 32*C cells; C = 4 halves the shuffles per cell and the
+    // recomputed halo fraction on wide tiles, C = 2 wastes less on narrow ones
+    // and keeps the 7-row rotation window within the register budget.
+    k->C = (!k->rot && k->W >= 480) ? 4 : 2;
+    const int hx = k->rot ? 8 : 4;
+    const int wo = 32 * k->C - 2 * hx;
+    const int strips = div_up(k->W, wo);
+    // about 8 resident warps per SM in one wave, segments of 32..256 rows
+    const long target = (long)k->num_sms * 8;
+    const int segs = std::max(1, (int)(target / std::max(1, strips)));
+    int sh = div_up(k->H, segs);
+    sh = std::max(32, std::min(256, sh));
+    k->seg_h = std::min(sh, std::max(1, k->H));
+    k->warps = 4;
+    k->ring = 4;
+}
+
+void geometry(const ts_b200_kernel *k, int *strips, int *segs, int *blocks, size_t *smem) {
+    const int hx = k->rot ? 8 : 4;
+    const int wo = 32 * k->C - 2 * hx;
+    *strips = div_up(k->W, wo);
+    *segs = div_up(k->H, k->seg_h);
+    const int tasks = *strips * *segs;
+    *blocks = div_up(tasks, k->warps);
+    *smem = (size_t)k->warps * k->ring * (slot_bytes(k->C, k->fp32, k->imag) + 8);
+}
+
+template <typename T>
+int launch_step_t(ts_b200_kernel *k, int exchange, bool dry = false) {
+    int strips, segs, blocks;
+    size_t smem;
+    geometry(k, &strips, &segs, &blocks, &smem);
+    if (dry) blocks = 0;
+    const size_t tasks = (size_t)strips * segs;
+    if (k->imag && tasks > k->partials_cap) {
+        if (k->partials) cudaFree(k->partials);
+        k->partials = nullptr;
+        TSB_CHECK(k, cudaMalloc(&k->partials, tasks * sizeof(double)));
+        k->partials_cap = tasks;
+    }
+    StepArgs<T> a{};
+    a.psi_in = k->psi[k->cur];
+    a.psi_out = k->psi[1 - k->cur];
+    a.pot = k->tab;
+    a.row_ab = k->row_ab;
+    a.col_ab = k->col_ab;
+    a.W = k->W;
+    a.H = k->H;
+    a.P = k->P;
+    a.ix0 = k->d.inner_x0;
+    a.ix1 = k->d.inner_x1;
+    a.iy0 = k->d.inner_y0;
+    a.iy1 = k->d.inner_y1;
+    a.n_strips = strips;
+    a.n_segs = segs;
+    a.seg_h = k->seg_h;
+    a.ring = k->ring;
+    a.aH = (T)k->d.a_h;
+    a.bH = (T)k->d.b_h;
+    a.aV = (T)k->d.a_v;
+    a.bV = (T)k->d.b_v;
+    a.ca = (T)k->d.coupling;
+    a.caa = (T)k->d.lhy_coupling;
+    a.partials = k->partials;
+    a.scal = k->scal;
+    a.dxdy = k->d.delta_x * k->d.delta_y;
+    a.norm0 = k->d.norm0;
+    cudaError_t e =
+        dispatch_step<T>(k->C, k->imag, k->rot, k->phase, a, k->warps, smem, blocks, k->stream);
+    if (e != cudaSuccess) return cuda_fail(k, e, "step kernel launch");
+    if (dry) return TS_B200_OK;
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    k->cur = 1 - k->cur;
+    if (exchange && (k->d.periodic_x || k->d.periodic_y)) {
+        const int hx = k->d.halo_x, hy = k->d.halo_y;
+        const int nx = k->d.periodic_x ? 2 * hx * k->H : 0;
+        const int ny = k->d.periodic_y ? 2 * hy * (k->d.periodic_x ? k->W - 2 * hx : k->W) : 0;
+        const int n = nx + ny;
+        if (n > 0) {
+            const int threads = 256;
+            const int nb = std::min(div_up(n, threads), 4096);
+            halo_kernel<T><<<nb, threads, 0, k->stream>>>(
+                reinterpret_cast<Cx<T> *>(k->psi[k->cur]), k->W, k->H, k->P, hx, hy,
+                k->d.periodic_x, k->d.periodic_y, k->d.inner_y0);
+            e = cudaGetLastError();
+            if (e != cudaSuccess) return cuda_fail(k, e, "halo kernel launch");
+            g_launches.fetch_add(1, std::memory_order_relaxed);
+        }
+    }
+    return TS_B200_OK;
+}
+
+int launch_step(ts_b200_kernel *k, int exchange, bool dry = false) {
+    return k->fp32 ? launch_step_t<float>(k, exchange, dry) : launch_step_t<double>(k, exchange, dry);
+}
+
+int kernels_per_step(const ts_b200_kernel *k, int exchange) {
+    return 1 + ((exchange && (k->d.periodic_x || k->d.periodic_y)) ? 1 : 0);
+}
+
+int check_device_error(ts_b200_kernel *k) {
+    int err = 0;
+    cudaError_t e = cudaMemcpyAsync(&err, &k->scal->error, sizeof(int), cudaMemcpyDeviceToHost,
+                                    k->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(k->stream);
+    if (e != cudaSuccess) return cuda_fail(k, e, "device status read");
+    if (err) {
+        int zero = 0;
+        cudaMemcpy(&k->scal->error, &zero, sizeof(int), cudaMemcpyHostToDevice);
+        return fail(k, TS_B200_DEVICE_TIMEOUT,
+                    "a bounded wait in the step kernel gave up (row copy did not complete)");
+    }
+    return TS_B200_OK;
+}
+
+void fill_red_args(ts_b200_kernel *k, RedArgs &a) {
+    a.psi = k->psi[k->cur];
+    a.W = k->W;
+    a.H = k->H;
+    a.P = k->P;
+    a.ix0 = k->d.inner_x0;
+    a.ix1 = k->d.inner_x1;
+    a.iy0 = k->d.inner_y0;
+    a.iy1 = k->d.inner_y1;
+    a.scal = k->scal;
+    a.use_scale = k->imag ? 1 : 0;
+    a.dx = k->d.delta_x;
+    a.dy = k->d.delta_y;
+    a.partials = k->red_partials;
+    a.out = k->red_out;
+    a.ticket = k->red_ticket;
+}
+
+int red_blocks(const ts_b200_kernel *k) {
+    const long n = (long)(k->d.inner_x1 - k->d.inner_x0) * (k->d.inner_y1 - k->d.inner_y0);
+    return std::max(1, std::min(RED_MAX_BLOCKS, div_up(n, RED_THREADS)));
+}
+
+int read_red(ts_b200_kernel *k, double *host, int nterms) {
+    TSB_CHECK(k, cudaMemcpyAsync(host, k->red_out, nterms * sizeof(double), cudaMemcpyDeviceToHost,
+                                 k->stream));
+    TSB_CHECK(k, cudaStreamSynchronize(k->stream));
+    return TS_B200_OK;
+}
+
+// Rotation coefficients per row and column, computed on the host with the
+// C library exactly as src/cpucartesian.cpp:146-147,165-166 does.
+template <typename T>
+int upload_rotation(ts_b200_kernel *k) {
+    const int W = k->W, H = k->H;
+    Cx<T> *rows = new (std::nothrow) Cx<T>[H];
+    Cx<T> *cols = new (std::nothrow) Cx<T>[W];
+    if (!rows || !cols) {
+        delete[] rows;
+        delete[] cols;
+        return fail(k, TS_B200_OUT_OF_MEMORY, "host allocation for rotation tables");
+    }
+    const int offx = (int)k->d.rot_offset_x, offy = (int)k->d.rot_offset_y;
+    for (int y = 0; y < H; ++y) {
+        const double ang = -0.5 * k->d.alpha_y * (y + offy);
+        const double a = k->imag ? std::cosh(ang) : std::cos(ang);
+        const double b = k->imag ? std::sinh(ang) : std::sin(ang);
+        rows[y] = Cx<T>{(T)a, (T)b};
+    }
+    for (int x = 0; x < W; ++x) {
+        const double ang = k->d.alpha_x * (x + offx);
+        const double a = k->imag ? std::cosh(ang) : std::cos(ang);
+        const double b = k->imag ? std::sinh(ang) : std::sin(ang);
+        cols[x] = Cx<T>{(T)a, (T)b};
+    }
+    cudaError_t e = cudaMemcpy(k->row_ab, rows, sizeof(Cx<T>) * H, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(k->col_ab, cols, sizeof(Cx<T>) * W, cudaMemcpyHostToDevice);
+    delete[] rows;
+    delete[] cols;
+    if (e != cudaSuccess) return cuda_fail(k, e, "rotation table upload");
+    return TS_B200_OK;
+}
+
+int grid_for(size_t n) { return (int)std::max<size_t>(1, std::min<size_t>((n + 255) / 256, 8192)); }
+
+}  // namespace
+
+// ================================================================ C ABI
+extern "C" {
+
+const char *ts_b200_version(void) { return "ts_b200 1.0 (sm_100a)"; }
+
+uint64_t ts_b200_launch_count(void) { return g_launches.load(); }
+
+const char *ts_b200_status_string(int s) {
+    switch (s) {
+        case TS_B200_OK: return "ok";
+        case TS_B200_INVALID_ARGUMENT: return "invalid argument";
+        case TS_B200_CUDA_ERROR: return "CUDA error";
+        case TS_B200_OUT_OF_MEMORY: return "out of device memory";
+        case TS_B200_UNSUPPORTED: return "unsupported configuration";
+        case TS_B200_DEVICE_TIMEOUT: return "device wait timed out";
+        case TS_B200_NO_DEVICE: return "no CUDA device";
+        default: return "unknown status";
+    }
+}
+
+const char *ts_b200_last_error(const ts_b200_kernel *k) { return k ? k->err.c_str() : ""; }
+
+int ts_b200_create(const ts_b200_desc *d, ts_b200_kernel **out) {
+    if (!d || !out) return TS_B200_INVALID_ARGUMENT;
+    *out = nullptr;
+    if (d->dim_x < 1 || d->dim_y < 1 || d->inner_x0 < 0 || d->inner_x1 > d->dim_x ||
+        d->inner_x0 >= d->inner_x1 || d->inner_y0 < 0 || d->inner_y1 > d->dim_y ||
+        d->inner_y0 >= d->inner_y1 || d->halo_x < 0 || d->halo_y < 0 ||
+        (d->precision != TS_B200_FP64 && d->precision != TS_B200_FP32))
+        return TS_B200_INVALID_ARGUMENT;
+    if ((long)d->dim_x * d->dim_y > (1L << 31) - 1) return TS_B200_UNSUPPORTED;
+    if (d->periodic_x && d->dim_x < 2 * d->halo_x) return TS_B200_INVALID_ARGUMENT;
+    if (d->periodic_y && d->dim_y < 2 * d->halo_y) return TS_B200_INVALID_ARGUMENT;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return TS_B200_NO_DEVICE;
+    ts_b200_kernel *k = new (std::nothrow) ts_b200_kernel();
+    if (!k) return TS_B200_OUT_OF_MEMORY;
+    k->d = *d;
+    k->W = d->dim_x;
+    k->H = d->dim_y;
+    k->P = (d->dim_x + 3) & ~3;
+    k->fp32 = d->precision == TS_B200_FP32;
+    k->imag = d->imag_time != 0;
+    k->rot = d->alpha_x != 0.0 && d->alpha_y != 0.0;
+    k->phase = d->coupling != 0.0 || d->lhy_coupling != 0.0;
+    k->cell = k->fp32 ? 8 : 16;
+    k->tab_cell = k->imag ? k->cell / 2 : k->cell;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&k->num_sms, cudaDevAttrMultiProcessorCount, dev);
+    choose_launch(k);
+    const size_t ncell = (size_t)k->P * k->H;
+    cudaError_t e = cudaSuccess;
+    auto alloc = [&](void **p, size_t bytes) {
+        if (e == cudaSuccess) e = cudaMalloc(p, bytes);
+        if (e == cudaSuccess) e = cudaMemset(*p, 0, bytes);
+    };
+    alloc(&k->psi[0], ncell * k->cell);
+    alloc(&k->psi[1], ncell * k->cell);
+    alloc(&k->tab, ncell * k->tab_cell);
+    alloc((void **)&k->scal, sizeof(Scalars));
+    alloc((void **)&k->staging, (size_t)2 * k->W * k->H * sizeof(double));
+    alloc((void **)&k->red_partials, (size_t)RED_MAX_BLOCKS * RED_MAX_TERMS * sizeof(double));
+    alloc((void **)&k->red_out, RED_MAX_TERMS * sizeof(double));
+    alloc((void **)&k->red_ticket, sizeof(unsigned int));
+    if (k->rot) {
+        alloc(&k->row_ab, (size_t)k->H * (k->fp32 ? 8 : 16));
+        alloc(&k->col_ab, (size_t)k->W * (k->fp32 ? 8 : 16));
+    }
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&k->own_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        int s = cuda_fail(nullptr, e, "allocation");
+        ts_b200_destroy(k);
+        return s;
+    }
+    k->stream = k->own_stream;
+    Scalars s0{};
+    s0.pending_inv = 1.0;
+    s0.renorm = (k->imag && d->norm0 != 0.0) ? 1 : 0;
+    e = cudaMemcpy(k->scal, &s0, sizeof s0, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        int s = cuda_fail(nullptr, e, "scalar init");
+        ts_b200_destroy(k);
+        return s;
+    }
+    if (k->rot) {
+        int s = k->fp32 ? upload_rotation<float>(k) : upload_rotation<double>(k);
+        if (s != TS_B200_OK) {
+            ts_b200_destroy(k);
+            return s;
+        }
+    }
+    *out = k;
+    return TS_B200_OK;
+}
+
+int ts_b200_destroy(ts_b200_kernel *k) {
+    if (!k) return TS_B200_OK;
+    drop_graph(k);
+    if (k->own_stream) cudaStreamSynchronize(k->own_stream);
+    if (k->stream && k->stream != k->own_stream) cudaStreamSynchronize(k->stream);
+    void *bufs[] = {k->psi[0], k->psi[1], k->tab, k->row_ab, k->col_ab, k->partials, k->scal,
+                    k->staging, k->vtab, k->red_partials, k->red_out, k->red_ticket};
+    for (void *b : bufs)
+        if (b) cudaFree(b);
+    if (k->own_stream) cudaStreamDestroy(k->own_stream);
+    delete k;
+    return TS_B200_OK;
+}
+
+int ts_b200_set_stream(ts_b200_kernel *k, void *stream) {
+    if (!k) return TS_B200_INVALID_ARGUMENT;
+    drop_graph(k);
+    k->stream = stream ? reinterpret_cast<cudaStream_t>(stream) : k->own_stream;
+    return TS_B200_OK;
+}
+
+int ts_b200_synchronize(ts_b200_kernel *k) {
+    if (!k) return TS_B200_INVALID_ARGUMENT;
+    TSB_CHECK(k, cudaStreamSynchronize(k->stream));
+    return check_device_error(k);
+}
+
+int ts_b200_set_state(ts_b200_kernel *k, const double *re, const double *im, size_t stride) {
+    if (!k || !re || !im || stride < (size_t)k->W) return TS_B200_INVALID_ARGUMENT;
+    double *sre = k->staging, *sim = k->staging + (size_t)k->W * k->H;
+    TSB_CHECK(k, cudaMemcpy2DAsync(sre, k->W * sizeof(double), re, stride * sizeof(double),
+                                   k->W * sizeof(double), k->H, cudaMemcpyHostToDevice, k->stream));
+    TSB_CHECK(k, cudaMemcpy2DAsync(sim, k->W * sizeof(double), im, stride * sizeof(double),
+                                   k->W * sizeof(double), k->H, cudaMemcpyHostToDevice, k->stream));
+    const size_t n = (size_t)k->P * k->H;
+    if (k->fp32)
+        pack_state_kernel<float><<<grid_for(n), 256, 0, k->stream>>>(
+            reinterpret_cast<Cx<float> *>(k->psi[k->cur]), k->W, k->H, k->P, sre, sim, k->W);
+    else
+        pack_state_kernel<double><<<grid_for(n), 256, 0, k->stream>>>(
+            reinterpret_cast<Cx<double> *>(k->psi[k->cur]), k->W, k->H, k->P, sre, sim, k->W);
+    TSB_CHECK(k, cudaGetLastError());
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    // a freshly uploaded state carries no pending renormalisation
+    const double one = 1.0;
+    TSB_CHECK(k, cudaMemcpyAsync(&k->scal->pending_inv, &one, sizeof(double), cudaMemcpyHostToDevice,
+                                 k->stream));
+    TSB_CHECK(k, cudaStreamSynchronize(k->stream));
+    return TS_B200_OK;
+}
+
+int ts_b200_set_exp_potential(ts_b200_kernel *k, const double *re, const double *im,
+                              size_t stride) {
+    if (!k || !re || (!im && !k->imag) || stride < (size_t)k->W) return TS_B200_INVALID_ARGUMENT;
+    double *sre = k->staging, *sim = k->staging + (size_t)k->W * k->H;
+    TSB_CHECK(k, cudaMemcpy2DAsync(sre, k->W * sizeof(double), re, stride * sizeof(double),
+                                   k->W * sizeof(double), k->H, cudaMemcpyHostToDevice, k->stream));
+    if (im)
+        TSB_CHECK(k, cudaMemcpy2DAsync(sim, k->W * sizeof(double), im, stride * sizeof(double),
+                                       k->W * sizeof(double), k->H, cudaMemcpyHostToDevice,
+                                       k->stream));
+    else
+        TSB_CHECK(k, cudaMemsetAsync(sim, 0, (size_t)k->W * k->H * sizeof(double), k->stream));
+    const size_t n = (size_t)k->P * k->H;
+    if (k->fp32)
+        pack_table_kernel<float><<<grid_for(n), 256, 0, k->stream>>>(k->tab, k->imag, k->W, k->H,
+                                                                      k->P, sre, sim, k->W);
+    else
+        pack_table_kernel<double><<<grid_for(n), 256, 0, k->stream>>>(k->tab, k->imag, k->W, k->H,
+                                                                       k->P, sre, sim, k->W);
+    TSB_CHECK(k, cudaGetLastError());
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    TSB_CHECK(k, cudaStreamSynchronize(k->stream));
+    return TS_B200_OK;
+}
+
+int ts_b200_set_state_device(ts_b200_kernel *k, const void *aos, size_t pitch) {
+    if (!k || !aos || pitch < (size_t)k->W) return TS_B200_INVALID_ARGUMENT;
+    TSB_CHECK(k, cudaMemcpy2DAsync(k->psi[k->cur], k->P * k->cell, aos, pitch * k->cell,
+                                   k->W * k->cell, k->H, cudaMemcpyDeviceToDevice, k->stream));
+    const double one = 1.0;
+    TSB_CHECK(k, cudaMemcpyAsync(&k->scal->pending_inv, &one, sizeof(double), cudaMemcpyHostToDevice,
+                                 k->stream));
+    return TS_B200_OK;
+}
+
+int ts_b200_get_state_device(ts_b200_kernel *k, void *aos, size_t pitch) {
+    if (!k || !aos || pitch < (size_t)k->W) return TS_B200_INVALID_ARGUMENT;
+    const size_t n = (size_t)k->W * k->H;
+    if (k->fp32)
+        copy_tile_kernel<float><<<grid_for(n), 256, 0, k->stream>>>(
+            reinterpret_cast<Cx<float> *>(aos), pitch,
+            reinterpret_cast<const Cx<float> *>(k->psi[k->cur]), k->P, k->W, k->H, k->scal,
+            k->imag ? 1 : 0);
+    else
+        copy_tile_kernel<double><<<grid_for(n), 256, 0, k->stream>>>(
+            reinterpret_cast<Cx<double> *>(aos), pitch,
+            reinterpret_cast<const Cx<double> *>(k->psi[k->cur]), k->P, k->W, k->H, k->scal,
+            k->imag ? 1 : 0);
+    TSB_CHECK(k, cudaGetLastError());
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    return TS_B200_OK;
+}
+
+int ts_b200_set_exp_potential_device(ts_b200_kernel *k, const void *table, size_t pitch) {
+    if (!k || !table || pitch < (size_t)k->W) return TS_B200_INVALID_ARGUMENT;
+    TSB_CHECK(k, cudaMemcpy2DAsync(k->tab, k->P * k->tab_cell, table, pitch * k->tab_cell,
+                                   k->W * k->tab_cell, k->H, cudaMemcpyDeviceToDevice, k->stream));
+    return TS_B200_OK;
+}
+
+int ts_b200_step(ts_b200_kernel *k, int exchange) {
+    if (!k) return TS_B200_INVALID_ARGUMENT;
+    return launch_step(k, exchange);
+}
+
+int ts_b200_evolve(ts_b200_kernel *k, int iterations) {
+    if (!k || iterations < 0) return TS_B200_INVALID_ARGUMENT;
+    if (iterations == 0) return TS_B200_OK;
+    // Steps 0 .. iterations-2 refresh the halo; the last one does not
+    // (src/solver.cpp:203-209).  Runs of G exchanging steps starting from
+    // buffer 0 are replayed from one CUDA graph (G even, so the graph leaves
+    // the buffers as it found them).
+    const int G = 32;
+    int remaining = iterations - 1;  // exchanging steps
+    if (remaining > 0 && k->cur != 0) {
+        int s = launch_step(k, 1);
+        if (s) return s;
+        --remaining;
+    }
+    if (remaining >= G) {
+        if (!k->graph || k->graph_steps != G) {
+            drop_graph(k);
+            int s0 = launch_step(k, 1, true);  // scratch and attributes before capture
+            if (s0) return s0;
+            cudaGraph_t g = nullptr;
+            TSB_CHECK(k, cudaStreamBeginCapture(k->stream, cudaStreamCaptureModeThreadLocal));
+            const uint64_t before = g_launches.load();
+            int s = TS_B200_OK;
+            for (int i = 0; i < G && s == TS_B200_OK; ++i) s = launch_step(k, 1);
+            cudaError_t e = cudaStreamEndCapture(k->stream, &g);
+            g_launches.store(before);  // captured launches are counted when replayed
+            if (s != TS_B200_OK) {
+                if (g) cudaGraphDestroy(g);
+                return s;
+            }
+            if (e != cudaSuccess) return cuda_fail(k, e, "graph capture");
+            e = cudaGraphInstantiate(&k->graph, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) return cuda_fail(k, e, "graph instantiate");
+            k->graph_steps = G;
+        }
+        const int per = kernels_per_step(k, 1);
+        while (remaining >= G) {
+            TSB_CHECK(k, cudaGraphLaunch(k->graph, k->stream));
+            g_launches.fetch_add((uint64_t)G * per, std::memory_order_relaxed);
+            remaining -= G;
+        }
+    }
+    for (; remaining > 0; --remaining) {
+        int s = launch_step(k, 1);
+        if (s) return s;
+    }
+    return launch_step(k, 0);
+}
+
+int ts_b200_get_sample(ts_b200_kernel *k, size_t dest_stride, size_t x, size_t y, size_t width,
+                       size_t height, double *re, double *im) {
+    if (!k || !re || !im || x + width > (size_t)k->W || y + height > (size_t)k->H ||
+        dest_stride < width)
+        return TS_B200_INVALID_ARGUMENT;
+    if (width == 0 || height == 0) return TS_B200_OK;
+    double *sre = k->staging, *sim = k->staging + width * height;
+    const size_t n = width * height;
+    if (k->fp32)
+        unpack_state_kernel<float><<<grid_for(n), 256, 0, k->stream>>>(
+            reinterpret_cast<const Cx<float> *>(k->psi[k->cur]), k->P, (int)x, (int)y, (int)width,
+            (int)height, k->scal, k->imag ? 1 : 0, sre, sim);
+    else
+        unpack_state_kernel<double><<<grid_for(n), 256, 0, k->stream>>>(
+            reinterpret_cast<const Cx<double> *>(k->psi[k->cur]), k->P, (int)x, (int)y,
+            (int)width, (int)height, k->scal, k->imag ? 1 : 0, sre, sim);
+    TSB_CHECK(k, cudaGetLastError());
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    TSB_CHECK(k, cudaMemcpy2DAsync(re, dest_stride * sizeof(double), sre, width * sizeof(double),
+                                   width * sizeof(double), height, cudaMemcpyDeviceToHost,
+                                   k->stream));
+    TSB_CHECK(k, cudaMemcpy2DAsync(im, dest_stride * sizeof(double), sim, width * sizeof(double),
+                                   width * sizeof(double), height, cudaMemcpyDeviceToHost,
+                                   k->stream));
+    TSB_CHECK(k, cudaStreamSynchronize(k->stream));
+    return check_device_error(k);
+}
+
+int ts_b200_squared_norm(ts_b200_kernel *k, double *out) {
+    if (!k || !out) return TS_B200_INVALID_ARGUMENT;
+    RedArgs a{};
+    fill_red_args(k, a);
+    const int nb = red_blocks(k);
+    if (k->fp32) norm_kernel<float><<<nb, RED_THREADS, 0, k->stream>>>(a);
+    else norm_kernel<double><<<nb, RED_THREADS, 0, k->stream>>>(a);
+    TSB_CHECK(k, cudaGetLastError());
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    double s = 0;
+    int st = read_red(k, &s, 1);
+    if (st) return st;
+    *out = s * k->d.delta_x * k->d.delta_y;
+    return TS_B200_OK;
+}
+
+int ts_b200_energies(ts_b200_kernel *k, const double *potential, const ts_b200_energy_params *p,
+                     ts_b200_energy_result *out) {
+    if (!k || !p || !out) return TS_B200_INVALID_ARGUMENT;
+    if (potential) {
+        if (!k->vtab) TSB_CHECK(k, cudaMalloc((void **)&k->vtab, (size_t)k->W * k->H * sizeof(double)));
+        TSB_CHECK(k, cudaMemcpyAsync(k->vtab, potential, (size_t)k->W * k->H * sizeof(double),
+                                     cudaMemcpyHostToDevice, k->stream));
+        k->have_v = true;
+    }
+    if (!k->have_v) return fail(k, TS_B200_INVALID_ARGUMENT, "no potential uploaded for energies");
+    RedArgs a{};
+    fill_red_args(k, a);
+    a.V = k->vtab;
+    a.start_x = p->start_x;
+    a.start_y = p->start_y;
+    a.gnx = p->global_no_halo_dim_x;
+    a.gny = p->global_no_halo_dim_y;
+    a.Lx = p->length_x;
+    a.Ly = p->length_y;
+    a.mass = p->mass;
+    a.g = p->coupling;
+    a.glhy = p->lhy_coupling;
+    a.omega = p->angular_velocity;
+    const int nb = red_blocks(k);
+    if (k->fp32) energy_kernel<float><<<nb, RED_THREADS, 0, k->stream>>>(a);
+    else energy_kernel<double><<<nb, RED_THREADS, 0, k->stream>>>(a);
+    TSB_CHECK(k, cudaGetLastError());
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    double s[7];
+    int st = read_red(k, s, 7);
+    if (st) return st;
+    // final arithmetic of src/solver.cpp:532-538,561
+    out->kinetic = s[2] / s[1];
+    out->rotational = s[4] / s[1];
+    out->potential = s[3] / s[0];
+    out->intra = s[5] / s[0];
+    out->lhy = s[6] / s[0];
+    out->total = out->kinetic + out->potential + out->intra + out->rotational + out->lhy;
+    out->norm2 = s[0] * (k->d.delta_y * p->length_x / p->global_no_halo_dim_x);
+    return TS_B200_OK;
+}
+
+int ts_b200_expectations(ts_b200_kernel *k, const ts_b200_energy_params *p,
+                         ts_b200_expectation_result *out) {
+    if (!k || !p || !out) return TS_B200_INVALID_ARGUMENT;
+    RedArgs a{};
+    fill_red_args(k, a);
+    a.start_x = p->start_x;
+    a.start_y = p->start_y;
+    a.gnx = p->global_no_halo_dim_x;
+    a.gny = p->global_no_halo_dim_y;
+    a.Lx = p->length_x;
+    a.Ly = p->length_y;
+    const int nb = red_blocks(k);
+    if (k->fp32) expect_kernel<float><<<nb, RED_THREADS, 0, k->stream>>>(a);
+    else expect_kernel<double><<<nb, RED_THREADS, 0, k->stream>>>(a);
+    TSB_CHECK(k, cudaGetLastError());
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    double s[10];
+    int st = read_red(k, s, 10);
+    if (st) return st;
+    // final arithmetic of src/model.cpp:456-534
+    const double ppx = -1. / k->d.delta_x, ppy = 1. / k->d.delta_y;
+    out->mean_x = s[1] / s[0];
+    out->mean_y = s[2] / s[0];
+    out->mean_xx = s[3] / s[0];
+    out->mean_yy = s[4] / s[0];
+    out->mean_px = -s[5] * ppx / s[0];
+    out->mean_py = -s[6] * ppy / s[0];
+    out->mean_pxpx = -s[7] * ppx * ppx / s[0];
+    out->mean_pypy = -s[8] * ppy * ppy / s[0];
+    out->mean_lz = s[9] / s[0];
+    out->norm2 = s[0] * (k->d.delta_x * k->d.delta_y);
+    return TS_B200_OK;
+}
+
+int ts_b200_launch_info(const ts_b200_kernel *k, ts_b200_launch_shape *out) {
+    if (!k || !out) return TS_B200_INVALID_ARGUMENT;
+    int strips, segs, blocks;
+    size_t smem;
+    geometry(k, &strips, &segs, &blocks, &smem);
+    out->cells_per_lane = k->C;
+    out->segment_rows = k->seg_h;
+    out->warps_per_block = k->warps;
+    out->ring_depth = k->ring;
+    out->strips = strips;
+    out->segments = segs;
+    out->blocks = blocks;
+    out->threads = k->warps * 32;
+    out->smem_bytes = (int64_t)smem;
+    return TS_B200_OK;
+}
+
+int ts_b200_set_launch(ts_b200_kernel *k, int C, int seg_h, int warps, int ring) {
+    if (!k) return TS_B200_INVALID_ARGUMENT;
+    if (C != 0 && C != 2 && C != 4) return TS_B200_INVALID_ARGUMENT;
+    if (C == 4 && k->rot) return fail(k, TS_B200_UNSUPPORTED, "rotation kernels use 2 cells per lane");
+    if (warps != 0 && warps != 1 && warps != 2 && warps != 4) return TS_B200_INVALID_ARGUMENT;
+    if (ring != 0 && (ring < 3 || ring > 12)) return TS_B200_INVALID_ARGUMENT;
+    if (seg_h < 0) return TS_B200_INVALID_ARGUMENT;
+    if (C) k->C = C;
+    if (seg_h) k->seg_h = seg_h;
+    if (warps) k->warps = warps;
+    if (ring) k->ring = ring;
+    int strips, segs, blocks;
+    size_t smem;
+    geometry(k, &strips, &segs, &blocks, &smem);
+    if (smem > 227 * 1024) return fail(k, TS_B200_INVALID_ARGUMENT, "ring does not fit in shared memory");
+    drop_graph(k);
+    return TS_B200_OK;
+}
+
+int ts_b200_host_alloc(void **ptr, size_t bytes) {
+    if (!ptr) return TS_B200_INVALID_ARGUMENT;
+    cudaError_t e = cudaHostAlloc(ptr, bytes, cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+        *ptr = nullptr;
+        return e == cudaErrorMemoryAllocation ? TS_B200_OUT_OF_MEMORY : TS_B200_CUDA_ERROR;
+    }
+    return TS_B200_OK;
+}
+
+int ts_b200_host_free(void *ptr) {
+    if (!ptr) return TS_B200_OK;
+    return cudaFreeHost(ptr) == cudaSuccess ? TS_B200_OK : TS_B200_CUDA_ERROR;
+}
+
+}  // extern "C"

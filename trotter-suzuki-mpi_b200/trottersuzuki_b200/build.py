@@ -1,0 +1,60 @@
+"""Build the CUDA library libtsb200.so (sm_100a) in-tree.
+
+    python -m trottersuzuki_b200.build          (from trotter-suzuki-mpi_b200/)
+
+Each .cu under csrc/ is compiled to an object under _build/ in parallel, then
+linked next to this file so that the package loads it from its own folder.
+"""
+import concurrent.futures as cf
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG_ROOT = os.path.dirname(HERE)
+REPO = os.path.dirname(PKG_ROOT)
+CSRC = os.path.join(PKG_ROOT, "csrc")
+INCLUDE = os.path.join(REPO, "include")
+BUILD = os.path.join(REPO, "_build")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + INCLUDE, "-I" + CSRC]
+
+
+def _stale(obj, deps):
+    if not os.path.exists(obj):
+        return True
+    t = os.path.getmtime(obj)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def _compile(src, extra):
+    obj = os.path.join(BUILD, os.path.basename(src) + ".o")
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
+    headers.append(os.path.join(INCLUDE, "ts_b200.h"))
+    if _stale(obj, [src] + headers):
+        cmd = [NVCC] + ARCH + FLAGS + extra + ["-c", src, "-o", obj + ".tmp"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"nvcc failed for {src}:\n{r.stdout}\n{r.stderr}")
+        os.replace(obj + ".tmp", obj)
+    return obj
+
+
+def build(verbose=True, extra=()):
+    os.makedirs(BUILD, exist_ok=True)
+    srcs = sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu"))
+    with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 4)) as ex:
+        objs = list(ex.map(lambda s: _compile(s, list(extra)), srcs))
+    out = os.path.join(HERE, "libtsb200.so")
+    if _stale(out, objs):
+        cmd = [NVCC] + ARCH + ["-shared", "-o", out + ".tmp"] + objs + ["-lcudart"]
+        subprocess.check_call(cmd)
+        os.replace(out + ".tmp", out)
+    if verbose:
+        print("built", out)
+    return out
+
+
+if __name__ == "__main__":
+    build(extra=sys.argv[1:])

@@ -1,0 +1,145 @@
+"""Python handle over the C ABI: one B200 kernel per lattice tile.
+
+This is the low-level object the Python Solver uses, the analogue of the
+reference's ITrotterKernel (src/trottersuzuki.h:502-520).  Host arrays are
+numpy complex128 tiles of shape (dim_y, dim_x) in the reference's tile layout.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _capi
+from ._capi import Desc, EnergyParams, EnergyResult, ExpectationResult, LaunchShape, check, lib
+
+FP64 = _capi.FP64
+FP32 = _capi.FP32
+
+
+def _soa(psi):
+    re = np.ascontiguousarray(np.real(psi), dtype=np.float64)
+    im = np.ascontiguousarray(np.imag(psi), dtype=np.float64)
+    return re, im
+
+
+class Kernel:
+    """A tile resident on the GPU plus its exponential table.
+
+    desc: a _capi.Desc with the tile geometry and the step constants.
+    """
+
+    def __init__(self, desc):
+        self.desc = desc
+        self._h = C.c_void_p()
+        check(lib().ts_b200_create(C.byref(desc), C.byref(self._h)))
+        self.shape = (desc.dim_y, desc.dim_x)
+
+    # -- lifetime -------------------------------------------------------
+    def close(self):
+        if self._h:
+            lib().ts_b200_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def _check(self, status):
+        check(status, self._h)
+
+    # -- data movement ------------------------------------------------------
+    def set_state(self, psi):
+        psi = np.asarray(psi)
+        if psi.shape != self.shape:
+            raise ValueError(f"state shape {psi.shape} != tile {self.shape}")
+        re, im = _soa(psi)
+        self._check(lib().ts_b200_set_state(self._h, re.ctypes.data, im.ctypes.data,
+                                            self.shape[1]))
+
+    def set_exp_potential(self, pot_re, pot_im=None):
+        pr = np.ascontiguousarray(pot_re, dtype=np.float64)
+        if pr.shape != self.shape:
+            raise ValueError("table shape mismatch")
+        pi = None if pot_im is None else np.ascontiguousarray(pot_im, dtype=np.float64)
+        self._check(lib().ts_b200_set_exp_potential(
+            self._h, pr.ctypes.data, None if pi is None else pi.ctypes.data, self.shape[1]))
+
+    def get_state(self, x=0, y=0, width=None, height=None):
+        width = self.shape[1] - x if width is None else width
+        height = self.shape[0] - y if height is None else height
+        re = np.empty((height, width), np.float64)
+        im = np.empty((height, width), np.float64)
+        self._check(lib().ts_b200_get_sample(self._h, width, x, y, width, height,
+                                             re.ctypes.data, im.ctypes.data))
+        return re + 1j * im
+
+    def set_state_device(self, ptr, pitch):
+        self._check(lib().ts_b200_set_state_device(self._h, C.c_void_p(ptr), pitch))
+
+    def get_state_device(self, ptr, pitch):
+        self._check(lib().ts_b200_get_state_device(self._h, C.c_void_p(ptr), pitch))
+
+    def set_exp_potential_device(self, ptr, pitch):
+        self._check(lib().ts_b200_set_exp_potential_device(self._h, C.c_void_p(ptr), pitch))
+
+    # -- evolution ---------------------------------------------------------
+    def step(self, exchange=True):
+        self._check(lib().ts_b200_step(self._h, int(bool(exchange))))
+
+    def evolve(self, iterations):
+        self._check(lib().ts_b200_evolve(self._h, int(iterations)))
+
+    def synchronize(self):
+        self._check(lib().ts_b200_synchronize(self._h))
+
+    def set_stream(self, stream_ptr):
+        self._check(lib().ts_b200_set_stream(self._h, C.c_void_p(stream_ptr)))
+
+    # -- reductions --------------------------------------------------------
+    def squared_norm(self):
+        out = C.c_double()
+        self._check(lib().ts_b200_squared_norm(self._h, C.byref(out)))
+        return out.value
+
+    def energies(self, potential, params):
+        """potential: tile of V values or None (reuse); params: EnergyParams."""
+        V = None if potential is None else np.ascontiguousarray(potential, np.float64)
+        out = EnergyResult()
+        self._check(lib().ts_b200_energies(self._h, None if V is None else V.ctypes.data,
+                                           C.byref(params), C.byref(out)))
+        return {n: getattr(out, n) for n, _ in EnergyResult._fields_}
+
+    def expectations(self, params):
+        out = ExpectationResult()
+        self._check(lib().ts_b200_expectations(self._h, C.byref(params), C.byref(out)))
+        return {n: getattr(out, n) for n, _ in ExpectationResult._fields_}
+
+    # -- launch shape ------------------------------------------------------
+    def launch_shape(self):
+        s = LaunchShape()
+        self._check(lib().ts_b200_launch_info(self._h, C.byref(s)))
+        return {n: getattr(s, n) for n, _ in LaunchShape._fields_}
+
+    def set_launch(self, cells_per_lane=0, segment_rows=0, warps_per_block=0, ring_depth=0):
+        self._check(lib().ts_b200_set_launch(self._h, cells_per_lane, segment_rows,
+                                             warps_per_block, ring_depth))
+
+
+def launch_count():
+    """Kernel launches made by this process through the library."""
+    return int(lib().ts_b200_launch_count())
+
+
+def version():
+    return lib().ts_b200_version().decode()
