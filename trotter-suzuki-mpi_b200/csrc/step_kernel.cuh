@@ -123,14 +123,16 @@ __device__ __forceinline__ uint64_t global_ns() {
     return t;
 }
 
-// Bounded wait: gives up after `limit_ns` nanoseconds of polling.
+// Bounded wait: gives up after `limit_ns` nanoseconds of polling.  Called by
+// all lanes of a warp for the same barrier and phase; the vote keeps the loop
+// warp-uniform.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity,
                                                   uint64_t limit_ns = 1000000000ull) {
-    if (mbar_try_wait(bar, parity)) return true;
+    if (__all_sync(0xffffffffu, mbar_try_wait(bar, parity))) return true;
     const uint64_t t0 = global_ns();
     while (true) {
-        if (mbar_try_wait(bar, parity)) return true;
-        if (global_ns() - t0 > limit_ns) return false;
+        if (__all_sync(0xffffffffu, mbar_try_wait(bar, parity))) return true;
+        if (__any_sync(0xffffffffu, global_ns() - t0 > limit_ns)) return false;
     }
 }
 
@@ -224,16 +226,19 @@ __device__ __forceinline__ void vsweep(Cx<T> (&up)[C], Cx<T> (&lo)[C], T a, T b)
 }
 
 // Horizontal kinetic sweep on one row: pairs (x, x+1) with (x + u) % 2 == s
-// start at lane cells with (i & 1) == PAR, PAR = (u + s) & 1.
-template <bool IMAG, int C, int PAR, typename T>
+// start at lane cells with (i & 1) == PAR, PAR = (u + s) & 1.  Only strips
+// that touch the tile edge (EDGE) mask pairs: in an interior strip the cells
+// of lanes 0 and 31 are recomputed halo that is never stored, so their
+// missing partners do not matter.
+template <bool IMAG, int C, int PAR, bool EDGE, typename T>
 __device__ __forceinline__ void hsweep(Cx<T> (&w)[C], T a, T b, const LaneMask<C> &m) {
     if (PAR == 0) {
 #pragma unroll
         for (int i = 0; i + 1 < C; i += 2) {
             Cx<T> p = w[i], q = w[i + 1];
             Cx<T> np = kin<IMAG>(p, q, a, b), nq = kin<IMAG>(q, p, a, b);
-            w[i] = m.pair_int[i] ? np : p;
-            w[i + 1] = m.pair_int[i] ? nq : q;
+            w[i] = (!EDGE || m.pair_int[i]) ? np : p;
+            w[i + 1] = (!EDGE || m.pair_int[i]) ? nq : q;
         }
     } else {
         Cx<T> right = shfl_down1(w[0]);
@@ -242,26 +247,26 @@ __device__ __forceinline__ void hsweep(Cx<T> (&w)[C], T a, T b, const LaneMask<C
         for (int i = 1; i + 1 < C; i += 2) {
             Cx<T> p = w[i], q = w[i + 1];
             Cx<T> np = kin<IMAG>(p, q, a, b), nq = kin<IMAG>(q, p, a, b);
-            w[i] = m.pair_int[i] ? np : p;
-            w[i + 1] = m.pair_int[i] ? nq : q;
+            w[i] = (!EDGE || m.pair_int[i]) ? np : p;
+            w[i + 1] = (!EDGE || m.pair_int[i]) ? nq : q;
         }
         Cx<T> n0 = kin<IMAG>(w[0], left, a, b);
         Cx<T> nl = kin<IMAG>(w[C - 1], right, a, b);
-        if (m.pair_left) w[0] = n0;
-        if (m.pair_right) w[C - 1] = nl;
+        if (!EDGE || m.pair_left) w[0] = n0;
+        if (!EDGE || m.pair_right) w[C - 1] = nl;
     }
 }
 
 // Rotation row sweep on one row: pairs (x, x+1) with x % 2 == PAR.
-template <bool IMAG, int C, int PAR, typename T>
+template <bool IMAG, int C, int PAR, bool EDGE, typename T>
 __device__ __forceinline__ void rrow(Cx<T> (&w)[C], T a, T b, const LaneMask<C> &m) {
     if (PAR == 0) {
 #pragma unroll
         for (int i = 0; i + 1 < C; i += 2) {
             Cx<T> f = w[i], s = w[i + 1];
             Cx<T> nf = rot_first<IMAG>(f, s, a, b), ns = rot_second<IMAG>(s, f, a, b);
-            w[i] = m.pair_int[i] ? nf : f;
-            w[i + 1] = m.pair_int[i] ? ns : s;
+            w[i] = (!EDGE || m.pair_int[i]) ? nf : f;
+            w[i + 1] = (!EDGE || m.pair_int[i]) ? ns : s;
         }
     } else {
         Cx<T> right = shfl_down1(w[0]);
@@ -270,13 +275,13 @@ __device__ __forceinline__ void rrow(Cx<T> (&w)[C], T a, T b, const LaneMask<C> 
         for (int i = 1; i + 1 < C; i += 2) {
             Cx<T> f = w[i], s = w[i + 1];
             Cx<T> nf = rot_first<IMAG>(f, s, a, b), ns = rot_second<IMAG>(s, f, a, b);
-            w[i] = m.pair_int[i] ? nf : f;
-            w[i + 1] = m.pair_int[i] ? ns : s;
+            w[i] = (!EDGE || m.pair_int[i]) ? nf : f;
+            w[i + 1] = (!EDGE || m.pair_int[i]) ? ns : s;
         }
         Cx<T> n0 = rot_second<IMAG>(w[0], left, a, b);
         Cx<T> nl = rot_first<IMAG>(w[C - 1], right, a, b);
-        if (m.pair_left) w[0] = n0;
-        if (m.pair_right) w[C - 1] = nl;
+        if (!EDGE || m.pair_left) w[0] = n0;
+        if (!EDGE || m.pair_right) w[C - 1] = nl;
     }
 }
 
@@ -291,16 +296,63 @@ __device__ __forceinline__ void rcol(Cx<T> (&up)[C], Cx<T> (&lo)[C], const Cx<T>
     }
 }
 
-__device__ __forceinline__ void sincos_t(double x, double *s, double *c) { sincos(x, s, c); }
-__device__ __forceinline__ void sincos_t(float x, float *s, float *c) { sincosf(x, s, c); }
-__device__ __forceinline__ double exp_t(double x) { return exp(x); }
-__device__ __forceinline__ float exp_t(float x) { return expf(x); }
+// Library paths for large phase arguments: kept out of line so that the
+// unrolled row loop does not carry copies of them.
+static __device__ __noinline__ void sincos_t(double x, double *s, double *c) { sincos(x, s, c); }
+static __device__ __noinline__ void sincos_t(float x, float *s, float *c) { sincosf(x, s, c); }
+static __device__ __noinline__ double exp_t(double x) { return exp(x); }
+static __device__ __noinline__ float exp_t(float x) { return expf(x); }
 __device__ __forceinline__ double sqrt_t(double x) { return sqrt(x); }
 __device__ __forceinline__ float sqrt_t(float x) { return sqrtf(x); }
 
+// Phase factors of the GPE / LHY term for small arguments.  The nonlinear
+// phase g*dt*|psi|^2 is far below 1/32 in practice, where the Maclaurin
+// series of cos, sin and exp truncated after the x^10 / x^11 / x^8 terms
+// (Horner's rule) leave a remainder below 1e-19, i.e. well under half an ulp
+// of double; larger arguments take the CUDA math library.
+template <typename T>
+__device__ __forceinline__ void phase_sincos(T th, T *s, T *c) {
+    // warp-uniform choice: the library path only if some lane needs it
+    if (!__any_sync(0xffffffffu, !(fabs((double)th) < 0.03125))) {
+        const T t = th * th;
+        T pc = T(-2.7557319223985893e-07);            // -1/10!
+        pc = fma_t(pc, t, T(2.4801587301587302e-05));  //  1/8!
+        pc = fma_t(pc, t, T(-1.3888888888888889e-03)); // -1/6!
+        pc = fma_t(pc, t, T(4.1666666666666664e-02));  //  1/4!
+        pc = fma_t(pc, t, T(-0.5));                    // -1/2!
+        *c = fma_t(pc, t, T(1));
+        T ps = T(-2.5052108385441720e-08);             // -1/11!
+        ps = fma_t(ps, t, T(2.7557319223985888e-06));  //  1/9!
+        ps = fma_t(ps, t, T(-1.9841269841269841e-04)); // -1/7!
+        ps = fma_t(ps, t, T(8.3333333333333332e-03));  //  1/5!
+        ps = fma_t(ps, t, T(-1.6666666666666666e-01)); // -1/3!
+        *s = fma_t(mul_t(ps, t), th, th);
+    } else {
+        sincos_t(th, s, c);
+    }
+}
+
+// exp(-th) for the imaginary-time nonlinear factor (same truncation rule).
+template <typename T>
+__device__ __forceinline__ T phase_expneg(T th) {
+    if (!__any_sync(0xffffffffu, !(fabs((double)th) < 0.03125))) {
+        const T x = -th;
+        T p = T(2.4801587301587302e-05);             // 1/8!
+        p = fma_t(p, x, T(1.9841269841269841e-04)); // 1/7!
+        p = fma_t(p, x, T(1.3888888888888889e-03)); // 1/6!
+        p = fma_t(p, x, T(8.3333333333333332e-03)); // 1/5!
+        p = fma_t(p, x, T(4.1666666666666664e-02)); // 1/4!
+        p = fma_t(p, x, T(1.6666666666666666e-01)); // 1/3!
+        p = fma_t(p, x, T(0.5));                    // 1/2!
+        p = fma_t(p, x, T(1));
+        return fma_t(p, x, T(1));
+    }
+    return exp_t(-th);
+}
+
 // Potential, GPE and LHY phase on one row (src/cpucartesian.cpp:96-106,130-134).
 // |psi|^2 is taken before the table multiply, as the reference does.
-template <bool IMAG, bool PHASE, int C, typename T, typename TabT>
+template <bool IMAG, bool PHASE, bool LHY, int C, typename T, typename TabT>
 __device__ __forceinline__ void potential_row(Cx<T> (&w)[C], const TabT *tab, T ca, T caa) {
 #pragma unroll
     for (int i = 0; i < C; ++i) {
@@ -310,8 +362,8 @@ __device__ __forceinline__ void potential_row(Cx<T> (&w)[C], const TabT *tab, T 
             if (PHASE) {
                 const T n2 = fma_t(v.re, v.re, mul_t(v.im, v.im));
                 T th = mul_t(ca, n2);
-                if (caa != T(0)) th = fma_t(caa, mul_t(n2, sqrt_t(n2)), th);
-                const T t = mul_t(exp_t(-th), pr);
+                if (LHY) th = fma_t(caa, mul_t(n2, sqrt_t(n2)), th);
+                const T t = mul_t(phase_expneg(th), pr);
                 v.re = mul_t(t, v.re);
                 v.im = mul_t(t, v.im);
             } else {
@@ -324,8 +376,8 @@ __device__ __forceinline__ void potential_row(Cx<T> (&w)[C], const TabT *tab, T 
             if (PHASE) {
                 const T n2 = fma_t(v.re, v.re, mul_t(v.im, v.im));
                 T th = mul_t(ca, n2);
-                if (caa != T(0)) th = fma_t(caa, mul_t(n2, sqrt_t(n2)), th);
-                sincos_t(th, &s, &c);
+                if (LHY) th = fma_t(caa, mul_t(n2, sqrt_t(n2)), th);
+                phase_sincos(th, &s, &c);
             }
             T t = v.re;
             v.re = fma_t(e.re, t, -mul_t(e.im, v.im));
@@ -369,16 +421,22 @@ __device__ __forceinline__ void st_cx_global(Cx<T> *p, Cx<T> v) {
 }
 
 // Compile-time description of a kernel variant.
-template <typename T_, int C_, bool IMAG_, bool ROT_, bool PHASE_>
+// PHASE: 0 no nonlinear phase, 1 g|psi|^2 only, 2 with the Lee-Huang-Yang term.
+template <typename T_, int C_, bool IMAG_, bool ROT_, int PHASE_>
 struct Variant {
     using T = T_;
     static constexpr int C = C_;
     static constexpr bool IMAG = IMAG_;
     static constexpr bool ROT = ROT_;
-    static constexpr bool PHASE = PHASE_;
+    static constexpr bool PHASE = PHASE_ != 0;
+    static constexpr bool LHY = PHASE_ == 2;
     static constexpr int HX = ROT_ ? 8 : 4;
     static constexpr int HY = ROT_ ? 6 : 4;
+    // Register window (rows); the body is unrolled over two windows so that
+    // the parity of every row index is a compile-time constant.
     static constexpr int NWIN = ROT_ ? 7 : 5;
+    static constexpr int UNROLL = 2 * NWIN;
+    static constexpr int OUT_LAG = NWIN - 1;
     static constexpr int SW = 32 * C_;
     static constexpr int WO = SW - 2 * HX;
     using TabT = typename std::conditional<IMAG_, T_, Cx<T_>>::type;
@@ -390,7 +448,9 @@ struct Variant {
 
 // Per-warp state of one segment walk.  Every member is indexed with
 // compile-time constants after inlining, so the whole struct lives in
-// registers.
+// registers.  Ring slots are tracked incrementally: row ra of a segment goes
+// to slot 0, row ra+1 to slot 1, ...; the parity each slot's mbarrier will
+// show next is kept in phase_bits (bit q for slot q) across segments.
 template <class V>
 struct Walk {
     using T = typename V::T;
@@ -402,32 +462,37 @@ struct Walk {
     LaneMask<C> m;
     bool present[C], out_col[C], norm_col[C];
     int ra, rb, oy0, oy1, xl, lane, D;
-    int cs;
+    int lslot;            // slot of the next row to load
+    int tslot;            // slot of the row whose table is read next
+    uint32_t phase_bits;  // expected completion parity of each slot
+    int issued_to;        // rows [ra, issued_to) have had their copy issued
+    int loaded_to;        // rows [ra, loaded_to) have been waited for
+    const unsigned char *gpsi, *gtab;  // row 0, column cs of psi and of the table
+    size_t gpsi_pitch, gtab_pitch;
     uint32_t psi_off, psi_bytes, tab_off, tab_bytes;
-    int next_issue;  // next row whose copy has not been issued
-    int consumed;    // rows [ra, consumed) have been waited for
     unsigned char *ring;
     uint64_t *bars;
     double nacc;
     bool failed;
     T inv;
+    T aH, bH, aV, bV, ca, caa;  // step constants, read from the parameters once
 
-    __device__ __forceinline__ void issue(const StepArgs<T> &a, int row) {
-        const int slot = (row - ra) % D;
-        unsigned char *sb = ring + (size_t)slot * V::SLOT;
+    __device__ __forceinline__ void issue(int row, int slot) {
+        unsigned char *sb = ring + slot * V::SLOT;
         mbar_expect_tx(&bars[slot], psi_bytes + tab_bytes);
-        const unsigned char *gp = reinterpret_cast<const unsigned char *>(a.psi_in) +
-                                  ((size_t)row * a.P + cs) * sizeof(Cx<T>);
-        bulk_g2s(sb + psi_off, gp, psi_bytes, &bars[slot]);
-        const unsigned char *gt = reinterpret_cast<const unsigned char *>(a.pot) +
-                                  ((size_t)row * a.P + cs) * sizeof(TabT);
-        bulk_g2s(sb + V::PSI_BYTES + tab_off, gt, tab_bytes, &bars[slot]);
+        bulk_g2s(sb + psi_off, gpsi + (size_t)row * gpsi_pitch, psi_bytes, &bars[slot]);
+        bulk_g2s(sb + V::PSI_BYTES + tab_off, gtab + (size_t)row * gtab_pitch, tab_bytes,
+                 &bars[slot]);
     }
+    __device__ __forceinline__ int next(int q) const { return q + 1 == D ? 0 : q + 1; }
 };
 
-// One iteration of the walk for row r = base + K (base even, so the parity
-// of every row index below is known at compile time).
-template <class V, int K>
+// One iteration of the walk for row r = base + K (base even, so the parity of
+// every row index below is known at compile time).
+// GUARD: the iteration may touch rows outside [ra, rb) (segment prologue and
+// epilogue); without it every stage is known to be valid.  EDGE: the strip
+// touches the tile edge and needs the per-lane masks.
+template <class V, int K, bool GUARD, bool EDGE>
 __device__ __forceinline__ void walk_row(Walk<V> &w, const StepArgs<typename V::T> &a, int r) {
     using T = typename V::T;
     using TabT = typename V::TabT;
@@ -436,96 +501,97 @@ __device__ __forceinline__ void walk_row(Walk<V> &w, const StepArgs<typename V::
     // row r - j lives in win[(K - j) mod NWIN]
 #define WS(j) w.win[((K) - (j) + 2 * NWIN) % NWIN]
     const int ra = w.ra, rb = w.rb;
-    const T aH = a.aH, bH = a.bH, aV = a.aV, bV = a.bV;
+    const T aH = w.aH, bH = w.bH, aV = w.aV, bV = w.bV;
 
     // ---- load row r
-    if (r >= ra && r < rb) {
-        const int slot = (r - ra) % w.D;
-        const uint32_t par = (uint32_t)(((r - ra) / w.D) & 1);
-        if (!mbar_wait_bounded(&w.bars[slot], par)) {
+    if (!GUARD || (r >= ra && r < rb)) {
+        const int q = w.lslot;
+        if (!mbar_wait_bounded(&w.bars[q], (w.phase_bits >> q) & 1u)) {
             w.failed = true;
             return;
         }
-        w.consumed = r + 1;
-        const Cx<T> *sp = reinterpret_cast<const Cx<T> *>(w.ring + (size_t)slot * V::SLOT);
+        w.phase_bits ^= 1u << q;
+        w.lslot = w.next(q);
+        w.loaded_to = r + 1;
+        const Cx<T> *sp = reinterpret_cast<const Cx<T> *>(w.ring + q * V::SLOT) + C * w.lane;
 #pragma unroll
         for (int i = 0; i < C; ++i) {
-            Cx<T> v = ld_cx_shared(sp + C * w.lane + i);
+            Cx<T> v = ld_cx_shared(sp + i);
             if (IMAG) {
                 v.re = v.re * w.inv;
                 v.im = v.im * w.inv;
             }
-            WS(0)[i] = w.present[i] ? v : Cx<T>{T(0), T(0)};
+            WS(0)[i] = (!EDGE || w.present[i]) ? v : Cx<T>{T(0), T(0)};
         }
     }
     // ---- S1: V0 on rows (r-1, r)
-    if (r - 1 >= ra && r < rb) vsweep<IMAG, C, ((K + 1) & 1)>(WS(1), WS(0), aV, bV);
+    if (!GUARD || (r - 1 >= ra && r < rb)) vsweep<IMAG, C, ((K + 1) & 1)>(WS(1), WS(0), aV, bV);
     // ---- S2: H0 on row r-1
-    if (r - 1 >= ra && r - 1 < rb) hsweep<IMAG, C, ((K + 1) & 1)>(WS(1), aH, bH, w.m);
+    if (!GUARD || (r - 1 >= ra && r - 1 < rb)) hsweep<IMAG, C, ((K + 1) & 1), EDGE>(WS(1), aH, bH, w.m);
     // ---- S3: V1 on rows (r-2, r-1)
-    if (r - 2 >= ra && r - 1 < rb) vsweep<IMAG, C, ((K + 1) & 1)>(WS(2), WS(1), aV, bV);
+    if (!GUARD || (r - 2 >= ra && r - 1 < rb)) vsweep<IMAG, C, ((K + 1) & 1)>(WS(2), WS(1), aV, bV);
     // ---- S4: H1, P, then H1 (or the rotation row sweeps) on row r-2; free its slot
-    if (r - 2 >= ra && r - 2 < rb) {
+    if (!GUARD || (r - 2 >= ra && r - 2 < rb)) {
         const int u = r - 2;
-        hsweep<IMAG, C, ((K + 1) & 1)>(WS(2), aH, bH, w.m);
-        const int slot = (u - ra) % w.D;
+        hsweep<IMAG, C, ((K + 1) & 1), EDGE>(WS(2), aH, bH, w.m);
+        const int q = w.tslot;
         const TabT *tp =
-            reinterpret_cast<const TabT *>(w.ring + (size_t)slot * V::SLOT + V::PSI_BYTES) +
-            C * w.lane;
-        potential_row<IMAG, PHASE, C>(WS(2), tp, a.ca, a.caa);
+            reinterpret_cast<const TabT *>(w.ring + q * V::SLOT + V::PSI_BYTES) + C * w.lane;
+        potential_row<IMAG, PHASE, V::LHY, C>(WS(2), tp, w.ca, w.caa);
         if constexpr (ROT) {
             const Cx<T> ab = reinterpret_cast<const Cx<T> *>(a.row_ab)[u];
-            rrow<IMAG, C, 0>(WS(2), ab.re, ab.im, w.m);
-            rrow<IMAG, C, 1>(WS(2), ab.re, ab.im, w.m);
+            rrow<IMAG, C, 0, EDGE>(WS(2), ab.re, ab.im, w.m);
+            rrow<IMAG, C, 1, EDGE>(WS(2), ab.re, ab.im, w.m);
         } else {
-            hsweep<IMAG, C, ((K + 1) & 1)>(WS(2), aH, bH, w.m);
+            hsweep<IMAG, C, ((K + 1) & 1), EDGE>(WS(2), aH, bH, w.m);
         }
         __syncwarp();
         if (u + w.D < rb) {
             if (w.lane == 0) {
                 // the slot's last generic-proxy reads happen-before the bulk copy refills it
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                w.issue(a, u + w.D);
+                w.issue(u + w.D, q);
             }
-            w.next_issue = u + w.D + 1;
+            w.issued_to = u + w.D + 1;
         }
+        w.tslot = w.next(q);
     }
     if constexpr (!ROT) {
         // ---- S5: V1 on rows (r-3, r-2)
-        if (r - 3 >= ra && r - 2 < rb) vsweep<IMAG, C, ((K) & 1)>(WS(3), WS(2), aV, bV);
+        if (!GUARD || (r - 3 >= ra && r - 2 < rb)) vsweep<IMAG, C, ((K) & 1)>(WS(3), WS(2), aV, bV);
         // ---- S6: H0 on row r-3
-        if (r - 3 >= ra && r - 3 < rb) hsweep<IMAG, C, ((K + 1) & 1)>(WS(3), aH, bH, w.m);
+        if (!GUARD || (r - 3 >= ra && r - 3 < rb)) hsweep<IMAG, C, ((K + 1) & 1), EDGE>(WS(3), aH, bH, w.m);
         // ---- S7: V0 on rows (r-4, r-3)
-        if (r - 4 >= ra && r - 3 < rb) vsweep<IMAG, C, ((K) & 1)>(WS(4), WS(3), aV, bV);
+        if (!GUARD || (r - 4 >= ra && r - 3 < rb)) vsweep<IMAG, C, ((K) & 1)>(WS(4), WS(3), aV, bV);
     } else {
         // ---- S5: rotation columns, even rows: pair (r-3, r-2) when r-3 is even
-        if (((K + 1) & 1) == 0 && r - 3 >= ra && r - 2 < rb) rcol<IMAG, C>(WS(3), WS(2), w.colab);
+        if (((K + 1) & 1) == 0 && (!GUARD || (r - 3 >= ra && r - 2 < rb))) rcol<IMAG, C>(WS(3), WS(2), w.colab);
         // ---- S6: rotation columns, odd rows: pair (r-4, r-3) when r-4 is odd
-        if (((K) & 1) == 1 && r - 4 >= ra && r - 3 < rb) rcol<IMAG, C>(WS(4), WS(3), w.colab);
+        if (((K) & 1) == 1 && (!GUARD || (r - 4 >= ra && r - 3 < rb))) rcol<IMAG, C>(WS(4), WS(3), w.colab);
         // ---- S7: rotation rows again, then H1, on row r-4
-        if (r - 4 >= ra && r - 4 < rb) {
+        if (!GUARD || (r - 4 >= ra && r - 4 < rb)) {
             const Cx<T> ab = reinterpret_cast<const Cx<T> *>(a.row_ab)[r - 4];
-            rrow<IMAG, C, 0>(WS(4), ab.re, ab.im, w.m);
-            rrow<IMAG, C, 1>(WS(4), ab.re, ab.im, w.m);
-            hsweep<IMAG, C, ((K + 1) & 1)>(WS(4), aH, bH, w.m);
+            rrow<IMAG, C, 0, EDGE>(WS(4), ab.re, ab.im, w.m);
+            rrow<IMAG, C, 1, EDGE>(WS(4), ab.re, ab.im, w.m);
+            hsweep<IMAG, C, ((K + 1) & 1), EDGE>(WS(4), aH, bH, w.m);
         }
         // ---- S8: V1 on rows (r-5, r-4)
-        if (r - 5 >= ra && r - 4 < rb) vsweep<IMAG, C, ((K) & 1)>(WS(5), WS(4), aV, bV);
+        if (!GUARD || (r - 5 >= ra && r - 4 < rb)) vsweep<IMAG, C, ((K) & 1)>(WS(5), WS(4), aV, bV);
         // ---- S9: H0 on row r-5
-        if (r - 5 >= ra && r - 5 < rb) hsweep<IMAG, C, ((K + 1) & 1)>(WS(5), aH, bH, w.m);
+        if (!GUARD || (r - 5 >= ra && r - 5 < rb)) hsweep<IMAG, C, ((K + 1) & 1), EDGE>(WS(5), aH, bH, w.m);
         // ---- S10: V0 on rows (r-6, r-5)
-        if (r - 6 >= ra && r - 5 < rb) vsweep<IMAG, C, ((K) & 1)>(WS(6), WS(5), aV, bV);
+        if (!GUARD || (r - 6 >= ra && r - 5 < rb)) vsweep<IMAG, C, ((K) & 1)>(WS(6), WS(5), aV, bV);
     }
     // ---- store the finished row r - (NWIN-1)
     {
         const int u = r - (NWIN - 1);
         if (u >= w.oy0 && u < w.oy1) {
-            Cx<T> *out = reinterpret_cast<Cx<T> *>(a.psi_out);
+            Cx<T> *orow = reinterpret_cast<Cx<T> *>(a.psi_out) + (size_t)u * a.P + w.xl;
             const bool norm_row = IMAG && u >= a.iy0 && u < a.iy1;
 #pragma unroll
             for (int i = 0; i < C; ++i) {
                 const Cx<T> v = WS(NWIN - 1)[i];
-                if (w.out_col[i]) st_cx_global(out + (size_t)u * a.P + (w.xl + i), v);
+                if (w.out_col[i]) st_cx_global(orow + i, v);
                 if (norm_row && w.norm_col[i])
                     w.nacc += (double)v.re * (double)v.re + (double)v.im * (double)v.im;
             }
@@ -534,17 +600,28 @@ __device__ __forceinline__ void walk_row(Walk<V> &w, const StepArgs<typename V::
 #undef WS
 }
 
-template <class V, int K>
+template <class V, int K, bool GUARD, bool EDGE>
 __device__ __forceinline__ void walk_rows(Walk<V> &w, const StepArgs<typename V::T> &a, int base,
                                           int rlast) {
-    if constexpr (K < 2 * V::NWIN) {
+    if constexpr (K < V::UNROLL) {
         const int r = base + K;
-        if (r > rlast || w.failed) return;
-        walk_row<V, K>(w, a, r);
-        walk_rows<V, K + 1>(w, a, base, rlast);
+        if (GUARD && (r > rlast || w.failed)) return;
+        walk_row<V, K, GUARD, EDGE>(w, a, r);
+        walk_rows<V, K + 1, GUARD, EDGE>(w, a, base, rlast);
     }
 }
 
+// Walk one segment in chunks of UNROLL rows (every stage checks its rows).
+template <class V, bool EDGE>
+__device__ __forceinline__ void walk_segment(Walk<V> &w, const StepArgs<typename V::T> &a) {
+    const int rlast = w.rb - 1 + V::OUT_LAG;
+    for (int base = w.ra & ~1; base <= rlast && !w.failed; base += V::UNROLL) {
+        walk_rows<V, 0, true, EDGE>(w, a, base, rlast);
+    }
+}
+
+// Grid: any number of blocks of 1..4 warps; each warp loops over the tasks
+// (strip, segment) t = warp_global, warp_global + total_warps, ...
 template <class V>
 __global__ void __launch_bounds__(128) step_kernel(StepArgs<typename V::T> a) {
     using T = typename V::T;
@@ -557,31 +634,73 @@ __global__ void __launch_bounds__(128) step_kernel(StepArgs<typename V::T> a) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int D = a.ring;
     const int n_tasks = a.n_strips * a.n_segs;
-    const int task = blockIdx.x * warps + warp;
 
     Walk<V> w;
     w.nacc = 0.0;
     w.failed = false;
     w.inv = IMAG ? (T)a.scal->pending_inv : T(1);
+    w.aH = a.aH;
+    w.bH = a.bH;
+    w.aV = a.aV;
+    w.bV = a.bV;
+    w.ca = a.ca;
+    w.caa = a.caa;
+    w.D = D;
+    w.lane = lane;
+    // each warp: D ring slots, then (after all warps' rings) D mbarriers
+    w.ring = smem + (size_t)warp * D * V::SLOT;
+    w.bars = reinterpret_cast<uint64_t *>(smem + (size_t)warps * D * V::SLOT) + warp * D;
+    w.phase_bits = 0u;
+    w.gpsi_pitch = (size_t)a.P * sizeof(Cx<T>);
+    w.gtab_pitch = (size_t)a.P * sizeof(TabT);
 
-    if (task < n_tasks) {
-        w.D = D;
-        w.lane = lane;
-        w.ring = smem + (size_t)warp * D * V::SLOT;
-        w.bars = reinterpret_cast<uint64_t *>(smem + (size_t)warps * D * V::SLOT) + warp * D;
-        const int strip = task % a.n_strips, seg = task / a.n_strips;
+    // Zero this warp's ring once: cells never written by a copy (outside the
+    // tile) are then finite, so masked-off pair updates cannot produce NaNs.
+    {
+        uint4 *z = reinterpret_cast<uint4 *>(w.ring);
+        const int n16 = D * V::SLOT / 16;
+        for (int i = lane; i < n16; i += 32) z[i] = make_uint4(0u, 0u, 0u, 0u);
+    }
+    if (lane == 0) {
+        for (int q = 0; q < D; ++q) mbar_init(&w.bars[q], 1);
+        fence_mbar_init();
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncwarp();
+
+    for (int task = blockIdx.x * warps + warp; task < n_tasks && !w.failed;
+         task += gridDim.x * warps) {
+        // tasks of interior strips come first and those of the first and last
+        // strip (the only ones that need masks) last, so that few SMs run both
+        // code paths
+        int strip, seg;
+        {
+            const int n_int = a.n_strips > 2 ? (a.n_strips - 2) * a.n_segs : 0;
+            if (task < n_int) {
+                strip = 1 + task % (a.n_strips - 2);
+                seg = task / (a.n_strips - 2);
+            } else {
+                const int e = task - n_int;
+                const int n_edge_strips = a.n_strips > 2 ? 2 : a.n_strips;
+                const int es = e % n_edge_strips;
+                strip = (a.n_strips > 2 && es == 1) ? a.n_strips - 1 : es;
+                seg = e / n_edge_strips;
+            }
+        }
         const int ox0 = strip * WO, ox1 = min(ox0 + WO, a.W);
         const int c0 = ox0 - HX;
         w.oy0 = seg * a.seg_h;
         w.oy1 = min(w.oy0 + a.seg_h, a.H);
         w.ra = max(w.oy0 - HY, 0);
         w.rb = min(w.oy1 + HY, a.H);
-        w.cs = max(c0, 0);
+        const int cs = max(c0, 0);
         const int ce = min(c0 + SW, a.P);
-        w.psi_off = (uint32_t)(w.cs - c0) * sizeof(Cx<T>);
-        w.psi_bytes = (uint32_t)(ce - w.cs) * sizeof(Cx<T>);
-        w.tab_off = (uint32_t)(w.cs - c0) * sizeof(TabT);
-        w.tab_bytes = (uint32_t)(ce - w.cs) * sizeof(TabT);
+        w.psi_off = (uint32_t)(cs - c0) * sizeof(Cx<T>);
+        w.psi_bytes = (uint32_t)(ce - cs) * sizeof(Cx<T>);
+        w.tab_off = (uint32_t)(cs - c0) * sizeof(TabT);
+        w.tab_bytes = (uint32_t)(ce - cs) * sizeof(TabT);
+        w.gpsi = reinterpret_cast<const unsigned char *>(a.psi_in) + (size_t)cs * sizeof(Cx<T>);
+        w.gtab = reinterpret_cast<const unsigned char *>(a.pot) + (size_t)cs * sizeof(TabT);
         w.xl = c0 + C * lane;
 #pragma unroll
         for (int i = 0; i < C; ++i) {
@@ -605,34 +724,35 @@ __global__ void __launch_bounds__(128) step_kernel(StepArgs<typename V::T> a) {
 #pragma unroll
             for (int i = 0; i < C; ++i) w.win[j][i] = Cx<T>{T(0), T(0)};
 
-        if (lane == 0) {
-            for (int q = 0; q < D; ++q) mbar_init(&w.bars[q], 1);
-            fence_mbar_init();
-        }
-        __syncwarp();
-        w.next_issue = min(w.ra + D, w.rb);
-        w.consumed = w.ra;
+        w.lslot = 0;
+        w.tslot = 0;
+        w.loaded_to = w.ra;
+        w.issued_to = min(w.ra + D, w.rb);
         if (lane == 0)
-            for (int row = w.ra; row < w.next_issue; ++row) w.issue(a, row);
+            for (int row = w.ra; row < w.issued_to; ++row) w.issue(row, row - w.ra);
 
-        const int rlast = w.rb - 1 + (NWIN - 1);
-        for (int base = w.ra & ~1; base <= rlast && !w.failed; base += 2 * NWIN)
-            walk_rows<V, 0>(w, a, base, rlast);
+        if (c0 >= 0 && c0 + SW <= a.W) walk_segment<V, false>(w, a);
+        else walk_segment<V, true>(w, a);
 
         if (w.failed) {
             if (lane == 0) atomicExch(&a.scal->error, 1);
             // let copies already issued land before the block can exit
-            for (int row = w.consumed; row < w.next_issue; ++row)
-                (void)mbar_wait_bounded(&w.bars[(row - w.ra) % D], (uint32_t)(((row - w.ra) / D) & 1),
-                                        100000000ull);
+            int q = w.lslot;
+            for (int row = w.loaded_to; row < w.issued_to; ++row) {
+                (void)mbar_wait_bounded(&w.bars[q], (w.phase_bits >> q) & 1u, 100000000ull);
+                w.phase_bits ^= 1u << q;
+                q = w.next(q);
+            }
         }
     }
 
     if constexpr (IMAG) {
+        // per-warp partial: a warp's tasks are summed in task order
         double nacc = w.nacc;
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) nacc += __shfl_xor_sync(0xffffffffu, nacc, off);
-        if (lane == 0 && task < n_tasks) a.partials[task] = nacc;
+        const int gw = blockIdx.x * warps + warp;
+        if (lane == 0) a.partials[gw] = nacc;
         __shared__ unsigned int s_last;
         __shared__ double red[128];
         __syncthreads();
@@ -644,9 +764,10 @@ __global__ void __launch_bounds__(128) step_kernel(StepArgs<typename V::T> a) {
         __syncthreads();
         if (s_last) {
             __threadfence();
-            // fixed order: thread t sums tasks t, t + blockDim, ..., then a fixed tree
+            // fixed order: thread t sums warps t, t + blockDim, ..., then a fixed tree
+            const int nw = gridDim.x * warps;
             double s = 0.0;
-            for (int t = threadIdx.x; t < n_tasks; t += blockDim.x) s += __ldcg(&a.partials[t]);
+            for (int t = threadIdx.x; t < nw; t += blockDim.x) s += __ldcg(&a.partials[t]);
             red[threadIdx.x] = s;
             __syncthreads();
             for (int h = blockDim.x >> 1; h > 0; h >>= 1) {

@@ -347,22 +347,22 @@ __global__ void __launch_bounds__(RED_THREADS) expect_kernel(RedArgs a) {
 // The step variants are instantiated in step_f64_real.cu, step_f64_imag.cu,
 // step_f32_real.cu and step_f32_imag.cu (compiled in parallel).
 template <typename T>
-cudaError_t dispatch_step(int C, bool imag, bool rot, bool phase, const StepArgs<T> &a, int warps,
-                          size_t smem, int blocks, cudaStream_t st);
+cudaError_t dispatch_step(int C, bool imag, bool rot, int phase, const StepArgs<T> &a, int warps,
+                          size_t smem, int blocks, cudaStream_t st, int *bps);
 
 template <>
-cudaError_t dispatch_step<double>(int C, bool imag, bool rot, bool phase,
+cudaError_t dispatch_step<double>(int C, bool imag, bool rot, int phase,
                                   const StepArgs<double> &a, int warps, size_t smem, int blocks,
-                                  cudaStream_t st) {
-    return imag ? tsb::launch_step_f64_imag(C, rot, phase, a, warps, smem, blocks, st)
-                : tsb::launch_step_f64_real(C, rot, phase, a, warps, smem, blocks, st);
+                                  cudaStream_t st, int *bps) {
+    return imag ? tsb::launch_step_f64_imag(C, rot, phase, a, warps, smem, blocks, st, bps)
+                : tsb::launch_step_f64_real(C, rot, phase, a, warps, smem, blocks, st, bps);
 }
 
 template <>
-cudaError_t dispatch_step<float>(int C, bool imag, bool rot, bool phase, const StepArgs<float> &a,
-                                 int warps, size_t smem, int blocks, cudaStream_t st) {
-    return imag ? tsb::launch_step_f32_imag(C, rot, phase, a, warps, smem, blocks, st)
-                : tsb::launch_step_f32_real(C, rot, phase, a, warps, smem, blocks, st);
+cudaError_t dispatch_step<float>(int C, bool imag, bool rot, int phase, const StepArgs<float> &a,
+                                 int warps, size_t smem, int blocks, cudaStream_t st, int *bps) {
+    return imag ? tsb::launch_step_f32_imag(C, rot, phase, a, warps, smem, blocks, st, bps)
+                : tsb::launch_step_f32_real(C, rot, phase, a, warps, smem, blocks, st, bps);
 }
 
 int slot_bytes(int C, bool fp32, bool imag) {
@@ -379,7 +379,8 @@ int div_up(long a, long b) { return (int)((a + b - 1) / b); }
 struct ts_b200_kernel {
     ts_b200_desc d{};
     int W = 0, H = 0, P = 0;
-    bool fp32 = false, imag = false, rot = false, phase = false;
+    bool fp32 = false, imag = false, rot = false;
+    int phase = 0;  // 0 none, 1 g|psi|^2, 2 with Lee-Huang-Yang
     size_t cell = 0, tab_cell = 0;
     void *psi[2] = {nullptr, nullptr};
     int cur = 0;
@@ -396,6 +397,8 @@ struct ts_b200_kernel {
     unsigned int *red_ticket = nullptr;
     cudaStream_t own_stream = nullptr, stream = nullptr;
     int C = 2, seg_h = 64, warps = 4, ring = 4;
+    int resident_blocks = 0;  // blocks of the current launch shape resident on the GPU (0: unknown)
+    bool auto_seg = true;     // pick the segment height from the resident grid
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
     int num_sms = 148;
@@ -430,21 +433,29 @@ void drop_graph(ts_b200_kernel *k) {
 }
 
 void choose_launch(ts_b200_kernel *k) {
-    // Column strips of 32*C cells; C = 4 halves the shuffles per cell and the
-    // recomputed halo fraction on wide tiles, C = 2 wastes less on narrow ones
-    // and keeps the 7-row rotation window within the register budget.
-    k->C = (!k->rot && k->W >= 480) ? 4 : 2;
+    // Column strips of 32*C cells with C = 2: the short 2-cell rows keep the
+    // register window small enough for 5 blocks of 4 warps per SM.  The
+    // segment height is fixed once the resident grid is known (auto_seg).
+    k->C = 2;
+    k->seg_h = 64;
+    k->auto_seg = true;
+    k->warps = 4;
+    k->ring = 4;
+}
+
+// A row's table is read two rows after its psi: the ring must hold those
+// three rows plus at least one in flight.
+int min_ring(const ts_b200_kernel *) { return 4; }
+
+// One round of tasks over the resident warps: as many row segments per strip
+// as there are resident warps per strip.
+void auto_segments(ts_b200_kernel *k) {
     const int hx = k->rot ? 8 : 4;
     const int wo = 32 * k->C - 2 * hx;
     const int strips = div_up(k->W, wo);
-    // about 8 resident warps per SM in one wave, segments of 32..256 rows
-    const long target = (long)k->num_sms * 8;
-    const int segs = std::max(1, (int)(target / std::max(1, strips)));
-    int sh = div_up(k->H, segs);
-    sh = std::max(32, std::min(256, sh));
-    k->seg_h = std::min(sh, std::max(1, k->H));
-    k->warps = 4;
-    k->ring = 4;
+    const long rw = (long)k->resident_blocks * k->warps;
+    const int per_strip = (int)std::max(1L, rw / std::max(1, strips));
+    k->seg_h = std::max(16, div_up(k->H, per_strip));
 }
 
 void geometry(const ts_b200_kernel *k, int *strips, int *segs, int *blocks, size_t *smem) {
@@ -454,21 +465,35 @@ void geometry(const ts_b200_kernel *k, int *strips, int *segs, int *blocks, size
     *segs = div_up(k->H, k->seg_h);
     const int tasks = *strips * *segs;
     *blocks = div_up(tasks, k->warps);
-    *smem = (size_t)k->warps * k->ring * (slot_bytes(k->C, k->fp32, k->imag) + 8);
+    if (k->resident_blocks > 0) *blocks = std::min(*blocks, k->resident_blocks);
+    // per warp: ring slots + one mbarrier per ring slot
+    *smem = (size_t)k->warps * (k->ring * slot_bytes(k->C, k->fp32, k->imag) + 8 * k->ring);
 }
 
 template <typename T>
 int launch_step_t(ts_b200_kernel *k, int exchange, bool dry = false) {
     int strips, segs, blocks;
     size_t smem;
+    if (k->resident_blocks <= 0) {
+        // resident blocks of this variant and shape: the persistent grid size
+        geometry(k, &strips, &segs, &blocks, &smem);
+        StepArgs<T> a0{};
+        int bps = 0;
+        cudaError_t e = dispatch_step<T>(k->C, k->imag, k->rot, k->phase, a0, k->warps, smem, 0,
+                                         k->stream, &bps);
+        if (e != cudaSuccess) return cuda_fail(k, e, "step kernel configuration");
+        if (bps < 1) return fail(k, TS_B200_UNSUPPORTED, "step kernel does not fit on an SM");
+        k->resident_blocks = bps * k->num_sms;
+        if (k->auto_seg) auto_segments(k);
+    }
     geometry(k, &strips, &segs, &blocks, &smem);
     if (dry) blocks = 0;
-    const size_t tasks = (size_t)strips * segs;
-    if (k->imag && tasks > k->partials_cap) {
+    const size_t nwarps = (size_t)std::max(blocks, 1) * k->warps;
+    if (k->imag && nwarps > k->partials_cap) {
         if (k->partials) cudaFree(k->partials);
         k->partials = nullptr;
-        TSB_CHECK(k, cudaMalloc(&k->partials, tasks * sizeof(double)));
-        k->partials_cap = tasks;
+        TSB_CHECK(k, cudaMalloc(&k->partials, nwarps * sizeof(double)));
+        k->partials_cap = nwarps;
     }
     StepArgs<T> a{};
     a.psi_in = k->psi[k->cur];
@@ -497,8 +522,8 @@ int launch_step_t(ts_b200_kernel *k, int exchange, bool dry = false) {
     a.scal = k->scal;
     a.dxdy = k->d.delta_x * k->d.delta_y;
     a.norm0 = k->d.norm0;
-    cudaError_t e =
-        dispatch_step<T>(k->C, k->imag, k->rot, k->phase, a, k->warps, smem, blocks, k->stream);
+    cudaError_t e = dispatch_step<T>(k->C, k->imag, k->rot, k->phase, a, k->warps, smem, blocks,
+                                     k->stream, nullptr);
     if (e != cudaSuccess) return cuda_fail(k, e, "step kernel launch");
     if (dry) return TS_B200_OK;
     g_launches.fetch_add(1, std::memory_order_relaxed);
@@ -656,7 +681,7 @@ int ts_b200_create(const ts_b200_desc *d, ts_b200_kernel **out) {
     k->fp32 = d->precision == TS_B200_FP32;
     k->imag = d->imag_time != 0;
     k->rot = d->alpha_x != 0.0 && d->alpha_y != 0.0;
-    k->phase = d->coupling != 0.0 || d->lhy_coupling != 0.0;
+    k->phase = d->lhy_coupling != 0.0 ? 2 : (d->coupling != 0.0 ? 1 : 0);
     k->cell = k->fp32 ? 8 : 16;
     k->tab_cell = k->imag ? k->cell / 2 : k->cell;
     int dev = 0;
@@ -1016,12 +1041,17 @@ int ts_b200_set_launch(ts_b200_kernel *k, int C, int seg_h, int warps, int ring)
     if (C != 0 && C != 2 && C != 4) return TS_B200_INVALID_ARGUMENT;
     if (C == 4 && k->rot) return fail(k, TS_B200_UNSUPPORTED, "rotation kernels use 2 cells per lane");
     if (warps != 0 && warps != 1 && warps != 2 && warps != 4) return TS_B200_INVALID_ARGUMENT;
-    if (ring != 0 && (ring < 3 || ring > 12)) return TS_B200_INVALID_ARGUMENT;
+    if (ring != 0 && (ring < min_ring(k) || ring > 16))
+        return fail(k, TS_B200_INVALID_ARGUMENT, "ring depth out of range for this variant");
     if (seg_h < 0) return TS_B200_INVALID_ARGUMENT;
     if (C) k->C = C;
-    if (seg_h) k->seg_h = seg_h;
+    if (seg_h) {
+        k->seg_h = seg_h;
+        k->auto_seg = false;
+    }
     if (warps) k->warps = warps;
     if (ring) k->ring = ring;
+    k->resident_blocks = 0;
     int strips, segs, blocks;
     size_t smem;
     geometry(k, &strips, &segs, &blocks, &smem);
