@@ -105,6 +105,12 @@ int ts_b200_set_exp_potential(ts_b200_kernel *k, const double *pot_real, const d
  *           (src/trottersuzuki.h:505-507,517-518; src/gpukernel.cu:439-521). */
 int ts_b200_step(ts_b200_kernel *k, int exchange);
 
+/* Refresh the periodic halo of the current tile (no-op for closed lattices).
+ * Replaces: ITrotterKernel::start_halo_exchange + finish_halo_exchange
+ *           (src/trottersuzuki.h:517-518; single process:
+ *           src/cpukernel.cpp:706-716,738-746). */
+int ts_b200_halo_exchange(ts_b200_kernel *k);
+
 /* `iterations` steps with the reference's evolve() semantics: the halo is
  * refreshed after every step but the last (src/solver.cpp:186-230).  Steps
  * are replayed from a CUDA graph; nothing synchronises the host. */

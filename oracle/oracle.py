@@ -260,3 +260,13 @@ def gaussian(lattice, omega_x, omega_y=-1.0, mean_x=0.0, mean_y=0.0, norm=1.0, p
     dy = Y - mean_y
     val = amp * np.exp(-(omega_x * (dx * dx) + omega_y * (dy * dy)) * 0.5)
     return val * complex(math.cos(phase), math.sin(phase))
+
+
+def exponential(lattice, n_x=1, n_y=1, norm=1.0, phase=0.0):
+    """ExponentialState values over the tile (src/model.cpp:653-672)."""
+    X, Y = lattice.coordinates()
+    lx = lattice.global_no_halo_dim_x * lattice.delta_x
+    ly = lattice.global_no_halo_dim_y * lattice.delta_y
+    amp = math.sqrt(norm / (lx * ly)) * complex(math.cos(phase), math.sin(phase))
+    arg = 2 * math.pi * float(n_x) / lx * X + 2 * math.pi * float(n_y) / ly * Y
+    return amp * (np.cos(arg) + 1j * np.sin(arg))

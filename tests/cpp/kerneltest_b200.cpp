@@ -1,0 +1,131 @@
+// Known-answer tests of the reference (test/kerneltest.cpp:7-175, tolerances
+// test/kerneltest.h:8-9) written against the C++ API of this engine, with
+// kernel_type "gpu".  A program written for the reference's API compiles
+// against trottersuzuki.h unchanged; this one shows it.  Exit status: the
+// number of failed checks.
+#include <cmath>
+#include <cstdio>
+#include <string>
+
+#include "trottersuzuki.h"
+
+static int failures = 0;
+
+static void check(bool ok, const char *test, const char *what, double got, double want) {
+    std::printf("%-44s %-12s got %.10g want %.10g  %s\n", test, what, got, want,
+                ok ? "ok" : "FAILED");
+    if (!ok) ++failures;
+}
+
+static const double TOLERANCE = 1.e-3, NORM_TOLERANCE = 1.e-5;
+static const int DIM = 250;
+static const double LENGTH = 100;
+
+static void free_particle(const std::string &kt) {
+    Lattice *grid = new Lattice2D(DIM, LENGTH, true, true);
+    State *state = new ExponentialState(static_cast<Lattice2D *>(grid));
+    Hamiltonian *ham = new Hamiltonian(grid, NULL);
+    Solver *solver = new Solver(grid, state, ham, 5.e-3, kt);
+    const double e0 = solver->get_total_energy(), n0 = solver->get_squared_norm();
+    solver->evolve(100);
+    const double e = solver->get_total_energy(), n = solver->get_squared_norm();
+    check(std::fabs(e0 - e) < TOLERANCE, "free_particle", "energy", e, e0);
+    check(std::fabs(n0 - n) < NORM_TOLERANCE, "free_particle", "norm", n, n0);
+    delete solver;
+    delete ham;
+    delete state;
+    delete grid;
+}
+
+static void imaginary_harmonic_oscillator(const std::string &kt) {
+    Lattice2D *grid = new Lattice2D(DIM, LENGTH);
+    State *state = new GaussianState(grid, 0.5);
+    Potential *pot = new HarmonicPotential(grid, 1., 1.);
+    Hamiltonian *ham = new Hamiltonian(grid, pot);
+    Solver *solver = new Solver(grid, state, ham, 5.e-3, kt);
+    const double n0 = solver->get_squared_norm();
+    solver->evolve(1000, true);
+    const double e = solver->get_total_energy(), n = solver->get_squared_norm();
+    check(std::fabs(1.00001 - e) < TOLERANCE, "imaginary_harmonic_oscillator", "energy", e, 1.00001);
+    check(std::fabs(n0 - n) < NORM_TOLERANCE, "imaginary_harmonic_oscillator", "norm", n, n0);
+    delete solver;
+    delete ham;
+    delete pot;
+    delete state;
+    delete grid;
+}
+
+static void intra_particle_interaction(const std::string &kt, bool imag) {
+    Lattice2D *grid = new Lattice2D(DIM, LENGTH);
+    State *state = new GaussianState(grid, 1);
+    Potential *pot = new HarmonicPotential(grid, 1., 1.);
+    Hamiltonian *ham = new Hamiltonian(grid, pot, 1., 10);
+    Solver *solver = new Solver(grid, state, ham, 1.e-3, kt);
+    const double e0 = solver->get_total_energy(), n0 = solver->get_squared_norm();
+    solver->evolve(1000, imag);
+    const double e = solver->get_total_energy(), n = solver->get_squared_norm();
+    const double xx = state->get_mean_xx();
+    const char *name = imag ? "imaginary_intra_particle_interaction" : "intra_particle_interaction";
+    if (imag) {
+        check(std::fabs(1.59273 - e) < TOLERANCE, name, "energy", e, 1.59273);
+        check(std::fabs(0.768148 - xx) < TOLERANCE, name, "<x^2>", xx, 0.768148);
+    } else {
+        check(std::fabs(e0 - e) < TOLERANCE, name, "energy", e, e0);
+        check(std::fabs(1.02321 - xx) < TOLERANCE, name, "<x^2>", xx, 1.02321);
+    }
+    check(std::fabs(n0 - n) < NORM_TOLERANCE, name, "norm", n, n0);
+    delete solver;
+    delete ham;
+    delete pot;
+    delete state;
+    delete grid;
+}
+
+static void rotating_frame(const std::string &kt, bool imag) {
+    const double w = 0.7;
+    Lattice2D *grid = new Lattice2D(300, 20, false, false, w);
+    State *state = new GaussianState(grid, 1);
+    Potential *pot = new HarmonicPotential(grid, 1., 1.);
+    Hamiltonian *ham = new Hamiltonian(grid, pot, 1., 100., w);
+    Solver *solver = new Solver(grid, state, ham, 1.e-4, kt);
+    const double e0 = solver->get_total_energy(), n0 = solver->get_squared_norm();
+    solver->evolve(1000, imag);
+    const double e = solver->get_total_energy(), n = solver->get_squared_norm();
+    const char *name = imag ? "imaginary_rotating_frame_of_reference" : "rotating_frame_of_reference";
+    // test/kerneltest.cpp:154 states 4.89895; the reference itself gives
+    // 4.9018077669 on this setup (its 5th Hamiltonian argument is now the
+    // Lee-Huang-Yang coupling), which is what is checked here.
+    if (imag)
+        check(std::fabs(4.9018077669 - e) < TOLERANCE, name, "energy", e, 4.9018077669);
+    else
+        check(std::fabs(e0 - e) < TOLERANCE * 10., name, "energy", e, e0);
+    check(std::fabs(n0 - n) < NORM_TOLERANCE, name, "norm", n, n0);
+    delete solver;
+    delete ham;
+    delete pot;
+    delete state;
+    delete grid;
+}
+
+int main(int argc, char **argv) {
+    const std::string kt = argc > 1 ? argv[1] : "gpu";
+    free_particle(kt);
+    imaginary_harmonic_oscillator(kt);
+    intra_particle_interaction(kt, false);
+    intra_particle_interaction(kt, true);
+    rotating_frame(kt, false);
+    rotating_frame(kt, true);
+    bool threw = false;
+    try {
+        Lattice2D g(16, 4.);
+        GaussianState s(&g, 1.);
+        Hamiltonian h(&g);
+        Solver solver(&g, &s, &h, 1e-3, "cpu");
+        solver.evolve(1);
+    } catch (std::exception &e) {
+        threw = std::string(e.what()).find("Unknown kernel") != std::string::npos;
+    }
+    check(threw, "unknown kernel type", "throws", threw, 1);
+    std::printf("%d failure(s)\n", failures);
+    return failures;
+}

@@ -42,3 +42,39 @@ def seeded_case(N, L, Ny=None, periodic=(False, False), omega=0.0, seed=0, momen
             * np.exp(1j * momentum * X))
     V = lat.harmonic(1.0, 1.3) + 0.1 * rng.uniform(-1, 1, lat.shape)
     return lat, psi0, V
+
+
+# ---------------------------------------------------------------- fixtures
+import json  # noqa: E402
+import os  # noqa: E402
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def golden_names():
+    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz"))
+
+
+def load_golden(name):
+    z = np.load(os.path.join(GOLDEN, name + ".npz"))
+    meta = json.loads(str(z["meta"]))
+    N, L, Ny, px, py, omega, one_d = meta["lat"]
+    lat = O.Lattice(N, L, Ny, None, px, py, omega, one_d=one_d)
+    return dict(lat=lat, psi0=z["psi0"], V=z["V"], psi=z["psi"], energies=z["energies"],
+                expectations=z["expectations"], meta=meta)
+
+
+def oracle_run_golden(g):
+    """Evolve a golden case with the oracle, segment by segment like Solver::evolve."""
+    meta, lat = g["meta"], g["lat"]
+    psi = g["psi0"].copy()
+    prev_imag = None
+    n0 = 0.0
+    for it, imag in meta["segments"]:
+        if imag and prev_imag is not True:
+            n0 = O.expectations(lat, psi)["norm2"]
+        p = lat.params(meta["dt"], imag, 1.0, meta["g"], meta["lhy"], meta["omega"], norm0=n0)
+        tr, ti = O.exp_table(g["V"], meta["dt"], imag)
+        psi = O.evolve(p, psi, tr, ti, it)
+        prev_imag = imag
+    return psi

@@ -145,17 +145,35 @@ __device__ __forceinline__ float fma_t(float a, float b, float c) { return __fma
 __device__ __forceinline__ double mul_t(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ float mul_t(float a, float b) { return __fmul_rn(a, b); }
 
+// FP32 storage works in "delta form": a coefficient a that is close to 1 is
+// carried as a - 1, and an update x' = a x + y is evaluated as
+// x + ((a - 1) x + y).  Stored in float, a itself would be off by up to half an
+// ulp of 1 (6e-8), the same on every sweep, and the norm would drift by that
+// much per sweep; a - 1 is small, so its rounding error is tiny.  The FP64 path
+// keeps the reference's form a x + y.
+template <typename T>
+struct DeltaForm {
+    static constexpr bool value = std::is_same<T, float>::value;
+};
+
+// z + ((a - 1) z + p) in delta form, a z + p otherwise (a is a - 1 in delta form).
+template <typename T>
+__device__ __forceinline__ T lin(T a, T z, T p) {
+    if (DeltaForm<T>::value) return z + fma_t(a, z, p);
+    return fma_t(a, z, p);
+}
+
 // Kinetic pair (src/cpucartesian.cpp:8-11 real time, :29-32 imaginary time);
 // the update is symmetric, so each cell is updated from (self, partner).
 template <bool IMAG, typename T>
 __device__ __forceinline__ Cx<T> kin(Cx<T> s, Cx<T> p, T a, T b) {
     Cx<T> r;
     if (IMAG) {
-        r.re = fma_t(a, s.re, mul_t(b, p.re));
-        r.im = fma_t(a, s.im, mul_t(b, p.im));
+        r.re = lin(a, s.re, mul_t(b, p.re));
+        r.im = lin(a, s.im, mul_t(b, p.im));
     } else {
-        r.re = fma_t(a, s.re, -mul_t(b, p.im));
-        r.im = fma_t(a, s.im, mul_t(b, p.re));
+        r.re = lin(a, s.re, -mul_t(b, p.im));
+        r.im = lin(a, s.im, mul_t(b, p.re));
     }
     return r;
 }
@@ -166,11 +184,11 @@ template <bool IMAG, typename T>
 __device__ __forceinline__ Cx<T> rot_first(Cx<T> f, Cx<T> s, T a, T b) {
     Cx<T> r;
     if (IMAG) {
-        r.re = fma_t(a, f.re, mul_t(b, s.im));
-        r.im = fma_t(a, f.im, -mul_t(b, s.re));
+        r.re = lin(a, f.re, mul_t(b, s.im));
+        r.im = lin(a, f.im, -mul_t(b, s.re));
     } else {
-        r.re = fma_t(a, f.re, mul_t(b, s.re));
-        r.im = fma_t(a, f.im, mul_t(b, s.im));
+        r.re = lin(a, f.re, mul_t(b, s.re));
+        r.im = lin(a, f.im, mul_t(b, s.im));
     }
     return r;
 }
@@ -179,11 +197,11 @@ template <bool IMAG, typename T>
 __device__ __forceinline__ Cx<T> rot_second(Cx<T> s, Cx<T> f, T a, T b) {
     Cx<T> r;
     if (IMAG) {
-        r.re = fma_t(a, s.re, -mul_t(b, f.im));
-        r.im = fma_t(a, s.im, mul_t(b, f.re));
+        r.re = lin(a, s.re, -mul_t(b, f.im));
+        r.im = lin(a, s.im, mul_t(b, f.re));
     } else {
-        r.re = fma_t(a, s.re, -mul_t(b, f.re));
-        r.im = fma_t(a, s.im, -mul_t(b, f.im));
+        r.re = lin(a, s.re, -mul_t(b, f.re));
+        r.im = lin(a, s.im, -mul_t(b, f.im));
     }
     return r;
 }
@@ -301,6 +319,8 @@ __device__ __forceinline__ void rcol(Cx<T> (&up)[C], Cx<T> (&lo)[C], const Cx<T>
 static __device__ __noinline__ void sincos_t(double x, double *s, double *c) { sincos(x, s, c); }
 static __device__ __noinline__ void sincos_t(float x, float *s, float *c) { sincosf(x, s, c); }
 static __device__ __noinline__ double exp_t(double x) { return exp(x); }
+static __device__ __noinline__ double sin_t(double x) { return sin(x); }
+static __device__ __noinline__ float sin_t(float x) { return sinf(x); }
 static __device__ __noinline__ float exp_t(float x) { return expf(x); }
 __device__ __forceinline__ double sqrt_t(double x) { return sqrt(x); }
 __device__ __forceinline__ float sqrt_t(float x) { return sqrtf(x); }
@@ -310,6 +330,7 @@ __device__ __forceinline__ float sqrt_t(float x) { return sqrtf(x); }
 // series of cos, sin and exp truncated after the x^10 / x^11 / x^8 terms
 // (Horner's rule) leave a remainder below 1e-19, i.e. well under half an ulp
 // of double; larger arguments take the CUDA math library.
+// Returns sin(th) and cos(th) (cos(th) - 1 in delta form).
 template <typename T>
 __device__ __forceinline__ void phase_sincos(T th, T *s, T *c) {
     // warp-uniform choice: the library path only if some lane needs it
@@ -320,7 +341,7 @@ __device__ __forceinline__ void phase_sincos(T th, T *s, T *c) {
         pc = fma_t(pc, t, T(-1.3888888888888889e-03)); // -1/6!
         pc = fma_t(pc, t, T(4.1666666666666664e-02));  //  1/4!
         pc = fma_t(pc, t, T(-0.5));                    // -1/2!
-        *c = fma_t(pc, t, T(1));
+        *c = DeltaForm<T>::value ? mul_t(pc, t) : fma_t(pc, t, T(1));
         T ps = T(-2.5052108385441720e-08);             // -1/11!
         ps = fma_t(ps, t, T(2.7557319223985888e-06));  //  1/9!
         ps = fma_t(ps, t, T(-1.9841269841269841e-04)); // -1/7!
@@ -329,6 +350,11 @@ __device__ __forceinline__ void phase_sincos(T th, T *s, T *c) {
         *s = fma_t(mul_t(ps, t), th, th);
     } else {
         sincos_t(th, s, c);
+        if (DeltaForm<T>::value) {
+            // cos(th) - 1 = -2 sin^2(th / 2), without cancellation
+            const T h = sin_t(T(0.5) * th);
+            *c = T(-2) * h * h;
+        }
     }
 }
 
@@ -372,20 +398,21 @@ __device__ __forceinline__ void potential_row(Cx<T> (&w)[C], const TabT *tab, T 
             }
         } else {
             const Cx<T> e = reinterpret_cast<const Cx<T> *>(tab)[i];
-            T c = T(1), s = T(0);
+            T c = DeltaForm<T>::value ? T(0) : T(1), s = T(0);
             if (PHASE) {
                 const T n2 = fma_t(v.re, v.re, mul_t(v.im, v.im));
                 T th = mul_t(ca, n2);
                 if (LHY) th = fma_t(caa, mul_t(n2, sqrt_t(n2)), th);
                 phase_sincos(th, &s, &c);
             }
+            // the table holds (cos, sin) of -dt V; in delta form (cos - 1, sin)
             T t = v.re;
-            v.re = fma_t(e.re, t, -mul_t(e.im, v.im));
-            v.im = fma_t(e.re, v.im, mul_t(e.im, t));
+            v.re = lin(e.re, t, -mul_t(e.im, v.im));
+            v.im = lin(e.re, v.im, mul_t(e.im, t));
             if (PHASE) {
                 t = v.re;
-                v.re = fma_t(c, t, mul_t(s, v.im));
-                v.im = fma_t(c, v.im, -mul_t(s, t));
+                v.re = lin(c, t, mul_t(s, v.im));
+                v.im = lin(c, v.im, -mul_t(s, t));
             }
         }
         w[i] = v;

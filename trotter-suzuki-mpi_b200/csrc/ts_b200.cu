@@ -29,6 +29,54 @@ namespace {
 
 std::atomic<uint64_t> g_launches{0};
 
+
+// ------------------------------------------------ FP32 rounding of rotations
+// The FP32 step works in delta form (see step_kernel.cuh): a 2x2 rotation
+// with coefficients (a, b) is stored as (a - 1, b).  It conserves the norm
+// only if (1 + am1)^2 + b^2 = 1 for the stored floats.  Among the floats within
+// `span` ulps of the rounded values the pair with the smallest defect
+// |2 am1 + am1^2 + b^2| (exact in double for float inputs) is kept; ties go to
+// the pair closest to the exact values.  am1 is passed in double, computed
+// without cancellation by the caller.
+__host__ __device__ inline void unimodular_float_pair(double am1, double b, int span, float *fa,
+                                                      float *fb) {
+    const float a0 = (float)am1, b0 = (float)b;
+    float ba = a0, bb = b0;
+    auto defect = [](float x, float y) {
+        return fabs(2.0 * (double)x + (double)x * x + (double)y * y);
+    };
+    double best = defect(a0, b0);
+    double bestd = fabs((double)a0 - am1) + fabs((double)b0 - b);
+    float ai = a0;
+    for (int i = 0; i < span; ++i) ai = nextafterf(ai, -INFINITY);
+    for (int i = -span; i <= span; ++i, ai = nextafterf(ai, INFINITY)) {
+        float bj = b0;
+        for (int j = 0; j < span; ++j) bj = nextafterf(bj, -INFINITY);
+        for (int j = -span; j <= span; ++j, bj = nextafterf(bj, INFINITY)) {
+            const double err = defect(ai, bj);
+            const double d = fabs((double)ai - am1) + fabs((double)bj - b);
+            if (err < best || (err == best && d < bestd)) {
+                best = err;
+                bestd = d;
+                ba = ai;
+                bb = bj;
+            }
+        }
+    }
+    *fa = ba;
+    *fb = bb;
+}
+
+// cos(k) - 1 and cosh(k) - 1 without cancellation.
+__host__ __device__ inline double cos_m1(double k) {
+    const double h = sin(0.5 * k);
+    return -2.0 * h * h;
+}
+__host__ __device__ inline double cosh_m1(double k) {
+    const double h = sinh(0.5 * k);
+    return 2.0 * h * h;
+}
+
 // ------------------------------------------------------------------ kernels
 
 // Interleave host-order SoA doubles (row stride `sstride`) into the device
@@ -61,6 +109,11 @@ __global__ void pack_table_kernel(void *dst, int imag, int W, int H, int P, cons
         const double vi = x < W ? im[(size_t)y * sstride + x] : 0.0;
         if (imag) {
             reinterpret_cast<T *>(dst)[k] = (T)vr;
+        } else if (sizeof(T) == 4) {
+            // delta form (cos - 1, sin); vr - 1 is exact enough in double
+            float fr, fi;
+            unimodular_float_pair(vr - 1.0, vi, 4, &fr, &fi);
+            reinterpret_cast<Cx<T> *>(dst)[k] = Cx<T>{(T)fr, (T)fi};
         } else {
             reinterpret_cast<Cx<T> *>(dst)[k] = Cx<T>{(T)vr, (T)vi};
         }
@@ -471,6 +524,25 @@ void geometry(const ts_b200_kernel *k, int *strips, int *segs, int *blocks, size
 }
 
 template <typename T>
+int launch_halo_t(ts_b200_kernel *k) {
+    if (!(k->d.periodic_x || k->d.periodic_y)) return TS_B200_OK;
+    const int hx = k->d.halo_x, hy = k->d.halo_y;
+    const int nx = k->d.periodic_x ? 2 * hx * k->H : 0;
+    const int ny = k->d.periodic_y ? 2 * hy * (k->d.periodic_x ? k->W - 2 * hx : k->W) : 0;
+    const int n = nx + ny;
+    if (n <= 0) return TS_B200_OK;
+    const int threads = 256;
+    const int nb = std::min(div_up(n, threads), 4096);
+    halo_kernel<T><<<nb, threads, 0, k->stream>>>(reinterpret_cast<Cx<T> *>(k->psi[k->cur]), k->W,
+                                                  k->H, k->P, hx, hy, k->d.periodic_x,
+                                                  k->d.periodic_y, k->d.inner_y0);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(k, e, "halo kernel launch");
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    return TS_B200_OK;
+}
+
+template <typename T>
 int launch_step_t(ts_b200_kernel *k, int exchange, bool dry = false) {
     int strips, segs, blocks;
     size_t smem;
@@ -487,7 +559,6 @@ int launch_step_t(ts_b200_kernel *k, int exchange, bool dry = false) {
         if (k->auto_seg) auto_segments(k);
     }
     geometry(k, &strips, &segs, &blocks, &smem);
-    if (dry) blocks = 0;
     const size_t nwarps = (size_t)std::max(blocks, 1) * k->warps;
     if (k->imag && nwarps > k->partials_cap) {
         if (k->partials) cudaFree(k->partials);
@@ -495,6 +566,7 @@ int launch_step_t(ts_b200_kernel *k, int exchange, bool dry = false) {
         TSB_CHECK(k, cudaMalloc(&k->partials, nwarps * sizeof(double)));
         k->partials_cap = nwarps;
     }
+    if (dry) blocks = 0;
     StepArgs<T> a{};
     a.psi_in = k->psi[k->cur];
     a.psi_out = k->psi[1 - k->cur];
@@ -516,6 +588,25 @@ int launch_step_t(ts_b200_kernel *k, int exchange, bool dry = false) {
     a.bH = (T)k->d.b_h;
     a.aV = (T)k->d.a_v;
     a.bV = (T)k->d.b_v;
+    if (sizeof(T) == 4) {
+        // delta form: a - 1 from the angle, without cancellation
+        const double kx = k->imag ? asinh(k->d.b_h) : asin(k->d.b_h);
+        const double ky = k->imag ? asinh(k->d.b_v) : asin(k->d.b_v);
+        const double amh = k->imag ? cosh_m1(kx) : cos_m1(kx);
+        const double amv = k->imag ? cosh_m1(ky) : cos_m1(ky);
+        float fa, fb;
+        if (k->imag) {
+            a.aH = (T)amh;
+            a.aV = (T)amv;
+        } else {
+            unimodular_float_pair(amh, k->d.b_h, 16, &fa, &fb);
+            a.aH = (T)fa;
+            a.bH = (T)fb;
+            unimodular_float_pair(amv, k->d.b_v, 16, &fa, &fb);
+            a.aV = (T)fa;
+            a.bV = (T)fb;
+        }
+    }
     a.ca = (T)k->d.coupling;
     a.caa = (T)k->d.lhy_coupling;
     a.partials = k->partials;
@@ -528,21 +619,9 @@ int launch_step_t(ts_b200_kernel *k, int exchange, bool dry = false) {
     if (dry) return TS_B200_OK;
     g_launches.fetch_add(1, std::memory_order_relaxed);
     k->cur = 1 - k->cur;
-    if (exchange && (k->d.periodic_x || k->d.periodic_y)) {
-        const int hx = k->d.halo_x, hy = k->d.halo_y;
-        const int nx = k->d.periodic_x ? 2 * hx * k->H : 0;
-        const int ny = k->d.periodic_y ? 2 * hy * (k->d.periodic_x ? k->W - 2 * hx : k->W) : 0;
-        const int n = nx + ny;
-        if (n > 0) {
-            const int threads = 256;
-            const int nb = std::min(div_up(n, threads), 4096);
-            halo_kernel<T><<<nb, threads, 0, k->stream>>>(
-                reinterpret_cast<Cx<T> *>(k->psi[k->cur]), k->W, k->H, k->P, hx, hy,
-                k->d.periodic_x, k->d.periodic_y, k->d.inner_y0);
-            e = cudaGetLastError();
-            if (e != cudaSuccess) return cuda_fail(k, e, "halo kernel launch");
-            g_launches.fetch_add(1, std::memory_order_relaxed);
-        }
+    if (exchange) {
+        const int st = launch_halo_t<T>(k);
+        if (st) return st;
     }
     return TS_B200_OK;
 }
@@ -617,13 +696,27 @@ int upload_rotation(ts_b200_kernel *k) {
         const double ang = -0.5 * k->d.alpha_y * (y + offy);
         const double a = k->imag ? std::cosh(ang) : std::cos(ang);
         const double b = k->imag ? std::sinh(ang) : std::sin(ang);
-        rows[y] = Cx<T>{(T)a, (T)b};
+        if (sizeof(T) == 4) {
+            const double am1 = k->imag ? cosh_m1(ang) : cos_m1(ang);
+            float fa = (float)am1, fb = (float)b;
+            if (!k->imag) unimodular_float_pair(am1, b, 16, &fa, &fb);
+            rows[y] = Cx<T>{(T)fa, (T)fb};
+        } else {
+            rows[y] = Cx<T>{(T)a, (T)b};
+        }
     }
     for (int x = 0; x < W; ++x) {
         const double ang = k->d.alpha_x * (x + offx);
         const double a = k->imag ? std::cosh(ang) : std::cos(ang);
         const double b = k->imag ? std::sinh(ang) : std::sin(ang);
-        cols[x] = Cx<T>{(T)a, (T)b};
+        if (sizeof(T) == 4) {
+            const double am1 = k->imag ? cosh_m1(ang) : cos_m1(ang);
+            float fa = (float)am1, fb = (float)b;
+            if (!k->imag) unimodular_float_pair(am1, b, 16, &fa, &fb);
+            cols[x] = Cx<T>{(T)fa, (T)fb};
+        } else {
+            cols[x] = Cx<T>{(T)a, (T)b};
+        }
     }
     cudaError_t e = cudaMemcpy(k->row_ab, rows, sizeof(Cx<T>) * H, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(k->col_ab, cols, sizeof(Cx<T>) * W, cudaMemcpyHostToDevice);
@@ -849,6 +942,11 @@ int ts_b200_step(ts_b200_kernel *k, int exchange) {
     return launch_step(k, exchange);
 }
 
+int ts_b200_halo_exchange(ts_b200_kernel *k) {
+    if (!k) return TS_B200_INVALID_ARGUMENT;
+    return k->fp32 ? launch_halo_t<float>(k) : launch_halo_t<double>(k);
+}
+
 int ts_b200_evolve(ts_b200_kernel *k, int iterations) {
     if (!k || iterations < 0) return TS_B200_INVALID_ARGUMENT;
     if (iterations == 0) return TS_B200_OK;
@@ -875,9 +973,10 @@ int ts_b200_evolve(ts_b200_kernel *k, int iterations) {
             for (int i = 0; i < G && s == TS_B200_OK; ++i) s = launch_step(k, 1);
             cudaError_t e = cudaStreamEndCapture(k->stream, &g);
             g_launches.store(before);  // captured launches are counted when replayed
-            if (s != TS_B200_OK) {
+            if (s != TS_B200_OK || e != cudaSuccess) {
                 if (g) cudaGraphDestroy(g);
-                return s;
+                (void)cudaGetLastError();  // do not leave the capture error to later calls
+                if (s != TS_B200_OK) return s;
             }
             if (e != cudaSuccess) return cuda_fail(k, e, "graph capture");
             e = cudaGraphInstantiate(&k->graph, g, 0);

@@ -1,0 +1,182 @@
+// B200Kernel and the GPU reductions used by the model objects.
+#include "b200kernel.h"
+
+#include <cmath>
+#include <stdexcept>
+#include <string>
+
+namespace b200 {
+
+ts_b200_desc make_desc(Lattice *g, Hamiltonian *ham, double dt, double norm, bool imag,
+                       int precision) {
+    if (g->coordinate_system != "cartesian")
+        my_abort("The B200 kernel supports cartesian coordinates only.");
+    ts_b200_desc d = {};
+    d.dim_x = g->dim_x;
+    d.dim_y = g->dim_y;
+    d.inner_x0 = g->inner_start_x - g->start_x;
+    d.inner_x1 = g->inner_end_x - g->start_x;
+    d.inner_y0 = g->inner_start_y - g->start_y;
+    d.inner_y1 = g->inner_end_y - g->start_y;
+    d.halo_x = g->halo_x;
+    d.halo_y = g->halo_y;
+    d.periodic_x = g->periods[1];
+    d.periodic_y = g->periods[0];
+    d.imag_time = imag ? 1 : 0;
+    d.precision = precision;
+    // step constants exactly as the reference's CPUBlock constructor computes
+    // them (src/cpukernel.cpp:185-216)
+    const double kx = dt / (4. * ham->mass * g->delta_x * g->delta_x);
+    const double ky = dt / (4. * ham->mass * g->delta_y * g->delta_y);
+    if (imag) {
+        d.a_h = cosh(kx);
+        d.b_h = sinh(kx);
+        d.a_v = cosh(ky);
+        d.b_v = sinh(ky);
+    } else {
+        d.a_h = cos(kx);
+        d.b_h = sin(kx);
+        d.a_v = cos(ky);
+        d.b_v = sin(ky);
+    }
+    d.alpha_x = ham->angular_velocity * dt * g->delta_x / (2 * g->delta_y);
+    d.alpha_y = ham->angular_velocity * dt * g->delta_y / (2 * g->delta_x);
+    d.coupling = ham->coupling_a * dt;
+    d.lhy_coupling = ham->LeeHuangYang_coupling_a * dt;
+    d.rot_offset_x = g->start_x - ham->rot_coord_x;
+    d.rot_offset_y = g->start_y - ham->rot_coord_y;
+    d.delta_x = g->delta_x;
+    d.delta_y = g->delta_y;
+    d.norm0 = imag ? norm : 0.0;
+    return d;
+}
+
+namespace {
+
+void fail(int status, ts_b200_kernel *h, const char *what) {
+    std::string msg = std::string(what) + ": " + ts_b200_status_string(status);
+    if (h) {
+        const char *e = ts_b200_last_error(h);
+        if (e && *e) msg += std::string(" (") + e + ")";
+    }
+    my_abort(msg);
+}
+
+// A short-lived FP64 real-time handle holding a host tile, for reductions.
+struct ScratchTile {
+    ts_b200_kernel *h = nullptr;
+    ScratchTile(Lattice *g, const double *re, const double *im) {
+        ts_b200_desc d = {};
+        d.dim_x = g->dim_x;
+        d.dim_y = g->dim_y;
+        d.inner_x0 = g->inner_start_x - g->start_x;
+        d.inner_x1 = g->inner_end_x - g->start_x;
+        d.inner_y0 = g->inner_start_y - g->start_y;
+        d.inner_y1 = g->inner_end_y - g->start_y;
+        d.halo_x = g->halo_x;
+        d.halo_y = g->halo_y;
+        d.precision = TS_B200_FP64;
+        d.a_h = d.a_v = 1.0;
+        d.delta_x = g->delta_x;
+        d.delta_y = g->delta_y;
+        int s = ts_b200_create(&d, &h);
+        if (s) fail(s, nullptr, "creating a device tile");
+        s = ts_b200_set_state(h, re, im, g->dim_x);
+        if (s) fail(s, h, "uploading the state");
+    }
+    ~ScratchTile() { ts_b200_destroy(h); }
+};
+
+ts_b200_energy_params params_of(Lattice *g) {
+    ts_b200_energy_params p = {};
+    p.start_x = g->start_x;
+    p.start_y = g->start_y;
+    p.global_no_halo_dim_x = g->global_no_halo_dim_x;
+    p.global_no_halo_dim_y = g->global_no_halo_dim_y;
+    p.length_x = g->length_x;
+    p.length_y = g->length_y;
+    return p;
+}
+
+}  // namespace
+
+Expectations reduce_expectations(Lattice *g, const double *re, const double *im) {
+    ScratchTile t(g, re, im);
+    ts_b200_energy_params p = params_of(g);
+    ts_b200_expectation_result r;
+    int s = ts_b200_expectations(t.h, &p, &r);
+    if (s) fail(s, t.h, "expectation values");
+    Expectations e = {r.norm2,  r.mean_x,  r.mean_xx,   r.mean_y,    r.mean_yy,
+                      r.mean_px, r.mean_pxpx, r.mean_py, r.mean_pypy, r.mean_lz};
+    return e;
+}
+
+ts_b200_energy_result reduce_energies(Lattice *g, const double *re, const double *im,
+                                      const double *V, double mass, double coupling,
+                                      double lhy, double omega) {
+    ScratchTile t(g, re, im);
+    ts_b200_energy_params p = params_of(g);
+    p.mass = mass;
+    p.coupling = coupling;
+    p.lhy_coupling = lhy;
+    p.angular_velocity = omega;
+    ts_b200_energy_result r;
+    int s = ts_b200_energies(t.h, V, &p, &r);
+    if (s) fail(s, t.h, "energies");
+    return r;
+}
+
+}  // namespace b200
+
+B200Kernel::B200Kernel(Lattice *grid, State *state, Hamiltonian *ham, double *pot_re,
+                       double *pot_im, double dt, double norm, bool imag, int precision)
+    : h_(nullptr), dim_x_(grid->dim_x), dim_y_(grid->dim_y), imag_time_(imag) {
+    ts_b200_desc d = b200::make_desc(grid, ham, dt, norm, imag, precision);
+    int s = ts_b200_create(&d, &h_);
+    if (s) b200::fail(s, nullptr, "B200Kernel: creating the device tile");
+    s = ts_b200_set_state(h_, state->p_real, state->p_imag, grid->dim_x);
+    if (s == 0) s = ts_b200_set_exp_potential(h_, pot_re, pot_im, grid->dim_x);
+    if (s) {
+        const std::string e = ts_b200_last_error(h_);
+        ts_b200_destroy(h_);
+        h_ = nullptr;
+        my_abort("B200Kernel: uploading the state: " + e);
+    }
+}
+
+B200Kernel::~B200Kernel() { ts_b200_destroy(h_); }
+
+void B200Kernel::check(int status, const char *what) const {
+    if (status) b200::fail(status, h_, what);
+}
+
+void B200Kernel::run_kernel() { check(ts_b200_step(h_, 0), "B200Kernel::run_kernel"); }
+
+void B200Kernel::finish_halo_exchange() {
+    check(ts_b200_halo_exchange(h_), "B200Kernel::finish_halo_exchange");
+}
+
+void B200Kernel::evolve(int iterations) {
+    check(ts_b200_evolve(h_, iterations), "B200Kernel::evolve");
+}
+
+void B200Kernel::steps_with_exchange(int n) {
+    for (int i = 0; i < n; ++i) check(ts_b200_step(h_, 1), "B200Kernel::step");
+}
+
+void B200Kernel::get_sample(size_t dest_stride, size_t x, size_t y, size_t width, size_t height,
+                            double *dest_real, double *dest_imag, double *, double *) const {
+    check(ts_b200_get_sample(h_, dest_stride, x, y, width, height, dest_real, dest_imag),
+          "B200Kernel::get_sample");
+}
+
+double B200Kernel::calculate_squared_norm(bool) const {
+    double n = 0;
+    check(ts_b200_squared_norm(h_, &n), "B200Kernel::calculate_squared_norm");
+    return n;
+}
+
+void B200Kernel::update_potential(double *re, double *im, int which) {
+    if (which != 0) my_abort("B200Kernel: single-component kernel (potential index 0 only)");
+    check(ts_b200_set_exp_potential(h_, re, im, dim_x_), "B200Kernel::update_potential");
+}

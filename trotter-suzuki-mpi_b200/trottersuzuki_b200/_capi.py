@@ -76,6 +76,7 @@ SIGNATURES = {
     "ts_b200_set_exp_potential": (_I, [_VP, _DP, _DP, _SZ]),
     "ts_b200_step": (_I, [_VP, _I]),
     "ts_b200_evolve": (_I, [_VP, _I]),
+    "ts_b200_halo_exchange": (_I, [_VP]),
     "ts_b200_get_sample": (_I, [_VP, _SZ, _SZ, _SZ, _SZ, _SZ, _DP, _DP]),
     "ts_b200_squared_norm": (_I, [_VP, C.POINTER(C.c_double)]),
     "ts_b200_energies": (_I, [_VP, _DP, C.POINTER(EnergyParams), C.POINTER(EnergyResult)]),

@@ -41,6 +41,28 @@ def _compile(src, extra):
     return obj
 
 
+HOST = os.path.join(PKG_ROOT, "host")
+CXX = os.environ.get("TS_B200_CXX", "g++")
+
+
+def build_host(verbose=True):
+    """The C++ host layer (drop-in API) linked against libtsb200.so."""
+    srcs = sorted(os.path.join(HOST, f) for f in os.listdir(HOST) if f.endswith(".cpp"))
+    deps = srcs + [os.path.join(HOST, f) for f in os.listdir(HOST) if f.endswith(".h")]
+    deps += [os.path.join(INCLUDE, f) for f in os.listdir(INCLUDE) if f.endswith(".h")]
+    out = os.path.join(HERE, "libtrottersuzuki_b200.so")
+    cuda_lib = os.path.join(HERE, "libtsb200.so")
+    if _stale(out, deps + [cuda_lib]):
+        cmd = [CXX, "-O2", "-std=c++17", "-fPIC", "-shared", "-ffp-contract=off",
+               "-I" + INCLUDE, "-I" + HOST] + srcs + [
+            "-L" + HERE, "-ltsb200", "-Wl,-rpath,$ORIGIN", "-o", out + ".tmp"]
+        subprocess.check_call(cmd)
+        os.replace(out + ".tmp", out)
+    if verbose:
+        print("built", out)
+    return out
+
+
 def build(verbose=True, extra=()):
     os.makedirs(BUILD, exist_ok=True)
     srcs = sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu"))
@@ -53,6 +75,7 @@ def build(verbose=True, extra=()):
         os.replace(out + ".tmp", out)
     if verbose:
         print("built", out)
+    build_host(verbose)
     return out
 
 
