@@ -1,0 +1,436 @@
+"""Benchmark of the B200 Trotter-Suzuki evolution.
+
+Workload (the configuration the headline metric is quoted on): 2D GPE
+imaginary-time ground state in FP64 on a 2048 x 2048 lattice over length 24,
+closed boundaries, harmonic trap omega_x = 1, omega_y = 1.5, g = 100,
+Omega = 0; initial state a normalised Gaussian (sigma 2) times
+(1 + 0.01 u), u seeded uniform in [-1, 1); dt = 1e-4, renormalised every step.
+One bench step = one evolve() of 2000 Trotter steps, so the default 10 timed
+steps are the configuration's 20000-step run.  Synthetic inputs of the
+configuration's shape; nothing is read from disk.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+With N > 1 (torchrun, one process per GPU) every rank evolves its own copy
+(replicas: a single lattice is not split across GPUs), times are the max over
+ranks and the value is the total site-steps of all ranks per second.
+
+The JSON line reports: value (device-resident, CUDA events on the kernel's
+stream), e2e (through the C ABI from pinned host buffers, state copied in and
+out every step), the roofline of the step kernel against the measured HBM
+peak, the FP32-storage form on the same workload, the reference's own CPU
+implementation timed on this host (cpu_baseline), clocks sampled during the
+timed region and the number of kernel launches.
+"""
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "trotter-suzuki-mpi_b200"))
+
+import numpy as np  # noqa: E402
+
+N_SIDE = 2048
+LENGTH = 24.0
+OMEGA_X, OMEGA_Y = 1.0, 1.5
+G = 100.0
+DT = 1e-4
+TROTTER_PER_STEP = 2000
+BYTES_PER_SITE_STEP = {"fp64": 40, "fp32": 20}  # imaginary time: psi in + psi out + real table
+SEED = 20240601
+WORKLOAD = "gpe_imaginary_time_2048"
+
+
+def initial_state(grid_info):
+    """Normalised Gaussian (sigma 2) x (1 + 0.01 u) over the tile (host numpy)."""
+    W, H = grid_info["dim_x"], grid_info["dim_y"]
+    dx, dy = grid_info["delta_x"], grid_info["delta_y"]
+    x = (np.arange(W) + 0.5) * dx - W * dx * 0.5
+    y = (np.arange(H) + 0.5) * dy - H * dy * 0.5
+    X, Y = np.meshgrid(x, y)
+    w = 1.0 / 4.0  # omega = 1 / sigma^2
+    psi = np.sqrt(w / math.pi) * np.exp(-(w * X * X + w * Y * Y) * 0.5)
+    rng = np.random.Generator(np.random.PCG64(SEED))
+    psi = psi * (1.0 + 0.01 * rng.uniform(-1.0, 1.0, psi.shape))
+    psi = psi / math.sqrt(np.sum(psi * psi) * dx * dy)
+    return psi.astype(np.complex128)
+
+
+def measured_peak():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def committed_traffic():
+    """DRAM bytes per step-kernel launch from the committed ncu summary, if any."""
+    path = os.path.join(REPO, "profiles", "step_kernel_traffic.json")
+    try:
+        with open(path) as f:
+            t = json.load(f)
+        return t
+    except Exception:
+        return None
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.tmp = None
+
+    def __enter__(self):
+        try:
+            self.tmp = tempfile.NamedTemporaryFile("w+", delete=False, suffix=".csv")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.tmp, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.tmp:
+            return None
+        try:
+            rows = [r.split(",") for r in open(self.tmp.name).read().strip().splitlines()]
+            os.unlink(self.tmp.name)
+        except Exception:
+            return None
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[0]))
+                mx.append(float(r[1]))
+                for n, v in zip(names, r[4:8]):
+                    if v.strip().lower() == "active":
+                        reasons.add(n)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl" if args.impl == "b200" else "gloo",
+                                timeout=datetime.timedelta(seconds=300))
+        pg = dist
+    return rank, world, local, pg
+
+
+def max_over_ranks(value, pg, device=None):
+    if pg is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+# --------------------------------------------------------------- CPU legs
+def cpu_reference_rate(psi0, budget_s=12.0, threads=None):
+    """The reference's own CPU implementation (oracle/_ref, compiled from the
+    reference sources; its -Ofast build when present) on the bench workload."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import tsref
+    flavour = "fast" if tsref.available("fast") else ("parity" if tsref.available() else None)
+    threads = threads or os.cpu_count() or 1
+
+    def run(steps):
+        cfg = tsref.make_config(N_SIDE, LENGTH, harmonic=(OMEGA_X, OMEGA_Y, 1.0, 0.0, 0.0),
+                                coupling=G, delta_t=DT, segments=((1, True), (steps, True)),
+                                omp_threads=threads)
+        _, res = tsref.run(cfg, psi0, None, flavour=flavour)
+        return res.seg_seconds[1]
+
+    if flavour is not None:
+        t = run(4)
+        steps = int(max(4, min(2000, budget_s / max(t / 4, 1e-6))))
+        secs = run(steps)
+        kind = "reference"
+        sample = (f"{N_SIDE}x{N_SIDE} GPE imaginary time, {steps} Trotter steps after 1 warm-up "
+                  f"step, reference CPUBlock ({'-Ofast' if flavour == 'fast' else '-O2'} "
+                  f"build), {threads} OpenMP threads")
+        return N_SIDE * N_SIDE * steps / secs, threads, kind, sample, steps
+    # the oracle restatement, single thread
+    import oracle as O
+    lat = O.Lattice(N_SIDE, LENGTH)
+    V = lat.harmonic(OMEGA_X, OMEGA_Y)
+    n0 = O.expectations(lat, psi0)["norm2"]
+    p = lat.params(DT, True, 1.0, G, 0.0, 0.0, norm0=n0)
+    tr, ti = O.exp_table(V, DT, True)
+    t0 = time.perf_counter()
+    O.evolve(p, psi0, tr, ti, 2)
+    t = time.perf_counter() - t0
+    steps = int(max(2, min(500, budget_s / max(t / 2, 1e-6))))
+    t0 = time.perf_counter()
+    O.evolve(p, psi0, tr, ti, steps)
+    secs = time.perf_counter() - t0
+    sample = f"{N_SIDE}x{N_SIDE} GPE imaginary time, {steps} Trotter steps, C restatement, 1 thread"
+    return N_SIDE * N_SIDE * steps / secs, 1, "port", sample, steps
+
+
+def run_reference_arm(args, rank, world, pg):
+    if rank != 0:
+        return
+    grid_info = {"dim_x": N_SIDE, "dim_y": N_SIDE, "delta_x": LENGTH / N_SIDE,
+                 "delta_y": LENGTH / N_SIDE}
+    psi0 = initial_state(grid_info)
+    for _ in range(args.warmup):
+        cpu_reference_rate(psi0, budget_s=2.0)
+    rates = []
+    last = None
+    for _ in range(args.steps):
+        last = cpu_reference_rate(psi0, budget_s=args.ref_budget)
+        rates.append(last[0])
+    rate = statistics.mean(rates)
+    _, cores, kind, sample, steps = last
+    line = {
+        "impl": "reference", "metric": "site-steps/s", "value": rate, "unit": "site-steps/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": N_SIDE * N_SIDE * steps / rate * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "lattice": f"{N_SIDE}x{N_SIDE}", "length": LENGTH,
+                   "trotter_steps_per_step": steps, "dt": DT, "g": G,
+                   "omega_xy": [OMEGA_X, OMEGA_Y], "boundary": "closed", "imag_time": True},
+        "cpu_baseline": {"value": rate, "unit": "site-steps/s", "cores": cores, "kind": kind,
+                         "sample": sample},
+        "e2e": {"value": rate, "unit": "site-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- GPU leg
+def build_solver(kernel_type):
+    import trottersuzuki_b200 as ts
+    grid = ts.Lattice2D(N_SIDE, LENGTH)
+    state = ts.State(grid)
+    info = {"dim_x": grid.dim_x, "dim_y": grid.dim_y, "delta_x": grid.delta_x,
+            "delta_y": grid.delta_y}
+    psi0 = initial_state(info)
+    state.init_state_matrix(psi0.real, psi0.imag)
+    pot = ts.HarmonicPotential(grid, OMEGA_X, OMEGA_Y)
+    ham = ts.Hamiltonian(grid, pot, 1.0, G)
+    solver = ts.Solver(grid, state, ham, DT, kernel_type=kernel_type)
+    return ts, grid, state, pot, ham, solver, psi0
+
+
+def time_device(solver, handle, stream, steps):
+    """K bench steps with the state resident in HBM: evolve(-T) keeps the tile
+    on the device (no copy back), events on the kernel's stream."""
+    import torch
+    from trottersuzuki_b200 import launch_count
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    l0 = launch_count()
+    e0.record(stream)
+    for _ in range(steps):
+        solver.evolve(-TROTTER_PER_STEP, True)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1), launch_count() - l0
+
+
+def run_b200_arm(args, rank, world, local, pg):
+    import torch
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    from trottersuzuki_b200 import _capi
+    L = _capi.lib()
+
+    # ---- FP64, device resident (value)
+    ts, grid, state, pot, ham, solver, psi0 = build_solver("gpu")
+    stream = torch.cuda.Stream(device=device)
+    solver.evolve(-1, True)  # builds the kernel (table, norm0, upload)
+    handle = solver.kernel_handle()
+    _capi.check(L.ts_b200_set_stream(handle, C.c_void_p(stream.cuda_stream)), handle)
+    for _ in range(args.warmup):
+        solver.evolve(-TROTTER_PER_STEP, True)
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    with Clocks(local) as clocks:
+        ms, launches = time_device(solver, handle, stream, args.steps)
+    if pg:
+        pg.barrier()
+    ms = max_over_ranks(ms, pg, device)
+    site_steps = float(N_SIDE) * N_SIDE * TROTTER_PER_STEP * args.steps
+    value = world * site_steps / (ms * 1e-3)
+    shape = _capi.LaunchShape()
+    L.ts_b200_launch_info(handle, C.byref(shape))
+
+    # energies of the final FP64 state (for the FP32 comparison)
+    solver.evolve(0, True)  # copies the tile back (get_sample)
+    e64 = solver.get_total_energy()
+    n64 = solver.get_squared_norm()
+
+    # ---- e2e: through the C ABI with pinned host buffers, every step copies
+    # the state in (H2D) and the result out (D2H)
+    W, H = grid.dim_x, grid.dim_y
+    nbytes = W * H * 8
+    bufs = []
+    for _ in range(4):
+        p = C.c_void_p()
+        _capi.check(L.ts_b200_host_alloc(C.byref(p), nbytes))
+        bufs.append(p)
+    re_in = np.ctypeslib.as_array(C.cast(bufs[0], C.POINTER(C.c_double)), shape=(H, W))
+    im_in = np.ctypeslib.as_array(C.cast(bufs[1], C.POINTER(C.c_double)), shape=(H, W))
+    re_in[...] = psi0.real
+    im_in[...] = psi0.imag
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+
+    def e2e_step():
+        _capi.check(L.ts_b200_set_state(handle, bufs[0], bufs[1], W), handle)
+        _capi.check(L.ts_b200_evolve(handle, TROTTER_PER_STEP), handle)
+        _capi.check(L.ts_b200_get_sample(handle, W, 0, 0, W, H, bufs[2], bufs[3]), handle)
+
+    for _ in range(args.warmup):
+        e2e_step()
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    e0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(stream)
+    e1.synchronize()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), pg, device)
+    e2e_value = world * site_steps / (e2e_ms * 1e-3)
+    for p in bufs:
+        L.ts_b200_host_free(p)
+    del solver, ham, pot, state, grid
+
+    # ---- FP32 storage on the same workload
+    fp32 = None
+    if not args.no_fp32:
+        ts, grid, state, pot, ham, solver32, _ = build_solver("gpu_fp32")
+        solver32.evolve(-1, True)
+        h32 = solver32.kernel_handle()
+        _capi.check(L.ts_b200_set_stream(h32, C.c_void_p(stream.cuda_stream)), h32)
+        for _ in range(args.warmup):
+            solver32.evolve(-TROTTER_PER_STEP, True)
+        torch.cuda.synchronize()
+        if pg:
+            pg.barrier()
+        ms32, _ = time_device(solver32, h32, stream, args.steps)
+        ms32 = max_over_ranks(ms32, pg, device)
+        solver32.evolve(0, True)
+        e32 = solver32.get_total_energy()
+        n32 = solver32.get_squared_norm()
+        v32 = world * site_steps / (ms32 * 1e-3)
+        fp32 = {"value": v32, "unit": "site-steps/s", "speedup_vs_fp64": v32 / value,
+                "rel_energy_err_vs_fp64": abs(e32 - e64) / abs(e64),
+                "rel_norm_err_vs_fp64": abs(n32 - n64) / abs(n64),
+                "bytes_per_site_step": BYTES_PER_SITE_STEP["fp32"]}
+        del solver32
+
+    if rank != 0:
+        return
+
+    # ---- roofline of the step kernel
+    peak, peak_kind = measured_peak()
+    per_launch_ms = ms / launches if launches else None  # this rank's launches; ms is the max
+    bytes_per_launch = BYTES_PER_SITE_STEP["fp64"] * N_SIDE * N_SIDE
+    achieved = bytes_per_launch / (per_launch_ms * 1e-3) / 1e9 if per_launch_ms else None
+    traffic = committed_traffic()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak if achieved else None, "peak_kind": peak_kind,
+                "traffic": traffic.get("dram_bytes_per_launch") if traffic else None,
+                "algorithmic_bytes_per_launch": bytes_per_launch,
+                "kernel": "tsb::step_kernel<double, C=2, imaginary, no rotation, GPE>"}
+
+    cpu = None
+    if not args.no_cpu_baseline:
+        rate, cores, kind, sample, _ = cpu_reference_rate(psi0, budget_s=args.ref_budget)
+        cpu = {"value": rate, "unit": "site-steps/s", "cores": cores, "kind": kind,
+               "sample": sample}
+
+    clk = clocks.summary()
+    line = {
+        "metric": "site-steps/s", "value": value, "unit": "site-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "lattice": f"{N_SIDE}x{N_SIDE}", "length": LENGTH,
+                   "trotter_steps_per_step": TROTTER_PER_STEP, "dt": DT, "g": G,
+                   "omega_xy": [OMEGA_X, OMEGA_Y], "boundary": "closed", "imag_time": True,
+                   "precision": "fp64", "parallelism": f"replicas{world}",
+                   "l2": "inputs larger than L2: 160 MiB read+written per Trotter step > 126 MiB",
+                   "launch": {k: getattr(shape, k) for k, _ in _capi.LaunchShape._fields_}},
+        "e2e": {"value": e2e_value, "unit": "site-steps/s", "h2d_bytes_per_step": 2 * nbytes,
+                "d2h_bytes_per_step": 2 * nbytes,
+                "path": "C ABI ts_b200_set_state / ts_b200_evolve / ts_b200_get_sample, "
+                        "pinned host buffers"},
+        "roofline": roofline,
+        "fp32_store": fp32,
+        "cpu_baseline": cpu,
+        "clocks": clk,
+        "gpu_launches": launches,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--ref-budget", type=float, default=12.0,
+                    help="seconds of reference CPU work per sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp32", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    rank, world, local, pg = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            run_reference_arm(args, rank, world, pg)
+        else:
+            run_b200_arm(args, rank, world, local, pg)
+    finally:
+        if pg is not None:
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

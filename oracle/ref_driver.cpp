@@ -56,6 +56,7 @@ struct tsref_result {
     double state_norm;
     double initial_total_energy, initial_squared_norm;
     double seconds;              // wall time of the evolve() calls only
+    double seg_seconds[8];       // wall time of each evolve() call
 };
 
 static char g_err[512];
@@ -148,8 +149,12 @@ int tsref_run(const tsref_config *cfg, double *psi_re, double *psi_im,
         res->initial_total_energy = solver->get_total_energy();
         res->initial_squared_norm = solver->get_squared_norm();
         auto t0 = std::chrono::steady_clock::now();
-        for (int s = 0; s < cfg->n_segments; ++s)
+        for (int s = 0; s < cfg->n_segments; ++s) {
+            auto ts = std::chrono::steady_clock::now();
             solver->evolve(cfg->seg_iterations[s], cfg->seg_imag[s] != 0);
+            res->seg_seconds[s] =
+                std::chrono::duration<double>(std::chrono::steady_clock::now() - ts).count();
+        }
         auto t1 = std::chrono::steady_clock::now();
         res->seconds = std::chrono::duration<double>(t1 - t0).count();
         res->total_energy = solver->get_total_energy();

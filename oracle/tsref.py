@@ -54,6 +54,7 @@ class Result(C.Structure):
         ("state_norm", C.c_double),
         ("initial_total_energy", C.c_double), ("initial_squared_norm", C.c_double),
         ("seconds", C.c_double),
+        ("seg_seconds", C.c_double * 8),
     ]
 
 
