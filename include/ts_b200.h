@@ -154,6 +154,23 @@ typedef struct {
 int ts_b200_expectations(ts_b200_kernel *k, const ts_b200_energy_params *params,
                          ts_b200_expectation_result *out);
 
+/* Squared norm of a caller-owned device tile (AoS complex in `precision`, row
+ * pitch `pitch` cells) over the inner region, times delta_x * delta_y, written
+ * to the device double `*out` on `stream` (a cudaStream_t, NULL for the
+ * default stream).  Allocates nothing: for callers that cannot call cudaMalloc
+ * (device memory owned by another allocator or fixed pool; no allocation, and
+ * so no implicit device synchronisation, after start-up).  Its scratch is a
+ * static device array of the library (128 KiB per GPU, kept until exit):
+ * tiles with more than 16384 inner rows are rejected (TS_B200_UNSUPPORTED);
+ * the first call on a device looks the array up (cudaGetSymbolAddress), so
+ * make it before any stream capture; calls that overlap on the GPU race on
+ * the shared scratch.  No counterpart in the reference (which reduces the
+ * norm on the host, src/cpukernel.cpp:526-549). */
+int ts_b200_squared_norm_noalloc(const void *psi, int precision, size_t pitch, int dim_x,
+                                 int dim_y, int inner_x0, int inner_x1, int inner_y0,
+                                 int inner_y1, double delta_x, double delta_y, double *out,
+                                 void *stream);
+
 /* Device-resident access (for callers that already hold device memory, such
  * as a torch binding or a benchmark).  `aos` is a device array of dim_y rows
  * of dim_x interleaved complex numbers in the kernel's precision with row

@@ -81,6 +81,8 @@ SIGNATURES = {
     "ts_b200_squared_norm": (_I, [_VP, C.POINTER(C.c_double)]),
     "ts_b200_energies": (_I, [_VP, _DP, C.POINTER(EnergyParams), C.POINTER(EnergyResult)]),
     "ts_b200_expectations": (_I, [_VP, C.POINTER(EnergyParams), C.POINTER(ExpectationResult)]),
+    "ts_b200_squared_norm_noalloc": (_I, [_VP, _I, _SZ, _I, _I, _I, _I, _I, _I, C.c_double,
+                                          C.c_double, _VP, _VP]),
     "ts_b200_set_state_device": (_I, [_VP, _VP, _SZ]),
     "ts_b200_get_state_device": (_I, [_VP, _VP, _SZ]),
     "ts_b200_set_exp_potential_device": (_I, [_VP, _VP, _SZ]),
