@@ -74,13 +74,15 @@ def measured_peak():
 
 
 def committed_traffic():
-    """DRAM bytes per step-kernel launch from the committed ncu summary, if any."""
-    path = os.path.join(REPO, "profiles", "step_kernel_traffic.json")
+    """DRAM bytes (read + write) per step-kernel launch on this workload, from
+    the committed ncu summary (a line `dram_bytes_per_launch: <int>`), if any."""
+    import re
+    path = os.path.join(REPO, "profiles", "step_kernel_gpe_imag_2048.md")
     try:
         with open(path) as f:
-            t = json.load(f)
-        return t
-    except Exception:
+            m = re.search(r"^dram_bytes_per_launch:\s*(\d+)", f.read(), re.M)
+        return int(m.group(1)) if m else None
+    except OSError:
         return None
 
 
@@ -374,7 +376,7 @@ def run_b200_arm(args, rank, world, local, pg):
     traffic = committed_traffic()
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak if achieved else None, "peak_kind": peak_kind,
-                "traffic": traffic.get("dram_bytes_per_launch") if traffic else None,
+                "traffic": traffic,
                 "algorithmic_bytes_per_launch": bytes_per_launch,
                 "kernel": "tsb::step_kernel<double, C=2, imaginary, no rotation, GPE>"}
 
