@@ -275,6 +275,25 @@ __device__ __forceinline__ void hsweep(Cx<T> (&w)[C], T a, T b, const LaneMask<C
     }
 }
 
+// Horizontal kinetic sweep with per-lane pair coefficients (2 cells per
+// lane): (ai, bi) for the pair inside the lane, (al, bl) for the pair with the
+// left neighbour lane, (ar, br) for the pair with the right one.  A pair whose
+// partner lies outside the tile carries the identity, (1, 0) ((0, 0) in delta
+// form), so one code path serves edge and interior strips alike.
+template <bool IMAG, int PAR, typename T>
+__device__ __forceinline__ void hsweep_lane(Cx<T> (&w)[2], T ai, T bi, T al, T bl, T ar, T br) {
+    if (PAR == 0) {
+        const Cx<T> p = w[0], q = w[1];
+        w[0] = kin<IMAG>(p, q, ai, bi);
+        w[1] = kin<IMAG>(q, p, ai, bi);
+    } else {
+        const Cx<T> right = shfl_down1(w[0]);
+        const Cx<T> left = shfl_up1(w[1]);
+        w[0] = kin<IMAG>(w[0], left, al, bl);
+        w[1] = kin<IMAG>(w[1], right, ar, br);
+    }
+}
+
 // Rotation row sweep on one row: pairs (x, x+1) with x % 2 == PAR.
 template <bool IMAG, int C, int PAR, bool EDGE, typename T>
 __device__ __forceinline__ void rrow(Cx<T> (&w)[C], T a, T b, const LaneMask<C> &m) {
@@ -466,6 +485,14 @@ struct Variant {
     static constexpr int OUT_LAG = NWIN - 1;
     static constexpr int SW = 32 * C_;
     static constexpr int WO = SW - 2 * HX;
+    // Per-lane horizontal coefficients instead of edge masks (no second,
+    // masked copy of the row body): variants with 2 cells per lane and no
+    // rotating frame.
+    static constexpr bool LANE_COEF = C_ == 2 && !ROT_;
+    // Resident blocks of 4 warps per SM the register allocation aims at (the
+    // step is latency-bound: more resident warps hide more of it): 5 blocks
+    // (96 registers) in double, 6 (80 registers) in float.
+    static constexpr int MIN_BLOCKS = LANE_COEF ? (sizeof(T_) == 4 ? 6 : 5) : 1;
     using TabT = typename std::conditional<IMAG_, T_, Cx<T_>>::type;
     static constexpr int PSI_BYTES = SW * (int)sizeof(Cx<T_>);
     static constexpr int TAB_BYTES = SW * (int)sizeof(TabT);
@@ -503,6 +530,7 @@ struct Walk {
     bool failed;
     T inv;
     T aH, bH, aV, bV, ca, caa;  // step constants, read from the parameters once
+    T hai, hbi, hal, hbl, har, hbr;  // LANE_COEF: this lane's horizontal pair coefficients
 
     __device__ __forceinline__ void issue(int row, int slot) {
         unsigned char *sb = ring + slot * V::SLOT;
@@ -513,6 +541,36 @@ struct Walk {
     }
     __device__ __forceinline__ int next(int q) const { return q + 1 == D ? 0 : q + 1; }
 };
+
+// Horizontal sweep of one window row, PAR the pair parity.
+template <class V, int PAR, bool EDGE>
+__device__ __forceinline__ void hsw(Walk<V> &w, Cx<typename V::T> (&row)[V::C]) {
+    if constexpr (V::LANE_COEF) {
+        hsweep_lane<V::IMAG, PAR>(row, w.hai, w.hbi, w.hal, w.hbl, w.har, w.hbr);
+    } else {
+        hsweep<V::IMAG, V::C, PAR, EDGE>(row, w.aH, w.bH, w.m);
+    }
+}
+
+// Zero the parts of this warp's ring slots that the current task's copies do
+// not cover (strips that reach past the row), so that cells outside the tile
+// read as 0 without a per-row mask.
+template <class V>
+__device__ __forceinline__ void zero_ring_outside(Walk<V> &w) {
+    uint32_t *ring32 = reinterpret_cast<uint32_t *>(w.ring);
+    const int words = w.D * V::SLOT / 4;
+    for (int i = w.lane; i < words; i += 32) {
+        const uint32_t off = (uint32_t)(i * 4) % (uint32_t)V::SLOT;
+        bool copied;
+        if (off < (uint32_t)V::PSI_BYTES) {
+            copied = off >= w.psi_off && off < w.psi_off + w.psi_bytes;
+        } else {
+            const uint32_t t = off - (uint32_t)V::PSI_BYTES;
+            copied = t >= w.tab_off && t < w.tab_off + w.tab_bytes;
+        }
+        if (!copied) ring32[i] = 0u;
+    }
+}
 
 // One iteration of the walk for row r = base + K (base even, so the parity of
 // every row index below is known at compile time).
@@ -554,13 +612,13 @@ __device__ __forceinline__ void walk_row(Walk<V> &w, const StepArgs<typename V::
     // ---- S1: V0 on rows (r-1, r)
     if (!GUARD || (r - 1 >= ra && r < rb)) vsweep<IMAG, C, ((K + 1) & 1)>(WS(1), WS(0), aV, bV);
     // ---- S2: H0 on row r-1
-    if (!GUARD || (r - 1 >= ra && r - 1 < rb)) hsweep<IMAG, C, ((K + 1) & 1), EDGE>(WS(1), aH, bH, w.m);
+    if (!GUARD || (r - 1 >= ra && r - 1 < rb)) hsw<V, ((K + 1) & 1), EDGE>(w, WS(1));
     // ---- S3: V1 on rows (r-2, r-1)
     if (!GUARD || (r - 2 >= ra && r - 1 < rb)) vsweep<IMAG, C, ((K + 1) & 1)>(WS(2), WS(1), aV, bV);
     // ---- S4: H1, P, then H1 (or the rotation row sweeps) on row r-2; free its slot
     if (!GUARD || (r - 2 >= ra && r - 2 < rb)) {
         const int u = r - 2;
-        hsweep<IMAG, C, ((K + 1) & 1), EDGE>(WS(2), aH, bH, w.m);
+        hsw<V, ((K + 1) & 1), EDGE>(w, WS(2));
         const int q = w.tslot;
         const TabT *tp =
             reinterpret_cast<const TabT *>(w.ring + q * V::SLOT + V::PSI_BYTES) + C * w.lane;
@@ -570,7 +628,7 @@ __device__ __forceinline__ void walk_row(Walk<V> &w, const StepArgs<typename V::
             rrow<IMAG, C, 0, EDGE>(WS(2), ab.re, ab.im, w.m);
             rrow<IMAG, C, 1, EDGE>(WS(2), ab.re, ab.im, w.m);
         } else {
-            hsweep<IMAG, C, ((K + 1) & 1), EDGE>(WS(2), aH, bH, w.m);
+            hsw<V, ((K + 1) & 1), EDGE>(w, WS(2));
         }
         __syncwarp();
         if (u + w.D < rb) {
@@ -587,7 +645,7 @@ __device__ __forceinline__ void walk_row(Walk<V> &w, const StepArgs<typename V::
         // ---- S5: V1 on rows (r-3, r-2)
         if (!GUARD || (r - 3 >= ra && r - 2 < rb)) vsweep<IMAG, C, ((K) & 1)>(WS(3), WS(2), aV, bV);
         // ---- S6: H0 on row r-3
-        if (!GUARD || (r - 3 >= ra && r - 3 < rb)) hsweep<IMAG, C, ((K + 1) & 1), EDGE>(WS(3), aH, bH, w.m);
+        if (!GUARD || (r - 3 >= ra && r - 3 < rb)) hsw<V, ((K + 1) & 1), EDGE>(w, WS(3));
         // ---- S7: V0 on rows (r-4, r-3)
         if (!GUARD || (r - 4 >= ra && r - 3 < rb)) vsweep<IMAG, C, ((K) & 1)>(WS(4), WS(3), aV, bV);
     } else {
@@ -600,12 +658,12 @@ __device__ __forceinline__ void walk_row(Walk<V> &w, const StepArgs<typename V::
             const Cx<T> ab = reinterpret_cast<const Cx<T> *>(a.row_ab)[r - 4];
             rrow<IMAG, C, 0, EDGE>(WS(4), ab.re, ab.im, w.m);
             rrow<IMAG, C, 1, EDGE>(WS(4), ab.re, ab.im, w.m);
-            hsweep<IMAG, C, ((K + 1) & 1), EDGE>(WS(4), aH, bH, w.m);
+            hsw<V, ((K + 1) & 1), EDGE>(w, WS(4));
         }
         // ---- S8: V1 on rows (r-5, r-4)
         if (!GUARD || (r - 5 >= ra && r - 4 < rb)) vsweep<IMAG, C, ((K) & 1)>(WS(5), WS(4), aV, bV);
         // ---- S9: H0 on row r-5
-        if (!GUARD || (r - 5 >= ra && r - 5 < rb)) hsweep<IMAG, C, ((K + 1) & 1), EDGE>(WS(5), aH, bH, w.m);
+        if (!GUARD || (r - 5 >= ra && r - 5 < rb)) hsw<V, ((K + 1) & 1), EDGE>(w, WS(5));
         // ---- S10: V0 on rows (r-6, r-5)
         if (!GUARD || (r - 6 >= ra && r - 5 < rb)) vsweep<IMAG, C, ((K) & 1)>(WS(6), WS(5), aV, bV);
     }
@@ -650,7 +708,7 @@ __device__ __forceinline__ void walk_segment(Walk<V> &w, const StepArgs<typename
 // Grid: any number of blocks of 1..4 warps; each warp loops over the tasks
 // (strip, segment) t = warp_global, warp_global + total_warps, ...
 template <class V>
-__global__ void __launch_bounds__(128) step_kernel(StepArgs<typename V::T> a) {
+__global__ void __launch_bounds__(128, V::MIN_BLOCKS) step_kernel(StepArgs<typename V::T> a) {
     using T = typename V::T;
     using TabT = typename V::TabT;
     constexpr int C = V::C, NWIN = V::NWIN, HX = V::HX, HY = V::HY, SW = V::SW, WO = V::WO;
@@ -741,6 +799,15 @@ __global__ void __launch_bounds__(128) step_kernel(StepArgs<typename V::T> a) {
         w.m.pair_int[C - 1] = false;
         w.m.pair_left = lane > 0 && w.present[0] && w.xl - 1 >= 0;
         w.m.pair_right = lane < 31 && w.present[C - 1] && w.xl + C < a.W;
+        if constexpr (V::LANE_COEF) {
+            const T one = DeltaForm<T>::value ? T(0) : T(1);
+            w.hai = w.m.pair_int[0] ? w.aH : one;
+            w.hbi = w.m.pair_int[0] ? w.bH : T(0);
+            w.hal = w.m.pair_left ? w.aH : one;
+            w.hbl = w.m.pair_left ? w.bH : T(0);
+            w.har = w.m.pair_right ? w.aH : one;
+            w.hbr = w.m.pair_right ? w.bH : T(0);
+        }
         if constexpr (ROT) {
 #pragma unroll
             for (int i = 0; i < C; ++i)
@@ -755,11 +822,24 @@ __global__ void __launch_bounds__(128) step_kernel(StepArgs<typename V::T> a) {
         w.tslot = 0;
         w.loaded_to = w.ra;
         w.issued_to = min(w.ra + D, w.rb);
-        if (lane == 0)
+        __syncwarp();  // the previous task's reads of the ring are done
+        if constexpr (V::LANE_COEF) {
+            if (c0 < 0 || c0 + SW > a.P) {
+                zero_ring_outside(w);
+                __syncwarp();
+            }
+        }
+        if (lane == 0) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             for (int row = w.ra; row < w.issued_to; ++row) w.issue(row, row - w.ra);
+        }
 
-        if (c0 >= 0 && c0 + SW <= a.W) walk_segment<V, false>(w, a);
-        else walk_segment<V, true>(w, a);
+        if constexpr (V::LANE_COEF) {
+            walk_segment<V, false>(w, a);
+        } else {
+            if (c0 >= 0 && c0 + SW <= a.W) walk_segment<V, false>(w, a);
+            else walk_segment<V, true>(w, a);
+        }
 
         if (w.failed) {
             if (lane == 0) atomicExch(&a.scal->error, 1);
@@ -774,16 +854,21 @@ __global__ void __launch_bounds__(128) step_kernel(StepArgs<typename V::T> a) {
     }
 
     if constexpr (IMAG) {
-        // per-warp partial: a warp's tasks are summed in task order
+        // block partial: the block's warps in warp order (a warp's tasks in
+        // task order); then the last block to finish sums the block partials
+        // in a fixed order, eight independent loads in flight per thread.
         double nacc = w.nacc;
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) nacc += __shfl_xor_sync(0xffffffffu, nacc, off);
-        const int gw = blockIdx.x * warps + warp;
-        if (lane == 0) a.partials[gw] = nacc;
+        __shared__ double s_warp[4];
         __shared__ unsigned int s_last;
         __shared__ double red[128];
+        if (lane == 0) s_warp[warp] = nacc;
         __syncthreads();
         if (threadIdx.x == 0) {
+            double b = 0.0;
+            for (int i = 0; i < warps; ++i) b += s_warp[i];
+            a.partials[blockIdx.x] = b;
             __threadfence();
             const unsigned int t = atomicAdd(&a.scal->ticket, 1u);
             s_last = (t == gridDim.x - 1) ? 1u : 0u;
@@ -791,11 +876,19 @@ __global__ void __launch_bounds__(128) step_kernel(StepArgs<typename V::T> a) {
         __syncthreads();
         if (s_last) {
             __threadfence();
-            // fixed order: thread t sums warps t, t + blockDim, ..., then a fixed tree
-            const int nw = gridDim.x * warps;
-            double s = 0.0;
-            for (int t = threadIdx.x; t < nw; t += blockDim.x) s += __ldcg(&a.partials[t]);
-            red[threadIdx.x] = s;
+            const int nb = gridDim.x;
+            double acc[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) acc[j] = 0.0;
+            for (int base = threadIdx.x; base < nb; base += 8 * (int)blockDim.x) {
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const int t = base + j * (int)blockDim.x;
+                    if (t < nb) acc[j] += __ldcg(&a.partials[t]);
+                }
+            }
+            red[threadIdx.x] = ((acc[0] + acc[1]) + (acc[2] + acc[3])) +
+                               ((acc[4] + acc[5]) + (acc[6] + acc[7]));
             __syncthreads();
             for (int h = blockDim.x >> 1; h > 0; h >>= 1) {
                 if ((int)threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
