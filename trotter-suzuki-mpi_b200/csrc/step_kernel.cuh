@@ -490,9 +490,10 @@ struct Variant {
     // rotating frame.
     static constexpr bool LANE_COEF = C_ == 2 && !ROT_;
     // Resident blocks of 4 warps per SM the register allocation aims at (the
-    // step is latency-bound: more resident warps hide more of it): 5 blocks
-    // (96 registers) in double, 6 (80 registers) in float.
-    static constexpr int MIN_BLOCKS = LANE_COEF ? (sizeof(T_) == 4 ? 6 : 5) : 1;
+    // step is latency-bound: more resident warps hide more of it): 6 blocks
+    // (80 registers) in double, 8 (64 registers) in float for the default
+    // variants, 4 (128 registers) for the others.
+    static constexpr int MIN_BLOCKS = LANE_COEF ? (sizeof(T_) == 4 ? 8 : 6) : 4;
     using TabT = typename std::conditional<IMAG_, T_, Cx<T_>>::type;
     static constexpr int PSI_BYTES = SW * (int)sizeof(Cx<T_>);
     static constexpr int TAB_BYTES = SW * (int)sizeof(TabT);
@@ -716,7 +717,10 @@ __global__ void __launch_bounds__(128, V::MIN_BLOCKS) step_kernel(StepArgs<typen
 
     extern __shared__ __align__(128) unsigned char smem[];
     const int warps = blockDim.x >> 5;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // broadcast from lane 0 so that the compiler knows the warp index, and
+    // every task quantity derived from it, to be warp-uniform
+    const int warp = __shfl_sync(0xffffffffu, (int)(threadIdx.x >> 5), 0);
+    const int lane = threadIdx.x & 31;
     const int D = a.ring;
     const int n_tasks = a.n_strips * a.n_segs;
 
