@@ -199,6 +199,48 @@ int ts_b200_launch_info(const ts_b200_kernel *k, ts_b200_launch_shape *out);
 int ts_b200_set_launch(ts_b200_kernel *k, int cells_per_lane, int segment_rows, int warps_per_block,
                        int ring_depth);
 
+/* ---- Batched evolution (no counterpart in the reference, which evolves one
+ * lattice per Solver; the batch replaces a loop of per-tile evolve() calls).
+ *
+ * A batch advances many tiles of uneven sizes together: each Trotter step is
+ * one persistent launch over the tasks of all tiles (plus, in imaginary time,
+ * one per-tile norm reduction launch, and for periodic tiles one batched halo
+ * refresh), 32-step runs replayed from a CUDA graph.  The batch borrows the
+ * tiles' device state: set states and tables, read results, energies and
+ * norms through the tiles' own calls.  All tiles must share precision, time
+ * mode and device and have no rotating frame (TS_B200_UNSUPPORTED); a tile
+ * appears once.  The batch orders itself after work queued on the tiles'
+ * streams and the tiles' streams after the batch's work. */
+typedef struct ts_b200_batch ts_b200_batch;
+
+int ts_b200_batch_create(ts_b200_kernel *const *kernels, int n, ts_b200_batch **out);
+void ts_b200_batch_destroy(ts_b200_batch *b);
+int ts_b200_batch_size(const ts_b200_batch *b);
+
+/* `iterations` Trotter steps of every tile, with the per-tile protocol of
+ * ts_b200_evolve (halo refresh after every step but the last). */
+int ts_b200_batch_evolve(ts_b200_batch *b, int iterations);
+
+/* Wait for the batch's queued work; TS_B200_DEVICE_TIMEOUT if a bounded wait
+ * in the batched step gave up. */
+int ts_b200_batch_synchronize(ts_b200_batch *b);
+
+/* Tile shape of the batched launch: rows per segment task (even; capped by
+ * each tile's height) and warps per block (1, 2 or 4).  Zero keeps a field. */
+int ts_b200_batch_set_launch(ts_b200_batch *b, int segment_rows, int warps_per_block);
+
+/* Autotuner: times `trial_steps` batched steps for each candidate shape (rows
+ * per segment 16..128, 2 or 4 warps per block) and keeps the fastest.  The
+ * trials read the tiles' current state and write only the scratch buffer, so
+ * the state is unchanged.  With use_cache != 0 a shape tuned earlier in this
+ * process for the same precision, time mode and tile sizes is reused
+ * without timing.  Synchronises the batch's stream. */
+int ts_b200_batch_autotune(ts_b200_batch *b, int trial_steps, int use_cache);
+
+/* Current shape: strips and segments are summed over the tiles. */
+int ts_b200_batch_launch_info(ts_b200_batch *b, ts_b200_launch_shape *out);
+const char *ts_b200_batch_last_error(const ts_b200_batch *b);
+
 /* Pinned host memory for the state arrays (page-locked so that host<->device
  * copies run at full PCIe/C2C rate). */
 int ts_b200_host_alloc(void **ptr, size_t bytes);

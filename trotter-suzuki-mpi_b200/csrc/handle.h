@@ -1,0 +1,63 @@
+// Internal: the per-tile handle behind the C ABI and the helpers the
+// batched path (batch.cu) shares with the single-tile path (ts_b200.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <string>
+
+#include "step_kernel.cuh"
+#include "ts_b200.h"
+
+// =================================================================== handle
+struct ts_b200_kernel {
+    ts_b200_desc d{};
+    int W = 0, H = 0, P = 0;
+    bool fp32 = false, imag = false, rot = false;
+    int phase = 0;  // 0 none, 1 g|psi|^2, 2 with Lee-Huang-Yang
+    size_t cell = 0, tab_cell = 0;
+    void *psi[2] = {nullptr, nullptr};
+    int cur = 0;
+    void *tab = nullptr;
+    void *row_ab = nullptr, *col_ab = nullptr;
+    double *partials = nullptr;
+    size_t partials_cap = 0;
+    tsb::Scalars *scal = nullptr;
+    double *staging = nullptr;  // 2 * W * H doubles
+    double *vtab = nullptr;     // V for energies (W * H)
+    bool have_v = false;
+    double *red_partials = nullptr;
+    double *red_out = nullptr;
+    unsigned int *red_ticket = nullptr;
+    cudaStream_t own_stream = nullptr, stream = nullptr;
+    int C = 2, seg_h = 64, warps = 4, ring = 4;
+    int resident_blocks = 0;  // blocks of the current launch shape resident on the GPU (0: unknown)
+    bool auto_seg = true;     // pick the segment height from the resident grid
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = 0;
+    int num_sms = 148;
+    int device = 0;
+    std::string err;
+};
+
+namespace tsbh {
+
+// Kernel launches made through the library (reported by ts_b200_launch_count).
+extern std::atomic<uint64_t> g_launches;
+
+inline int div_up(long a, long b) { return (int)((a + b - 1) / b); }
+
+// Bytes of one ring slot: a row of 32*C cells of psi and of the table.
+inline int slot_bytes(int C, bool fp32, bool imag) {
+    const int cell = fp32 ? 8 : 16;
+    const int tab = imag ? cell / 2 : cell;
+    return 32 * C * (cell + tab);
+}
+
+// Step constants of a tile in the kernel's precision (delta form in float):
+// every StepArgs field except the buffers, the task geometry and the scratch.
+template <typename T>
+void fill_step_constants(const ts_b200_kernel *k, tsb::StepArgs<T> &a);
+
+}  // namespace tsbh

@@ -706,43 +706,20 @@ __device__ __forceinline__ void walk_segment(Walk<V> &w, const StepArgs<typename
     }
 }
 
-// Grid: any number of blocks of 1..4 warps; each warp loops over the tasks
-// (strip, segment) t = warp_global, warp_global + total_warps, ...
+// ------------------------------------------------------------ task pieces
+// Per-warp set-up shared by the single-tile and the batched kernels: this
+// warp's ring slots (D of them) and their mbarriers.
 template <class V>
-__global__ void __launch_bounds__(128, V::MIN_BLOCKS) step_kernel(StepArgs<typename V::T> a) {
-    using T = typename V::T;
-    using TabT = typename V::TabT;
-    constexpr int C = V::C, NWIN = V::NWIN, HX = V::HX, HY = V::HY, SW = V::SW, WO = V::WO;
-    constexpr bool IMAG = V::IMAG, ROT = V::ROT;
-
-    extern __shared__ __align__(128) unsigned char smem[];
-    const int warps = blockDim.x >> 5;
-    // broadcast from lane 0 so that the compiler knows the warp index, and
-    // every task quantity derived from it, to be warp-uniform
-    const int warp = __shfl_sync(0xffffffffu, (int)(threadIdx.x >> 5), 0);
-    const int lane = threadIdx.x & 31;
-    const int D = a.ring;
-    const int n_tasks = a.n_strips * a.n_segs;
-
-    Walk<V> w;
+__device__ __forceinline__ void warp_setup(Walk<V> &w, unsigned char *smem, int warps, int warp,
+                                           int lane, int D) {
     w.nacc = 0.0;
     w.failed = false;
-    w.inv = IMAG ? (T)a.scal->pending_inv : T(1);
-    w.aH = a.aH;
-    w.bH = a.bH;
-    w.aV = a.aV;
-    w.bV = a.bV;
-    w.ca = a.ca;
-    w.caa = a.caa;
     w.D = D;
     w.lane = lane;
     // each warp: D ring slots, then (after all warps' rings) D mbarriers
     w.ring = smem + (size_t)warp * D * V::SLOT;
     w.bars = reinterpret_cast<uint64_t *>(smem + (size_t)warps * D * V::SLOT) + warp * D;
     w.phase_bits = 0u;
-    w.gpsi_pitch = (size_t)a.P * sizeof(Cx<T>);
-    w.gtab_pitch = (size_t)a.P * sizeof(TabT);
-
     // Zero this warp's ring once: cells never written by a copy (outside the
     // tile) are then finite, so masked-off pair updates cannot produce NaNs.
     {
@@ -756,106 +733,149 @@ __global__ void __launch_bounds__(128, V::MIN_BLOCKS) step_kernel(StepArgs<typen
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
     __syncwarp();
+}
 
-    for (int task = blockIdx.x * warps + warp; task < n_tasks && !w.failed;
-         task += gridDim.x * warps) {
-        // tasks of interior strips come first and those of the first and last
-        // strip (the only ones that need masks) last, so that few SMs run both
-        // code paths
-        int strip, seg;
-        {
-            const int n_int = a.n_strips > 2 ? (a.n_strips - 2) * a.n_segs : 0;
-            if (task < n_int) {
-                strip = 1 + task % (a.n_strips - 2);
-                seg = task / (a.n_strips - 2);
-            } else {
-                const int e = task - n_int;
-                const int n_edge_strips = a.n_strips > 2 ? 2 : a.n_strips;
-                const int es = e % n_edge_strips;
-                strip = (a.n_strips > 2 && es == 1) ? a.n_strips - 1 : es;
-                seg = e / n_edge_strips;
-            }
-        }
-        const int ox0 = strip * WO, ox1 = min(ox0 + WO, a.W);
-        const int c0 = ox0 - HX;
-        w.oy0 = seg * a.seg_h;
-        w.oy1 = min(w.oy0 + a.seg_h, a.H);
-        w.ra = max(w.oy0 - HY, 0);
-        w.rb = min(w.oy1 + HY, a.H);
-        const int cs = max(c0, 0);
-        const int ce = min(c0 + SW, a.P);
-        w.psi_off = (uint32_t)(cs - c0) * sizeof(Cx<T>);
-        w.psi_bytes = (uint32_t)(ce - cs) * sizeof(Cx<T>);
-        w.tab_off = (uint32_t)(cs - c0) * sizeof(TabT);
-        w.tab_bytes = (uint32_t)(ce - cs) * sizeof(TabT);
-        w.gpsi = reinterpret_cast<const unsigned char *>(a.psi_in) + (size_t)cs * sizeof(Cx<T>);
-        w.gtab = reinterpret_cast<const unsigned char *>(a.pot) + (size_t)cs * sizeof(TabT);
-        w.xl = c0 + C * lane;
-#pragma unroll
-        for (int i = 0; i < C; ++i) {
-            const int x = w.xl + i;
-            w.present[i] = x >= 0 && x < a.W;
-            w.out_col[i] = x >= ox0 && x < ox1;
-            w.norm_col[i] = w.out_col[i] && x >= a.ix0 && x < a.ix1;
-        }
-#pragma unroll
-        for (int i = 0; i + 1 < C; ++i) w.m.pair_int[i] = w.present[i] && w.present[i + 1];
-        w.m.pair_int[C - 1] = false;
-        w.m.pair_left = lane > 0 && w.present[0] && w.xl - 1 >= 0;
-        w.m.pair_right = lane < 31 && w.present[C - 1] && w.xl + C < a.W;
-        if constexpr (V::LANE_COEF) {
-            const T one = DeltaForm<T>::value ? T(0) : T(1);
-            w.hai = w.m.pair_int[0] ? w.aH : one;
-            w.hbi = w.m.pair_int[0] ? w.bH : T(0);
-            w.hal = w.m.pair_left ? w.aH : one;
-            w.hbl = w.m.pair_left ? w.bH : T(0);
-            w.har = w.m.pair_right ? w.aH : one;
-            w.hbr = w.m.pair_right ? w.bH : T(0);
-        }
-        if constexpr (ROT) {
-#pragma unroll
-            for (int i = 0; i < C; ++i)
-                w.colab[i] = reinterpret_cast<const Cx<T> *>(a.col_ab)[w.present[i] ? w.xl + i : 0];
-        }
-#pragma unroll
-        for (int j = 0; j < NWIN; ++j)
-#pragma unroll
-            for (int i = 0; i < C; ++i) w.win[j][i] = Cx<T>{T(0), T(0)};
+// The step constants of one tile.
+template <class V>
+__device__ __forceinline__ void bind_args(Walk<V> &w, const StepArgs<typename V::T> &a) {
+    using T = typename V::T;
+    w.inv = V::IMAG ? (T)a.scal->pending_inv : T(1);
+    w.aH = a.aH;
+    w.bH = a.bH;
+    w.aV = a.aV;
+    w.bV = a.bV;
+    w.ca = a.ca;
+    w.caa = a.caa;
+    w.gpsi_pitch = (size_t)a.P * sizeof(Cx<T>);
+    w.gtab_pitch = (size_t)a.P * sizeof(typename V::TabT);
+}
 
-        w.lslot = 0;
-        w.tslot = 0;
-        w.loaded_to = w.ra;
-        w.issued_to = min(w.ra + D, w.rb);
-        __syncwarp();  // the previous task's reads of the ring are done
-        if constexpr (V::LANE_COEF) {
-            if (c0 < 0 || c0 + SW > a.P) {
-                zero_ring_outside(w);
-                __syncwarp();
-            }
-        }
-        if (lane == 0) {
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            for (int row = w.ra; row < w.issued_to; ++row) w.issue(row, row - w.ra);
-        }
-
-        if constexpr (V::LANE_COEF) {
-            walk_segment<V, false>(w, a);
+// One task of a tile: strip x segment `task`, interior strips first.
+template <class V>
+__device__ __forceinline__ void run_task(Walk<V> &w, const StepArgs<typename V::T> &a, int task) {
+    using T = typename V::T;
+    using TabT = typename V::TabT;
+    constexpr int C = V::C, NWIN = V::NWIN, HX = V::HX, HY = V::HY, SW = V::SW, WO = V::WO;
+    constexpr bool ROT = V::ROT;
+    const int lane = w.lane;
+    const int D = w.D;
+    // tasks of interior strips come first and those of the first and last
+    // strip (the only ones that need masks) last, so that few SMs run both
+    // code paths
+    int strip, seg;
+    {
+        const int n_int = a.n_strips > 2 ? (a.n_strips - 2) * a.n_segs : 0;
+        if (task < n_int) {
+            strip = 1 + task % (a.n_strips - 2);
+            seg = task / (a.n_strips - 2);
         } else {
-            if (c0 >= 0 && c0 + SW <= a.W) walk_segment<V, false>(w, a);
-            else walk_segment<V, true>(w, a);
-        }
-
-        if (w.failed) {
-            if (lane == 0) atomicExch(&a.scal->error, 1);
-            // let copies already issued land before the block can exit
-            int q = w.lslot;
-            for (int row = w.loaded_to; row < w.issued_to; ++row) {
-                (void)mbar_wait_bounded(&w.bars[q], (w.phase_bits >> q) & 1u, 100000000ull);
-                w.phase_bits ^= 1u << q;
-                q = w.next(q);
-            }
+            const int e = task - n_int;
+            const int n_edge_strips = a.n_strips > 2 ? 2 : a.n_strips;
+            const int es = e % n_edge_strips;
+            strip = (a.n_strips > 2 && es == 1) ? a.n_strips - 1 : es;
+            seg = e / n_edge_strips;
         }
     }
+    const int ox0 = strip * WO, ox1 = min(ox0 + WO, a.W);
+    const int c0 = ox0 - HX;
+    w.oy0 = seg * a.seg_h;
+    w.oy1 = min(w.oy0 + a.seg_h, a.H);
+    w.ra = max(w.oy0 - HY, 0);
+    w.rb = min(w.oy1 + HY, a.H);
+    const int cs = max(c0, 0);
+    const int ce = min(c0 + SW, a.P);
+    w.psi_off = (uint32_t)(cs - c0) * sizeof(Cx<T>);
+    w.psi_bytes = (uint32_t)(ce - cs) * sizeof(Cx<T>);
+    w.tab_off = (uint32_t)(cs - c0) * sizeof(TabT);
+    w.tab_bytes = (uint32_t)(ce - cs) * sizeof(TabT);
+    w.gpsi = reinterpret_cast<const unsigned char *>(a.psi_in) + (size_t)cs * sizeof(Cx<T>);
+    w.gtab = reinterpret_cast<const unsigned char *>(a.pot) + (size_t)cs * sizeof(TabT);
+    w.xl = c0 + C * lane;
+#pragma unroll
+    for (int i = 0; i < C; ++i) {
+        const int x = w.xl + i;
+        w.present[i] = x >= 0 && x < a.W;
+        w.out_col[i] = x >= ox0 && x < ox1;
+        w.norm_col[i] = w.out_col[i] && x >= a.ix0 && x < a.ix1;
+    }
+#pragma unroll
+    for (int i = 0; i + 1 < C; ++i) w.m.pair_int[i] = w.present[i] && w.present[i + 1];
+    w.m.pair_int[C - 1] = false;
+    w.m.pair_left = lane > 0 && w.present[0] && w.xl - 1 >= 0;
+    w.m.pair_right = lane < 31 && w.present[C - 1] && w.xl + C < a.W;
+    if constexpr (V::LANE_COEF) {
+        const T one = DeltaForm<T>::value ? T(0) : T(1);
+        w.hai = w.m.pair_int[0] ? w.aH : one;
+        w.hbi = w.m.pair_int[0] ? w.bH : T(0);
+        w.hal = w.m.pair_left ? w.aH : one;
+        w.hbl = w.m.pair_left ? w.bH : T(0);
+        w.har = w.m.pair_right ? w.aH : one;
+        w.hbr = w.m.pair_right ? w.bH : T(0);
+    }
+    if constexpr (ROT) {
+#pragma unroll
+        for (int i = 0; i < C; ++i)
+            w.colab[i] = reinterpret_cast<const Cx<T> *>(a.col_ab)[w.present[i] ? w.xl + i : 0];
+    }
+#pragma unroll
+    for (int j = 0; j < NWIN; ++j)
+#pragma unroll
+        for (int i = 0; i < C; ++i) w.win[j][i] = Cx<T>{T(0), T(0)};
+
+    w.lslot = 0;
+    w.tslot = 0;
+    w.loaded_to = w.ra;
+    w.issued_to = min(w.ra + D, w.rb);
+    __syncwarp();  // the previous task's reads of the ring are done
+    if constexpr (V::LANE_COEF) {
+        if (c0 < 0 || c0 + SW > a.P) {
+            zero_ring_outside(w);
+            __syncwarp();
+        }
+    }
+    if (lane == 0) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        for (int row = w.ra; row < w.issued_to; ++row) w.issue(row, row - w.ra);
+    }
+
+    if constexpr (V::LANE_COEF) {
+        walk_segment<V, false>(w, a);
+    } else {
+        if (c0 >= 0 && c0 + SW <= a.W) walk_segment<V, false>(w, a);
+        else walk_segment<V, true>(w, a);
+    }
+
+    if (w.failed) {
+        if (lane == 0) atomicExch(&a.scal->error, 1);
+        // let copies already issued land before the block can exit
+        int q = w.lslot;
+        for (int row = w.loaded_to; row < w.issued_to; ++row) {
+            (void)mbar_wait_bounded(&w.bars[q], (w.phase_bits >> q) & 1u, 100000000ull);
+            w.phase_bits ^= 1u << q;
+            q = w.next(q);
+        }
+    }
+}
+
+// Grid: any number of blocks of 1..4 warps; each warp loops over the tasks
+// (strip, segment) t = warp_global, warp_global + total_warps, ...
+template <class V>
+__global__ void __launch_bounds__(128, V::MIN_BLOCKS) step_kernel(StepArgs<typename V::T> a) {
+    constexpr bool IMAG = V::IMAG;
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int warps = blockDim.x >> 5;
+    // broadcast from lane 0 so that the compiler knows the warp index, and
+    // every task quantity derived from it, to be warp-uniform
+    const int warp = __shfl_sync(0xffffffffu, (int)(threadIdx.x >> 5), 0);
+    const int lane = threadIdx.x & 31;
+    const int n_tasks = a.n_strips * a.n_segs;
+
+    Walk<V> w;
+    warp_setup(w, smem, warps, warp, lane, a.ring);
+    bind_args(w, a);
+    for (int task = blockIdx.x * warps + warp; task < n_tasks && !w.failed;
+         task += gridDim.x * warps)
+        run_task(w, a, task);
 
     if constexpr (IMAG) {
         // block partial: the block's warps in warp order (a warp's tasks in
@@ -906,6 +926,93 @@ __global__ void __launch_bounds__(128, V::MIN_BLOCKS) step_kernel(StepArgs<typen
             }
         }
     }
+}
+
+// ------------------------------------------------------------------ batch
+// Many tiles of uneven sizes advanced by one Trotter step in one launch: the
+// tasks (strip x segment) of all tiles form one list that the persistent
+// grid walks; each task binds its tile's buffers and constants.
+template <typename T>
+struct BatchArgs {
+    const StepArgs<T> *inst;  // per tile: this step's buffers, constants and task geometry
+    const int2 *tasks;        // (tile, task of the tile), tile-major
+    double *task_norm;        // imaginary time: squared norm of each task's inner cells
+    int *error;               // set when a bounded wait gives up
+    int n_tasks;
+    int ring;
+};
+
+template <typename X>
+__device__ __forceinline__ X bcast0(X x) {
+    return __shfl_sync(0xffffffffu, x, 0);
+}
+template <typename X>
+__device__ __forceinline__ X *ldg_ptr(X *const *addr) {
+    return reinterpret_cast<X *>(__ldg(reinterpret_cast<const unsigned long long *>(addr)));
+}
+template <typename X>
+__device__ __forceinline__ X *bcast0_ptr(X *p) {
+    return reinterpret_cast<X *>(__shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(p), 0));
+}
+
+// The tile's arguments as warp-uniform values (read by every lane from the
+// same address, broadcast from lane 0 so that the compiler knows it).
+template <typename T>
+__device__ __forceinline__ StepArgs<T> load_tile_args(const StepArgs<T> *p) {
+    StepArgs<T> a;
+    a.psi_in = bcast0_ptr(ldg_ptr(&p->psi_in));
+    a.psi_out = bcast0_ptr(ldg_ptr(&p->psi_out));
+    a.pot = bcast0_ptr(ldg_ptr(&p->pot));
+    a.row_ab = bcast0_ptr(ldg_ptr(&p->row_ab));
+    a.col_ab = bcast0_ptr(ldg_ptr(&p->col_ab));
+    a.W = bcast0(__ldg(&p->W));
+    a.H = bcast0(__ldg(&p->H));
+    a.P = bcast0(__ldg(&p->P));
+    a.ix0 = bcast0(__ldg(&p->ix0));
+    a.ix1 = bcast0(__ldg(&p->ix1));
+    a.iy0 = bcast0(__ldg(&p->iy0));
+    a.iy1 = bcast0(__ldg(&p->iy1));
+    a.n_strips = bcast0(__ldg(&p->n_strips));
+    a.n_segs = bcast0(__ldg(&p->n_segs));
+    a.seg_h = bcast0(__ldg(&p->seg_h));
+    a.ring = bcast0(__ldg(&p->ring));
+    a.aH = bcast0(__ldg(&p->aH));
+    a.bH = bcast0(__ldg(&p->bH));
+    a.aV = bcast0(__ldg(&p->aV));
+    a.bV = bcast0(__ldg(&p->bV));
+    a.ca = bcast0(__ldg(&p->ca));
+    a.caa = bcast0(__ldg(&p->caa));
+    a.partials = nullptr;
+    a.scal = bcast0_ptr(ldg_ptr(&p->scal));
+    a.dxdy = bcast0(__ldg(&p->dxdy));
+    a.norm0 = bcast0(__ldg(&p->norm0));
+    return a;
+}
+
+template <class V>
+__global__ void __launch_bounds__(128, V::MIN_BLOCKS) batch_step_kernel(BatchArgs<typename V::T> b) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int warps = blockDim.x >> 5;
+    const int warp = __shfl_sync(0xffffffffu, (int)(threadIdx.x >> 5), 0);
+    const int lane = threadIdx.x & 31;
+
+    Walk<V> w;
+    warp_setup(w, smem, warps, warp, lane, b.ring);
+    for (int t = blockIdx.x * warps + warp; t < b.n_tasks && !w.failed; t += gridDim.x * warps) {
+        const int2 it = __ldg(&b.tasks[t]);
+        const int tile = bcast0(it.x), task = bcast0(it.y);
+        const StepArgs<typename V::T> a = load_tile_args(b.inst + tile);
+        bind_args(w, a);
+        w.nacc = 0.0;
+        run_task(w, a, task);
+        if constexpr (V::IMAG) {
+            double n = w.nacc;
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) n += __shfl_xor_sync(0xffffffffu, n, off);
+            if (lane == 0) b.task_norm[t] = n;
+        }
+    }
+    if (w.failed && lane == 0) atomicExch(b.error, 1);
 }
 
 }  // namespace tsb

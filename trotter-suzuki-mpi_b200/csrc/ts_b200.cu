@@ -18,6 +18,8 @@
 #include <type_traits>
 
 #include "step_kernel.cuh"
+#include "handle.h"
+#include "halo.cuh"
 #include "step_launch.h"
 #include "ts_b200.h"
 
@@ -25,9 +27,12 @@ using tsb::Cx;
 using tsb::Scalars;
 using tsb::StepArgs;
 
-namespace {
-
+namespace tsbh {
 std::atomic<uint64_t> g_launches{0};
+}  // namespace tsbh
+using tsbh::g_launches;
+
+namespace {
 
 
 // ------------------------------------------------ FP32 rounding of rotations
@@ -162,37 +167,8 @@ __global__ void copy_tile_kernel(Cx<T> *dst, size_t dpitch, const Cx<T> *src, si
 template <typename T>
 __global__ void halo_kernel(Cx<T> *psi, int W, int H, int P, int hx, int hy, int px, int py,
                             int iy0) {
-    const int nx_dest = px ? 2 * hx * H : 0;
-    const int ncols_b = px ? W - 2 * hx : W;  // y-halo cells outside the x-halo columns
-    const int ny_dest = py ? 2 * hy * ncols_b : 0;
-    const int n = nx_dest + ny_dest;
-    const int Nx = W - 2 * hx, Ny = H - 2 * hy;
-    const int xr0 = iy0, xr1 = iy0 + H - 2 * hy;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        int x, y;
-        if (k < nx_dest) {
-            y = k / (2 * hx);
-            const int c = k % (2 * hx);
-            x = c < hx ? c : W - 2 * hx + c;
-        } else {
-            const int kk = k - nx_dest;
-            const int rr = kk / ncols_b, c = kk % ncols_b;
-            y = rr < hy ? rr : H - 2 * hy + rr;
-            x = px ? hx + c : c;
-        }
-        int ys = y;
-        if (py) {
-            if (y < hy) ys = y + Ny;
-            else if (y >= H - hy) ys = y - Ny;
-        }
-        int xs = x;
-        if (px && ys >= xr0 && ys < xr1) {
-            if (x < hx) xs = x + Nx;
-            else if (x >= W - hx) xs = x - Nx;
-        }
-        if (xs == x && ys == y) continue;
-        psi[(size_t)y * P + x] = psi[(size_t)ys * P + xs];
-    }
+    tsb::halo_cells(psi, W, H, P, hx, hy, px, py, iy0, blockIdx.x * blockDim.x + threadIdx.x,
+                    gridDim.x * blockDim.x);
 }
 
 // -------------------------------------------------------------- reductions
@@ -418,45 +394,11 @@ cudaError_t dispatch_step<float>(int C, bool imag, bool rot, int phase, const St
                 : tsb::launch_step_f32_real(C, rot, phase, a, warps, smem, blocks, st, bps);
 }
 
-int slot_bytes(int C, bool fp32, bool imag) {
-    const int cell = fp32 ? 8 : 16;
-    const int tab = imag ? cell / 2 : cell;
-    return 32 * C * (cell + tab);
-}
-
-int div_up(long a, long b) { return (int)((a + b - 1) / b); }
+using tsbh::div_up;
+using tsbh::slot_bytes;
 
 }  // namespace
 
-// =================================================================== handle
-struct ts_b200_kernel {
-    ts_b200_desc d{};
-    int W = 0, H = 0, P = 0;
-    bool fp32 = false, imag = false, rot = false;
-    int phase = 0;  // 0 none, 1 g|psi|^2, 2 with Lee-Huang-Yang
-    size_t cell = 0, tab_cell = 0;
-    void *psi[2] = {nullptr, nullptr};
-    int cur = 0;
-    void *tab = nullptr;
-    void *row_ab = nullptr, *col_ab = nullptr;
-    double *partials = nullptr;
-    size_t partials_cap = 0;
-    Scalars *scal = nullptr;
-    double *staging = nullptr;  // 2 * W * H doubles
-    double *vtab = nullptr;     // V for energies (W * H)
-    bool have_v = false;
-    double *red_partials = nullptr;
-    double *red_out = nullptr;
-    unsigned int *red_ticket = nullptr;
-    cudaStream_t own_stream = nullptr, stream = nullptr;
-    int C = 2, seg_h = 64, warps = 4, ring = 4;
-    int resident_blocks = 0;  // blocks of the current launch shape resident on the GPU (0: unknown)
-    bool auto_seg = true;     // pick the segment height from the resident grid
-    cudaGraphExec_t graph = nullptr;
-    int graph_steps = 0;
-    int num_sms = 148;
-    std::string err;
-};
 
 namespace {
 
@@ -542,6 +484,54 @@ int launch_halo_t(ts_b200_kernel *k) {
     return TS_B200_OK;
 }
 
+}  // namespace
+
+template <typename T>
+void tsbh::fill_step_constants(const ts_b200_kernel *k, StepArgs<T> &a) {
+    a.pot = k->tab;
+    a.row_ab = k->row_ab;
+    a.col_ab = k->col_ab;
+    a.W = k->W;
+    a.H = k->H;
+    a.P = k->P;
+    a.ix0 = k->d.inner_x0;
+    a.ix1 = k->d.inner_x1;
+    a.iy0 = k->d.inner_y0;
+    a.iy1 = k->d.inner_y1;
+    a.aH = (T)k->d.a_h;
+    a.bH = (T)k->d.b_h;
+    a.aV = (T)k->d.a_v;
+    a.bV = (T)k->d.b_v;
+    if (sizeof(T) == 4) {
+        // delta form: a - 1 from the angle, without cancellation
+        const double kx = k->imag ? asinh(k->d.b_h) : asin(k->d.b_h);
+        const double ky = k->imag ? asinh(k->d.b_v) : asin(k->d.b_v);
+        const double amh = k->imag ? cosh_m1(kx) : cos_m1(kx);
+        const double amv = k->imag ? cosh_m1(ky) : cos_m1(ky);
+        float fa, fb;
+        if (k->imag) {
+            a.aH = (T)amh;
+            a.aV = (T)amv;
+        } else {
+            unimodular_float_pair(amh, k->d.b_h, 16, &fa, &fb);
+            a.aH = (T)fa;
+            a.bH = (T)fb;
+            unimodular_float_pair(amv, k->d.b_v, 16, &fa, &fb);
+            a.aV = (T)fa;
+            a.bV = (T)fb;
+        }
+    }
+    a.ca = (T)k->d.coupling;
+    a.caa = (T)k->d.lhy_coupling;
+    a.scal = k->scal;
+    a.dxdy = k->d.delta_x * k->d.delta_y;
+    a.norm0 = k->d.norm0;
+}
+template void tsbh::fill_step_constants<double>(const ts_b200_kernel *, StepArgs<double> &);
+template void tsbh::fill_step_constants<float>(const ts_b200_kernel *, StepArgs<float> &);
+
+namespace {
+
 template <typename T>
 int launch_step_t(ts_b200_kernel *k, int exchange, bool dry = false) {
     int strips, segs, blocks;
@@ -570,49 +560,12 @@ int launch_step_t(ts_b200_kernel *k, int exchange, bool dry = false) {
     StepArgs<T> a{};
     a.psi_in = k->psi[k->cur];
     a.psi_out = k->psi[1 - k->cur];
-    a.pot = k->tab;
-    a.row_ab = k->row_ab;
-    a.col_ab = k->col_ab;
-    a.W = k->W;
-    a.H = k->H;
-    a.P = k->P;
-    a.ix0 = k->d.inner_x0;
-    a.ix1 = k->d.inner_x1;
-    a.iy0 = k->d.inner_y0;
-    a.iy1 = k->d.inner_y1;
+    tsbh::fill_step_constants(k, a);
     a.n_strips = strips;
     a.n_segs = segs;
     a.seg_h = k->seg_h;
     a.ring = k->ring;
-    a.aH = (T)k->d.a_h;
-    a.bH = (T)k->d.b_h;
-    a.aV = (T)k->d.a_v;
-    a.bV = (T)k->d.b_v;
-    if (sizeof(T) == 4) {
-        // delta form: a - 1 from the angle, without cancellation
-        const double kx = k->imag ? asinh(k->d.b_h) : asin(k->d.b_h);
-        const double ky = k->imag ? asinh(k->d.b_v) : asin(k->d.b_v);
-        const double amh = k->imag ? cosh_m1(kx) : cos_m1(kx);
-        const double amv = k->imag ? cosh_m1(ky) : cos_m1(ky);
-        float fa, fb;
-        if (k->imag) {
-            a.aH = (T)amh;
-            a.aV = (T)amv;
-        } else {
-            unimodular_float_pair(amh, k->d.b_h, 16, &fa, &fb);
-            a.aH = (T)fa;
-            a.bH = (T)fb;
-            unimodular_float_pair(amv, k->d.b_v, 16, &fa, &fb);
-            a.aV = (T)fa;
-            a.bV = (T)fb;
-        }
-    }
-    a.ca = (T)k->d.coupling;
-    a.caa = (T)k->d.lhy_coupling;
     a.partials = k->partials;
-    a.scal = k->scal;
-    a.dxdy = k->d.delta_x * k->d.delta_y;
-    a.norm0 = k->d.norm0;
     cudaError_t e = dispatch_step<T>(k->C, k->imag, k->rot, k->phase, a, k->warps, smem, blocks,
                                      k->stream, nullptr);
     if (e != cudaSuccess) return cuda_fail(k, e, "step kernel launch");
@@ -780,6 +733,7 @@ int ts_b200_create(const ts_b200_desc *d, ts_b200_kernel **out) {
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&k->num_sms, cudaDevAttrMultiProcessorCount, dev);
+    k->device = dev;
     choose_launch(k);
     const size_t ncell = (size_t)k->P * k->H;
     cudaError_t e = cudaSuccess;

@@ -90,6 +90,15 @@ SIGNATURES = {
     "ts_b200_synchronize": (_I, [_VP]),
     "ts_b200_launch_info": (_I, [_VP, C.POINTER(LaunchShape)]),
     "ts_b200_set_launch": (_I, [_VP, _I, _I, _I, _I]),
+    "ts_b200_batch_create": (_I, [C.POINTER(_VP), _I, C.POINTER(_VP)]),
+    "ts_b200_batch_destroy": (None, [_VP]),
+    "ts_b200_batch_size": (_I, [_VP]),
+    "ts_b200_batch_evolve": (_I, [_VP, _I]),
+    "ts_b200_batch_synchronize": (_I, [_VP]),
+    "ts_b200_batch_set_launch": (_I, [_VP, _I, _I]),
+    "ts_b200_batch_autotune": (_I, [_VP, _I, _I]),
+    "ts_b200_batch_launch_info": (_I, [_VP, C.POINTER(LaunchShape)]),
+    "ts_b200_batch_last_error": (C.c_char_p, [_VP]),
     "ts_b200_host_alloc": (_I, [C.POINTER(_VP), _SZ]),
     "ts_b200_host_free": (_I, [_VP]),
     "ts_b200_last_error": (C.c_char_p, [_VP]),
@@ -126,7 +135,10 @@ def lib():
     return _lib
 
 
-def check(status, handle=None):
+def check(status, handle=None, batch=None):
     if status != OK:
-        msg = lib().ts_b200_last_error(handle).decode() if handle else ""
+        if batch:
+            msg = lib().ts_b200_batch_last_error(batch).decode()
+        else:
+            msg = lib().ts_b200_last_error(handle).decode() if handle else ""
         raise B200Error(status, msg or STATUS.get(status, ""))

@@ -136,6 +136,62 @@ class Kernel:
                                              warps_per_block, ring_depth))
 
 
+class Batch:
+    """Many tiles advanced together, one persistent launch per Trotter step.
+
+    kernels: Kernel objects of the same precision and time mode (no rotating
+    frame).  The batch borrows their device state: set states and read
+    results through the Kernel objects; they must outlive the batch.
+    """
+
+    def __init__(self, kernels):
+        self.kernels = list(kernels)
+        arr = (C.c_void_p * len(self.kernels))(*[k.handle.value for k in self.kernels])
+        self._b = C.c_void_p()
+        check(lib().ts_b200_batch_create(arr, len(self.kernels), C.byref(self._b)))
+
+    def close(self):
+        if self._b:
+            lib().ts_b200_batch_destroy(self._b)
+            self._b = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __len__(self):
+        return len(self.kernels)
+
+    def _check(self, status):
+        check(status, batch=self._b)
+
+    def evolve(self, iterations):
+        self._check(lib().ts_b200_batch_evolve(self._b, int(iterations)))
+
+    def synchronize(self):
+        self._check(lib().ts_b200_batch_synchronize(self._b))
+
+    def set_launch(self, segment_rows=0, warps_per_block=0):
+        self._check(lib().ts_b200_batch_set_launch(self._b, segment_rows, warps_per_block))
+
+    def autotune(self, trial_steps=3, use_cache=True):
+        self._check(lib().ts_b200_batch_autotune(self._b, int(trial_steps), int(bool(use_cache))))
+        return self.launch_shape()
+
+    def launch_shape(self):
+        s = LaunchShape()
+        self._check(lib().ts_b200_batch_launch_info(self._b, C.byref(s)))
+        return {n: getattr(s, n) for n, _ in LaunchShape._fields_}
+
+
 def launch_count():
     """Kernel launches made by this process through the library."""
     return int(lib().ts_b200_launch_count())
