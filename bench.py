@@ -411,6 +411,211 @@ def run_b200_arm(args, rank, world, local, pg):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------- batched workload
+# 512 independent real-time GPE instances of uneven sizes in one persistent
+# launch per Trotter step.  Sides uniform in {128, 192, ..., 1024}; per
+# instance omega ~ U[0.5, 2], g ~ U[0, 200], Gaussian centre ~ U[-2, 2]^2,
+# width ~ U[0.5, 2]; length 20 per side (the configuration leaves it open),
+# closed boundaries, dt = 1e-4.  One bench step = 200 Trotter steps, so 10
+# bench steps are the configuration's 2000-step run.
+BATCH_N = 512
+BATCH_SIDES = tuple(range(128, 1025, 64))
+BATCH_LENGTH = 20.0
+BATCH_DT = 1e-4
+BATCH_TROTTER_PER_STEP = 200
+BATCH_SEED = 20240602
+BATCH_BYTES = {"fp64": 48, "fp32": 24}  # real time: psi in + psi out + complex table
+
+
+def batch_config(n=BATCH_N, seed=BATCH_SEED):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    sides = rng.choice(np.array(BATCH_SIDES), n)
+    omega = rng.uniform(0.5, 2.0, n)
+    g = rng.uniform(0.0, 200.0, n)
+    centre = rng.uniform(-2.0, 2.0, (n, 2))
+    width = rng.uniform(0.5, 2.0, n)
+    return [dict(side=int(sides[i]), omega=float(omega[i]), g=float(g[i]),
+                 cx=float(centre[i, 0]), cy=float(centre[i, 1]), width=float(width[i]))
+            for i in range(n)]
+
+
+def batch_solvers(ts, cfgs, kernel_type):
+    out = []
+    for c in cfgs:
+        grid = ts.Lattice2D(c["side"], BATCH_LENGTH)
+        w = 1.0 / c["width"] ** 2
+        state = ts.GaussianState(grid, w, w, c["cx"], c["cy"])
+        pot = ts.HarmonicPotential(grid, c["omega"], c["omega"])
+        ham = ts.Hamiltonian(grid, pot, 1.0, c["g"])
+        out.append((ts.Solver(grid, state, ham, BATCH_DT, kernel_type=kernel_type),
+                    (grid, state, pot, ham)))
+    return out
+
+
+def batch_cpu_rate(cfgs, budget_s=10.0):
+    """The reference's CPUBlock (oracle/_ref) on the first instances of the batch."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import tsref
+    flavour = "fast" if tsref.available("fast") else ("parity" if tsref.available() else None)
+    if flavour is None:
+        return None
+    threads = os.cpu_count() or 1
+    sites = 0.0
+    secs = 0.0
+    used = 0
+    for c in cfgs:
+        w = 1.0 / c["width"] ** 2
+        cfg = tsref.make_config(c["side"], BATCH_LENGTH, gaussian=(w, w, c["cx"], c["cy"], 1.0, 0.0),
+                                harmonic=(c["omega"], c["omega"], 1.0, 0.0, 0.0), coupling=c["g"],
+                                delta_t=BATCH_DT, segments=((1, False), (20, False)),
+                                omp_threads=threads)
+        _, res = tsref.run(cfg, None, None, flavour=flavour)
+        sites += c["side"] ** 2 * 20
+        secs += res.seg_seconds[1]
+        used += 1
+        if secs > budget_s:
+            break
+    return {"value": sites / secs, "unit": "site-steps/s", "cores": threads, "kind": "reference",
+            "sample": f"first {used} instances of the batch, 20 real-time Trotter steps each, "
+                      f"reference CPUBlock ({'-Ofast' if flavour == 'fast' else '-O2'} build), "
+                      f"{threads} OpenMP threads"}
+
+
+def run_batch_workload(args, rank, world, local, pg):
+    import torch
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    import trottersuzuki_b200 as ts
+    from trottersuzuki_b200 import _capi, launch_count
+    L = _capi.lib()
+    cfgs = batch_config()
+    total_sites = float(sum(c["side"] ** 2 for c in cfgs))
+    T = BATCH_TROTTER_PER_STEP
+    stream = torch.cuda.Stream(device=device)
+    res = {}
+    clk = None
+    e2e = None
+    launches = 0
+    for kernel_type, prec in (("gpu", "fp64"), ("gpu_fp32", "fp32")):
+        solvers = batch_solvers(ts, cfgs, kernel_type)
+        sb = ts.SolverBatch([s for s, _ in solvers])
+        sb.batch.set_stream(stream.cuda_stream)
+        handles = [s.kernel_handle() for s, _ in solvers]
+        for h in handles:
+            _capi.check(L.ts_b200_set_stream(C.c_void_p(h), C.c_void_p(stream.cuda_stream)))
+        t0 = time.perf_counter()
+        shape = sb.autotune(trial_steps=3, use_cache=False)
+        tune_s = time.perf_counter() - t0
+        for _ in range(args.warmup):
+            sb.batch.evolve(T)
+        torch.cuda.synchronize()
+        if pg:
+            pg.barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        l0 = launch_count()
+        with Clocks(local) as clocks:
+            e0.record(stream)
+            for _ in range(args.steps):
+                sb.batch.evolve(T)
+            e1.record(stream)
+            e1.synchronize()
+        if prec == "fp64":
+            clk = clocks.summary()
+            launches = launch_count() - l0
+        ms = max_over_ranks(e0.elapsed_time(e1), pg, device)
+        value = world * total_sites * T * args.steps / (ms * 1e-3)
+        # per-instance launch loop on the same stream (each tile's own
+        # graph-replayed evolve, one tile after the other)
+        loop_steps = max(1, args.steps // 5)
+        for h in handles:
+            _capi.check(L.ts_b200_evolve(C.c_void_p(h), T))
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(loop_steps):
+            for h in handles:
+                _capi.check(L.ts_b200_evolve(C.c_void_p(h), T))
+        e1.record(stream)
+        e1.synchronize()
+        ms_loop = max_over_ranks(e0.elapsed_time(e1), pg, device)
+        loop_value = world * total_sites * T * loop_steps / (ms_loop * 1e-3)
+        res[prec] = {"value": value, "ms_per_step": ms / args.steps, "loop_value": loop_value,
+                     "speedup_vs_loop": value / loop_value, "autotune_s": tune_s,
+                     "shape": {k: shape[k] for k in ("segment_rows", "warps_per_block", "blocks")}}
+        if prec == "fp64":
+            # e2e: every bench step uploads all initial states from host
+            # arrays, evolves the batch and reads every state back
+            init = []
+            for c in cfgs:
+                n_side = c["side"]
+                dx = BATCH_LENGTH / n_side
+                x = (np.arange(n_side) + 0.5) * dx - BATCH_LENGTH * 0.5
+                X, Y = np.meshgrid(x, x)
+                w = 1.0 / c["width"] ** 2
+                g0 = np.sqrt(w / math.pi) * np.exp(-0.5 * w * ((X - c["cx"]) ** 2 + (Y - c["cy"]) ** 2))
+                init.append((np.ascontiguousarray(g0), np.zeros_like(g0)))
+            outs = [(np.empty_like(a), np.empty_like(a)) for a, _ in init]
+            h2d = sum(a.nbytes + b.nbytes for a, b in init)
+
+            def e2e_step():
+                for h, (a, b), c in zip(handles, init, cfgs):
+                    _capi.check(L.ts_b200_set_state(C.c_void_p(h), a.ctypes.data, b.ctypes.data,
+                                                    c["side"]))
+                sb.batch.evolve(T)
+                for h, (a, b), c in zip(handles, outs, cfgs):
+                    n_side = c["side"]
+                    _capi.check(L.ts_b200_get_sample(C.c_void_p(h), n_side, 0, 0, n_side, n_side,
+                                                     a.ctypes.data, b.ctypes.data))
+            e2e_step()
+            torch.cuda.synchronize()
+            e0.record(stream)
+            for _ in range(args.steps):
+                e2e_step()
+            e1.record(stream)
+            e1.synchronize()
+            e2e_ms = max_over_ranks(e0.elapsed_time(e1), pg, device)
+            e2e = {"value": world * total_sites * T * args.steps / (e2e_ms * 1e-3),
+                   "unit": "site-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d,
+                   "path": "ts_b200_set_state x512, ts_b200_batch_evolve, ts_b200_get_sample x512"}
+        sb.close()
+        del solvers, sb
+        torch.cuda.synchronize()
+    if rank != 0:
+        return
+    peak, peak_kind = measured_peak()
+    bytes_step = BATCH_BYTES["fp64"] * total_sites
+    achieved = bytes_step / (res["fp64"]["ms_per_step"] * 1e-3 / T) / 1e9
+    cpu = None if args.no_cpu_baseline else batch_cpu_rate(cfgs)
+    line = {
+        "metric": "site-steps/s", "value": res["fp64"]["value"], "unit": "site-steps/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": res["fp64"]["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "batch512_real_time", "instances": BATCH_N,
+                   "sides": list(BATCH_SIDES), "total_sites": total_sites, "length": BATCH_LENGTH,
+                   "dt": BATCH_DT, "trotter_steps_per_step": T, "boundary": "closed",
+                   "imag_time": False, "seed": BATCH_SEED, "parallelism": f"replicas{world}",
+                   "l2": "inputs larger than L2: %.1f GB moved per Trotter step" % (bytes_step / 1e9)},
+        "per_instance_loop": {"value": res["fp64"]["loop_value"], "unit": "site-steps/s",
+                              "speedup_batch_vs_loop": res["fp64"]["speedup_vs_loop"]},
+        "autotune": {"fp64": res["fp64"]["shape"], "fp32": res["fp32"]["shape"],
+                     "seconds_fp64": res["fp64"]["autotune_s"]},
+        "fp32_store": {"value": res["fp32"]["value"], "unit": "site-steps/s",
+                       "speedup_vs_fp64": res["fp32"]["value"] / res["fp64"]["value"],
+                       "loop_value": res["fp32"]["loop_value"],
+                       "speedup_batch_vs_loop": res["fp32"]["speedup_vs_loop"]},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                     "algorithmic_bytes_per_launch": bytes_step,
+                     "kernel": "tsb::batch_step_kernel<double, C=2, real, no rotation, GPE>"},
+        "e2e": e2e,
+        "cpu_baseline": cpu,
+        "clocks": clk,
+        "gpu_launches": launches,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -421,12 +626,16 @@ def main():
                     help="seconds of reference CPU work per sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32", action="store_true")
+    ap.add_argument("--workload", choices=["gpe_imaginary_time_2048", "batch512"],
+                    default="gpe_imaginary_time_2048")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     rank, world, local, pg = dist_setup(args)
     try:
         if args.impl == "reference":
             run_reference_arm(args, rank, world, pg)
+        elif args.workload == "batch512":
+            run_batch_workload(args, rank, world, local, pg)
         else:
             run_b200_arm(args, rank, world, local, pg)
     finally:

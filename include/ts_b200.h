@@ -225,12 +225,16 @@ int ts_b200_batch_evolve(ts_b200_batch *b, int iterations);
  * in the batched step gave up. */
 int ts_b200_batch_synchronize(ts_b200_batch *b);
 
+/* Queue the batch's work on `stream` (a cudaStream_t); NULL restores the
+ * batch's own stream. */
+int ts_b200_batch_set_stream(ts_b200_batch *b, void *stream);
+
 /* Tile shape of the batched launch: rows per segment task (even; capped by
  * each tile's height) and warps per block (1, 2 or 4).  Zero keeps a field. */
 int ts_b200_batch_set_launch(ts_b200_batch *b, int segment_rows, int warps_per_block);
 
 /* Autotuner: times `trial_steps` batched steps for each candidate shape (rows
- * per segment 16..128, 2 or 4 warps per block) and keeps the fastest.  The
+ * per segment 16..256, 2 or 4 warps per block) and keeps the fastest.  The
  * trials read the tiles' current state and write only the scratch buffer, so
  * the state is unchanged.  With use_cache != 0 a shape tuned earlier in this
  * process for the same precision, time mode and tile sizes is reused

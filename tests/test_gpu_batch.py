@@ -116,7 +116,7 @@ def test_autotune_keeps_state_and_results():
     before = [t["k"].get_state() for t in tiles]
     with Batch([t["k"] for t in tiles]) as b:
         shape = b.autotune(trial_steps=2, use_cache=False)
-        assert shape["segment_rows"] in (16, 24, 32, 48, 64, 96, 128)
+        assert shape["segment_rows"] in (16, 32, 64, 96, 128, 192, 256)
         assert shape["warps_per_block"] in (2, 4)
         after = [t["k"].get_state() for t in tiles]
         for x, y in zip(before, after):
@@ -161,3 +161,35 @@ def test_batch_rejects_mixed_or_unsupported_tiles():
             Batch([kr])
     close_all(t64)
     close_all(t32)
+
+
+def _solver(ts, N, L, omega, g, centre, width, kernel_type="gpu"):
+    grid = ts.Lattice2D(N, L)
+    state = ts.GaussianState(grid, 1.0 / width ** 2, 1.0 / width ** 2, centre[0], centre[1])
+    pot = ts.HarmonicPotential(grid, omega, omega)
+    ham = ts.Hamiltonian(grid, pot, 1.0, g)
+    return ts.Solver(grid, state, ham, 1e-4, kernel_type=kernel_type), state
+
+
+@pytest.mark.parametrize("imag", [False, True], ids=["real", "imag"])
+def test_solver_batch_matches_solver_loop(imag):
+    """The drop-in level: SolverBatch(solvers).evolve(T) == for s: s.evolve(T)."""
+    import trottersuzuki_b200 as ts
+    cfg = [(128, 20.0, 1.0, 50.0, (0.5, -1.0), 1.0), (192, 20.0, 1.7, 0.0, (-1.5, 0.3), 0.7),
+           (96, 20.0, 0.6, 150.0, (0.0, 1.2), 1.8)]
+    batch = [_solver(ts, *c) for c in cfg]
+    loop = [_solver(ts, *c) for c in cfg]
+    sb = ts.SolverBatch([s for s, _ in batch], imag_time=imag)
+    sb.autotune(trial_steps=1)
+    sb.evolve(70)
+    for (s1, st1), (s2, st2) in zip(batch, loop):
+        s2.evolve(70, imag)
+        a = np.asarray(st1.get_particle_density())
+        b = np.asarray(st2.get_particle_density())
+        if imag:
+            assert np.abs(a - b).max() <= 1e-12 * np.abs(b).max()
+            assert abs(s1.get_total_energy() - s2.get_total_energy()) <= 1e-11 * abs(s2.get_total_energy())
+        else:
+            assert np.array_equal(a, b)
+            assert s1.get_total_energy() == s2.get_total_energy()
+    sb.close()

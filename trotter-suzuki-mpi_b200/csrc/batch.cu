@@ -94,7 +94,7 @@ struct ts_b200_batch {
     bool fp32 = false, imag = false;
     int phase = 0;
     int device = 0, num_sms = 148;
-    Shape shape{32, 4};
+    Shape shape{128, 4};
     int ring = 4;
     int resident_blocks = 0;  // of the current shape (0: unknown)
     int n_tasks = 0;
@@ -110,7 +110,7 @@ struct ts_b200_batch {
     int *d_error = nullptr;
     std::vector<int> args_cur;    // cur of each tile the argument tables were built for
     bool layout_valid = false;
-    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr, stream = nullptr;
     cudaEvent_t ev = nullptr;
     cudaGraphExec_t graph = nullptr;
     std::string err;
@@ -420,7 +420,7 @@ int autotune_t(ts_b200_batch *b, int trial_steps, int use_cache) {
     }
     int s = join_tiles(b, true);
     if (s) return s;
-    static const int kSegRows[] = {16, 24, 32, 48, 64, 96, 128};
+    static const int kSegRows[] = {16, 32, 64, 96, 128, 192, 256};
     static const int kWarps[] = {4, 2};
     Shape best = b->shape;
     float best_ms = -1.0f;
@@ -482,7 +482,8 @@ int ts_b200_batch_create(ts_b200_kernel *const *kernels, int n, ts_b200_batch **
     b->num_sms = k0->num_sms;
     b->args_bytes = b->fp32 ? sizeof(StepArgs<float>) : sizeof(StepArgs<double>);
     cudaError_t e = cudaSetDevice(b->device);
-    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->own_stream, cudaStreamNonBlocking);
+    b->stream = b->own_stream;
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev, cudaEventDisableTiming);
     for (int p = 0; p < 2 && e == cudaSuccess; ++p) e = cudaMalloc(&b->d_args[p], n * b->args_bytes);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_norm, n * sizeof(TileNorm));
@@ -509,7 +510,7 @@ void ts_b200_batch_destroy(ts_b200_batch *b) {
     cudaFree(b->d_halo);
     cudaFree(b->d_error);
     if (b->ev) cudaEventDestroy(b->ev);
-    if (b->stream) cudaStreamDestroy(b->stream);
+    if (b->own_stream) cudaStreamDestroy(b->own_stream);
     delete b;
 }
 
@@ -525,6 +526,14 @@ int ts_b200_batch_synchronize(ts_b200_batch *b) {
     TSBB_CHECK(b, cudaMemcpyAsync(&err, b->d_error, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
     TSBB_CHECK(b, cudaStreamSynchronize(b->stream));
     if (err) return bfail(b, TS_B200_DEVICE_TIMEOUT, "a bounded wait in the batched step gave up");
+    return TS_B200_OK;
+}
+
+int ts_b200_batch_set_stream(ts_b200_batch *b, void *stream) {
+    if (!b) return TS_B200_INVALID_ARGUMENT;
+    // work queued so far finishes before the batch moves to the other stream
+    TSBB_CHECK(b, cudaStreamSynchronize(b->stream));
+    b->stream = stream ? static_cast<cudaStream_t>(stream) : b->own_stream;
     return TS_B200_OK;
 }
 

@@ -9,12 +9,13 @@ Batch -- many Kernel tiles of uneven sizes advanced by one persistent launch per
 from ._capi import B200Error, Desc, EnergyParams  # noqa: F401
 from .api import (ExponentialState, GaussianState, Hamiltonian, Hamiltonian2Component,  # noqa: F401
                   HarmonicPotential, Lattice1D, Lattice2D, Potential, SinusoidState, Solver,
-                  State, map_lattice_to_coordinate_space)
+                  SolverBatch, State, map_lattice_to_coordinate_space)
 from .kernel import FP32, FP64, Batch, Kernel, launch_count, version  # noqa: F401
 
 __version__ = "1.6.2+b200"
 
 __all__ = ["Lattice1D", "Lattice2D", "State", "ExponentialState", "GaussianState",
            "SinusoidState", "Potential", "HarmonicPotential", "Hamiltonian",
-           "Hamiltonian2Component", "Solver", "map_lattice_to_coordinate_space", "Kernel", "Batch",
+           "Hamiltonian2Component", "Solver", "SolverBatch", "map_lattice_to_coordinate_space",
+           "Kernel", "Batch",
            "B200Error"]

@@ -95,6 +95,7 @@ SIGNATURES = {
     "ts_b200_batch_size": (_I, [_VP]),
     "ts_b200_batch_evolve": (_I, [_VP, _I]),
     "ts_b200_batch_synchronize": (_I, [_VP]),
+    "ts_b200_batch_set_stream": (_I, [_VP, _VP]),
     "ts_b200_batch_set_launch": (_I, [_VP, _I, _I]),
     "ts_b200_batch_autotune": (_I, [_VP, _I, _I]),
     "ts_b200_batch_launch_info": (_I, [_VP, C.POINTER(LaunchShape)]),

@@ -468,3 +468,42 @@ class Solver(_Handle):
         out = C.c_void_p()
         _chk(host().tsh_solver_kernel_handle(self._h, C.byref(out)))
         return out.value
+
+
+class SolverBatch:
+    """Evolve many Solvers together: one persistent launch per Trotter step.
+
+    No counterpart in the reference, where each Solver evolves on its own; a
+    loop of solver.evolve(T) calls becomes SolverBatch(solvers).evolve(T).
+    The solvers must share kernel_type and have no rotating frame and no
+    time-dependent potential.  Each solver's kernel is built (or rebuilt for
+    the time mode) here, from its current State; evolve() leaves the results
+    in the solvers' States, as Solver.evolve does.
+    """
+
+    def __init__(self, solvers, imag_time=False):
+        from .kernel import Batch
+        self.solvers = list(solvers)
+        self.imag_time = bool(imag_time)
+        for s in self.solvers:
+            s.evolve(0, self.imag_time)  # (re)builds the kernel from the State, no step
+        self.batch = Batch([s.kernel_handle() for s in self.solvers])
+
+    def autotune(self, trial_steps=3, use_cache=True):
+        return self.batch.autotune(trial_steps, use_cache)
+
+    def evolve(self, iterations, copy_back=True):
+        """iterations Trotter steps of every solver; with copy_back the States
+        receive the results (else they stay on the device until the next
+        Solver call that reads them)."""
+        n = int(iterations)
+        self.batch.evolve(n)
+        for s in self.solvers:
+            s.current_evolution_time += s.delta_t * n
+            if copy_back:
+                s.evolve(0, self.imag_time)  # copies the tile back into the State
+        if not copy_back:
+            self.batch.synchronize()
+
+    def close(self):
+        self.batch.close()

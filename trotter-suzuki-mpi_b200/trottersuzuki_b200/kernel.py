@@ -139,14 +139,20 @@ class Kernel:
 class Batch:
     """Many tiles advanced together, one persistent launch per Trotter step.
 
-    kernels: Kernel objects of the same precision and time mode (no rotating
-    frame).  The batch borrows their device state: set states and read
-    results through the Kernel objects; they must outlive the batch.
+    kernels: Kernel objects (or raw ts_b200_kernel* handles, as
+    Solver.kernel_handle() returns) of the same precision and time mode, no
+    rotating frame.  The batch borrows their device state: set states and
+    read results through the tiles' own calls; they must outlive the batch.
     """
 
     def __init__(self, kernels):
         self.kernels = list(kernels)
-        arr = (C.c_void_p * len(self.kernels))(*[k.handle.value for k in self.kernels])
+
+        def raw(k):  # a Kernel, a c_void_p or an integer ts_b200_kernel* address
+            if hasattr(k, "handle"):
+                return k.handle.value
+            return k.value if isinstance(k, C.c_void_p) else int(k)
+        arr = (C.c_void_p * len(self.kernels))(*[raw(k) for k in self.kernels])
         self._b = C.c_void_p()
         check(lib().ts_b200_batch_create(arr, len(self.kernels), C.byref(self._b)))
 
@@ -178,6 +184,9 @@ class Batch:
 
     def synchronize(self):
         self._check(lib().ts_b200_batch_synchronize(self._b))
+
+    def set_stream(self, stream_ptr):
+        self._check(lib().ts_b200_batch_set_stream(self._b, C.c_void_p(stream_ptr)))
 
     def set_launch(self, segment_rows=0, warps_per_block=0):
         self._check(lib().ts_b200_batch_set_launch(self._b, segment_rows, warps_per_block))
