@@ -245,6 +245,38 @@ int ts_b200_batch_autotune(ts_b200_batch *b, int trial_steps, int use_cache);
 int ts_b200_batch_launch_info(ts_b200_batch *b, ts_b200_launch_shape *out);
 const char *ts_b200_batch_last_error(const ts_b200_batch *b);
 
+/* ---- Adjoint (reverse mode) of a real-time evolution (no counterpart in the
+ * reference, which has no derivatives).  For a loss L(psi(T)) the reverse
+ * pass turns dL/dpsi(T) into dL/dpsi(0) and dL/dV(x, y) for the `steps`
+ * Trotter steps of the forward pass.  Complex fields are device arrays of
+ * interleaved doubles (re, im) with row stride dim_x cells; gradients follow
+ * the real-pair convention dL/dre + i dL/dim.  The potential V is a device
+ * array of dim_x * dim_y doubles; its table exp(-i V dt) is built on the
+ * device.  Real time, FP64, closed boundaries, no rotating frame
+ * (TS_B200_UNSUPPORTED otherwise).
+ * checkpoint_every == 0: the reverse pass recovers the forward states by
+ * inverse steps; linear evolution only (coupling = lhy_coupling = 0, else
+ * TS_B200_INVALID_ARGUMENT).  checkpoint_every = k > 0: the forward pass
+ * stores every k-th state and the reverse pass recomputes each segment
+ * (device memory: ceil(steps / k) + k - 1 extra states).  One backward per
+ * forward; the engine works on its own stream (ts_b200_adjoint_set_stream). */
+typedef struct ts_b200_adjoint ts_b200_adjoint;
+
+int ts_b200_adjoint_create(const ts_b200_desc *d, double delta_t, int steps, int checkpoint_every,
+                           ts_b200_adjoint **out);
+void ts_b200_adjoint_destroy(ts_b200_adjoint *a);
+int ts_b200_adjoint_set_stream(ts_b200_adjoint *a, void *stream);
+/* psi_t may be NULL (the final state stays in the engine). */
+int ts_b200_adjoint_forward(ts_b200_adjoint *a, const double *potential, const void *psi0,
+                            void *psi_t);
+/* grad_potential and grad_psi0 may be NULL. */
+int ts_b200_adjoint_backward(ts_b200_adjoint *a, const void *grad_psi_t, double *grad_potential,
+                             void *grad_psi0);
+/* Wait for the engine's queued work; TS_B200_DEVICE_TIMEOUT if a bounded
+ * wait gave up. */
+int ts_b200_adjoint_synchronize(ts_b200_adjoint *a);
+const char *ts_b200_adjoint_last_error(const ts_b200_adjoint *a);
+
 /* Pinned host memory for the state arrays (page-locked so that host<->device
  * copies run at full PCIe/C2C rate). */
 int ts_b200_host_alloc(void **ptr, size_t bytes);

@@ -15,6 +15,8 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include "ts_b200.h"
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -83,6 +85,13 @@ int tsh_solver_update_parameters(void *solver);
 /* The device handle of the solver's kernel (NULL before the first evolve). */
 int tsh_solver_kernel_handle(void *solver, void **out);
 int tsh_solver_free(void *solver);
+
+/* The step descriptor the solver's kernel would get for this lattice and
+ * Hamiltonian (the constants of the reference's CPUBlock constructor,
+ * src/cpukernel.cpp:172-272), for the adjoint engine and other direct users
+ * of include/ts_b200.h.  No counterpart in the reference. */
+int tsh_make_desc(void *lattice, void *hamiltonian, double delta_t, double norm, int imag_time,
+                  int precision, ts_b200_desc *out);
 
 #ifdef __cplusplus
 }

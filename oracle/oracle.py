@@ -88,6 +88,9 @@ def lib():
         L.tso_energies.argtypes = [C.POINTER(Geometry), dp, dp, dp, C.c_double, C.c_double,
                                    C.c_double, C.c_double, C.POINTER(Energies)]
         L.tso_expectations.argtypes = [C.POINTER(Geometry), dp, dp, C.POINTER(Expectations)]
+        L.tso_adjoint_real.argtypes = [C.POINTER(Params), dp, dp, C.c_double, dp, dp, C.c_int,
+                                       dp, dp, dp, dp, dp]
+        L.tso_adjoint_real.restype = C.c_int
         _lib = L
     return _lib
 
@@ -270,3 +273,23 @@ def exponential(lattice, n_x=1, n_y=1, norm=1.0, phase=0.0):
     amp = math.sqrt(norm / (lx * ly)) * complex(math.cos(phase), math.sin(phase))
     arg = 2 * math.pi * float(n_x) / lx * X + 2 * math.pi * float(n_y) / ly * Y
     return amp * (np.cos(arg) + 1j * np.sin(arg))
+
+
+def adjoint_real(p, tab_re, tab_im, delta_t, psi0, steps, lam_t):
+    """Reverse mode of `steps` closed real-time steps (CPU FP64 check of the B200
+    adjoint; oracle/ts_oracle.c tso_adjoint_real).  lam_t = dL/dre + i dL/dim at
+    psi(T); returns (dL/dV, dL/dpsi0) with the same convention."""
+    shape = (p.H, p.W)
+    a = lambda z: np.ascontiguousarray(z, np.float64)
+    r0, i0 = a(np.real(psi0)), a(np.imag(psi0))
+    lr, li = a(np.real(lam_t)), a(np.imag(lam_t))
+    tr, ti = a(tab_re), a(tab_im)
+    gv = np.zeros(shape)
+    gr = np.zeros(shape)
+    gi = np.zeros(shape)
+    rc = lib().tso_adjoint_real(C.byref(p), tr.ctypes.data, ti.ctypes.data, float(delta_t),
+                                r0.ctypes.data, i0.ctypes.data, int(steps), lr.ctypes.data,
+                                li.ctypes.data, gv.ctypes.data, gr.ctypes.data, gi.ctypes.data)
+    if rc != 0:
+        raise RuntimeError(f"tso_adjoint_real: status {rc}")
+    return gv, gr + 1j * gi

@@ -222,6 +222,90 @@ void tso_evolve(const tso_params *p, double *re, double *im, const double *pot_r
     }
 }
 
+/* ---- reverse mode of tso_evolve (real time, closed tile) ----------------
+ * Not a restatement of the reference (it has no derivatives): the
+ * transpose, stage by stage, of the forward step above, used as the FP64
+ * CPU check of the B200 adjoint kernel.  Every pair sweep is orthogonal as a
+ * real map, so its transpose is the same sweep with b -> -b.  The potential
+ * stage psi' = exp(-i theta(|x|^2)) E x (x its input) has the transpose
+ *     lambda = conj(E) exp(+i theta) lambda' + 2 theta' q x,
+ *     q = Im(conj(lambda') psi'),   dL/dV += dt q   (dE/dV = -i dt E),
+ * with theta = g|x|^2 + g_lhy|x|^3 (g, g_lhy already times dt) and
+ * theta' = g + 1.5 g_lhy |x|.  All forward states are stored (small tiles). */
+static void forward_half(const tso_params *p, double *re, double *im) {
+    const int vert = p->H > 1;
+    if (vert) sweep_vertical(p, 0, p->aV, p->bV, re, im);
+    sweep_horizontal(p, 0, p->aH, p->bH, re, im);
+    if (vert) sweep_vertical(p, 1, p->aV, p->bV, re, im);
+    sweep_horizontal(p, 1, p->aH, p->bH, re, im);
+}
+
+static void adjoint_potential(const tso_params *p, const double *pot_re, const double *pot_im,
+                              double dt, const double *xr, const double *xi, double *lr,
+                              double *li, double *grad_v) {
+    const size_t n = (size_t)p->W * p->H;
+    for (size_t k = 0; k < n; ++k) {
+        double n2 = xr[k] * xr[k] + xi[k] * xi[k];
+        double r = sqrt(n2);
+        double th = p->coupling * n2 + p->lhy_coupling * n2 * r;
+        double dth = p->coupling + 1.5 * p->lhy_coupling * r;
+        double c = cos(th), s = sin(th);
+        double tr = pot_re[k] * xr[k] - pot_im[k] * xi[k];
+        double ti = pot_re[k] * xi[k] + pot_im[k] * xr[k];
+        double pr = c * tr + s * ti, pi = c * ti - s * tr;
+        double q = lr[k] * pi - li[k] * pr;
+        grad_v[k] += dt * q;
+        double ur = c * lr[k] - s * li[k], ui = c * li[k] + s * lr[k];
+        double nr = pot_re[k] * ur + pot_im[k] * ui + 2. * dth * q * xr[k];
+        double ni = pot_re[k] * ui - pot_im[k] * ur + 2. * dth * q * xi[k];
+        lr[k] = nr;
+        li[k] = ni;
+    }
+}
+
+int tso_adjoint_real(const tso_params *p, const double *pot_re, const double *pot_im, double dt,
+                     const double *psi0_re, const double *psi0_im, int steps,
+                     const double *lam_re, const double *lam_im, double *grad_v,
+                     double *grad_re, double *grad_im) {
+    const size_t n = (size_t)p->W * p->H;
+    const int vert = p->H > 1;
+    if (p->imag_time || p->periodic_x || p->periodic_y || (p->alpha_x != 0. && p->alpha_y != 0.))
+        return 1;
+    double *states = (double *)malloc(sizeof(double) * 2 * n * (size_t)steps);
+    double *xr = (double *)malloc(sizeof(double) * n), *xi = (double *)malloc(sizeof(double) * n);
+    if (!states || !xr || !xi) {
+        free(states); free(xr); free(xi);
+        return 2;
+    }
+    double *cr = states, *ci = states + n;
+    memcpy(cr, psi0_re, sizeof(double) * n);
+    memcpy(ci, psi0_im, sizeof(double) * n);
+    for (int s = 1; s < steps; ++s) {
+        double *pr = states + 2 * n * (size_t)(s - 1), *nr = states + 2 * n * (size_t)s;
+        memcpy(nr, pr, sizeof(double) * 2 * n);
+        tso_full_step(p, nr, nr + n, pot_re, pot_im);
+    }
+    memcpy(grad_re, lam_re, sizeof(double) * n);
+    memcpy(grad_im, lam_im, sizeof(double) * n);
+    memset(grad_v, 0, sizeof(double) * n);
+    for (int s = steps - 1; s >= 0; --s) {
+        memcpy(xr, states + 2 * n * (size_t)s, sizeof(double) * n);
+        memcpy(xi, states + 2 * n * (size_t)s + n, sizeof(double) * n);
+        forward_half(p, xr, xi);  /* x: the potential stage's input */
+        if (vert) sweep_vertical(p, 0, p->aV, -p->bV, grad_re, grad_im);
+        sweep_horizontal(p, 0, p->aH, -p->bH, grad_re, grad_im);
+        if (vert) sweep_vertical(p, 1, p->aV, -p->bV, grad_re, grad_im);
+        sweep_horizontal(p, 1, p->aH, -p->bH, grad_re, grad_im);
+        adjoint_potential(p, pot_re, pot_im, dt, xr, xi, grad_re, grad_im, grad_v);
+        sweep_horizontal(p, 1, p->aH, -p->bH, grad_re, grad_im);
+        if (vert) sweep_vertical(p, 1, p->aV, -p->bV, grad_re, grad_im);
+        sweep_horizontal(p, 0, p->aH, -p->bH, grad_re, grad_im);
+        if (vert) sweep_vertical(p, 0, p->aV, -p->bV, grad_re, grad_im);
+    }
+    free(states); free(xr); free(xi);
+    return 0;
+}
+
 /* ---- step constants (src/cpukernel.cpp:185-217) and table (src/solver.cpp:74-109) */
 void tso_init_constants(tso_params *p, double delta_t, double mass, double g, double g_lhy,
                         double omega, double delta_x, double delta_y) {

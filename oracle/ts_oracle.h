@@ -46,6 +46,15 @@ void tso_full_step(const tso_params *p, double *re, double *im, const double *po
                    const double *pot_im);
 void tso_halo_exchange(const tso_params *p, double *re, double *im);
 double tso_squared_norm(const tso_params *p, const double *re, const double *im);
+/* Reverse mode of `steps` real-time steps on a closed tile (test check of
+ * the B200 adjoint; not in the reference): from lambda = dL/dpsi(T) (real
+ * pairs) to dL/dV (dt = time step) and dL/dpsi0.  Returns non-zero for
+ * unsupported tiles or when out of memory. */
+int tso_adjoint_real(const tso_params *p, const double *pot_re, const double *pot_im, double dt,
+                     const double *psi0_re, const double *psi0_im, int steps,
+                     const double *lam_re, const double *lam_im, double *grad_v,
+                     double *grad_re, double *grad_im);
+
 void tso_evolve(const tso_params *p, double *re, double *im, const double *pot_re,
                 const double *pot_im, int iterations);
 void tso_coordinates(const tso_geometry *g, int x_in, int y_in, double *x_out, double *y_out);

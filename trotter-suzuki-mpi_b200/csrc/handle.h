@@ -60,4 +60,8 @@ inline int slot_bytes(int C, bool fp32, bool imag) {
 template <typename T>
 void fill_step_constants(const ts_b200_kernel *k, tsb::StepArgs<T> &a);
 
+// One fused step of the tile from device buffer `in` to `out` (tile layout,
+// row pitch k->P), on the tile's stream; the tile's own buffers are untouched.
+int launch_step_buffers(ts_b200_kernel *k, const void *in, void *out);
+
 }  // namespace tsbh

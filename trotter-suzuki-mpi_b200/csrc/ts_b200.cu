@@ -532,8 +532,10 @@ template void tsbh::fill_step_constants<float>(const ts_b200_kernel *, StepArgs<
 
 namespace {
 
+// One fused step from buffer `in` to buffer `out` (no buffer flip, no halo);
+// dry: configure and size the scratch only.
 template <typename T>
-int launch_step_t(ts_b200_kernel *k, int exchange, bool dry = false) {
+int launch_step_buffers_t(ts_b200_kernel *k, const void *in, void *out, bool dry) {
     int strips, segs, blocks;
     size_t smem;
     if (k->resident_blocks <= 0) {
@@ -558,8 +560,8 @@ int launch_step_t(ts_b200_kernel *k, int exchange, bool dry = false) {
     }
     if (dry) blocks = 0;
     StepArgs<T> a{};
-    a.psi_in = k->psi[k->cur];
-    a.psi_out = k->psi[1 - k->cur];
+    a.psi_in = in;
+    a.psi_out = out;
     tsbh::fill_step_constants(k, a);
     a.n_strips = strips;
     a.n_segs = segs;
@@ -569,8 +571,14 @@ int launch_step_t(ts_b200_kernel *k, int exchange, bool dry = false) {
     cudaError_t e = dispatch_step<T>(k->C, k->imag, k->rot, k->phase, a, k->warps, smem, blocks,
                                      k->stream, nullptr);
     if (e != cudaSuccess) return cuda_fail(k, e, "step kernel launch");
-    if (dry) return TS_B200_OK;
-    g_launches.fetch_add(1, std::memory_order_relaxed);
+    if (!dry) g_launches.fetch_add(1, std::memory_order_relaxed);
+    return TS_B200_OK;
+}
+
+template <typename T>
+int launch_step_t(ts_b200_kernel *k, int exchange, bool dry = false) {
+    const int s = launch_step_buffers_t<T>(k, k->psi[k->cur], k->psi[1 - k->cur], dry);
+    if (s || dry) return s;
     k->cur = 1 - k->cur;
     if (exchange) {
         const int st = launch_halo_t<T>(k);
@@ -582,6 +590,15 @@ int launch_step_t(ts_b200_kernel *k, int exchange, bool dry = false) {
 int launch_step(ts_b200_kernel *k, int exchange, bool dry = false) {
     return k->fp32 ? launch_step_t<float>(k, exchange, dry) : launch_step_t<double>(k, exchange, dry);
 }
+
+}  // namespace
+
+int tsbh::launch_step_buffers(ts_b200_kernel *k, const void *in, void *out) {
+    return k->fp32 ? launch_step_buffers_t<float>(k, in, out, false)
+                   : launch_step_buffers_t<double>(k, in, out, false);
+}
+
+namespace {
 
 int kernels_per_step(const ts_b200_kernel *k, int exchange) {
     return 1 + ((exchange && (k->d.periodic_x || k->d.periodic_y)) ? 1 : 0);

@@ -228,6 +228,14 @@ int tsh_solver_kernel_handle(void *svp, void **out) {
     });
 }
 
+int tsh_make_desc(void *lattice, void *hamiltonian, double delta_t, double norm, int imag_time,
+                  int precision, ts_b200_desc *out) {
+    return guard([&] {
+        *out = b200::make_desc(static_cast<Lattice *>(lattice), static_cast<Hamiltonian *>(hamiltonian),
+                               delta_t, norm, imag_time != 0, precision);
+    });
+}
+
 int tsh_solver_free(void *svp) {
     return guard([&] { delete static_cast<Solver *>(svp); });
 }

@@ -9,7 +9,7 @@ Batch -- many Kernel tiles of uneven sizes advanced by one persistent launch per
 from ._capi import B200Error, Desc, EnergyParams  # noqa: F401
 from .api import (ExponentialState, GaussianState, Hamiltonian, Hamiltonian2Component,  # noqa: F401
                   HarmonicPotential, Lattice1D, Lattice2D, Potential, SinusoidState, Solver,
-                  SolverBatch, State, map_lattice_to_coordinate_space)
+                  SolverBatch, State, make_desc, map_lattice_to_coordinate_space)
 from .kernel import FP32, FP64, Batch, Kernel, launch_count, version  # noqa: F401
 
 __version__ = "1.6.2+b200"

@@ -100,6 +100,13 @@ SIGNATURES = {
     "ts_b200_batch_autotune": (_I, [_VP, _I, _I]),
     "ts_b200_batch_launch_info": (_I, [_VP, C.POINTER(LaunchShape)]),
     "ts_b200_batch_last_error": (C.c_char_p, [_VP]),
+    "ts_b200_adjoint_create": (_I, [C.POINTER(Desc), C.c_double, _I, _I, C.POINTER(_VP)]),
+    "ts_b200_adjoint_destroy": (None, [_VP]),
+    "ts_b200_adjoint_set_stream": (_I, [_VP, _VP]),
+    "ts_b200_adjoint_forward": (_I, [_VP, _VP, _VP, _VP]),
+    "ts_b200_adjoint_backward": (_I, [_VP, _VP, _VP, _VP]),
+    "ts_b200_adjoint_synchronize": (_I, [_VP]),
+    "ts_b200_adjoint_last_error": (C.c_char_p, [_VP]),
     "ts_b200_host_alloc": (_I, [C.POINTER(_VP), _SZ]),
     "ts_b200_host_free": (_I, [_VP]),
     "ts_b200_last_error": (C.c_char_p, [_VP]),
@@ -136,9 +143,11 @@ def lib():
     return _lib
 
 
-def check(status, handle=None, batch=None):
+def check(status, handle=None, batch=None, adjoint=None):
     if status != OK:
-        if batch:
+        if adjoint:
+            msg = lib().ts_b200_adjoint_last_error(adjoint).decode()
+        elif batch:
             msg = lib().ts_b200_batch_last_error(batch).decode()
         else:
             msg = lib().ts_b200_last_error(handle).decode() if handle else ""

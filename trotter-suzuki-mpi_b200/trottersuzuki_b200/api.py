@@ -75,6 +75,7 @@ def host():
             "tsh_solver_update_parameters": (i, [vp]),
             "tsh_solver_kernel_handle": (i, [vp, P(vp)]),
             "tsh_solver_free": (i, [vp]),
+            "tsh_make_desc": (i, [vp, vp, d, d, i, i, P(_capi.Desc)]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -468,6 +469,15 @@ class Solver(_Handle):
         out = C.c_void_p()
         _chk(host().tsh_solver_kernel_handle(self._h, C.byref(out)))
         return out.value
+
+
+def make_desc(grid, hamiltonian, delta_t, imag_time=False, norm=0.0, precision=0):
+    """The C-ABI step descriptor (include/ts_b200.h) of a lattice and Hamiltonian,
+    with the reference CPUBlock's constants (src/cpukernel.cpp:172-272)."""
+    out = _capi.Desc()
+    _chk(host().tsh_make_desc(grid._h, hamiltonian._h, float(delta_t), float(norm),
+                              int(bool(imag_time)), int(precision), C.byref(out)))
+    return out
 
 
 class SolverBatch:
