@@ -616,6 +616,154 @@ def run_batch_workload(args, rank, world, local, pg):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------- differentiation workload
+# 512 x 512 over length 20, real time, FP64, closed boundaries; V = harmonic
+# (omega 1) + 16 Gaussians (amplitude U[-0.5, 0.5], width U[1, 3], centres
+# uniform over the box); psi0 = normalised Gaussian (sigma 1) at (-3, 0) times
+# exp(2 i x); dt = 1e-4, 3000 steps; L = sum_{x > 0} |psi(T)|^2 dx dy.  Run
+# linear (inverse steps) and with g = 50 (checkpoints every 100 steps).
+ADJ_N = 512
+ADJ_LENGTH = 20.0
+ADJ_DT = 1e-4
+ADJ_STEPS = 3000
+ADJ_SEED = 20240603
+ADJ_SITES = 64
+
+
+def adjoint_setup(n=ADJ_N, seed=ADJ_SEED):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    dx = ADJ_LENGTH / n
+    x = (np.arange(n) + 0.5) * dx - ADJ_LENGTH * 0.5
+    X, Y = np.meshgrid(x, x)
+    V = 0.5 * (X * X + Y * Y)
+    amp = rng.uniform(-0.5, 0.5, 16)
+    wid = rng.uniform(1.0, 3.0, 16)
+    cen = rng.uniform(-ADJ_LENGTH * 0.5, ADJ_LENGTH * 0.5, (16, 2))
+    for a, w, (cx, cy) in zip(amp, wid, cen):
+        V += a * np.exp(-((X - cx) ** 2 + (Y - cy) ** 2) / (2 * w * w))
+    psi0 = np.exp(-0.5 * ((X + 3.0) ** 2 + Y ** 2)) * np.exp(2j * X)
+    psi0 /= math.sqrt((np.abs(psi0) ** 2).sum() * dx * dx)
+    mask = (X > 0).astype(np.float64)
+    # FD sites where the wave packet travels (|x|, |y| < 6)
+    sites = [(int(a), int(b)) for a, b in
+             zip(rng.integers(int(n * 0.2), int(n * 0.8), ADJ_SITES),
+                 rng.integers(int(n * 0.2), int(n * 0.8), ADJ_SITES))]
+    return V, psi0.astype(np.complex128), mask, dx, sites
+
+
+def run_adjoint_workload(args, rank, world, local, pg):
+    import torch
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    import trottersuzuki_b200 as ts
+    from trottersuzuki_b200 import launch_count
+    from trottersuzuki_b200.adjoint import AdjointEngine
+    V, psi0, mask, dx, sites = adjoint_setup()
+    dA = dx * dx
+    stream = torch.cuda.Stream(device=device)
+    m = torch.tensor(mask, device=device)
+    out = {}
+    clk = None
+    launches = 0
+    for label, g, every in (("linear_inverse_steps", 0.0, 0), ("gpe_g50_checkpoint100", 50.0, 100)):
+        grid = ts.Lattice2D(ADJ_N, ADJ_LENGTH)
+        ham = ts.Hamiltonian(grid, None, 1.0, g)
+        desc = ts.make_desc(grid, ham, ADJ_DT)
+        eng = AdjointEngine(desc, ADJ_DT, ADJ_STEPS, every)
+        with torch.cuda.stream(stream):
+            Vt = torch.tensor(V, dtype=torch.float64, device=device)
+            p0 = torch.tensor(psi0, dtype=torch.complex128, device=device)
+
+            def loss_of(psi_t):
+                return float(((psi_t.abs() ** 2) * m).sum().item() * dA)
+
+            fwd_ms, bwd_ms = [], []
+            for it in range(args.warmup + args.steps):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e2 = torch.cuda.Event(enable_timing=True)
+                l0 = launch_count()
+                timed = it >= args.warmup
+                clocks = Clocks(local) if (timed and label == "linear_inverse_steps" and
+                                            it == args.warmup) else None
+                if clocks:
+                    clocks.__enter__()
+                e0.record(stream)
+                psi_t = eng.forward(Vt, p0)
+                e1.record(stream)
+                grad_t = (2.0 * dA) * m * psi_t
+                gv, gp = eng.backward(grad_t)
+                e2.record(stream)
+                e2.synchronize()
+                if clocks:
+                    clocks.__exit__(None, None, None)
+                    clk = clocks.summary()
+                if timed:
+                    fwd_ms.append(e0.elapsed_time(e1))
+                    bwd_ms.append(e1.elapsed_time(e2))
+                    if label == "linear_inverse_steps":
+                        launches = launch_count() - l0
+            L0 = loss_of(psi_t)
+            gv = gv.cpu().numpy()
+            gp = gp.cpu().numpy()
+            # central differences of the B200 forward pass at the seeded sites
+            hv, hp = 1e-4, 1e-5
+            fd_v, fd_r, fd_i = [], [], []
+            for (y, x) in sites:
+                e = torch.zeros_like(Vt)
+                e[y, x] = hv
+                fd_v.append((loss_of(eng.forward(Vt + e, p0)) - loss_of(eng.forward(Vt - e, p0)))
+                            / (2 * hv))
+                ec = torch.zeros_like(p0)
+                ec[y, x] = hp
+                fd_r.append((loss_of(eng.forward(Vt, p0 + ec)) - loss_of(eng.forward(Vt, p0 - ec)))
+                            / (2 * hp))
+                fd_i.append((loss_of(eng.forward(Vt, p0 + 1j * ec))
+                             - loss_of(eng.forward(Vt, p0 - 1j * ec))) / (2 * hp))
+        ys, xs = zip(*sites)
+
+        def rel(a, b):
+            b = np.asarray(b)
+            return float(np.abs(np.asarray(a) - b).max() / np.abs(b).max())
+
+        f = statistics.median(fwd_ms)
+        b = statistics.median(bwd_ms)
+        out[label] = {
+            "loss": L0, "forward_ms": f, "adjoint_ms": b, "adjoint_over_forward": b / f,
+            "forward_site_steps_per_s": ADJ_N * ADJ_N * ADJ_STEPS / (f * 1e-3),
+            "fd_rel_err": {"dL_dV": rel(gv[ys, xs], fd_v), "dL_dre_psi0": rel(gp.real[ys, xs], fd_r),
+                           "dL_dim_psi0": rel(gp.imag[ys, xs], fd_i)},
+            "fd_sites": len(sites), "fd_step": {"V": hv, "psi0": hp},
+            "checkpoint_every": every, "g": g}
+        eng.close()
+    if rank != 0:
+        return
+    lin = out["linear_inverse_steps"]
+    peak, peak_kind = measured_peak()
+    # adjoint step: psi, lambda in and out, table, dL/dV in and out
+    bytes_step = 96.0 * ADJ_N * ADJ_N
+    achieved = bytes_step * ADJ_STEPS / (lin["adjoint_ms"] * 1e-3) / 1e9
+    line = {
+        "metric": "adjoint/forward cost", "value": lin["adjoint_over_forward"], "unit": "ratio",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": lin["forward_ms"] + lin["adjoint_ms"], "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "adjoint512_real_time", "lattice": f"{ADJ_N}x{ADJ_N}",
+                   "length": ADJ_LENGTH, "dt": ADJ_DT, "trotter_steps": ADJ_STEPS,
+                   "boundary": "closed", "seed": ADJ_SEED, "loss": "sum_{x>0} |psi(T)|^2 dx dy",
+                   "parallelism": f"replicas{world}",
+                   "l2": "state 4 MiB is L2-resident: a latency-bound size"},
+        "runs": out,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                     "algorithmic_bytes_per_launch": bytes_step,
+                     "kernel": "tsb::adjoint_kernel<inverse steps>"},
+        "clocks": clk,
+        "gpu_launches": launches,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -626,7 +774,7 @@ def main():
                     help="seconds of reference CPU work per sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32", action="store_true")
-    ap.add_argument("--workload", choices=["gpe_imaginary_time_2048", "batch512"],
+    ap.add_argument("--workload", choices=["gpe_imaginary_time_2048", "batch512", "adjoint512"],
                     default="gpe_imaginary_time_2048")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
@@ -636,6 +784,8 @@ def main():
             run_reference_arm(args, rank, world, pg)
         elif args.workload == "batch512":
             run_batch_workload(args, rank, world, local, pg)
+        elif args.workload == "adjoint512":
+            run_adjoint_workload(args, rank, world, local, pg)
         else:
             run_b200_arm(args, rank, world, local, pg)
     finally:

@@ -38,12 +38,16 @@ struct ts_b200_adjoint {
     int *error = nullptr;
     int seg_h = 32, warps = 2, ring = 4, blocks = 0;
     bool forward_done = false;
+    void *state0 = nullptr;           // a segment's first state (graph-fixed address)
+    cudaGraphExec_t inv_graph = nullptr;  // kInvGraphSteps inverse adjoint steps
+    cudaGraphExec_t seg_graph = nullptr;  // one full checkpoint segment
     std::string err;
 };
 
 namespace {
 
 constexpr int kAdjThreadsPerWarp = 32;
+constexpr int kInvGraphSteps = 32;  // even: the buffers end where they started
 
 int afail(ts_b200_adjoint *a, int status, const std::string &msg) {
     if (a) a->err = msg;
@@ -165,6 +169,44 @@ int tile_status(ts_b200_adjoint *a, int s) {
     return s;
 }
 
+// Capture the launches `body` queues on the tile's stream into *exec.
+template <class F>
+int capture(ts_b200_adjoint *a, cudaGraphExec_t *exec, F body) {
+    cudaStream_t st = a->k->stream;
+    cudaGraph_t g = nullptr;
+    TSBA_CHECK(a, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    const uint64_t before = g_launches.load();
+    const int s = body();
+    cudaError_t e = cudaStreamEndCapture(st, &g);
+    g_launches.store(before);  // counted when replayed
+    if (s != TS_B200_OK || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        (void)cudaGetLastError();
+        if (s != TS_B200_OK) return s;
+        return acuda(a, e, "adjoint graph capture");
+    }
+    e = cudaGraphInstantiate(exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return acuda(a, e, "adjoint graph instantiate");
+    return TS_B200_OK;
+}
+
+// Reverse pass of one checkpoint segment of `len` steps starting from the
+// state in a->state0: recompute states 1 .. len-1, then len adjoint steps
+// (lambda ping-pongs from lam[l]).
+int segment_pass(ts_b200_adjoint *a, int len, int l) {
+    int s = TS_B200_OK;
+    for (int i = 1; i < len && s == TS_B200_OK; ++i)
+        s = tile_status(a, tsbh::launch_step_buffers(a->k, i == 1 ? a->state0 : seg_at(a, i - 1),
+                                                     seg_at(a, i)));
+    for (int i = len - 1; i >= 0 && s == TS_B200_OK; --i) {
+        const void *psi_n = i == 0 ? a->state0 : seg_at(a, i);
+        s = adj_step(a, 1, psi_n, nullptr, a->lam[l], a->lam[l ^ 1]);
+        l ^= 1;
+    }
+    return s;
+}
+
 }  // namespace
 
 extern "C" {
@@ -206,6 +248,7 @@ int ts_b200_adjoint_create(const ts_b200_desc *d, double delta_t, int steps, int
         a->n_ckpt = (steps + a->every - 1) / a->every;  // states at 0, every, 2 every, ...
         alloc(&a->ckpt, sb * a->n_ckpt);
         if (a->every > 1) alloc(&a->seg, sb * (a->every - 1));
+        alloc(&a->state0, sb);
     }
     if (e == cudaSuccess) {
         int bps = 0;
@@ -213,6 +256,11 @@ int ts_b200_adjoint_create(const ts_b200_desc *d, double delta_t, int steps, int
         e = launch_adj(a, a->every > 0 ? 1 : 0, a->k->phase, x, 0, &bps);
         if (e == cudaSuccess && bps < 1) e = cudaErrorInvalidConfiguration;
         a->blocks = bps * a->k->num_sms;
+        // one round of tasks over the resident warps (the tile is often small)
+        const int strips = div_up(a->W, AdjVariant<0, 0>::WO);
+        const int per_strip = std::max(1, a->blocks * a->warps / strips);
+        a->seg_h = std::max(8, div_up(a->H, per_strip));
+        a->seg_h += a->seg_h & 1;
     }
     if (e != cudaSuccess) {
         const int st = e == cudaErrorMemoryAllocation ? TS_B200_OUT_OF_MEMORY : TS_B200_CUDA_ERROR;
@@ -232,6 +280,9 @@ void ts_b200_adjoint_destroy(ts_b200_adjoint *a) {
     cudaFree(a->ckpt);
     cudaFree(a->seg);
     cudaFree(a->error);
+    cudaFree(a->state0);
+    if (a->inv_graph) cudaGraphExecDestroy(a->inv_graph);
+    if (a->seg_graph) cudaGraphExecDestroy(a->seg_graph);
     ts_b200_destroy(a->k);
     delete a;
 }
@@ -282,8 +333,29 @@ int ts_b200_adjoint_backward(ts_b200_adjoint *a, const void *grad_psi_t, double 
     int l = 0;
     int s = TS_B200_OK;
     if (a->every == 0) {
+        // ping-pong from (psi[cur], lam[0]); runs of kInvGraphSteps replayed
         int c = k->cur;  // psi(T)
-        for (int n = a->steps - 1; n >= 0 && s == TS_B200_OK; --n) {
+        int n = a->steps;
+        if (n >= kInvGraphSteps && c == 0) {
+            if (!a->inv_graph) {
+                s = capture(a, &a->inv_graph, [&] {
+                    int st = TS_B200_OK, cc = 0, ll = 0;
+                    for (int i = 0; i < kInvGraphSteps && st == TS_B200_OK; ++i) {
+                        st = adj_step(a, 0, k->psi[cc], k->psi[cc ^ 1], a->lam[ll], a->lam[ll ^ 1]);
+                        cc ^= 1;
+                        ll ^= 1;
+                    }
+                    return st;
+                });
+                if (s) return s;
+            }
+            while (n >= kInvGraphSteps) {
+                TSBA_CHECK(a, cudaGraphLaunch(a->inv_graph, k->stream));
+                g_launches.fetch_add(kInvGraphSteps, std::memory_order_relaxed);
+                n -= kInvGraphSteps;
+            }
+        }
+        for (; n > 0 && s == TS_B200_OK; --n) {
             s = adj_step(a, 0, k->psi[c], k->psi[c ^ 1], a->lam[l], a->lam[l ^ 1]);
             c ^= 1;
             l ^= 1;
@@ -292,14 +364,24 @@ int ts_b200_adjoint_backward(ts_b200_adjoint *a, const void *grad_psi_t, double 
     } else {
         for (int j = a->n_ckpt - 1; j >= 0 && s == TS_B200_OK; --j) {
             const int len = std::min(a->every, a->steps - j * a->every);
-            // states 1 .. len-1 of the segment from its checkpoint
-            for (int i = 1; i < len && s == TS_B200_OK; ++i)
-                s = tile_status(a, tsbh::launch_step_buffers(
-                                       k, i == 1 ? ckpt_at(a, j) : seg_at(a, i - 1), seg_at(a, i)));
-            for (int i = len - 1; i >= 0 && s == TS_B200_OK; --i) {
-                const void *psi_n = i == 0 ? ckpt_at(a, j) : seg_at(a, i);
-                s = adj_step(a, 1, psi_n, nullptr, a->lam[l], a->lam[l ^ 1]);
-                l ^= 1;
+            TSBA_CHECK(a, cudaMemcpyAsync(a->state0, ckpt_at(a, j), state_bytes(a),
+                                          cudaMemcpyDeviceToDevice, k->stream));
+            if (len == a->every && (len & 1) == 0) {
+                // full segments of an even length leave lambda in lam[l]
+                if (!a->seg_graph) {
+                    s = capture(a, &a->seg_graph, [&] { return segment_pass(a, len, 0); });
+                    if (s) return s;
+                }
+                if (l != 0) {  // the graph starts from lam[0]
+                    TSBA_CHECK(a, cudaMemcpyAsync(a->lam[0], a->lam[1], state_bytes(a),
+                                                  cudaMemcpyDeviceToDevice, k->stream));
+                    l = 0;
+                }
+                TSBA_CHECK(a, cudaGraphLaunch(a->seg_graph, k->stream));
+                g_launches.fetch_add(2 * len - 1, std::memory_order_relaxed);
+            } else {
+                s = segment_pass(a, len, l);
+                if (len & 1) l ^= 1;
             }
         }
     }
