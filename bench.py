@@ -764,6 +764,132 @@ def run_adjoint_workload(args, rank, world, local, pg):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------- precision workload
+# 8192 x 8192 periodic lattice over length 40, real-time GPE in the rotating
+# frame: harmonic trap omega = 1, g = 500, Omega = 0.7, dt = 5e-5, 5000 steps.
+# psi0 = Thomas-Fermi profile sqrt(max(0, mu - V) / g) (norm 1: mu = sqrt(g / pi)
+# for this trap) times exp(i theta_k) windings around 8 seeded centres uniform
+# in the disk of radius 10.  The FP32-storage path runs against the FP64 path
+# (the oracle here: the reference refuses periodic boundaries with a rotating
+# frame, src/model.cpp:936-940).
+VORTEX_N = 8192
+VORTEX_LENGTH = 40.0
+VORTEX_G = 500.0
+VORTEX_OMEGA = 0.7
+VORTEX_DT = 5e-5
+VORTEX_STEPS = 5000
+VORTEX_SEED = 20240604
+VORTEX_BYTES = {"fp64": 48, "fp32": 24}
+
+
+def vortex_initial(grid):
+    from trottersuzuki_b200.api import _coordinate_grid
+    X, Y = _coordinate_grid(grid)
+    rng = np.random.Generator(np.random.PCG64(VORTEX_SEED))
+    r = 10.0 * np.sqrt(rng.uniform(0.0, 1.0, 8))
+    phi = rng.uniform(0.0, 2.0 * math.pi, 8)
+    centres = np.stack([r * np.cos(phi), r * np.sin(phi)], axis=1)
+    mu = math.sqrt(VORTEX_G / math.pi)
+    dens = np.maximum(0.0, (mu - 0.5 * (X * X + Y * Y)) / VORTEX_G)
+    psi = np.sqrt(dens).astype(np.complex128)
+    for cx, cy in centres:
+        psi *= np.exp(1j * np.arctan2(Y - cy, X - cx))
+    return psi, centres
+
+
+def run_vortex_workload(args, rank, world, local, pg):
+    import torch
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    import trottersuzuki_b200 as ts
+    from trottersuzuki_b200 import _capi, launch_count
+    L = _capi.lib()
+    stream = torch.cuda.Stream(device=device)
+    res = {}
+    clk = None
+    launches = 0
+    psi64 = None
+    for kernel_type, prec in (("gpu", "fp64"), ("gpu_fp32", "fp32")):
+        grid = ts.Lattice2D(VORTEX_N, VORTEX_LENGTH, periodic_x_axis=True, periodic_y_axis=True,
+                            angular_velocity=VORTEX_OMEGA)
+        state = ts.State(grid)
+        psi0, centres = vortex_initial(grid)
+        state.init_state_matrix(psi0.real, psi0.imag)
+        pot = ts.HarmonicPotential(grid, 1.0, 1.0)
+        ham = ts.Hamiltonian(grid, pot, 1.0, VORTEX_G, 0.0, VORTEX_OMEGA)
+        solver = ts.Solver(grid, state, ham, VORTEX_DT, kernel_type=kernel_type)
+        e0_energy = solver.get_total_energy()
+        # warm-up steps, then the state is reset and the kernel rebuilt from it
+        solver.evolve(-args.warmup)
+        torch.cuda.synchronize()
+        state.init_state_matrix(psi0.real, psi0.imag)
+        solver.update_parameters()
+        solver.evolve(0)
+        h = solver.kernel_handle()
+        _capi.check(L.ts_b200_set_stream(C.c_void_p(h), C.c_void_p(stream.cuda_stream)))
+        torch.cuda.synchronize()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        l0 = launch_count()
+        with Clocks(local) as clocks:
+            ev0.record(stream)
+            solver.evolve(-VORTEX_STEPS)
+            ev1.record(stream)
+            ev1.synchronize()
+        ms = max_over_ranks(ev0.elapsed_time(ev1), pg, device)
+        if prec == "fp64":
+            clk = clocks.summary()
+            launches = launch_count() - l0
+        solver.evolve(0)  # copies the tile back
+        psi = np.array(state.p_real) + 1j * np.array(state.p_imag)
+        sh = VORTEX_N * VORTEX_N
+        res[prec] = {"value": world * sh * VORTEX_STEPS / (ms * 1e-3), "ms": ms,
+                     "energy": solver.get_total_energy(), "norm": solver.get_squared_norm(),
+                     "initial_energy": e0_energy}
+        if prec == "fp64":
+            psi64 = psi
+            inner = (slice(grid.inner_start_y - grid.start_y, grid.inner_end_y - grid.start_y),
+                     slice(grid.inner_start_x - grid.start_x, grid.inner_end_x - grid.start_x))
+        else:
+            d = psi[inner] - psi64[inner]
+            res["errors"] = {
+                "psi_rel_l2": float(np.linalg.norm(d) / np.linalg.norm(psi64[inner])),
+                "psi_max_abs": float(np.abs(d).max()),
+                "psi_max_abs_over_max": float(np.abs(d).max() / np.abs(psi64[inner]).max()),
+                "norm_rel": abs(res["fp32"]["norm"] - res["fp64"]["norm"]) / abs(res["fp64"]["norm"]),
+                "energy_rel": abs(res["fp32"]["energy"] - res["fp64"]["energy"]) /
+                              abs(res["fp64"]["energy"])}
+        del solver, ham, pot, state, grid
+        torch.cuda.synchronize()
+    if rank != 0:
+        return
+    peak, peak_kind = measured_peak()
+    ms_launch = res["fp64"]["ms"] / VORTEX_STEPS
+    achieved = VORTEX_BYTES["fp64"] * VORTEX_N * VORTEX_N / (ms_launch * 1e-3) / 1e9
+    line = {
+        "metric": "site-steps/s", "value": res["fp64"]["value"], "unit": "site-steps/s",
+        "n_gpus": world, "steps": 1, "warmup": args.warmup,
+        "ms_per_step": res["fp64"]["ms"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "vortex8192_precision", "lattice": f"{VORTEX_N}x{VORTEX_N}",
+                   "length": VORTEX_LENGTH, "boundary": "periodic", "g": VORTEX_G,
+                   "omega_rot": VORTEX_OMEGA, "dt": VORTEX_DT, "trotter_steps": VORTEX_STEPS,
+                   "initial": "Thomas-Fermi x 8 windings (radius 10)", "seed": VORTEX_SEED,
+                   "parallelism": f"replicas{world}",
+                   "l2": "inputs larger than L2: 3 GiB moved per Trotter step in FP64"},
+        "fp64": res["fp64"],
+        "fp32_store": dict(res["fp32"], speedup_vs_fp64=res["fp32"]["value"] / res["fp64"]["value"]),
+        "fp32_vs_fp64_errors": res["errors"],
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                     "algorithmic_bytes_per_launch": VORTEX_BYTES["fp64"] * VORTEX_N * VORTEX_N,
+                     "kernel": "tsb::step_kernel<double, C=2, real, rotating frame, GPE> + halo"},
+        "clocks": clk,
+        "gpu_launches": launches,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -774,7 +900,8 @@ def main():
                     help="seconds of reference CPU work per sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32", action="store_true")
-    ap.add_argument("--workload", choices=["gpe_imaginary_time_2048", "batch512", "adjoint512"],
+    ap.add_argument("--workload", choices=["gpe_imaginary_time_2048", "batch512", "adjoint512",
+                                           "vortex8192"],
                     default="gpe_imaginary_time_2048")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
@@ -786,6 +913,8 @@ def main():
             run_batch_workload(args, rank, world, local, pg)
         elif args.workload == "adjoint512":
             run_adjoint_workload(args, rank, world, local, pg)
+        elif args.workload == "vortex8192":
+            run_vortex_workload(args, rank, world, local, pg)
         else:
             run_b200_arm(args, rank, world, local, pg)
     finally:
