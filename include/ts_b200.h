@@ -204,7 +204,8 @@ int ts_b200_set_launch(ts_b200_kernel *k, int cells_per_lane, int segment_rows, 
  *
  * A batch advances many tiles of uneven sizes together: each Trotter step is
  * one persistent launch over the tasks of all tiles (plus, in imaginary time,
- * one per-tile norm reduction launch, and for periodic tiles one batched halo
+ * one per-tile norm reduction launch, in FP32 real time one launch advancing
+ * the tiles' coefficient schedules, and for periodic tiles one batched halo
  * refresh), 32-step runs replayed from a CUDA graph.  The batch borrows the
  * tiles' device state: set states and tables, read results, energies and
  * norms through the tiles' own calls.  All tiles must share precision, time

@@ -70,6 +70,13 @@ __global__ void batch_norm_kernel(const TileNorm *tn, const double *task_norm) {
     }
 }
 
+// FP32 real time: every tile's coefficient schedule advances by one step
+// (the single-tile kernel's last block does this for its own tile).
+__global__ void batch_step_count_kernel(const TileNorm *tn, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) tn[i].scal->step += 1u;
+}
+
 // blockIdx.y: periodic tile; the x blocks stride over its destination cells.
 template <typename T>
 __global__ void batch_halo_kernel(const StepArgs<T> *inst, const TileHalo *th) {
@@ -278,6 +285,13 @@ int launch_batch_step(ts_b200_batch *b, int p, bool exchange, bool renorm_pass =
     cudaError_t e = launch_batch_kernel<T>(b, a, blocks, nullptr);
     if (e != cudaSuccess) return bcuda(b, e, "batch step launch");
     g_launches.fetch_add(1, std::memory_order_relaxed);
+    if (b->fp32 && !b->imag && renorm_pass) {
+        const int n = (int)b->k.size();
+        batch_step_count_kernel<<<div_up(n, 256), 256, 0, b->stream>>>(b->d_norm, n);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return bcuda(b, e, "batch step count launch");
+        g_launches.fetch_add(1, std::memory_order_relaxed);
+    }
     if (b->imag && renorm_pass) {
         batch_norm_kernel<<<(unsigned)b->k.size(), kNormThreads, 0, b->stream>>>(b->d_norm,
                                                                                b->d_task_norm);
@@ -297,7 +311,7 @@ int launch_batch_step(ts_b200_batch *b, int p, bool exchange, bool renorm_pass =
 }
 
 int kernels_per_batch_step(const ts_b200_batch *b, bool exchange) {
-    return 1 + (b->imag ? 1 : 0) + ((exchange && b->n_halo > 0) ? 1 : 0);
+    return 1 + ((b->imag || b->fp32) ? 1 : 0) + ((exchange && b->n_halo > 0) ? 1 : 0);
 }
 
 // The batch stream waits for every tile's queued work, or the tiles' streams

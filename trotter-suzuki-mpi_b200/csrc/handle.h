@@ -36,6 +36,7 @@ struct ts_b200_kernel {
     bool auto_seg = true;     // pick the segment height from the resident grid
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
+    float4 *kin_sched = nullptr;  // FP32 real time: per-step kinetic coefficients
     int num_sms = 148;
     int device = 0;
     std::string err;
@@ -47,6 +48,9 @@ namespace tsbh {
 extern std::atomic<uint64_t> g_launches;
 
 inline int div_up(long a, long b) { return (int)((a + b - 1) / b); }
+
+// Entries of the FP32 real-time kinetic coefficient schedule (repeats after).
+constexpr int kSchedLen = 4096;
 
 // Bytes of one ring slot: a row of 32*C cells of psi and of the table.
 inline int slot_bytes(int C, bool fp32, bool imag) {

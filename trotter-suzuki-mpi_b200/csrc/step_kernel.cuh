@@ -55,7 +55,7 @@ struct Scalars {
     unsigned int ticket; // blocks finished in the current launch
     int error;           // non-zero: a bounded wait gave up
     int renorm;          // imaginary-time renormalisation enabled (norm0 != 0)
-    int pad;
+    unsigned int step;   // steps taken (indexes the coefficient schedule)
 };
 
 template <typename T>
@@ -71,6 +71,10 @@ struct StepArgs {
     T aH, bH, aV, bV;
     T ca, caa;           // g*dt and g_LHY*dt
     double *partials;    // one per task (imaginary time)
+    // FP32 real time: per-step kinetic coefficients (aH-1, bH, aV-1, bV),
+    // entry scal->step mod sched_len; null: aH..bV above
+    const float4 *kin_sched;
+    int sched_len;
     Scalars *scal;
     double dxdy, norm0;
 };
@@ -735,7 +739,12 @@ __device__ __forceinline__ void warp_setup(Walk<V> &w, unsigned char *smem, int 
     __syncwarp();
 }
 
-// The step constants of one tile.
+// The step constants of one tile.  In FP32 real time the kinetic
+// coefficients come from a per-step schedule: float pairs rounded with the
+// carried error of the previous steps (sigma-delta), so that the coefficient
+// error summed over any run of steps stays within half an ulp instead of
+// growing with the step count (a fixed float pair would rotate every step
+// by the same wrong angle and scale the norm by the same factor).
 template <class V>
 __device__ __forceinline__ void bind_args(Walk<V> &w, const StepArgs<typename V::T> &a) {
     using T = typename V::T;
@@ -744,6 +753,16 @@ __device__ __forceinline__ void bind_args(Walk<V> &w, const StepArgs<typename V:
     w.bH = a.bH;
     w.aV = a.aV;
     w.bV = a.bV;
+    if constexpr (DeltaForm<T>::value && !V::IMAG) {
+        if (a.kin_sched) {
+            const unsigned int step = __ldcg(&a.scal->step);
+            const float4 c = __ldg(&a.kin_sched[step % (unsigned int)a.sched_len]);
+            w.aH = c.x;
+            w.bH = c.y;
+            w.aV = c.z;
+            w.bV = c.w;
+        }
+    }
     w.ca = a.ca;
     w.caa = a.caa;
     w.gpsi_pitch = (size_t)a.P * sizeof(Cx<T>);
@@ -877,6 +896,22 @@ __global__ void __launch_bounds__(128, V::MIN_BLOCKS) step_kernel(StepArgs<typen
          task += gridDim.x * warps)
         run_task(w, a, task);
 
+    if constexpr (!IMAG && DeltaForm<typename V::T>::value) {
+        // the last block to finish advances the schedule's step (every block
+        // has read it: each takes a ticket only after its whole walk)
+        if (a.kin_sched) {
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                __threadfence();
+                if (atomicAdd(&a.scal->ticket, 1u) == gridDim.x - 1) {
+                    a.scal->step += 1u;
+                    a.scal->ticket = 0u;
+                    __threadfence();
+                }
+            }
+        }
+    }
+
     if constexpr (IMAG) {
         // block partial: the block's warps in warp order (a warp's tasks in
         // task order); then the last block to finish sums the block partials
@@ -983,6 +1018,8 @@ __device__ __forceinline__ StepArgs<T> load_tile_args(const StepArgs<T> *p) {
     a.ca = bcast0(__ldg(&p->ca));
     a.caa = bcast0(__ldg(&p->caa));
     a.partials = nullptr;
+    a.kin_sched = bcast0_ptr(ldg_ptr(&p->kin_sched));
+    a.sched_len = bcast0(__ldg(&p->sched_len));
     a.scal = bcast0_ptr(ldg_ptr(&p->scal));
     a.dxdy = bcast0(__ldg(&p->dxdy));
     a.norm0 = bcast0(__ldg(&p->norm0));

@@ -396,6 +396,7 @@ cudaError_t dispatch_step<float>(int C, bool imag, bool rot, int phase, const St
 
 using tsbh::div_up;
 using tsbh::slot_bytes;
+using tsbh::kSchedLen;
 
 }  // namespace
 
@@ -524,6 +525,8 @@ void tsbh::fill_step_constants(const ts_b200_kernel *k, StepArgs<T> &a) {
     a.ca = (T)k->d.coupling;
     a.caa = (T)k->d.lhy_coupling;
     a.scal = k->scal;
+    a.kin_sched = k->kin_sched;
+    a.sched_len = kSchedLen;
     a.dxdy = k->d.delta_x * k->d.delta_y;
     a.norm0 = k->d.norm0;
 }
@@ -696,6 +699,31 @@ int upload_rotation(ts_b200_kernel *k) {
     return TS_B200_OK;
 }
 
+// FP32 real time: kinetic coefficients per step in delta form, each the
+// float nearest to the exact value plus the error carried from the previous
+// entries (first-order sigma-delta), so that any run of consecutive entries
+// sums to the exact total within half an ulp.
+int upload_kinetic_schedule(ts_b200_kernel *k) {
+    const double kx = asin(k->d.b_h), ky = asin(k->d.b_v);
+    const double exact[4] = {cos_m1(kx), k->d.b_h, cos_m1(ky), k->d.b_v};
+    double carry[4] = {0.0, 0.0, 0.0, 0.0};
+    float4 *host = new (std::nothrow) float4[kSchedLen];
+    if (!host) return fail(k, TS_B200_OUT_OF_MEMORY, "host allocation for the kinetic schedule");
+    for (int i = 0; i < kSchedLen; ++i) {
+        float c[4];
+        for (int j = 0; j < 4; ++j) {
+            c[j] = (float)(exact[j] + carry[j]);
+            carry[j] += exact[j] - (double)c[j];
+        }
+        host[i] = make_float4(c[0], c[1], c[2], c[3]);
+    }
+    cudaError_t e = cudaMemcpy(k->kin_sched, host, (size_t)kSchedLen * sizeof(float4),
+                               cudaMemcpyHostToDevice);
+    delete[] host;
+    if (e != cudaSuccess) return cuda_fail(k, e, "kinetic schedule upload");
+    return TS_B200_OK;
+}
+
 int grid_for(size_t n) { return (int)std::max<size_t>(1, std::min<size_t>((n + 255) / 256, 8192)); }
 
 }  // namespace
@@ -770,6 +798,7 @@ int ts_b200_create(const ts_b200_desc *d, ts_b200_kernel **out) {
         alloc(&k->row_ab, (size_t)k->H * (k->fp32 ? 8 : 16));
         alloc(&k->col_ab, (size_t)k->W * (k->fp32 ? 8 : 16));
     }
+    if (k->fp32 && !k->imag) alloc((void **)&k->kin_sched, (size_t)kSchedLen * sizeof(float4));
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&k->own_stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
         int s = cuda_fail(nullptr, e, "allocation");
@@ -793,6 +822,13 @@ int ts_b200_create(const ts_b200_desc *d, ts_b200_kernel **out) {
             return s;
         }
     }
+    if (k->kin_sched) {
+        int s = upload_kinetic_schedule(k);
+        if (s != TS_B200_OK) {
+            ts_b200_destroy(k);
+            return s;
+        }
+    }
     *out = k;
     return TS_B200_OK;
 }
@@ -803,7 +839,8 @@ int ts_b200_destroy(ts_b200_kernel *k) {
     if (k->own_stream) cudaStreamSynchronize(k->own_stream);
     if (k->stream && k->stream != k->own_stream) cudaStreamSynchronize(k->stream);
     void *bufs[] = {k->psi[0], k->psi[1], k->tab, k->row_ab, k->col_ab, k->partials, k->scal,
-                    k->staging, k->vtab, k->red_partials, k->red_out, k->red_ticket};
+                    k->staging, k->vtab, k->red_partials, k->red_out, k->red_ticket,
+                    k->kin_sched};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (k->own_stream) cudaStreamDestroy(k->own_stream);
