@@ -278,6 +278,14 @@ int ts_b200_adjoint_backward(ts_b200_adjoint *a, const void *grad_psi_t, double 
 int ts_b200_adjoint_synchronize(ts_b200_adjoint *a);
 const char *ts_b200_adjoint_last_error(const ts_b200_adjoint *a);
 
+/* Autotuner for this tile: times `trial_steps` steps for each balanced launch
+ * shape (rows per segment such that every SM holds the same number of
+ * blocks, for 1 .. the resident blocks per SM, 4 or 2 warps per block) and
+ * keeps the fastest.  The trials read the current state and write the other
+ * buffer, the scalars a step updates are restored: the state is unchanged.
+ * Synchronises the tile's stream.  No counterpart in the reference. */
+int ts_b200_autotune(ts_b200_kernel *k, int trial_steps);
+
 /* Pinned host memory for the state arrays (page-locked so that host<->device
  * copies run at full PCIe/C2C rate). */
 int ts_b200_host_alloc(void **ptr, size_t bytes);

@@ -143,3 +143,30 @@ def test_energies_and_expectations_match_oracle(case):
         assert abs(e[key] - v) <= 1e-9 * max(1.0, abs(v)), (key, e[key], v)
     for key, v in x_ref.items():
         assert abs(x[key] - v) <= 1e-9 * max(1.0, abs(v)), (key, x[key], v)
+
+
+@pytest.mark.parametrize("imag", [False, True], ids=["real", "imag"])
+def test_autotune_keeps_state_and_results(imag):
+    """ts_b200_autotune times shapes on the current state without changing it;
+    afterwards the evolution equals the untuned one (bitwise in real time; in
+    imaginary time the norm is summed over a different grid: 1e-13)."""
+    from trottersuzuki_b200 import Kernel
+    lat, psi0, V = seeded_case(300, 12.0, 260, (False, False))
+    p, tr, ti, _ = run_oracle(lat, psi0, V, 1e-3, imag, 3.0, 0.0, 0.0, 0)
+    res = []
+    for tune in (False, True):
+        with Kernel(desc_from_params(p)) as k:
+            k.set_state(psi0)
+            k.set_exp_potential(tr, ti)
+            k.evolve(3)
+            if tune:
+                before = k.get_state()
+                shape = k.autotune(2)
+                assert shape["blocks"] >= 1
+                assert np.array_equal(k.get_state(), before)
+            k.evolve(17)
+            res.append(k.get_state())
+    if imag:
+        assert np.abs(res[0] - res[1]).max() <= 1e-13 * np.abs(res[0]).max()
+    else:
+        assert np.array_equal(res[0], res[1])

@@ -445,13 +445,23 @@ int min_ring(const ts_b200_kernel *) { return 4; }
 
 // One round of tasks over the resident warps: as many row segments per strip
 // as there are resident warps per strip.
-void auto_segments(ts_b200_kernel *k) {
+// Rows per segment for a grid of `blocks_per_sm` blocks on every SM, one
+// task per warp: every SM then holds the same number of tasks (the launch
+// time is that of the most loaded SM).
+int balanced_segments(const ts_b200_kernel *k, int blocks_per_sm, int warps) {
     const int hx = k->rot ? 8 : 4;
     const int wo = 32 * k->C - 2 * hx;
     const int strips = div_up(k->W, wo);
-    const long rw = (long)k->resident_blocks * k->warps;
+    const long rw = (long)blocks_per_sm * k->num_sms * warps;
     const int per_strip = (int)std::max(1L, rw / std::max(1, strips));
-    k->seg_h = std::max(16, div_up(k->H, per_strip));
+    return std::max(8, div_up(k->H, per_strip));
+}
+
+// Default: 4 blocks of 4 warps per SM (fewer, taller tasks than a grid
+// filling every resident slot: less halo work per row, the same balance).
+void auto_segments(ts_b200_kernel *k) {
+    const int bps = std::max(1, k->resident_blocks / std::max(1, k->num_sms));
+    k->seg_h = balanced_segments(k, std::min(4, bps), k->warps);
 }
 
 void geometry(const ts_b200_kernel *k, int *strips, int *segs, int *blocks, size_t *smem) {
@@ -1165,6 +1175,74 @@ int ts_b200_set_launch(ts_b200_kernel *k, int C, int seg_h, int warps, int ring)
     if (smem > 227 * 1024) return fail(k, TS_B200_INVALID_ARGUMENT, "ring does not fit in shared memory");
     drop_graph(k);
     return TS_B200_OK;
+}
+
+int ts_b200_autotune(ts_b200_kernel *k, int trial_steps) {
+    if (!k || trial_steps < 1) return TS_B200_INVALID_ARGUMENT;
+    // the trials step from the current buffer into the other one without
+    // flipping, so the state is untouched; the scalars the step writes
+    // (renormalisation, schedule step) are restored afterwards
+    Scalars saved{};
+    TSB_CHECK(k, cudaMemcpyAsync(&saved, k->scal, sizeof saved, cudaMemcpyDeviceToHost, k->stream));
+    TSB_CHECK(k, cudaStreamSynchronize(k->stream));
+    const int C0 = k->C, seg0 = k->seg_h, warps0 = k->warps;
+    const bool auto0 = k->auto_seg;
+    cudaEvent_t e0, e1;
+    TSB_CHECK(k, cudaEventCreate(&e0));
+    TSB_CHECK(k, cudaEventCreate(&e1));
+    float best_ms = -1.0f;
+    int best_seg = seg0, best_warps = warps0;
+    int st = TS_B200_OK;
+    for (int warps : {4, 2}) {
+        k->warps = warps;
+        k->resident_blocks = 0;
+        k->auto_seg = false;
+        // resident blocks of this shape (the step kernel's occupancy)
+        st = launch_step(k, 0, true);
+        if (st) break;
+        const int bps = std::max(1, k->resident_blocks / std::max(1, k->num_sms));
+        for (int b = 1; b <= bps && st == TS_B200_OK; ++b) {
+            k->seg_h = balanced_segments(k, b, warps);
+            st = tsbh::launch_step_buffers(k, k->psi[k->cur], k->psi[1 - k->cur]);
+            if (st) break;
+            cudaEventRecord(e0, k->stream);
+            for (int i = 0; i < trial_steps && st == TS_B200_OK; ++i)
+                st = tsbh::launch_step_buffers(k, k->psi[k->cur], k->psi[1 - k->cur]);
+            cudaEventRecord(e1, k->stream);
+            cudaError_t e = cudaEventSynchronize(e1);
+            float ms = 0.0f;
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+            if (e != cudaSuccess) {
+                st = cuda_fail(k, e, "autotune timing");
+                break;
+            }
+            if (best_ms < 0.0f || ms < best_ms) {
+                best_ms = ms;
+                best_seg = k->seg_h;
+                best_warps = warps;
+            }
+        }
+        if (st) break;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st) {
+        k->C = C0;
+        k->seg_h = seg0;
+        k->warps = warps0;
+        k->auto_seg = auto0;
+        k->resident_blocks = 0;
+        return st;
+    }
+    k->C = C0;
+    k->seg_h = best_seg;
+    k->warps = best_warps;
+    k->auto_seg = false;
+    k->resident_blocks = 0;
+    drop_graph(k);
+    TSB_CHECK(k, cudaMemcpyAsync(k->scal, &saved, sizeof saved, cudaMemcpyHostToDevice, k->stream));
+    TSB_CHECK(k, cudaStreamSynchronize(k->stream));
+    return launch_step(k, 0, true);  // resident grid of the chosen shape
 }
 
 int ts_b200_host_alloc(void **ptr, size_t bytes) {

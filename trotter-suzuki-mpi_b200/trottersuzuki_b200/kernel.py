@@ -131,6 +131,11 @@ class Kernel:
         self._check(lib().ts_b200_launch_info(self._h, C.byref(s)))
         return {n: getattr(s, n) for n, _ in LaunchShape._fields_}
 
+    def autotune(self, trial_steps=3):
+        """Pick the fastest balanced launch shape (state unchanged)."""
+        self._check(lib().ts_b200_autotune(self._h, int(trial_steps)))
+        return self.launch_shape()
+
     def set_launch(self, cells_per_lane=0, segment_rows=0, warps_per_block=0, ring_depth=0):
         self._check(lib().ts_b200_set_launch(self._h, cells_per_lane, segment_rows,
                                              warps_per_block, ring_depth))
