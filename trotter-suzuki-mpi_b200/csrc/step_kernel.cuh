@@ -493,11 +493,15 @@ struct Variant {
     // masked copy of the row body): variants with 2 cells per lane and no
     // rotating frame.
     static constexpr bool LANE_COEF = C_ == 2 && !ROT_;
-    // Resident blocks of 4 warps per SM the register allocation aims at (the
-    // step is latency-bound: more resident warps hide more of it): 6 blocks
-    // (80 registers) in double, 8 (64 registers) in float for the default
-    // variants, 4 (128 registers) for the others.
-    static constexpr int MIN_BLOCKS = LANE_COEF ? (sizeof(T_) == 4 ? 8 : 6) : 4;
+    // Resident blocks of 4 warps per SM the register allocation aims at.  The
+    // default launch runs 4 blocks per SM (balanced tasks, fewer and taller
+    // segments); a cap of 4 lets the compiler keep ~90 registers in double,
+    // which schedules the row body better (46 vs 54 us per 2048^2 step than
+    // the 80-register cap of 6 blocks); float keeps a cap of 6.
+    static constexpr int MIN_BLOCKS = LANE_COEF ? (sizeof(T_) == 4 ? 6 : 4) : 4;
+    // The batched kernel runs many tasks per warp: more resident warps (6
+    // blocks in double, 8 in float: 80 / 64 registers) hide more latency.
+    static constexpr int BATCH_MIN_BLOCKS = LANE_COEF ? (sizeof(T_) == 4 ? 8 : 6) : 4;
     using TabT = typename std::conditional<IMAG_, T_, Cx<T_>>::type;
     static constexpr int PSI_BYTES = SW * (int)sizeof(Cx<T_>);
     static constexpr int TAB_BYTES = SW * (int)sizeof(TabT);
@@ -1027,7 +1031,7 @@ __device__ __forceinline__ StepArgs<T> load_tile_args(const StepArgs<T> *p) {
 }
 
 template <class V>
-__global__ void __launch_bounds__(128, V::MIN_BLOCKS) batch_step_kernel(BatchArgs<typename V::T> b) {
+__global__ void __launch_bounds__(128, V::BATCH_MIN_BLOCKS) batch_step_kernel(BatchArgs<typename V::T> b) {
     extern __shared__ __align__(128) unsigned char smem[];
     const int warps = blockDim.x >> 5;
     const int warp = __shfl_sync(0xffffffffu, (int)(threadIdx.x >> 5), 0);
