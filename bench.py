@@ -284,7 +284,6 @@ def run_b200_arm(args, rank, world, local, pg):
     solver.evolve(-1, True)  # builds the kernel (table, norm0, upload)
     handle = solver.kernel_handle()
     _capi.check(L.ts_b200_set_stream(handle, C.c_void_p(stream.cuda_stream)), handle)
-    _capi.check(L.ts_b200_autotune(handle, 5), handle)  # launch shape for this tile
     for _ in range(args.warmup):
         solver.evolve(-TROTTER_PER_STEP, True)
     torch.cuda.synchronize()
@@ -349,7 +348,6 @@ def run_b200_arm(args, rank, world, local, pg):
         solver32.evolve(-1, True)
         h32 = solver32.kernel_handle()
         _capi.check(L.ts_b200_set_stream(h32, C.c_void_p(stream.cuda_stream)), h32)
-        _capi.check(L.ts_b200_autotune(h32, 5), h32)
         for _ in range(args.warmup):
             solver32.evolve(-TROTTER_PER_STEP, True)
         torch.cuda.synchronize()
