@@ -298,6 +298,32 @@ __device__ __forceinline__ void hsweep_lane(Cx<T> (&w)[2], T ai, T bi, T al, T b
     }
 }
 
+// The same for C cells per lane: (pa[i], pb[i]) for the pair (i, i+1) inside
+// the lane, (al, bl) / (ar, br) for the pairs with the neighbour lanes.
+template <bool IMAG, int PAR, int C, typename T>
+__device__ __forceinline__ void hsweep_lanes(Cx<T> (&w)[C], const T (&pa)[C - 1],
+                                             const T (&pb)[C - 1], T al, T bl, T ar, T br) {
+    if (PAR == 0) {
+#pragma unroll
+        for (int i = 0; i + 1 < C; i += 2) {
+            const Cx<T> p = w[i], q = w[i + 1];
+            w[i] = kin<IMAG>(p, q, pa[i], pb[i]);
+            w[i + 1] = kin<IMAG>(q, p, pa[i], pb[i]);
+        }
+    } else {
+        const Cx<T> right = shfl_down1(w[0]);
+        const Cx<T> left = shfl_up1(w[C - 1]);
+#pragma unroll
+        for (int i = 1; i + 1 < C; i += 2) {
+            const Cx<T> p = w[i], q = w[i + 1];
+            w[i] = kin<IMAG>(p, q, pa[i], pb[i]);
+            w[i + 1] = kin<IMAG>(q, p, pa[i], pb[i]);
+        }
+        w[0] = kin<IMAG>(w[0], left, al, bl);
+        w[C - 1] = kin<IMAG>(w[C - 1], right, ar, br);
+    }
+}
+
 // Rotation row sweep on one row: pairs (x, x+1) with x % 2 == PAR.
 template <bool IMAG, int C, int PAR, bool EDGE, typename T>
 __device__ __forceinline__ void rrow(Cx<T> (&w)[C], T a, T b, const LaneMask<C> &m) {
@@ -492,16 +518,17 @@ struct Variant {
     // Per-lane horizontal coefficients instead of edge masks (no second,
     // masked copy of the row body): variants with 2 cells per lane and no
     // rotating frame.
-    static constexpr bool LANE_COEF = C_ == 2 && !ROT_;
+    static constexpr bool LANE_COEF = !ROT_;
     // Resident blocks of 4 warps per SM the register allocation aims at.  The
     // default launch runs 4 blocks per SM (balanced tasks, fewer and taller
     // segments); a cap of 4 lets the compiler keep ~90 registers in double,
     // which schedules the row body better (46 vs 54 us per 2048^2 step than
     // the 80-register cap of 6 blocks); float keeps a cap of 6.
-    static constexpr int MIN_BLOCKS = LANE_COEF ? (sizeof(T_) == 4 ? 6 : 4) : 4;
+    static constexpr int MIN_BLOCKS =
+        LANE_COEF ? (C_ == 2 ? (sizeof(T_) == 4 ? 6 : 4) : (sizeof(T_) == 4 ? 4 : 2)) : 4;
     // The batched kernel runs many tasks per warp: more resident warps (6
     // blocks in double, 8 in float: 80 / 64 registers) hide more latency.
-    static constexpr int BATCH_MIN_BLOCKS = LANE_COEF ? (sizeof(T_) == 4 ? 8 : 6) : 4;
+    static constexpr int BATCH_MIN_BLOCKS = LANE_COEF ? (sizeof(T_) == 4 ? 8 : 6) : 4;  // C = 2
     using TabT = typename std::conditional<IMAG_, T_, Cx<T_>>::type;
     static constexpr int PSI_BYTES = SW * (int)sizeof(Cx<T_>);
     static constexpr int TAB_BYTES = SW * (int)sizeof(TabT);
@@ -539,7 +566,8 @@ struct Walk {
     bool failed;
     T inv;
     T aH, bH, aV, bV, ca, caa;  // step constants, read from the parameters once
-    T hai, hbi, hal, hbl, har, hbr;  // LANE_COEF: this lane's horizontal pair coefficients
+    T hpa[C - 1], hpb[C - 1];        // LANE_COEF: this lane's pairs (i, i+1)
+    T hal, hbl, har, hbr;            //   and its pairs with the neighbour lanes
 
     __device__ __forceinline__ void issue(int row, int slot) {
         unsigned char *sb = ring + slot * V::SLOT;
@@ -555,7 +583,7 @@ struct Walk {
 template <class V, int PAR, bool EDGE>
 __device__ __forceinline__ void hsw(Walk<V> &w, Cx<typename V::T> (&row)[V::C]) {
     if constexpr (V::LANE_COEF) {
-        hsweep_lane<V::IMAG, PAR>(row, w.hai, w.hbi, w.hal, w.hbl, w.har, w.hbr);
+        hsweep_lanes<V::IMAG, PAR, V::C>(row, w.hpa, w.hpb, w.hal, w.hbl, w.har, w.hbr);
     } else {
         hsweep<V::IMAG, V::C, PAR, EDGE>(row, w.aH, w.bH, w.m);
     }
@@ -828,8 +856,11 @@ __device__ __forceinline__ void run_task(Walk<V> &w, const StepArgs<typename V::
     w.m.pair_right = lane < 31 && w.present[C - 1] && w.xl + C < a.W;
     if constexpr (V::LANE_COEF) {
         const T one = DeltaForm<T>::value ? T(0) : T(1);
-        w.hai = w.m.pair_int[0] ? w.aH : one;
-        w.hbi = w.m.pair_int[0] ? w.bH : T(0);
+#pragma unroll
+        for (int i = 0; i + 1 < C; ++i) {
+            w.hpa[i] = w.m.pair_int[i] ? w.aH : one;
+            w.hpb[i] = w.m.pair_int[i] ? w.bH : T(0);
+        }
         w.hal = w.m.pair_left ? w.aH : one;
         w.hbl = w.m.pair_left ? w.bH : T(0);
         w.har = w.m.pair_right ? w.aH : one;
