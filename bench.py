@@ -897,6 +897,133 @@ def run_vortex_workload(args, rank, world, local, pg):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------ time-dependent potential workload
+# Real-time GPE in a trap whose centre oscillates along x,
+# V(x, y, t) = 1/2 ((x - a sin(w t))^2 + (1.5 y)^2), FP64, on the headline
+# lattice (2048^2 over length 24, closed, g = 100, dt = 1e-4) from the headline
+# initial state.  The reference re-tabulates V and its exponential on the host
+# before every step; DevicePotential evaluates V with torch on the GPU and
+# builds the table on the device.  One bench step = 200 Trotter steps through
+# Solver.evolve; the host path is timed on a bounded sample of steps.
+MT_AMP, MT_FREQ = 1.0, 5.0
+MT_STEPS = 200
+MT_HOST_STEPS = 4
+
+
+MT_TIME_BATCH = 16
+
+
+def moving_trap(x, y, t):
+    return 0.5 * ((x - MT_AMP * math.sin(MT_FREQ * t)) ** 2 + (OMEGA_Y * y) ** 2)
+
+
+def moving_trap_batched(x, y, t):
+    """moving_trap for a tensor t of step times (DevicePotential time_batch mode)."""
+    import torch
+    return 0.5 * ((x - MT_AMP * torch.sin(MT_FREQ * t)) ** 2 + (OMEGA_Y * y) ** 2)
+
+
+def run_moving_trap_workload(args, rank, world, local, pg):
+    import torch
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    import trottersuzuki_b200 as ts
+    from trottersuzuki_b200 import launch_count
+
+    def solver_for(kind):
+        grid = ts.Lattice2D(N_SIDE, LENGTH)
+        state = ts.State(grid)
+        info = {"dim_x": grid.dim_x, "dim_y": grid.dim_y, "delta_x": grid.delta_x,
+                "delta_y": grid.delta_y}
+        psi0 = initial_state(info)
+        state.init_state_matrix(psi0.real, psi0.imag)
+        if kind == "device":
+            pot = ts.DevicePotential(grid, moving_trap_batched, device=device,
+                                     time_batch=MT_TIME_BATCH)
+        elif kind == "device_per_step":
+            pot = ts.DevicePotential(grid, moving_trap, device=device)
+        elif kind == "host":
+            pot = ts.Potential(grid)
+            pot.init_potential(moving_trap)
+        else:
+            pot = ts.HarmonicPotential(grid, OMEGA_X, OMEGA_Y)
+        ham = ts.Hamiltonian(grid, pot, 1.0, G)
+        return ts.Solver(grid, state, ham, DT, kernel_type="gpu"), (grid, state, pot, ham)
+
+    def timed(solver, n, calls):
+        cur = torch.cuda.current_stream(device)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        if pg:
+            pg.barrier()
+        l0 = launch_count()
+        e0.record(cur)
+        for _ in range(calls):
+            solver.evolve(n)
+        torch.cuda.synchronize()  # the static solver queues on its kernel's own stream
+        e1.record(cur)
+        e1.synchronize()
+        return max_over_ranks(e0.elapsed_time(e1), pg, device), launch_count() - l0
+
+    sites = float(N_SIDE) * N_SIDE
+    dev, keep_dev = solver_for("device")
+    for _ in range(args.warmup):
+        dev.evolve(-MT_STEPS)
+    with Clocks(local) as clocks:
+        ms_dev, launches = timed(dev, -MT_STEPS, args.steps)  # state stays on the device
+    ms_e2e, _ = timed(dev, MT_STEPS, max(1, args.steps // 2))  # copied into the State per call
+    e2e_calls = max(1, args.steps // 2)
+    del dev, keep_dev
+    # one pot_function call per step (Python float t)
+    dps, keep_dps = solver_for("device_per_step")
+    dps.evolve(-MT_STEPS)
+    ms_dps, _ = timed(dps, -MT_STEPS, args.steps)
+    del dps, keep_dps
+    # the same kernel with a static table: the step alone
+    static, keep_static = solver_for("static")
+    static.evolve(-MT_STEPS)
+    ms_static, _ = timed(static, -MT_STEPS, args.steps)
+    del static, keep_static
+    # the host path (numpy V, host exponential, upload) on a bounded sample
+    hst, keep_host = solver_for("host")
+    hst.evolve(-1)
+    ms_host, _ = timed(hst, -MT_HOST_STEPS, 1)
+    del hst, keep_host
+    if rank != 0:
+        return
+    v_dev = world * sites * MT_STEPS * args.steps / (ms_dev * 1e-3)
+    v_static = world * sites * MT_STEPS * args.steps / (ms_static * 1e-3)
+    v_host = world * sites * MT_HOST_STEPS / (ms_host * 1e-3)
+    v_e2e = world * sites * MT_STEPS * e2e_calls / (ms_e2e * 1e-3)
+    v_dps = world * sites * MT_STEPS * args.steps / (ms_dps * 1e-3)
+    line = {
+        "metric": "site-steps/s", "value": v_dev, "unit": "site-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_dev / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "moving_trap_2048", "lattice": f"{N_SIDE}x{N_SIDE}",
+                   "length": LENGTH, "boundary": "closed", "g": G, "dt": DT,
+                   "potential": f"1/2((x - {MT_AMP} sin({MT_FREQ} t))^2 + ({OMEGA_Y} y)^2)",
+                   "trotter_steps_per_step": MT_STEPS, "imag_time": False,
+                   "time_batch": MT_TIME_BATCH,
+                   "parallelism": f"replicas{world}",
+                   "l2": "inputs larger than L2: 192 MiB moved per Trotter step"},
+        "e2e": {"value": v_e2e, "unit": "site-steps/s", "h2d_bytes_per_step": 8 * MT_STEPS,
+                "d2h_bytes_per_step": 2 * 8 * int(sites),
+                "path": "Solver.evolve(200) with DevicePotential (step times uploaded, "
+                        "state copied into the State after each call)"},
+        "static_potential_same_kernel": {"value": v_static, "unit": "site-steps/s"},
+        "device_potential_per_step_call": {"value": v_dps, "unit": "site-steps/s"},
+        "host_potential_path": {"value": v_host, "unit": "site-steps/s",
+                                "sample": f"{MT_HOST_STEPS} Trotter steps",
+                                "speedup_of_device_path": v_dev / v_host},
+        "clocks": clocks.summary(),
+        "gpu_launches": launches,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -908,7 +1035,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--workload", choices=["gpe_imaginary_time_2048", "batch512", "adjoint512",
-                                           "vortex8192"],
+                                           "vortex8192", "moving_trap_2048"],
                     default="gpe_imaginary_time_2048")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
@@ -922,6 +1049,8 @@ def main():
             run_adjoint_workload(args, rank, world, local, pg)
         elif args.workload == "vortex8192":
             run_vortex_workload(args, rank, world, local, pg)
+        elif args.workload == "moving_trap_2048":
+            run_moving_trap_workload(args, rank, world, local, pg)
         else:
             run_b200_arm(args, rank, world, local, pg)
     finally:

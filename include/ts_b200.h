@@ -179,6 +179,25 @@ int ts_b200_set_state_device(ts_b200_kernel *k, const void *aos, size_t pitch);
 int ts_b200_get_state_device(ts_b200_kernel *k, void *aos, size_t pitch);
 int ts_b200_set_exp_potential_device(ts_b200_kernel *k, const void *table, size_t pitch);
 
+/* The exponential table from a potential already on the device: `potential`
+ * holds dim_y rows of dim_x doubles V(x, y) with row pitch `pitch` doubles;
+ * the table exp(-i dt V) (real time) or exp(-dt V) (imaginary time) is built
+ * on the device in the kernel's precision.  Replaces, for a potential that
+ * changes every step, the host re-tabulation and upload of the reference's
+ * Solver::evolve (src/solver.cpp:187-200 with initialize_exp_potential,
+ * src/solver.cpp:74-109, and the kernel's update_potential). */
+int ts_b200_set_potential_device(ts_b200_kernel *k, const double *potential, size_t pitch,
+                                 double delta_t);
+
+/* `count` steps, step i with the potential V_i already on the device:
+ * V_i = potentials + i * slab doubles (dim_y rows, row pitch `pitch`), its
+ * table built as by ts_b200_set_potential_device before the step.  Every
+ * step refreshes the halo when `exchange` is nonzero, none does otherwise
+ * (a run of the reference's per-step Python loop, classes_extension.py:
+ * 393-403, where each step is an evolve call of its own). */
+int ts_b200_evolve_potentials(ts_b200_kernel *k, const double *potentials, size_t pitch,
+                              size_t slab, int count, double delta_t, int exchange);
+
 /* Queue all work of this handle on `stream` (a cudaStream_t); NULL restores
  * the handle's own stream. */
 int ts_b200_set_stream(ts_b200_kernel *k, void *stream);
@@ -281,7 +300,8 @@ const char *ts_b200_adjoint_last_error(const ts_b200_adjoint *a);
 /* Autotuner for this tile: times `trial_steps` steps for each balanced launch
  * shape (rows per segment such that every SM holds the same number of
  * blocks, for 1 .. the resident blocks per SM, 4 or 2 warps per block) and
- * keeps the fastest.  The trials read the current state and write the other
+ * for segments of 32, 64 and 128 rows taken by the persistent warps in turn,
+ * and keeps the fastest.  The trials read the current state and write the other
  * buffer, the scalars a step updates are restored: the state is unchanged.
  * Synchronises the tile's stream.  No counterpart in the reference. */
 int ts_b200_autotune(ts_b200_kernel *k, int trial_steps);

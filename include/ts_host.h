@@ -82,6 +82,9 @@ int tsh_solver_energies(void *solver, double out[7]);
 int tsh_solver_set_exp_potential(void *solver, const double *re, const double *im, int length,
                                  int which);
 int tsh_solver_update_parameters(void *solver);
+/* Build (or rebuild) the solver's kernel for the time mode as evolve() does
+ * (src/solver.cpp:150-171), without a step or a copy back into the State. */
+int tsh_solver_prepare(void *solver, int imag_time);
 /* The device handle of the solver's kernel (NULL before the first evolve). */
 int tsh_solver_kernel_handle(void *solver, void **out);
 int tsh_solver_free(void *solver);

@@ -72,6 +72,53 @@ __host__ __device__ inline void unimodular_float_pair(double am1, double b, int 
     *fb = bb;
 }
 
+// The same objective as unimodular_float_pair (smallest defect, then the
+// closest pair) in a fraction of the work, for tables rebuilt every step.  For
+// each float b_j within `span` ulps of round(b), the exact unimodular partner
+// a(b_j) is followed from (am1, b) along the circle to second order
+// (da = -b/(1+a) db - db^2 / (2 (1+a)^3), from (1+a)^2 + b^2 = 1), and only the
+// two floats bracketing it are scored: 2a + a^2 is monotone there, so they
+// hold the smallest defect over ALL floats a for that b_j (a superset of the
+// exhaustive search's candidates).  Near |angle| = pi/2 (|1 + am1| < 1/4) the
+// expansion is not used and the exhaustive search runs instead.
+__host__ __device__ inline void unimodular_float_pair_fast(double am1, double b, int span,
+                                                           float *fa, float *fb) {
+    const double c = 1.0 + am1;
+    if (!(fabs(c) >= 0.25)) {
+        unimodular_float_pair(am1, b, span, fa, fb);
+        return;
+    }
+    const double inv = 1.0 / c;
+    auto defect = [](float x, float y) {
+        return fabs(2.0 * (double)x + (double)x * x + (double)y * y);
+    };
+    const float b0 = (float)b;
+    float ba = (float)am1, bb = b0;
+    double best = defect(ba, bb);
+    double bestd = fabs((double)ba - am1) + fabs((double)bb - b);
+    float bj = b0;
+    for (int j = 0; j < span; ++j) bj = nextafterf(bj, -INFINITY);
+    for (int j = -span; j <= span; ++j, bj = nextafterf(bj, INFINITY)) {
+        const double db = (double)bj - b;
+        const double am = am1 - b * inv * db - 0.5 * inv * inv * inv * db * db;
+        const float a1 = (float)am;
+        const float a2 = nextafterf(a1, (double)a1 < am ? INFINITY : -INFINITY);
+        for (int t = 0; t < 2; ++t) {
+            const float ai = t ? a2 : a1;
+            const double err = defect(ai, bj);
+            const double d = fabs((double)ai - am1) + fabs((double)bj - b);
+            if (err < best || (err == best && d < bestd)) {
+                best = err;
+                bestd = d;
+                ba = ai;
+                bb = bj;
+            }
+        }
+    }
+    *fa = ba;
+    *fb = bb;
+}
+
 // cos(k) - 1 and cosh(k) - 1 without cancellation.
 __host__ __device__ inline double cos_m1(double k) {
     const double h = sin(0.5 * k);
@@ -123,6 +170,81 @@ __global__ void pack_table_kernel(void *dst, int imag, int W, int H, int P, cons
             reinterpret_cast<Cx<T> *>(dst)[k] = Cx<T>{(T)vr, (T)vi};
         }
     }
+}
+
+// sin(a) and cos(a) - 1 for |a| <= 1/16 from their Maclaurin series (Horner's
+// rule in a^2).  With the last terms a^9/9! and a^10/10! the truncation error
+// is below 2^-64 relative, and a, -a^2/2 carry the leading bits exactly, so
+// both are within about half an ulp of the true values: no range reduction
+// and a few FMAs instead of a full sincos.
+constexpr double kSmallAngle = 0.0625;
+__device__ inline void small_angle_sincos(double a, double *s, double *cm1) {
+    const double a2 = a * a;
+    double ps = 1.0 / 362880.0;  // 1/9!
+    ps = fma(ps, a2, -1.0 / 5040.0);
+    ps = fma(ps, a2, 1.0 / 120.0);
+    ps = fma(ps, a2, -1.0 / 6.0);
+    *s = fma(a * a2, ps, a);
+    double pc = -1.0 / 3628800.0;  // -1/10!
+    pc = fma(pc, a2, 1.0 / 40320.0);
+    pc = fma(pc, a2, -1.0 / 720.0);
+    pc = fma(pc, a2, 1.0 / 24.0);
+    pc = fma(pc, a2, -0.5);
+    *cm1 = a2 * pc;
+}
+
+// The table from a potential on the device: exp(-i dt V) in real time
+// ((cos - 1, -sin) in float: delta form, pair chosen by the fast search),
+// exp(-dt V) in imaginary time; the host path tabulates the same with
+// std::exp(complex) (src/solver.cpp:74-109).  V: W x H doubles, row pitch vp.
+// One thread per cell of a row (blockIdx.y strides over the rows): no index
+// division, coalesced in both arrays.
+template <typename T>
+__global__ void table_from_potential_kernel(void *dst, int imag, int W, int H, int P,
+                                            const double *V, size_t vp, double dt) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= P) return;
+    for (int y = blockIdx.y; y < H; y += gridDim.y) {
+        const size_t k = (size_t)y * P + x;
+        const double ang = x < W ? dt * V[(size_t)y * vp + x] : 0.0;
+        if (imag) {
+            reinterpret_cast<T *>(dst)[k] = x < W ? (T)exp(-ang) : T(0);
+            continue;
+        }
+        double s, cm1;
+        if (fabs(ang) <= kSmallAngle) {
+            small_angle_sincos(ang, &s, &cm1);
+        } else {
+            double c;
+            sincos(ang, &s, &c);
+            cm1 = sizeof(T) == 4 ? cos_m1(ang) : c - 1.0;
+            if (sizeof(T) == 8) {
+                reinterpret_cast<Cx<T> *>(dst)[k] =
+                    x < W ? Cx<T>{(T)c, (T)-s} : Cx<T>{T(0), T(0)};
+                continue;
+            }
+        }
+        if (sizeof(T) == 4) {
+            float fr, fi;
+            // span 1: about the defect of the exhaustive span-4 search at a
+            // sixth of the FP64 work of span 4, for a table made every step
+            unimodular_float_pair_fast(x < W ? cm1 : -1.0, x < W ? -s : 0.0, 1, &fr, &fi);
+            reinterpret_cast<Cx<T> *>(dst)[k] = Cx<T>{(T)fr, (T)fi};
+        } else {
+            reinterpret_cast<Cx<T> *>(dst)[k] =
+                x < W ? Cx<T>{(T)(1.0 + cm1), (T)-s} : Cx<T>{T(0), T(0)};
+        }
+    }
+}
+
+void launch_table_from_potential(ts_b200_kernel *k, const double *V, size_t vp, double dt) {
+    const dim3 grid((k->P + 255) / 256, std::min(k->H, 65535));
+    if (k->fp32)
+        table_from_potential_kernel<float><<<grid, 256, 0, k->stream>>>(
+            k->tab, k->imag ? 1 : 0, k->W, k->H, k->P, V, vp, dt);
+    else
+        table_from_potential_kernel<double><<<grid, 256, 0, k->stream>>>(
+            k->tab, k->imag ? 1 : 0, k->W, k->H, k->P, V, vp, dt);
 }
 
 // De-interleave a w x h window at (x0, y0) into SoA doubles with stride w,
@@ -458,10 +580,15 @@ int balanced_segments(const ts_b200_kernel *k, int blocks_per_sm, int warps) {
 }
 
 // Default: 4 blocks of 4 warps per SM (fewer, taller tasks than a grid
-// filling every resident slot: less halo work per row, the same balance).
+// filling every resident slot: less halo work per row, the same balance),
+// with segments of at most kMaxAutoSegment rows: on large tiles one task per
+// warp means segments of hundreds of rows, which ran 1.3-1.6x slower than
+// 64-128-row segments taken by the persistent warps in turn (8192^2 rotating
+// frame: 2.02 -> 1.35 ms per step in double, 1.72 -> 1.07 in float).
+constexpr int kMaxAutoSegment = 128;
 void auto_segments(ts_b200_kernel *k) {
     const int bps = std::max(1, k->resident_blocks / std::max(1, k->num_sms));
-    k->seg_h = balanced_segments(k, std::min(4, bps), k->warps);
+    k->seg_h = std::min(kMaxAutoSegment, balanced_segments(k, std::min(4, bps), k->warps));
 }
 
 void geometry(const ts_b200_kernel *k, int *strips, int *segs, int *blocks, size_t *smem) {
@@ -955,6 +1082,31 @@ int ts_b200_set_exp_potential_device(ts_b200_kernel *k, const void *table, size_
     return TS_B200_OK;
 }
 
+int ts_b200_set_potential_device(ts_b200_kernel *k, const double *potential, size_t pitch,
+                                 double delta_t) {
+    if (!k || !potential || pitch < (size_t)k->W || !(delta_t > 0.0))
+        return TS_B200_INVALID_ARGUMENT;
+    launch_table_from_potential(k, potential, pitch, delta_t);
+    TSB_CHECK(k, cudaGetLastError());
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    return TS_B200_OK;
+}
+
+int ts_b200_evolve_potentials(ts_b200_kernel *k, const double *potentials, size_t pitch,
+                              size_t slab, int count, double delta_t, int exchange) {
+    if (!k || !potentials || count < 0 || pitch < (size_t)k->W || slab < pitch * k->H ||
+        !(delta_t > 0.0))
+        return TS_B200_INVALID_ARGUMENT;
+    for (int i = 0; i < count; ++i) {
+        launch_table_from_potential(k, potentials + (size_t)i * slab, pitch, delta_t);
+        TSB_CHECK(k, cudaGetLastError());
+        g_launches.fetch_add(1, std::memory_order_relaxed);
+        const int s = launch_step(k, exchange);
+        if (s) return s;
+    }
+    return TS_B200_OK;
+}
+
 int ts_b200_step(ts_b200_kernel *k, int exchange) {
     if (!k) return TS_B200_INVALID_ARGUMENT;
     return launch_step(k, exchange);
@@ -1201,8 +1353,17 @@ int ts_b200_autotune(ts_b200_kernel *k, int trial_steps) {
         st = launch_step(k, 0, true);
         if (st) break;
         const int bps = std::max(1, k->resident_blocks / std::max(1, k->num_sms));
-        for (int b = 1; b <= bps && st == TS_B200_OK; ++b) {
-            k->seg_h = balanced_segments(k, b, warps);
+        // balanced shapes (one task per warp at b blocks per SM) and short
+        // segments taken by the persistent warps in turn
+        int cand[24], nc = 0;
+        for (int b = 1; b <= bps && nc < 20; ++b) cand[nc++] = balanced_segments(k, b, warps);
+        for (int sh : {32, 64, 128})
+            if (sh < k->H) cand[nc++] = sh;
+        for (int c = 0; c < nc && st == TS_B200_OK; ++c) {
+            bool seen = false;
+            for (int d = 0; d < c; ++d) seen = seen || cand[d] == cand[c];
+            if (seen) continue;
+            k->seg_h = cand[c];
             st = tsbh::launch_step_buffers(k, k->psi[k->cur], k->psi[1 - k->cur]);
             if (st) break;
             cudaEventRecord(e0, k->stream);

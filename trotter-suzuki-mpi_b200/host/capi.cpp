@@ -196,6 +196,10 @@ int tsh_solver_evolve(void *svp, int iterations, int imag) {
     return guard([&] { static_cast<Solver *>(svp)->evolve(iterations, imag != 0); });
 }
 
+int tsh_solver_prepare(void *svp, int imag) {
+    return guard([&] { static_cast<Solver *>(svp)->prepare_kernel(imag != 0); });
+}
+
 int tsh_solver_energies(void *svp, double out[7]) {
     return guard([&] {
         Solver *s = static_cast<Solver *>(svp);

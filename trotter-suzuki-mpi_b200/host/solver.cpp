@@ -75,6 +75,10 @@ void Solver::set_exp_potential(double *re, int re_len, double *im, int im_len, i
     is_python = true;
     memcpy(external_pot_real[which], re, sizeof(double) * re_len);
     memcpy(external_pot_imag[which], im, sizeof(double) * im_len);
+    // The reference's CPU kernel reads these arrays in place, so a new table
+    // takes effect at the next step; the device kernel holds its own copy.
+    if (kernel != NULL && which == 0)
+        kernel->update_potential(external_pot_real[0], external_pot_imag[0], 0);
 }
 
 void Solver::init_kernel() {
@@ -95,7 +99,7 @@ void Solver::init_kernel() {
     kernel_state_current = true;
 }
 
-void Solver::evolve(int iterations, bool _imag_time) {
+void Solver::prepare_kernel(bool _imag_time) {
     if (_imag_time != imag_time || kernel == NULL || has_parameters_changed) {
         imag_time = _imag_time;
         if (imag_time) {
@@ -107,6 +111,10 @@ void Solver::evolve(int iterations, bool _imag_time) {
         init_kernel();
         has_parameters_changed = false;
     }
+}
+
+void Solver::evolve(int iterations, bool _imag_time) {
+    prepare_kernel(_imag_time);
     bool soft_update = false;
     if (iterations < 0) {
         iterations = -iterations;

@@ -287,6 +287,9 @@ public:
                            int which);
     /** The kernel currently in use (NULL before the first evolve). */
     ITrotterKernel *get_kernel() { return kernel; }
+    /** Build (or rebuild) the kernel for the time mode as evolve() does, with
+     *  no step and no copy back into the State. */
+    void prepare_kernel(bool imag_time);
 
 private:
     bool imag_time;

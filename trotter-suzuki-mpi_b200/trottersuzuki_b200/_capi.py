@@ -86,6 +86,8 @@ SIGNATURES = {
     "ts_b200_set_state_device": (_I, [_VP, _VP, _SZ]),
     "ts_b200_get_state_device": (_I, [_VP, _VP, _SZ]),
     "ts_b200_set_exp_potential_device": (_I, [_VP, _VP, _SZ]),
+    "ts_b200_set_potential_device": (_I, [_VP, _VP, _SZ, C.c_double]),
+    "ts_b200_evolve_potentials": (_I, [_VP, _VP, _SZ, _SZ, C.c_int, C.c_double, C.c_int]),
     "ts_b200_set_stream": (_I, [_VP, _VP]),
     "ts_b200_synchronize": (_I, [_VP]),
     "ts_b200_launch_info": (_I, [_VP, C.POINTER(LaunchShape)]),

@@ -70,6 +70,7 @@ def host():
             "tsh_hamiltonian_free": (i, [vp]),
             "tsh_solver_new": (i, [vp, vp, vp, d, C.c_char_p, P(vp)]),
             "tsh_solver_evolve": (i, [vp, i, i]),
+            "tsh_solver_prepare": (i, [vp, i]),
             "tsh_solver_energies": (i, [vp, P(d)]),
             "tsh_solver_set_exp_potential": (i, [vp, vp, vp, i, i]),
             "tsh_solver_update_parameters": (i, [vp]),
@@ -368,6 +369,70 @@ class Potential(_Handle):
         return np.exp(-1j * delta_t * V)
 
 
+class DevicePotential(Potential):
+    """A time-dependent potential V(x, y, t) evaluated on the GPU.
+
+    No counterpart in the reference, where a Python V(x, y, t) is tabulated
+    on the host and uploaded before every step (classes_extension.py:360-366,
+    388-403).  Here pot_function(X, Y, t) receives the tile's coordinates
+    (the points of map_lattice_to_coordinate_space) as float64 CUDA tensors,
+    X a 1 x dim_x row and Y a dim_y x 1 column that broadcast against each
+    other, and a Python float t; it returns V as a tensor broadcastable to
+    dim_y x dim_x.  Broadcast coordinates keep the terms that depend on x or
+    on y alone as vectors, so only the final combination costs a pass over
+    the tile.  The exponential table is
+    then built on the device (ts_b200_set_potential_device), so a real-time
+    step moves nothing between host and device.  The time schedule is the
+    reference's: step i of an evolve() call uses V(t0 + i dt).  As in the
+    reference, energies use V at t = 0 and imaginary-time evolution uses
+    V(x, y, 0) throughout.
+
+    time_batch = B > 0 evaluates B steps' potentials in one call: t is then
+    a B x 1 x 1 float64 CUDA tensor of step times (write pot_function with
+    torch operations, e.g. torch.sin(t)), the result is B x dim_y x dim_x,
+    and the B steps run from one library call (ts_b200_evolve_potentials),
+    which takes the per-step Python work off the critical path.  B tiles
+    of doubles are held on the device meanwhile.
+    """
+
+    def __init__(self, grid, pot_function, device="cuda", time_batch=0):
+        import torch
+        self.grid = grid
+        self.pot_function = pot_function
+        self.time_batch = int(time_batch)
+        self.updated_potential_matrix = True
+        X, Y = _coordinate_grid(grid)
+        self._X = torch.tensor(np.ascontiguousarray(X[:1, :]), dtype=torch.float64,
+                               device=device)
+        self._Y = torch.tensor(np.ascontiguousarray(Y[:, :1]), dtype=torch.float64,
+                               device=device)
+        self.shape = (grid.dim_y, grid.dim_x)
+        self.init_potential_matrix(self.device_values(0.0).cpu().numpy())
+
+    def device_values(self, t):
+        """V(x, y, t) over the tile: a contiguous dim_y x dim_x float64 tensor
+        on the device."""
+        if self.time_batch:
+            return self.device_values_batch([float(t)])[0]
+        import torch
+        v = torch.as_tensor(self.pot_function(self._X, self._Y, float(t)),
+                            dtype=torch.float64, device=self._X.device)
+        return v.expand(self.shape).contiguous()
+
+    def device_values_batch(self, times):
+        """V at each of `times` (time_batch mode): len(times) x dim_y x dim_x."""
+        import torch
+        # from pinned memory, so the copy does not wait for the queued steps
+        tt = torch.tensor(times, dtype=torch.float64).pin_memory().to(self._X.device,
+                                                                       non_blocking=True)
+        v = torch.as_tensor(self.pot_function(self._X, self._Y, tt.view(-1, 1, 1)),
+                            dtype=torch.float64, device=self._X.device)
+        return v.expand((len(times),) + self.shape).contiguous()
+
+    def exponential_update(self, delta_t, t):
+        return np.exp(-1j * delta_t * self.device_values(t).cpu().numpy())
+
+
 class HarmonicPotential(Potential):
     def __init__(self, grid, omegax, omegay, mass=1., mean_x=0., mean_y=0.):
         self.grid = grid
@@ -424,16 +489,65 @@ class Solver(_Handle):
             self.current_evolution_time += self.delta_t * abs(int(iterations))
             return
         # time-dependent Python potential: re-tabulate before every step
-        # (classes_extension.py:388-403)
-        for i in range(int(iterations)):
+        # (classes_extension.py:388-403); iterations < 0 leaves the result
+        # on the device, as the C++ evolve does
+        n, copy_back = abs(int(iterations)), int(iterations) > 0
+        if isinstance(pot, DevicePotential):
+            self._evolve_device_potential(pot, n, copy_back)
+            return
+        for i in range(n):
             e = pot.exponential_update(self.delta_t, self.current_evolution_time)
             re = np.ascontiguousarray(e.real).ravel()
             im = np.ascontiguousarray(e.imag).ravel()
             _chk(host().tsh_solver_set_exp_potential(self._h, re.ctypes.data, im.ctypes.data,
                                                      re.size, 0))
-            last = i == int(iterations) - 1
+            last = i == n - 1 and copy_back
             _chk(host().tsh_solver_evolve(self._h, 1 if last else -1, 0))
             self.current_evolution_time += self.delta_t
+
+    def _evolve_device_potential(self, pot, iterations, copy_back=True):
+        """The loop above with V(x, y, t) and its table made on the device:
+        per step (or per time_batch steps), pot_function on a side stream,
+        then the table kernel and one step per potential (no halo refresh, as
+        each per-step evolve call of the reference loop ends its own
+        iterations)."""
+        import torch
+        if iterations <= 0:
+            return
+        _chk(host().tsh_solver_prepare(self._h, 0))
+        k = self.kernel_handle()
+        lib = _capi.lib()
+        # one side stream per solver, so the caching allocator reuses the
+        # potential buffers of earlier calls
+        stream = getattr(self, "_potential_stream", None)
+        if stream is None or stream.device != pot._X.device:
+            stream = self._potential_stream = torch.cuda.Stream(device=pot._X.device)
+        stream.wait_stream(torch.cuda.current_stream(pot._X.device))
+        _capi.check(lib.ts_b200_set_stream(k, C.c_void_p(stream.cuda_stream)), k)
+        dt = float(self.delta_t)
+        try:
+            with torch.cuda.stream(stream):
+                done = 0
+                while done < iterations:
+                    # the host path's times: t advanced by repeated addition
+                    b = min(max(pot.time_batch, 1), iterations - done)
+                    times = []
+                    for _ in range(b):
+                        times.append(self.current_evolution_time)
+                        self.current_evolution_time += dt
+                    if pot.time_batch:
+                        V = pot.device_values_batch(times)
+                    else:
+                        V = pot.device_values(times[0])
+                    W = V.shape[-1]
+                    _capi.check(lib.ts_b200_evolve_potentials(
+                        k, C.c_void_p(V.data_ptr()), W, W * V.shape[-2], b, dt, 0), k)
+                    done += b
+            stream.synchronize()
+        finally:
+            lib.ts_b200_set_stream(k, None)
+        if copy_back:
+            _chk(host().tsh_solver_evolve(self._h, 0, 0))  # copies the tile into the State
 
     def update_parameters(self):
         _chk(host().tsh_solver_update_parameters(self._h))

@@ -93,6 +93,19 @@ class Kernel:
     def set_exp_potential_device(self, ptr, pitch):
         self._check(lib().ts_b200_set_exp_potential_device(self._h, C.c_void_p(ptr), pitch))
 
+    def set_potential_device(self, ptr, pitch, delta_t):
+        """The table exp(-i dt V) (exp(-dt V) in imaginary time) built on the
+        device from V: dim_y rows of float64 at `ptr`, row pitch `pitch`."""
+        self._check(lib().ts_b200_set_potential_device(self._h, C.c_void_p(ptr), pitch,
+                                                       float(delta_t)))
+
+    def evolve_potentials(self, ptr, pitch, slab, count, delta_t, exchange=False):
+        """`count` steps, step i with the potential at ptr + i * slab doubles
+        (each dim_y rows of row pitch `pitch`) tabulated on the device."""
+        self._check(lib().ts_b200_evolve_potentials(self._h, C.c_void_p(ptr), pitch, slab,
+                                                    int(count), float(delta_t),
+                                                    int(bool(exchange))))
+
     # -- evolution ---------------------------------------------------------
     def step(self, exchange=True):
         self._check(lib().ts_b200_step(self._h, int(bool(exchange))))
