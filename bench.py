@@ -15,6 +15,10 @@ With N > 1 (torchrun, one process per GPU) every rank evolves its own copy
 (replicas: a single lattice is not split across GPUs), times are the max over
 ranks and the value is the total site-steps of all ranks per second.
 
+`--impl reference` times the reference's own CPU implementation (the
+reference arm's value) and, on the same GPU, the reference's own CUDA kernel
+(`reference_gpu_kernel`).
+
 The JSON line reports: value (device-resident, CUDA events on the kernel's
 stream), e2e (through the C ABI from pinned host buffers, state copied in and
 out every step), the roofline of the step kernel against the measured HBM
@@ -207,6 +211,34 @@ def cpu_reference_rate(psi0, budget_s=12.0, threads=None):
     return N_SIDE * N_SIDE * steps / secs, 1, "port", sample, steps
 
 
+def reference_gpu_kernel_rate(psi0, steps=TROTTER_PER_STEP):
+    """The reference's own CUDA kernel (CC2Kernel, src/gpukernel.cu and
+    src/gpucartesian.cu, kernel_type "gpu"; compiled for sm_100a into
+    oracle/_ref/libtsref_gpu.so) on the bench workload, on this box's GPU.
+    Its per-step device synchronisation and cuBLAS renormalisation are part of
+    what is timed, as in the reference.  None when the library or a GPU is
+    missing."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import tsref
+    try:
+        import torch
+        if not torch.cuda.is_available() or not tsref.available("gpu"):
+            return None
+    except ImportError:
+        return None
+    cfg = tsref.make_config(N_SIDE, LENGTH, harmonic=(OMEGA_X, OMEGA_Y, 1.0, 0.0, 0.0),
+                            coupling=G, delta_t=DT, segments=((1, True), (steps, True)),
+                            omp_threads=os.cpu_count() or 1, kernel_gpu=True)
+    _, res = tsref.run(cfg, psi0, None, flavour="gpu")
+    secs = res.seg_seconds[1]
+    return {"value": N_SIDE * N_SIDE * steps / secs, "unit": "site-steps/s",
+            "sample": f"{N_SIDE}x{N_SIDE} GPE imaginary time, {steps} Trotter steps after 1 "
+                      f"warm-up step, one evolve() call, wall time",
+            "kernel": "reference CC2Kernel (src/gpukernel.cu, src/gpucartesian.cu) built for "
+                      "sm_100a, same GPU",
+            "energy_after": res.total_energy}
+
+
 def run_reference_arm(args, rank, world, pg):
     if rank != 0:
         return
@@ -222,6 +254,7 @@ def run_reference_arm(args, rank, world, pg):
         rates.append(last[0])
     rate = statistics.mean(rates)
     _, cores, kind, sample, steps = last
+    ref_gpu = None if args.no_ref_gpu else reference_gpu_kernel_rate(psi0)
     line = {
         "impl": "reference", "metric": "site-steps/s", "value": rate, "unit": "site-steps/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -234,6 +267,7 @@ def run_reference_arm(args, rank, world, pg):
                          "sample": sample},
         "e2e": {"value": rate, "unit": "site-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
+        "reference_gpu_kernel": ref_gpu,
     }
     print(json.dumps(line), flush=True)
 
@@ -1034,6 +1068,8 @@ def main():
                     help="seconds of reference CPU work per sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32", action="store_true")
+    ap.add_argument("--no-ref-gpu", action="store_true",
+                    help="reference arm: skip timing the reference's CUDA kernel")
     ap.add_argument("--workload", choices=["gpe_imaginary_time_2048", "batch512", "adjoint512",
                                            "vortex8192", "moving_trap_2048"],
                     default="gpe_imaginary_time_2048")

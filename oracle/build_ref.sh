@@ -9,6 +9,7 @@
 #                     -fopenmp                    flags (configure.ac:37 uses -Ofast
 #                                                 -march=native; x86-64-v3 keeps the
 #                                                 binary runnable on another host CPU)
+#   libtsref_gpu.so   nvcc -DCUDA -O2, sm_100a    adds the reference's CUDA kernel
 #
 # Usage: oracle/build_ref.sh [reference_root]   (default /root/reference)
 set -eu
@@ -27,4 +28,15 @@ $CXX -O2 -fopenmp -fPIC -shared -w -I"$SRC" $FILES -o "$OUT/libtsref.so.tmp"
 mv "$OUT/libtsref.so.tmp" "$OUT/libtsref.so"
 $CXX -Ofast -march=x86-64-v3 -fopenmp -fPIC -shared -w -I"$SRC" $FILES -o "$OUT/libtsref_fast.so.tmp"
 mv "$OUT/libtsref_fast.so.tmp" "$OUT/libtsref_fast.so"
+# libtsref_gpu.so: the same sources plus the reference's own CUDA kernel
+# (CC2Kernel, src/gpukernel.cu + src/gpucartesian.cu, selected by
+# kernel_type "gpu"), -DCUDA as the reference's configure sets it, for sm_100a.
+NVCC=${NVCC:-/usr/local/cuda/bin/nvcc}
+if [ -x "$NVCC" ]; then
+    "$NVCC" -DCUDA -O2 -gencode arch=compute_100a,code=sm_100a -Xcompiler -fPIC,-fopenmp \
+        -shared -w -I"$SRC" $FILES "$SRC/gpukernel.cu" "$SRC/gpucartesian.cu" -lcublas -lgomp \
+        -o "$OUT/libtsref_gpu.so.tmp"
+    mv "$OUT/libtsref_gpu.so.tmp" "$OUT/libtsref_gpu.so"
+    echo "built $OUT/libtsref_gpu.so"
+fi
 echo "built $OUT/libtsref.so $OUT/libtsref_fast.so"

@@ -9,7 +9,8 @@
 //
 // The driver builds the reference objects through the reference's public API
 // (Lattice1D/Lattice2D, State/GaussianState/ExponentialState, Potential/
-// HarmonicPotential, Hamiltonian, Solver with kernel_type "cpu",
+// HarmonicPotential, Hamiltonian, Solver with kernel_type "cpu", or "gpu" in
+// the build that also compiles the reference's CUDA kernel,
 // src/trottersuzuki.h:34-597), runs Solver::evolve (src/solver.cpp:150-242)
 // and returns the tile, the energies (src/solver.cpp:566-680) and the state
 // expectation values (src/model.cpp:385-536).
@@ -43,6 +44,8 @@ struct tsref_config {
     int seg_iterations[8];
     int seg_imag[8];
     int omp_threads;             // <= 0: leave OpenMP's default
+    int kernel_gpu;              // 1: kernel_type "gpu", the reference's CUDA kernel
+                                 // (CC2Kernel, src/gpukernel.cu; libtsref_gpu.so only)
 };
 
 struct tsref_result {
@@ -145,7 +148,8 @@ int tsref_run(const tsref_config *cfg, double *psi_re, double *psi_im,
                                cfg->rot_coord_y / grid->delta_y;
             ham->potential = pot ? pot : new Potential(grid, const_potential);
         }
-        Solver *solver = new Solver(grid, state, ham, cfg->delta_t, "cpu");
+        Solver *solver = new Solver(grid, state, ham, cfg->delta_t,
+                                    cfg->kernel_gpu ? "gpu" : "cpu");
         res->initial_total_energy = solver->get_total_energy();
         res->initial_squared_norm = solver->get_squared_norm();
         auto t0 = std::chrono::steady_clock::now();

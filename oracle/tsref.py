@@ -1,9 +1,10 @@
 """ctypes binding of the reference's own CPU implementation (test infrastructure).
 
 oracle/build_ref.sh compiles the reference's unmodified C++ sources with
-oracle/ref_driver.cpp into oracle/_ref/libtsref.so (parity flavour, -O2) and
-libtsref_fast.so (the reference's -Ofast flags).  Only tests/, the golden
-fixture generator and bench.py's CPU-baseline leg use this module.
+oracle/ref_driver.cpp into oracle/_ref/libtsref.so (parity flavour, -O2),
+libtsref_fast.so (the reference's -Ofast flags) and libtsref_gpu.so (with the
+reference's CUDA kernel, kernel_gpu=True).  Only tests/, the golden fixture
+generator and bench.py's reference legs use this module.
 """
 import ctypes as C
 import os
@@ -35,6 +36,7 @@ class Config(C.Structure):
         ("seg_iterations", C.c_int * 8),
         ("seg_imag", C.c_int * 8),
         ("omp_threads", C.c_int),
+        ("kernel_gpu", C.c_int),
     ]
 
 
@@ -61,15 +63,16 @@ class Result(C.Structure):
 _libs = {}
 
 
+_NAMES = {"parity": "libtsref.so", "fast": "libtsref_fast.so", "gpu": "libtsref_gpu.so"}
+
+
 def available(flavour="parity"):
-    name = "libtsref.so" if flavour == "parity" else "libtsref_fast.so"
-    return os.path.exists(os.path.join(REF_DIR, name))
+    return os.path.exists(os.path.join(REF_DIR, _NAMES[flavour]))
 
 
 def _lib(flavour="parity"):
     if flavour not in _libs:
-        name = "libtsref.so" if flavour == "parity" else "libtsref_fast.so"
-        lib = C.CDLL(os.path.join(REF_DIR, name))
+        lib = C.CDLL(os.path.join(REF_DIR, _NAMES[flavour]))
         lib.tsref_run.argtypes = [C.POINTER(Config), C.c_void_p, C.c_void_p, C.c_void_p,
                                   C.POINTER(Result)]
         lib.tsref_run.restype = C.c_int
@@ -84,7 +87,7 @@ def make_config(dim_x, length_x, dim_y=None, length_y=None, periodic_x=False, pe
                 lattice_angular_velocity=None, *, gaussian=None, exponential=None,
                 harmonic=None, mass=1.0, coupling=0.0, lhy_coupling=0.0, angular_velocity=0.0,
                 rot_coord=(0.0, 0.0), force_rotation_periodic=False, delta_t=1e-4,
-                segments=((1, False),), omp_threads=1):
+                segments=((1, False),), omp_threads=1, kernel_gpu=False):
     """Build a Config.  dim_y == 0 selects a 1D lattice.
 
     gaussian = (omega_x, omega_y, mean_x, mean_y, norm, phase) -> GaussianState;
@@ -130,6 +133,7 @@ def make_config(dim_x, length_x, dim_y=None, length_y=None, periodic_x=False, pe
         c.seg_iterations[i] = int(it)
         c.seg_imag[i] = int(bool(imag))
     c.omp_threads = omp_threads
+    c.kernel_gpu = int(bool(kernel_gpu))
     return c
 
 
