@@ -91,6 +91,14 @@ def lib():
         L.tso_adjoint_real.argtypes = [C.POINTER(Params), dp, dp, C.c_double, dp, dp, C.c_int,
                                        dp, dp, dp, dp, dp]
         L.tso_adjoint_real.restype = C.c_int
+        L.tso_full_step2.argtypes = [C.POINTER(Params), C.c_double, dp, dp, dp, dp, dp, dp]
+        L.tso_rabi.argtypes = [C.POINTER(Params), C.c_double, C.c_double, C.c_double,
+                               C.c_double, dp, dp, dp, dp]
+        L.tso_evolve2.argtypes = [C.POINTER(Params), C.POINTER(Params)] + [C.c_double] * 4 + \
+            [dp, C.c_double] + [dp] * 8 + [C.c_int, C.c_int]
+        L.tso_evolve2.restype = C.c_int
+        L.tso_cross_energies.argtypes = [C.POINTER(Geometry), dp, dp, dp, dp, C.c_double,
+                                         C.c_double, C.c_double, dp, dp]
         _lib = L
     return _lib
 
@@ -222,6 +230,51 @@ def evolve(params, psi, pot_re, pot_im, iterations):
     pi = np.ascontiguousarray(pot_im, np.float64)
     lib().tso_evolve(C.byref(params), _ptr(re), _ptr(im), _ptr(pr), _ptr(pi), int(iterations))
     return re + 1j * im
+
+
+def _soa(psi):
+    return (np.ascontiguousarray(np.real(psi), np.float64).copy(),
+            np.ascontiguousarray(np.imag(psi), np.float64).copy())
+
+
+def evolve2(pa, pb, coupling_ab, omega_r, omega_i, delta_t, psi_a, psi_b, table_a, table_b,
+            iterations, norms=(0.0, 0.0), tot_norm=None, rabi_first_half=True):
+    """`iterations` steps of the two-component loop (src/solver.cpp:172-230).
+    pa.coupling / pb.coupling are g_a dt / g_b dt, coupling_ab is g_ab dt;
+    norms are the per-component norms kept in imaginary time.  Returns
+    (psi_a, psi_b, norms)."""
+    ar, ai = _soa(psi_a)
+    br, bi = _soa(psi_b)
+    tar, tai = (np.ascontiguousarray(t, np.float64) for t in table_a)
+    tbr, tbi = (np.ascontiguousarray(t, np.float64) for t in table_b)
+    nrm = np.array(norms, np.float64)
+    tot = float(nrm.sum()) if tot_norm is None else float(tot_norm)
+    rc = lib().tso_evolve2(C.byref(pa), C.byref(pb), coupling_ab, omega_r, omega_i, delta_t,
+                           _ptr(nrm), tot, _ptr(ar), _ptr(ai), _ptr(br), _ptr(bi), _ptr(tar),
+                           _ptr(tai), _ptr(tbr), _ptr(tbi), int(iterations),
+                           int(bool(rabi_first_half)))
+    if rc != 0:
+        raise MemoryError("tso_evolve2")
+    return ar + 1j * ai, br + 1j * bi, (float(nrm[0]), float(nrm[1]))
+
+
+def rabi(params, omega_r, omega_i, var, delta_t, psi_a, psi_b):
+    ar, ai = _soa(psi_a)
+    br, bi = _soa(psi_b)
+    lib().tso_rabi(C.byref(params), omega_r, omega_i, var, delta_t, _ptr(ar), _ptr(ai), _ptr(br),
+                   _ptr(bi))
+    return ar + 1j * ai, br + 1j * bi
+
+
+def cross_energies(lattice, psi_a, psi_b, coupling_ab, omega_r, omega_i):
+    """(inter-species, Rabi) energies of src/solver.cpp:340-353,549-550."""
+    ar, ai = _soa(psi_a)
+    br, bi = _soa(psi_b)
+    inter, rab = C.c_double(), C.c_double()
+    g = lattice.geometry()
+    lib().tso_cross_energies(C.byref(g), _ptr(ar), _ptr(ai), _ptr(br), _ptr(bi), coupling_ab,
+                             omega_r, omega_i, C.byref(inter), C.byref(rab))
+    return inter.value, rab.value
 
 
 def squared_norm(params, psi):

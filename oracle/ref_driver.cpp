@@ -203,4 +203,78 @@ int tsref_run(const tsref_config *cfg, double *psi_re, double *psi_im,
     return 0;
 }
 
+// Two components: Hamiltonian2Component and the two-state Solver
+// (src/trottersuzuki.h:455-497,541-569).  Lattice and time fields come from
+// `cfg` (arrays given for both states, matrix potentials for both); the
+// second component's constants from `c2`.
+struct tsref_config2 {
+    double mass_b, coupling_b, coupling_ab, omega_r, omega_i;
+};
+
+struct tsref_result2 {
+    double total_energy;
+    double kinetic[2], potential[2], rotational[2], intra[2];
+    double inter_species, rabi;
+    double squared_norm[2];
+    double seconds;
+    double seg_seconds[8];
+};
+
+int tsref_run2(const tsref_config *cfg, const tsref_config2 *c2, double *a_re, double *a_im,
+               double *b_re, double *b_im, const double *pot_a, const double *pot_b,
+               tsref_result2 *res) {
+    try {
+#ifdef _OPENMP
+        if (cfg->omp_threads > 0) omp_set_num_threads(cfg->omp_threads);
+#endif
+        Lattice2D *grid = new Lattice2D(cfg->dim_x, cfg->length_x, cfg->dim_y, cfg->length_y,
+                                        cfg->periodic_x != 0, cfg->periodic_y != 0, 0.);
+        const size_t n = size_t(grid->dim_x) * grid->dim_y;
+        std::vector<double> ar(a_re, a_re + n), ai(a_im, a_im + n), br(b_re, b_re + n),
+            bi(b_im, b_im + n), va(pot_a, pot_a + n), vb(pot_b, pot_b + n);
+        State *sa = new State(grid, 0, ar.data(), ai.data());
+        State *sb = new State(grid, 0, br.data(), bi.data());
+        Potential *pa = new Potential(grid, va.data());
+        Potential *pb = new Potential(grid, vb.data());
+        Hamiltonian2Component *ham = new Hamiltonian2Component(
+            grid, pa, pb, cfg->mass, c2->mass_b, cfg->coupling, c2->coupling_ab, c2->coupling_b,
+            c2->omega_r, c2->omega_i, 0., 0., 0.);
+        Solver *solver = new Solver(grid, sa, sb, ham, cfg->delta_t,
+                                    cfg->kernel_gpu ? "gpu" : "cpu");
+        auto t0 = std::chrono::steady_clock::now();
+        for (int s = 0; s < cfg->n_segments; ++s) {
+            auto ts = std::chrono::steady_clock::now();
+            solver->evolve(cfg->seg_iterations[s], cfg->seg_imag[s] != 0);
+            res->seg_seconds[s] =
+                std::chrono::duration<double>(std::chrono::steady_clock::now() - ts).count();
+        }
+        res->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        res->total_energy = solver->get_total_energy();
+        for (int c = 0; c < 2; ++c) {
+            res->kinetic[c] = solver->get_kinetic_energy(c + 1);
+            res->potential[c] = solver->get_potential_energy(c + 1);
+            res->rotational[c] = solver->get_rotational_energy(c + 1);
+            res->intra[c] = solver->get_intra_species_energy(c + 1);
+            res->squared_norm[c] = solver->get_squared_norm(c + 1);
+        }
+        res->inter_species = solver->get_inter_species_energy();
+        res->rabi = solver->get_rabi_energy();
+        memcpy(a_re, sa->p_real, n * sizeof(double));
+        memcpy(a_im, sa->p_imag, n * sizeof(double));
+        memcpy(b_re, sb->p_real, n * sizeof(double));
+        memcpy(b_im, sb->p_imag, n * sizeof(double));
+        delete solver;
+        delete ham;
+        delete pa;
+        delete pb;
+        delete sa;
+        delete sb;
+        delete grid;
+    } catch (std::exception &e) {
+        snprintf(g_err, sizeof g_err, "%s", e.what());
+        return 1;
+    }
+    return 0;
+}
+
 }  // extern "C"

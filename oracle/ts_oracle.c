@@ -15,6 +15,8 @@
  *   - imaginary-time renorm   src/cpukernel.cpp:526-570
  *   - evolve loop             src/solver.cpp:150-242
  *   - energies                src/solver.cpp:244-564 (single component)
+ *   - two components          src/cpucartesian.cpp:73-126,264-290,
+ *                             src/cpukernel.cpp:581-667, src/solver.cpp:172-230
  *   - expectation values      src/model.cpp:385-536
  *
  * The reference evolves the tile in 128x128 cache blocks with a 4 (8 with
@@ -220,6 +222,148 @@ void tso_evolve(const tso_params *p, double *re, double *im, const double *pot_r
         if (i != iterations - 1) tso_halo_exchange(p, re, im);
         renormalise(p, re, im);
     }
+}
+
+/* ---- two components ------------------------------------------------------
+ * The two-wavefunction path of the reference: the step of one component with
+ * the other's density in the nonlinear phase (src/cpucartesian.cpp:73-92,
+ * 113-126: exp(-i (g dt |a|^2 + g_ab dt |b|^2)), |b|^2 from the other
+ * component's buffer at the start of the component's step), the Rabi
+ * rotation (src/cpucartesian.cpp:264-290 with the angle of
+ * src/cpukernel.cpp:581-606) and, in imaginary time with a Rabi coupling,
+ * the joint normalisation (src/cpukernel.cpp:608-667); the loop is
+ * src/solver.cpp:172-230 (B steps with A's state from before A's step). */
+static void potential_step2(const tso_params *p, double coupling_ab, const double *pot_re,
+                            const double *pot_im, const double *pb_re, const double *pb_im,
+                            double *re, double *im) {
+    const size_t n = (size_t)p->W * p->H;
+    for (size_t k = 0; k < n; ++k) {
+        double n2 = re[k] * re[k] + im[k] * im[k];
+        double n2b = pb_re[k] * pb_re[k] + pb_im[k] * pb_im[k];
+        if (p->imag_time) {
+            double t = exp(-1. * (p->coupling * n2 + coupling_ab * n2b));
+            re[k] = t * pot_re[k] * re[k];
+            im[k] = t * pot_re[k] * im[k];
+        } else {
+            double c = cos(p->coupling * n2 + coupling_ab * n2b);
+            double s = sin(p->coupling * n2 + coupling_ab * n2b);
+            double t = re[k];
+            re[k] = pot_re[k] * t - pot_im[k] * im[k];
+            im[k] = pot_re[k] * im[k] + pot_im[k] * t;
+            t = re[k];
+            re[k] = c * t + s * im[k];
+            im[k] = c * im[k] - s * t;
+        }
+    }
+}
+
+void tso_full_step2(const tso_params *p, double coupling_ab, double *re, double *im,
+                    const double *pot_re, const double *pot_im, const double *pb_re,
+                    const double *pb_im) {
+    const int vert = p->H > 1;
+    if (vert) sweep_vertical(p, 0, p->aV, p->bV, re, im);
+    sweep_horizontal(p, 0, p->aH, p->bH, re, im);
+    if (vert) sweep_vertical(p, 1, p->aV, p->bV, re, im);
+    sweep_horizontal(p, 1, p->aH, p->bH, re, im);
+    potential_step2(p, coupling_ab, pot_re, pot_im, pb_re, pb_im, re, im);
+    if (p->alpha_x != 0. && p->alpha_y != 0.) {
+        rotation_rows(p, re, im);
+        rotation_cols(p, re, im);
+        rotation_rows(p, re, im);
+    }
+    sweep_horizontal(p, 1, p->aH, p->bH, re, im);
+    if (vert) sweep_vertical(p, 1, p->aV, p->bV, re, im);
+    sweep_horizontal(p, 0, p->aH, p->bH, re, im);
+    if (vert) sweep_vertical(p, 0, p->aV, p->bV, re, im);
+}
+
+void tso_rabi(const tso_params *p, double omega_r, double omega_i, double var, double delta_t,
+              double *a_re, double *a_im, double *b_re, double *b_im) {
+    const double c3 = 0.5 * omega_r, c4 = 0.5 * omega_i;
+    const double norm_omega = sqrt(c3 * c3 + c4 * c4);
+    double cc, cs_r, cs_i;
+    if (p->imag_time) {
+        cc = cosh(-delta_t * var * norm_omega);
+        cs_r = norm_omega == 0 ? 0 : c3 / norm_omega * sinh(-delta_t * var * norm_omega);
+        cs_i = norm_omega == 0 ? 0 : c4 / norm_omega * sinh(-delta_t * var * norm_omega);
+    } else {
+        cc = cos(-delta_t * var * norm_omega);
+        cs_r = norm_omega == 0 ? 0 : c3 / norm_omega * sin(-delta_t * var * norm_omega);
+        cs_i = norm_omega == 0 ? 0 : c4 / norm_omega * sin(-delta_t * var * norm_omega);
+    }
+    const size_t n = (size_t)p->W * p->H;
+    for (size_t k = 0; k < n; ++k) {
+        double r = a_re[k], i = a_im[k];
+        if (p->imag_time) {
+            a_re[k] = cc * r + cs_r * b_re[k] - cs_i * b_im[k];
+            a_im[k] = cc * i + cs_i * b_re[k] + cs_r * b_im[k];
+            b_re[k] = cc * b_re[k] + cs_r * r + cs_i * i;
+            b_im[k] = cc * b_im[k] - cs_i * r + cs_r * i;
+        } else {
+            a_re[k] = cc * r - cs_i * b_re[k] - cs_r * b_im[k];
+            a_im[k] = cc * i + cs_r * b_re[k] - cs_i * b_im[k];
+            b_re[k] = cc * b_re[k] + cs_i * r - cs_r * i;
+            b_im[k] = cc * b_im[k] + cs_r * r + cs_i * i;
+        }
+    }
+}
+
+static double inner_sum(const tso_params *p, const double *re, const double *im) {
+    double s = 0.;
+    for (int y = p->iy0; y < p->iy1; ++y)
+        for (int x = p->ix0; x < p->ix1; ++x) {
+            size_t k = (size_t)y * p->W + x;
+            s += re[k] * re[k] + im[k] * im[k];
+        }
+    return s;
+}
+
+static void scale_tile(const tso_params *p, double f, double *re, double *im) {
+    const size_t n = (size_t)p->W * p->H;
+    for (size_t k = 0; k < n; ++k) {
+        re[k] /= f;
+        im[k] /= f;
+    }
+}
+
+int tso_evolve2(const tso_params *pa, const tso_params *pb, double coupling_ab, double omega_r,
+                double omega_i, double delta_t, double *norms, double tot_norm, double *a_re,
+                double *a_im, double *b_re, double *b_im, const double *ta_re,
+                const double *ta_im, const double *tb_re, const double *tb_im, int iterations,
+                int rabi_first_half) {
+    const size_t n = (size_t)pa->W * pa->H;
+    double *old_re = malloc(n * sizeof(double)), *old_im = malloc(n * sizeof(double));
+    if (!old_re || !old_im) {
+        free(old_re);
+        free(old_im);
+        return 1;
+    }
+    if (rabi_first_half) tso_rabi(pa, omega_r, omega_i, 0.5, delta_t, a_re, a_im, b_re, b_im);
+    for (int i = 0; i < iterations; ++i) {
+        memcpy(old_re, a_re, n * sizeof(double));
+        memcpy(old_im, a_im, n * sizeof(double));
+        tso_full_step2(pa, coupling_ab, a_re, a_im, ta_re, ta_im, b_re, b_im);
+        if (i != iterations - 1) tso_halo_exchange(pa, a_re, a_im);
+        if (pa->imag_time && norms[0] != 0)
+            scale_tile(pa, sqrt(tso_squared_norm(pa, a_re, a_im) / norms[0]), a_re, a_im);
+        tso_full_step2(pb, coupling_ab, b_re, b_im, tb_re, tb_im, old_re, old_im);
+        if (i != iterations - 1) tso_halo_exchange(pb, b_re, b_im);
+        if (pb->imag_time && norms[1] != 0)
+            scale_tile(pb, sqrt(tso_squared_norm(pb, b_re, b_im) / norms[1]), b_re, b_im);
+        tso_rabi(pa, omega_r, omega_i, i == iterations - 1 ? 0.5 : 1., delta_t, a_re, a_im, b_re,
+                 b_im);
+        if (pa->imag_time && (omega_r != 0 || omega_i != 0)) {
+            double sa = inner_sum(pa, a_re, a_im), sb = inner_sum(pa, b_re, b_im);
+            double f = sqrt((sa + sb) * pa->delta_x * pa->delta_y / tot_norm);
+            scale_tile(pa, f, a_re, a_im);
+            scale_tile(pa, f, b_re, b_im);
+            norms[0] = sa / (sa + sb) * tot_norm;
+            norms[1] = sb / (sa + sb) * tot_norm;
+        }
+    }
+    free(old_re);
+    free(old_im);
+    return 0;
 }
 
 /* ---- reverse mode of tso_evolve (real time, closed tile) ----------------
@@ -507,4 +651,37 @@ void tso_expectations(const tso_geometry *g, const double *re, const double *im,
     out->mean_pypy = -spypy * param_py * param_py / s_n2;
     out->mean_lz = slz / s_n2;
     out->norm2 = s_n2 * (g->delta_x * g->delta_y);
+}
+
+/* Cross terms of the two-component energy (src/solver.cpp:340-353,438-439,
+ * 549-550), kept as the reference writes them: g_ab |a|^4 |b|^4 summed and
+ * divided by (sum |a|^2)(sum |b|^2), and 0.5 * sum |a|^2 |b|^2 2 Re(conj(a) b
+ * omega) likewise. */
+void tso_cross_energies(const tso_geometry *g, const double *a_re, const double *a_im,
+                        const double *b_re, const double *b_im, double coupling_ab,
+                        double omega_r, double omega_i, double *inter, double *rabi) {
+    double s_a = 0, s_b = 0, s_inter = 0, s_rabi = 0;
+    for (int i = g->iy0; i < g->iy1; ++i)
+        for (int j = g->ix0; j < g->ix1; ++j) {
+            size_t k = (size_t)i * g->W + j;
+            cplx a = cload(a_re, a_im, k), b = cload(b_re, b_im, k);
+            cplx om = {omega_r, omega_i};
+            double na = cmul(conjc(a), a).re, nb = cmul(conjc(b), b).re;
+            s_a += na;
+            s_b += nb;
+            /* left to right, as the reference's expressions evaluate */
+            cplx t = cmul(conjc(a), a);
+            t = cmul(t, conjc(a));
+            t = cmul(t, a);
+            t = cmul(t, conjc(b));
+            t = cmul(t, b);
+            t = cmul(t, conjc(b));
+            t = cmul(t, b);
+            s_inter += cmul(t, (cplx){coupling_ab, 0.}).re;
+            cplx u = cadd(cmul(cmul(conjc(a), b), om), cmul(conjc(cmul(b, om)), a));
+            cplx v = cmul(cmul(cmul(conjc(a), a), conjc(b)), b);
+            s_rabi += cmul(v, u).re;
+        }
+    *inter = s_inter / (s_a * s_b);
+    *rabi = 0.5 * s_rabi / (s_a * s_b);
 }

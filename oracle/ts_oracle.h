@@ -57,7 +57,25 @@ int tso_adjoint_real(const tso_params *p, const double *pot_re, const double *po
 
 void tso_evolve(const tso_params *p, double *re, double *im, const double *pot_re,
                 const double *pot_im, int iterations);
+/* Two components: one component's step with the other's density (pb) in
+ * the phase; the Rabi rotation of both tiles; `iterations` steps of the
+ * two-component loop.  norms[2] (the per-component norms kept in imaginary
+ * time) are updated by the joint normalisation; tot_norm is their initial
+ * sum.  Returns non-zero when out of memory. */
+void tso_full_step2(const tso_params *p, double coupling_ab, double *re, double *im,
+                    const double *pot_re, const double *pot_im, const double *pb_re,
+                    const double *pb_im);
+void tso_rabi(const tso_params *p, double omega_r, double omega_i, double var, double delta_t,
+              double *a_re, double *a_im, double *b_re, double *b_im);
+int tso_evolve2(const tso_params *pa, const tso_params *pb, double coupling_ab, double omega_r,
+                double omega_i, double delta_t, double *norms, double tot_norm, double *a_re,
+                double *a_im, double *b_re, double *b_im, const double *ta_re,
+                const double *ta_im, const double *tb_re, const double *tb_im, int iterations,
+                int rabi_first_half);
 void tso_coordinates(const tso_geometry *g, int x_in, int y_in, double *x_out, double *y_out);
+void tso_cross_energies(const tso_geometry *g, const double *a_re, const double *a_im,
+                        const double *b_re, const double *b_im, double coupling_ab,
+                        double omega_r, double omega_i, double *inter, double *rabi);
 void tso_energies(const tso_geometry *g, const double *re, const double *im, const double *V,
                   double mass, double g_coupling, double g_lhy, double omega,
                   tso_energy_result *out);

@@ -60,6 +60,22 @@ class Result(C.Structure):
     ]
 
 
+class Config2(C.Structure):
+    _fields_ = [(n, C.c_double) for n in
+                ("mass_b", "coupling_b", "coupling_ab", "omega_r", "omega_i")]
+
+
+class Result2(C.Structure):
+    _fields_ = [
+        ("total_energy", C.c_double),
+        ("kinetic", C.c_double * 2), ("potential", C.c_double * 2),
+        ("rotational", C.c_double * 2), ("intra", C.c_double * 2),
+        ("inter_species", C.c_double), ("rabi", C.c_double),
+        ("squared_norm", C.c_double * 2),
+        ("seconds", C.c_double), ("seg_seconds", C.c_double * 8),
+    ]
+
+
 _libs = {}
 
 
@@ -79,6 +95,9 @@ def _lib(flavour="parity"):
         lib.tsref_geometry.argtypes = [C.POINTER(Config), C.POINTER(Result)]
         lib.tsref_geometry.restype = C.c_int
         lib.tsref_last_error.restype = C.c_char_p
+        lib.tsref_run2.argtypes = [C.POINTER(Config), C.POINTER(Config2)] + [C.c_void_p] * 6 + \
+            [C.POINTER(Result2)]
+        lib.tsref_run2.restype = C.c_int
         _libs[flavour] = lib
     return _libs[flavour]
 
@@ -160,3 +179,23 @@ def run(cfg, psi=None, potential=None, flavour="parity"):
     if rc != 0:
         raise RuntimeError(_lib(flavour).tsref_last_error().decode())
     return re + 1j * im, res
+
+
+def run2(cfg, c2, psi_a, psi_b, pot_a, pot_b, flavour="parity"):
+    """Two components (arrays and matrix potentials for both): returns
+    (psi_a, psi_b, Result2)."""
+    geo = geometry(cfg, flavour)
+    shape = (geo.dim_y, geo.dim_x)
+    arrs = []
+    for psi in (psi_a, psi_b):
+        re = np.ascontiguousarray(np.real(psi), np.float64).reshape(shape).copy()
+        im = np.ascontiguousarray(np.imag(psi), np.float64).reshape(shape).copy()
+        arrs += [re, im]
+    va = np.ascontiguousarray(pot_a, np.float64)
+    vb = np.ascontiguousarray(pot_b, np.float64)
+    res = Result2()
+    rc = _lib(flavour).tsref_run2(C.byref(cfg), C.byref(c2), *[a.ctypes.data for a in arrs],
+                                  va.ctypes.data, vb.ctypes.data, C.byref(res))
+    if rc != 0:
+        raise RuntimeError(_lib(flavour).tsref_last_error().decode())
+    return arrs[0] + 1j * arrs[1], arrs[2] + 1j * arrs[3], res

@@ -8,6 +8,8 @@ values) as a compressed .npz.  The reference ships no golden vectors of its
 own; these fixtures pin both the oracle restatement and the B200 kernel.
 
     python tests/golden/gen_golden.py        (needs oracle/_ref, i.e. the reference sources)
+
+Two-component cases (Hamiltonian2Component, the two-state Solver) go to two/.
 """
 import json
 import os
@@ -59,6 +61,56 @@ def inputs(case, seed):
     return lat, psi0, V
 
 
+# Two components (files under two/): lattice (N, L, Ny, periodic_x, periodic_y),
+# g_a, g_b, g_ab, mass_b, Rabi omega = (omega_r, omega_i), evolve segments.
+CASES2 = {
+    "two_real_rabi": dict(lat=(40, 8.0, None, False, False), g=2.0, g_b=1.0, g_ab=1.5,
+                          mass_b=1.5, omega=(3.0, 1.0), dt=1e-3, segments=[(15, False), (6, False)]),
+    "two_imag_rabi": dict(lat=(40, 8.0, None, False, False), g=2.0, g_b=1.0, g_ab=1.5,
+                          mass_b=1.5, omega=(3.0, 1.0), dt=1e-3, segments=[(20, True)]),
+    "two_imag_norabi": dict(lat=(36, 8.0, 30, False, False), g=4.0, g_b=2.0, g_ab=3.0,
+                            mass_b=1.0, omega=(0.0, 0.0), dt=1e-3, segments=[(20, True)]),
+    "two_periodic_real": dict(lat=(36, 8.0, 32, True, True), g=1.0, g_b=2.0, g_ab=0.5,
+                              mass_b=0.8, omega=(2.0, 0.0), dt=1e-3, segments=[(10, False)]),
+}
+
+
+def inputs2(case, seed):
+    N, L, Ny, px, py = case["lat"]
+    lat = O.Lattice(N, L, Ny, None, px, py, 0.0)
+    rng = np.random.default_rng(seed)
+    X, Y = lat.coordinates()
+    dxdy = lat.delta_x * lat.delta_y
+    a = np.exp(-((X - 0.4) ** 2 + (Y + 0.3) ** 2) / 2.0) * np.exp(1j * 0.5 * X)
+    a = a * (1 + 0.02 * rng.uniform(-1, 1, lat.shape))
+    a = a / np.sqrt(np.sum(np.abs(a) ** 2) * dxdy)
+    b = np.exp(-((X + 0.5) ** 2 + (Y - 0.2) ** 2) / 1.5) * np.exp(-1j * 0.3 * Y)
+    b = b * (1 + 0.02 * rng.uniform(-1, 1, lat.shape))
+    b = 0.7 * b / np.sqrt(np.sum(np.abs(b) ** 2) * dxdy)
+    Va = 0.5 * (X ** 2 + 1.3 * Y ** 2) + 0.1 * rng.uniform(-1, 1, lat.shape)
+    Vb = 0.5 * (1.2 * (X - 0.3) ** 2 + Y ** 2) + 0.1 * rng.uniform(-1, 1, lat.shape)
+    return lat, a, b, Va, Vb
+
+
+def main2():
+    os.makedirs(os.path.join(HERE, "two"), exist_ok=True)
+    for i, (name, case) in enumerate(sorted(CASES2.items())):
+        lat, a, b, Va, Vb = inputs2(case, seed=2000 + i)
+        N, L, Ny, px, py = case["lat"]
+        cfg = tsref.make_config(N, L, Ny, None, px, py, 0.0, harmonic=None, coupling=case["g"],
+                                delta_t=case["dt"], segments=case["segments"], omp_threads=1)
+        c2 = tsref.Config2(case["mass_b"], case["g_b"], case["g_ab"], *case["omega"])
+        pa, pb, res = tsref.run2(cfg, c2, a, b, Va, Vb)
+        meta = dict(case, name=name)
+        np.savez_compressed(
+            os.path.join(HERE, "two", name + ".npz"), psi0_a=a, psi0_b=b, Va=Va, Vb=Vb,
+            psi_a=pa, psi_b=pb,
+            energies=np.array([res.total_energy, *res.kinetic, *res.potential, *res.rotational,
+                               *res.intra, res.inter_species, res.rabi, *res.squared_norm]),
+            meta=json.dumps(meta))
+        print(f"{name}: tile {pa.shape}, E = {res.total_energy:.15g}")
+
+
 def main():
     if not tsref.available():
         raise SystemExit("oracle/_ref/libtsref.so is missing: run oracle/build_ref.sh first")
@@ -81,6 +133,7 @@ def main():
                                    res.mean_pypy, res.mean_lz]),
             meta=json.dumps(meta))
         print(f"{name}: tile {psi.shape}, E = {res.total_energy:.15g}")
+    main2()
 
 
 if __name__ == "__main__":
