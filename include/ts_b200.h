@@ -297,6 +297,42 @@ int ts_b200_adjoint_backward(ts_b200_adjoint *a, const void *grad_psi_t, double 
 int ts_b200_adjoint_synchronize(ts_b200_adjoint *a);
 const char *ts_b200_adjoint_last_error(const ts_b200_adjoint *a);
 
+/* ------------------------------------------------------------ two components
+ * Two species evolved together: the reference's two-wavefunction kernel and
+ * loop (CPUBlock two-state constructor src/cpukernel.cpp:274-392,
+ * rabi_coupling / normalization src/cpukernel.cpp:581-667, the coupled phase
+ * src/cpucartesian.cpp:73-92,113-126, the Rabi rotation
+ * src/cpucartesian.cpp:264-290, Solver::evolve src/solver.cpp:172-230).
+ * `a` and `b` are two tiles of the same geometry, precision and time mode,
+ * each with its own state, table and step constants (mass, g * dt, norm0 of
+ * its ts_b200_desc); no rotating frame and no Lee-Huang-Yang term, as in the
+ * reference's two-component path.  While paired the tiles step only through
+ * the pair (ts_b200_step / ts_b200_evolve on them return
+ * TS_B200_UNSUPPORTED); their states are read and written with the tiles' own
+ * calls, and b's work is queued on a's stream. */
+typedef struct ts_b200_pair ts_b200_pair;
+
+/* coupling_ab: g_ab; omega_r, omega_i: the Rabi coupling omega (the
+ * reference's Hamiltonian2Component::omega_r, omega_i). */
+int ts_b200_pair_create(ts_b200_kernel *a, ts_b200_kernel *b, double coupling_ab,
+                        double omega_r, double omega_i, double delta_t, ts_b200_pair **out);
+/* The Rabi rotation by var * delta_t alone: Solver::evolve's half step before
+ * the loop (src/solver.cpp:172-177, rabi_coupling(0.5, delta_t)). */
+int ts_b200_pair_rabi(ts_b200_pair *p, double var);
+/* `iterations` steps of the loop: species a, species b (with a's state from
+ * before a's step), the Rabi rotation (a half one on the last step), and in
+ * imaginary time with a Rabi coupling the joint normalisation.  Every step
+ * but the last refreshes the halos. */
+int ts_b200_pair_evolve(ts_b200_pair *p, int iterations);
+/* Inter-species and Rabi energies of Solver::calculate_energy_expected_values
+ * (src/solver.cpp:340-353,438-439,549-550), as the reference writes them:
+ * sum g_ab |a|^4 |b|^4 and 0.5 sum |a|^2 |b|^2 2 Re(conj(a) b omega), each over
+ * (sum |a|^2)(sum |b|^2) on the inner region.  Synchronises a's stream. */
+int ts_b200_pair_cross_energies(ts_b200_pair *p, double *inter_species, double *rabi);
+const char *ts_b200_pair_last_error(const ts_b200_pair *p);
+/* Unpairs the tiles (each then steps alone again) and frees the pair. */
+int ts_b200_pair_destroy(ts_b200_pair *p);
+
 /* Autotuner for this tile: times `trial_steps` steps for each balanced launch
  * shape (rows per segment such that every SM holds the same number of
  * blocks, for 1 .. the resident blocks per SM, 4 or 2 warps per block) and

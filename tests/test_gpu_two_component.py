@@ -1,0 +1,114 @@
+"""Two components on the GPU (ts_b200_pair_*) against the reference's
+two-state Solver (golden fixtures under tests/golden/two/) and the oracle.
+
+One evolve() call of the reference's two-component Solver is a Rabi half step
+followed by the loop (src/solver.cpp:172-230); here that is pair.rabi(0.5)
+then pair.evolve(n).  The species' tiles keep their own states, tables and
+step constants; the cross energies come from the pair.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from helpers import desc_from_params, energy_params
+from test_oracle_two import load_two, oracle_two, two_names
+
+pytestmark = pytest.mark.gpu
+
+
+def run_pair(lat, meta, z, precision=0, segments=None):
+    from trottersuzuki_b200 import Kernel, Pair
+    dt, imag = meta["dt"], meta["segments"][0][1]
+    a0, b0 = z["psi0_a"], z["psi0_b"]
+    na = O.expectations(lat, a0)["norm2"] if imag else 0.0
+    nb = O.expectations(lat, b0)["norm2"] if imag else 0.0
+    pa = lat.params(dt, imag, 1.0, meta["g"], 0.0, 0.0, norm0=na)
+    pb = lat.params(dt, imag, meta["mass_b"], meta["g_b"], 0.0, 0.0, norm0=nb)
+    ka, kb = Kernel(desc_from_params(pa, precision)), Kernel(desc_from_params(pb, precision))
+    ka.set_state(a0)
+    kb.set_state(b0)
+    ka.set_exp_potential(*O.exp_table(z["Va"], dt, imag))
+    kb.set_exp_potential(*O.exp_table(z["Vb"], dt, imag))
+    pair = Pair(ka, kb, meta["g_ab"], meta["omega"][0], meta["omega"][1], dt)
+    for it, seg_imag in (segments or meta["segments"]):
+        assert seg_imag == imag
+        pair.rabi(0.5)
+        pair.evolve(it)
+    return ka, kb, pair
+
+
+def gpu_energies(lat, meta, z, ka, kb, pair):
+    ea = ka.energies(z["Va"], energy_params(lat, 1.0, meta["g"]))
+    eb = kb.energies(z["Vb"], energy_params(lat, meta["mass_b"], meta["g_b"]))
+    inter, rabi = pair.cross_energies()
+    total = sum(e[k] for e in (ea, eb) for k in ("kinetic", "potential", "intra", "rotational"))
+    total += inter + rabi
+    return np.array([total, ea["kinetic"], eb["kinetic"], ea["potential"], eb["potential"],
+                     ea["rotational"], eb["rotational"], ea["intra"], eb["intra"], inter, rabi,
+                     ea["norm2"], eb["norm2"]])
+
+
+@pytest.mark.parametrize("name", two_names())
+def test_pair_matches_reference_fixture(name):
+    lat, meta, z = load_two(name)
+    ka, kb, pair = run_pair(lat, meta, z)
+    a, b = ka.get_state(), kb.get_state()
+    assert np.abs(a - z["psi_a"]).max() <= 1e-10
+    assert np.abs(b - z["psi_b"]).max() <= 1e-10
+    e = gpu_energies(lat, meta, z, ka, kb, pair)
+    assert np.allclose(e, z["energies"], rtol=1e-10, atol=1e-12), (e, z["energies"])
+    pair.close()
+
+
+@pytest.mark.parametrize("name", ["two_real_rabi", "two_imag_rabi"])
+def test_pair_fp32_storage(name):
+    lat, meta, z = load_two(name)
+    ka, kb, pair = run_pair(lat, meta, z, precision=1)
+    a, b = ka.get_state(), kb.get_state()
+    for got, want in ((a, z["psi_a"]), (b, z["psi_b"])):
+        assert np.abs(got - want).max() <= 2e-5 * np.abs(want).max()
+    e = gpu_energies(lat, meta, z, ka, kb, pair)
+    assert np.allclose(e, z["energies"], rtol=2e-5, atol=1e-9)
+    pair.close()
+
+
+def test_pair_longer_run_matches_oracle():
+    """Many steps, odd step counts per call (buffer parities of both species)."""
+    lat, meta, z = load_two("two_imag_rabi")
+    segs = [(33, True), (8, True)]
+    ka, kb, pair = run_pair(lat, meta, z, segments=segs)
+    ref_a, ref_b, _ = oracle_two(lat, dict(meta, segments=segs), z)
+    assert np.abs(ka.get_state() - ref_a).max() <= 1e-10
+    assert np.abs(kb.get_state() - ref_b).max() <= 1e-10
+    pair.close()
+
+
+def test_pair_rules():
+    from trottersuzuki_b200 import B200Error, Kernel, Pair
+    lat, meta, z = load_two("two_real_rabi")
+    p = lat.params(1e-3, False, 1.0, 1.0, 0.0, 0.0)
+    ka, kb = Kernel(desc_from_params(p)), Kernel(desc_from_params(p))
+    for k, s in ((ka, z["psi0_a"]), (kb, z["psi0_b"])):
+        k.set_state(s)
+        k.set_exp_potential(*O.exp_table(z["Va"], 1e-3, False))
+    with pytest.raises(B200Error):
+        Pair(ka, ka, 1.0, 0.0, 0.0, 1e-3)  # the same tile twice
+    other = O.Lattice(32, 8.0)
+    kc = Kernel(desc_from_params(other.params(1e-3, False)))
+    with pytest.raises(B200Error):
+        Pair(ka, kc, 1.0, 0.0, 0.0, 1e-3)  # different geometry
+    pair = Pair(ka, kb, 1.0, 2.0, 0.0, 1e-3)
+    with pytest.raises(B200Error):
+        ka.evolve(1)  # a paired tile steps only through the pair
+    with pytest.raises(B200Error):
+        Pair(ka, kc, 1.0, 0.0, 0.0, 1e-3)  # already paired
+    pair.evolve(3)
+    pair.close()
+    # unpaired, each tile steps alone again and matches a fresh single tile
+    psi = ka.get_state()
+    ka.evolve(5)
+    with Kernel(desc_from_params(p)) as k1:
+        k1.set_state(psi)
+        k1.set_exp_potential(*O.exp_table(z["Va"], 1e-3, False))
+        k1.evolve(5)
+        assert np.array_equal(k1.get_state(), ka.get_state())

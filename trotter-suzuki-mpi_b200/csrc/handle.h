@@ -15,7 +15,7 @@ struct ts_b200_kernel {
     ts_b200_desc d{};
     int W = 0, H = 0, P = 0;
     bool fp32 = false, imag = false, rot = false;
-    int phase = 0;  // 0 none, 1 g|psi|^2, 2 with Lee-Huang-Yang
+    int phase = 0;  // 0 none, 1 g|psi|^2, 2 with Lee-Huang-Yang, 3 one component of a pair
     size_t cell = 0, tab_cell = 0;
     void *psi[2] = {nullptr, nullptr};
     int cur = 0;
@@ -39,6 +39,13 @@ struct ts_b200_kernel {
     float4 *kin_sched = nullptr;  // FP32 real time: per-step kinetic coefficients
     int num_sms = 148;
     int device = 0;
+    // two components (pair.cu): the tile is one species of a ts_b200_pair;
+    // pb / pb_scale / cab are the other species' tile for the next step
+    bool pair_mode = false;
+    int phase_alone = 0;  // phase outside the pair
+    const void *pb = nullptr;
+    const double *pb_scale = nullptr;
+    double cab = 0.0;
     std::string err;
 };
 
@@ -52,12 +59,16 @@ inline int div_up(long a, long b) { return (int)((a + b - 1) / b); }
 // Entries of the FP32 real-time kinetic coefficient schedule (repeats after).
 constexpr int kSchedLen = 4096;
 
-// Bytes of one ring slot: a row of 32*C cells of psi and of the table.
-inline int slot_bytes(int C, bool fp32, bool imag) {
+// Bytes of one ring slot: a row of 32*C cells of psi and of the table (and,
+// for one species of a pair, of the other species).
+inline int slot_bytes(int C, bool fp32, bool imag, bool pb = false) {
     const int cell = fp32 ? 8 : 16;
     const int tab = imag ? cell / 2 : cell;
-    return 32 * C * (cell + tab);
+    return 32 * C * (cell + tab + (pb ? cell : 0));
 }
+
+// Kernel launches of one step of the tile (exchange: with the halo refresh).
+int launch_step_tile(ts_b200_kernel *k, int exchange);
 
 // Step constants of a tile in the kernel's precision (delta form in float):
 // every StepArgs field except the buffers, the task geometry and the scratch.

@@ -56,6 +56,10 @@ struct Scalars {
     int error;           // non-zero: a bounded wait gave up
     int renorm;          // imaginary-time renormalisation enabled (norm0 != 0)
     unsigned int step;   // steps taken (indexes the coefficient schedule)
+    // two components: pending_inv before the last step's update (the factor
+    // of the buffer that step read) and the norm the next step keeps
+    double prev_inv;
+    double norm_target;
 };
 
 template <typename T>
@@ -77,6 +81,11 @@ struct StepArgs {
     int sched_len;
     Scalars *scal;
     double dxdy, norm0;
+    // two components: the other species' tile at the start of this step, the
+    // factor that normalises it, and g_ab * dt
+    const void *pb;
+    const double *pb_scale;
+    T cab;
 };
 
 // ---------------------------------------------------------------- PTX helpers
@@ -425,49 +434,6 @@ __device__ __forceinline__ T phase_expneg(T th) {
     return exp_t(-th);
 }
 
-// Potential, GPE and LHY phase on one row (src/cpucartesian.cpp:96-106,130-134).
-// |psi|^2 is taken before the table multiply, as the reference does.
-template <bool IMAG, bool PHASE, bool LHY, int C, typename T, typename TabT>
-__device__ __forceinline__ void potential_row(Cx<T> (&w)[C], const TabT *tab, T ca, T caa) {
-#pragma unroll
-    for (int i = 0; i < C; ++i) {
-        Cx<T> v = w[i];
-        if (IMAG) {
-            const T pr = reinterpret_cast<const T *>(tab)[i];
-            if (PHASE) {
-                const T n2 = fma_t(v.re, v.re, mul_t(v.im, v.im));
-                T th = mul_t(ca, n2);
-                if (LHY) th = fma_t(caa, mul_t(n2, sqrt_t(n2)), th);
-                const T t = mul_t(phase_expneg(th), pr);
-                v.re = mul_t(t, v.re);
-                v.im = mul_t(t, v.im);
-            } else {
-                v.re = mul_t(pr, v.re);
-                v.im = mul_t(pr, v.im);
-            }
-        } else {
-            const Cx<T> e = reinterpret_cast<const Cx<T> *>(tab)[i];
-            T c = DeltaForm<T>::value ? T(0) : T(1), s = T(0);
-            if (PHASE) {
-                const T n2 = fma_t(v.re, v.re, mul_t(v.im, v.im));
-                T th = mul_t(ca, n2);
-                if (LHY) th = fma_t(caa, mul_t(n2, sqrt_t(n2)), th);
-                phase_sincos(th, &s, &c);
-            }
-            // the table holds (cos, sin) of -dt V; in delta form (cos - 1, sin)
-            T t = v.re;
-            v.re = lin(e.re, t, -mul_t(e.im, v.im));
-            v.im = lin(e.re, v.im, mul_t(e.im, t));
-            if (PHASE) {
-                t = v.re;
-                v.re = lin(c, t, mul_t(s, v.im));
-                v.im = lin(c, v.im, -mul_t(s, t));
-            }
-        }
-        w[i] = v;
-    }
-}
-
 template <typename T>
 struct Vec2T;
 template <>
@@ -496,8 +462,66 @@ __device__ __forceinline__ void st_cx_global(Cx<T> *p, Cx<T> v) {
     *reinterpret_cast<typename Vec2T<T>::type *>(p) = o;
 }
 
+// Potential, GPE and LHY phase on one row (src/cpucartesian.cpp:96-106,130-134).
+// |psi|^2 is taken before the table multiply, as the reference does.
+// PB (two components): the phase adds g_ab dt |psi_b|^2, psi_b the other
+// species' cell (row `pb`, times `pbs`) at the start of this step
+// (src/cpucartesian.cpp:73-92,113-126).
+template <bool IMAG, bool PHASE, bool LHY, bool PB, int C, typename T, typename TabT>
+__device__ __forceinline__ void potential_row(Cx<T> (&w)[C], const TabT *tab, T ca, T caa,
+                                              const Cx<T> *pb = nullptr, T pbs = T(1),
+                                              T cab = T(0)) {
+#pragma unroll
+    for (int i = 0; i < C; ++i) {
+        Cx<T> v = w[i];
+        T thb = T(0);
+        if (PB) {
+            const Cx<T> u = ld_cx_shared(pb + i);
+            const T ur = mul_t(u.re, pbs), ui = mul_t(u.im, pbs);
+            thb = mul_t(cab, fma_t(ur, ur, mul_t(ui, ui)));
+        }
+        if (IMAG) {
+            const T pr = reinterpret_cast<const T *>(tab)[i];
+            if (PHASE) {
+                const T n2 = fma_t(v.re, v.re, mul_t(v.im, v.im));
+                T th = mul_t(ca, n2);
+                if (LHY) th = fma_t(caa, mul_t(n2, sqrt_t(n2)), th);
+                if (PB) th = th + thb;
+                const T t = mul_t(phase_expneg(th), pr);
+                v.re = mul_t(t, v.re);
+                v.im = mul_t(t, v.im);
+            } else {
+                v.re = mul_t(pr, v.re);
+                v.im = mul_t(pr, v.im);
+            }
+        } else {
+            const Cx<T> e = reinterpret_cast<const Cx<T> *>(tab)[i];
+            T c = DeltaForm<T>::value ? T(0) : T(1), s = T(0);
+            if (PHASE) {
+                const T n2 = fma_t(v.re, v.re, mul_t(v.im, v.im));
+                T th = mul_t(ca, n2);
+                if (LHY) th = fma_t(caa, mul_t(n2, sqrt_t(n2)), th);
+                if (PB) th = th + thb;
+                phase_sincos(th, &s, &c);
+            }
+            // the table holds (cos, sin) of -dt V; in delta form (cos - 1, sin)
+            T t = v.re;
+            v.re = lin(e.re, t, -mul_t(e.im, v.im));
+            v.im = lin(e.re, v.im, mul_t(e.im, t));
+            if (PHASE) {
+                t = v.re;
+                v.re = lin(c, t, mul_t(s, v.im));
+                v.im = lin(c, v.im, -mul_t(s, t));
+            }
+        }
+        w[i] = v;
+    }
+}
+
+
 // Compile-time description of a kernel variant.
-// PHASE: 0 no nonlinear phase, 1 g|psi|^2 only, 2 with the Lee-Huang-Yang term.
+// PHASE: 0 no nonlinear phase, 1 g|psi|^2 only, 2 with the Lee-Huang-Yang term,
+// 3 g|psi|^2 + g_ab|psi_b|^2 (one component of a two-component system).
 template <typename T_, int C_, bool IMAG_, bool ROT_, int PHASE_>
 struct Variant {
     using T = T_;
@@ -506,6 +530,7 @@ struct Variant {
     static constexpr bool ROT = ROT_;
     static constexpr bool PHASE = PHASE_ != 0;
     static constexpr bool LHY = PHASE_ == 2;
+    static constexpr bool PB = PHASE_ == 3;
     static constexpr int HX = ROT_ ? 8 : 4;
     static constexpr int HY = ROT_ ? 6 : 4;
     // Register window (rows); the body is unrolled over two windows so that
@@ -532,7 +557,8 @@ struct Variant {
     using TabT = typename std::conditional<IMAG_, T_, Cx<T_>>::type;
     static constexpr int PSI_BYTES = SW * (int)sizeof(Cx<T_>);
     static constexpr int TAB_BYTES = SW * (int)sizeof(TabT);
-    static constexpr int SLOT = PSI_BYTES + TAB_BYTES;
+    // a slot: one row of psi, of the table and (PB) of the other species
+    static constexpr int SLOT = PSI_BYTES + TAB_BYTES + (PB ? PSI_BYTES : 0);
 };
 
 
@@ -558,6 +584,7 @@ struct Walk {
     int issued_to;        // rows [ra, issued_to) have had their copy issued
     int loaded_to;        // rows [ra, loaded_to) have been waited for
     const unsigned char *gpsi, *gtab;  // row 0, column cs of psi and of the table
+    const unsigned char *gpb;          // PB: row 0, column cs of the other species
     size_t gpsi_pitch, gtab_pitch;
     uint32_t psi_off, psi_bytes, tab_off, tab_bytes;
     unsigned char *ring;
@@ -566,15 +593,19 @@ struct Walk {
     bool failed;
     T inv;
     T aH, bH, aV, bV, ca, caa;  // step constants, read from the parameters once
+    T pbs, cab;                 // PB: factor of the other species' tile, g_ab * dt
     T hpa[C - 1], hpb[C - 1];        // LANE_COEF: this lane's pairs (i, i+1)
     T hal, hbl, har, hbr;            //   and its pairs with the neighbour lanes
 
     __device__ __forceinline__ void issue(int row, int slot) {
         unsigned char *sb = ring + slot * V::SLOT;
-        mbar_expect_tx(&bars[slot], psi_bytes + tab_bytes);
+        mbar_expect_tx(&bars[slot], psi_bytes + tab_bytes + (V::PB ? psi_bytes : 0u));
         bulk_g2s(sb + psi_off, gpsi + (size_t)row * gpsi_pitch, psi_bytes, &bars[slot]);
         bulk_g2s(sb + V::PSI_BYTES + tab_off, gtab + (size_t)row * gtab_pitch, tab_bytes,
                  &bars[slot]);
+        if constexpr (V::PB)
+            bulk_g2s(sb + V::PSI_BYTES + V::TAB_BYTES + psi_off, gpb + (size_t)row * gpsi_pitch,
+                     psi_bytes, &bars[slot]);
     }
     __device__ __forceinline__ int next(int q) const { return q + 1 == D ? 0 : q + 1; }
 };
@@ -601,9 +632,12 @@ __device__ __forceinline__ void zero_ring_outside(Walk<V> &w) {
         bool copied;
         if (off < (uint32_t)V::PSI_BYTES) {
             copied = off >= w.psi_off && off < w.psi_off + w.psi_bytes;
-        } else {
+        } else if (off < (uint32_t)(V::PSI_BYTES + V::TAB_BYTES)) {
             const uint32_t t = off - (uint32_t)V::PSI_BYTES;
             copied = t >= w.tab_off && t < w.tab_off + w.tab_bytes;
+        } else {
+            const uint32_t t = off - (uint32_t)(V::PSI_BYTES + V::TAB_BYTES);
+            copied = t >= w.psi_off && t < w.psi_off + w.psi_bytes;
         }
         if (!copied) ring32[i] = 0u;
     }
@@ -659,7 +693,14 @@ __device__ __forceinline__ void walk_row(Walk<V> &w, const StepArgs<typename V::
         const int q = w.tslot;
         const TabT *tp =
             reinterpret_cast<const TabT *>(w.ring + q * V::SLOT + V::PSI_BYTES) + C * w.lane;
-        potential_row<IMAG, PHASE, V::LHY, C>(WS(2), tp, w.ca, w.caa);
+        if constexpr (V::PB) {
+            const Cx<T> *bp = reinterpret_cast<const Cx<T> *>(w.ring + q * V::SLOT +
+                                                              V::PSI_BYTES + V::TAB_BYTES) +
+                              C * w.lane;
+            potential_row<IMAG, PHASE, false, true, C>(WS(2), tp, w.ca, w.caa, bp, w.pbs, w.cab);
+        } else {
+            potential_row<IMAG, PHASE, V::LHY, false, C>(WS(2), tp, w.ca, w.caa);
+        }
         if constexpr (ROT) {
             const Cx<T> ab = reinterpret_cast<const Cx<T> *>(a.row_ab)[u];
             rrow<IMAG, C, 0, EDGE>(WS(2), ab.re, ab.im, w.m);
@@ -808,6 +849,10 @@ __device__ __forceinline__ void bind_args(Walk<V> &w, const StepArgs<typename V:
     }
     w.ca = a.ca;
     w.caa = a.caa;
+    if constexpr (V::PB) {
+        w.pbs = (T)__ldcg(a.pb_scale);
+        w.cab = a.cab;
+    }
     w.gpsi_pitch = (size_t)a.P * sizeof(Cx<T>);
     w.gtab_pitch = (size_t)a.P * sizeof(typename V::TabT);
 }
@@ -852,6 +897,8 @@ __device__ __forceinline__ void run_task(Walk<V> &w, const StepArgs<typename V::
     w.tab_bytes = (uint32_t)(ce - cs) * sizeof(TabT);
     w.gpsi = reinterpret_cast<const unsigned char *>(a.psi_in) + (size_t)cs * sizeof(Cx<T>);
     w.gtab = reinterpret_cast<const unsigned char *>(a.pot) + (size_t)cs * sizeof(TabT);
+    if constexpr (V::PB)
+        w.gpb = reinterpret_cast<const unsigned char *>(a.pb) + (size_t)cs * sizeof(Cx<T>);
     w.xl = c0 + C * lane;
 #pragma unroll
     for (int i = 0; i < C; ++i) {
@@ -1002,7 +1049,15 @@ __global__ void __launch_bounds__(128, V::MIN_BLOCKS) step_kernel(StepArgs<typen
             if (threadIdx.x == 0) {
                 const double tot = red[0] * a.dxdy;
                 a.scal->last_norm = tot;
-                if (a.scal->renorm) a.scal->pending_inv = 1.0 / sqrt(tot / a.norm0);
+                if constexpr (V::PB) {
+                    // the other species' next step reads this step's input
+                    // buffer with the factor that was pending on it
+                    a.scal->prev_inv = a.scal->pending_inv;
+                    const double n0 = a.scal->norm_target;
+                    if (a.scal->renorm && n0 != 0.0) a.scal->pending_inv = 1.0 / sqrt(tot / n0);
+                } else {
+                    if (a.scal->renorm) a.scal->pending_inv = 1.0 / sqrt(tot / a.norm0);
+                }
                 a.scal->ticket = 0u;
             }
         }

@@ -42,12 +42,17 @@ cudaError_t launch_step_variant(const StepArgs<typename V::T> &a, int warps, siz
 template <typename T, bool IMAG, int C, bool ROT>
 cudaError_t launch_phase(int phase, const StepArgs<T> &a, int warps, size_t smem, int blocks,
                          cudaStream_t st, int *bps) {
+    if constexpr (C == 2 && !ROT) {
+        if (phase == 3)
+            return launch_step_variant<Variant<T, C, IMAG, ROT, 3>>(a, warps, smem, blocks, st, bps);
+    }
     if (phase == 2) return launch_step_variant<Variant<T, C, IMAG, ROT, 2>>(a, warps, smem, blocks, st, bps);
     if (phase == 1) return launch_step_variant<Variant<T, C, IMAG, ROT, 1>>(a, warps, smem, blocks, st, bps);
     return launch_step_variant<Variant<T, C, IMAG, ROT, 0>>(a, warps, smem, blocks, st, bps);
 }
 
-// phase: 0 none, 1 g|psi|^2, 2 g|psi|^2 + Lee-Huang-Yang.
+// phase: 0 none, 1 g|psi|^2, 2 g|psi|^2 + Lee-Huang-Yang, 3 two components
+// (g|psi|^2 + g_ab|psi_b|^2; 2 cells per lane, no rotating frame).
 template <typename T, bool IMAG>
 cudaError_t launch_step_imag_t(int C, bool rot, int phase, const StepArgs<T> &a, int warps,
                                size_t smem, int blocks, cudaStream_t st, int *bps) {

@@ -600,7 +600,8 @@ void geometry(const ts_b200_kernel *k, int *strips, int *segs, int *blocks, size
     *blocks = div_up(tasks, k->warps);
     if (k->resident_blocks > 0) *blocks = std::min(*blocks, k->resident_blocks);
     // per warp: ring slots + one mbarrier per ring slot
-    *smem = (size_t)k->warps * (k->ring * slot_bytes(k->C, k->fp32, k->imag) + 8 * k->ring);
+    *smem = (size_t)k->warps *
+            (k->ring * slot_bytes(k->C, k->fp32, k->imag, k->phase == 3) + 8 * k->ring);
 }
 
 template <typename T>
@@ -666,6 +667,9 @@ void tsbh::fill_step_constants(const ts_b200_kernel *k, StepArgs<T> &a) {
     a.sched_len = kSchedLen;
     a.dxdy = k->d.delta_x * k->d.delta_y;
     a.norm0 = k->d.norm0;
+    a.pb = k->pb;
+    a.pb_scale = k->pb_scale;
+    a.cab = (T)k->cab;
 }
 template void tsbh::fill_step_constants<double>(const ts_b200_kernel *, StepArgs<double> &);
 template void tsbh::fill_step_constants<float>(const ts_b200_kernel *, StepArgs<float> &);
@@ -732,6 +736,8 @@ int launch_step(ts_b200_kernel *k, int exchange, bool dry = false) {
 }
 
 }  // namespace
+
+int tsbh::launch_step_tile(ts_b200_kernel *k, int exchange) { return launch_step(k, exchange); }
 
 int tsbh::launch_step_buffers(ts_b200_kernel *k, const void *in, void *out) {
     return k->fp32 ? launch_step_buffers_t<float>(k, in, out, false)
@@ -863,6 +869,11 @@ int upload_kinetic_schedule(ts_b200_kernel *k) {
 
 int grid_for(size_t n) { return (int)std::max<size_t>(1, std::min<size_t>((n + 255) / 256, 8192)); }
 
+// A tile that is one species of a pair steps only through the pair.
+int reject_pair_mode(ts_b200_kernel *k) {
+    return fail(k, TS_B200_UNSUPPORTED, "the tile is one component of a pair: step the pair");
+}
+
 }  // namespace
 
 // ================================================================ C ABI
@@ -945,6 +956,8 @@ int ts_b200_create(const ts_b200_desc *d, ts_b200_kernel **out) {
     k->stream = k->own_stream;
     Scalars s0{};
     s0.pending_inv = 1.0;
+    s0.prev_inv = 1.0;
+    s0.norm_target = d->norm0;
     s0.renorm = (k->imag && d->norm0 != 0.0) ? 1 : 0;
     e = cudaMemcpy(k->scal, &s0, sizeof s0, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
@@ -1097,6 +1110,7 @@ int ts_b200_evolve_potentials(ts_b200_kernel *k, const double *potentials, size_
     if (!k || !potentials || count < 0 || pitch < (size_t)k->W || slab < pitch * k->H ||
         !(delta_t > 0.0))
         return TS_B200_INVALID_ARGUMENT;
+    if (k->pair_mode) return reject_pair_mode(k);
     for (int i = 0; i < count; ++i) {
         launch_table_from_potential(k, potentials + (size_t)i * slab, pitch, delta_t);
         TSB_CHECK(k, cudaGetLastError());
@@ -1109,6 +1123,7 @@ int ts_b200_evolve_potentials(ts_b200_kernel *k, const double *potentials, size_
 
 int ts_b200_step(ts_b200_kernel *k, int exchange) {
     if (!k) return TS_B200_INVALID_ARGUMENT;
+    if (k->pair_mode) return reject_pair_mode(k);
     return launch_step(k, exchange);
 }
 
@@ -1119,6 +1134,7 @@ int ts_b200_halo_exchange(ts_b200_kernel *k) {
 
 int ts_b200_evolve(ts_b200_kernel *k, int iterations) {
     if (!k || iterations < 0) return TS_B200_INVALID_ARGUMENT;
+    if (k->pair_mode) return reject_pair_mode(k);
     if (iterations == 0) return TS_B200_OK;
     // Steps 0 .. iterations-2 refresh the halo; the last one does not
     // (src/solver.cpp:203-209).  Runs of G exchanging steps starting from
@@ -1309,6 +1325,7 @@ int ts_b200_set_launch(ts_b200_kernel *k, int C, int seg_h, int warps, int ring)
     if (!k) return TS_B200_INVALID_ARGUMENT;
     if (C != 0 && C != 2 && C != 4) return TS_B200_INVALID_ARGUMENT;
     if (C == 4 && k->rot) return fail(k, TS_B200_UNSUPPORTED, "rotation kernels use 2 cells per lane");
+    if (C == 4 && k->pair_mode) return fail(k, TS_B200_UNSUPPORTED, "pair kernels use 2 cells per lane");
     if (warps != 0 && warps != 1 && warps != 2 && warps != 4) return TS_B200_INVALID_ARGUMENT;
     if (ring != 0 && (ring < min_ring(k) || ring > 16))
         return fail(k, TS_B200_INVALID_ARGUMENT, "ring depth out of range for this variant");
@@ -1331,6 +1348,7 @@ int ts_b200_set_launch(ts_b200_kernel *k, int C, int seg_h, int warps, int ring)
 
 int ts_b200_autotune(ts_b200_kernel *k, int trial_steps) {
     if (!k || trial_steps < 1) return TS_B200_INVALID_ARGUMENT;
+    if (k->pair_mode) return reject_pair_mode(k);
     // the trials step from the current buffer into the other one without
     // flipping, so the state is untouched; the scalars the step writes
     // (renormalisation, schedule step) are restored afterwards

@@ -12,12 +12,12 @@ from .api import (DevicePotential, ExponentialState, GaussianState, Hamiltonian,
                   Hamiltonian2Component,
                   HarmonicPotential, Lattice1D, Lattice2D, Potential, SinusoidState, Solver,
                   SolverBatch, State, make_desc, map_lattice_to_coordinate_space)
-from .kernel import FP32, FP64, Batch, Kernel, launch_count, version  # noqa: F401
+from .kernel import FP32, FP64, Batch, Kernel, Pair, launch_count, version  # noqa: F401
 
 __version__ = "1.6.2+b200"
 
 __all__ = ["Lattice1D", "Lattice2D", "State", "ExponentialState", "GaussianState",
            "SinusoidState", "Potential", "DevicePotential", "HarmonicPotential", "Hamiltonian",
            "Hamiltonian2Component", "Solver", "SolverBatch", "map_lattice_to_coordinate_space",
-           "Kernel", "Batch",
+           "Kernel", "Batch", "Pair",
            "B200Error"]

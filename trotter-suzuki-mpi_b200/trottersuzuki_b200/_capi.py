@@ -89,6 +89,13 @@ SIGNATURES = {
     "ts_b200_set_potential_device": (_I, [_VP, _VP, _SZ, C.c_double]),
     "ts_b200_evolve_potentials": (_I, [_VP, _VP, _SZ, _SZ, C.c_int, C.c_double, C.c_int]),
     "ts_b200_set_stream": (_I, [_VP, _VP]),
+    "ts_b200_pair_create": (_I, [_VP, _VP, C.c_double, C.c_double, C.c_double, C.c_double,
+                                 C.POINTER(_VP)]),
+    "ts_b200_pair_rabi": (_I, [_VP, C.c_double]),
+    "ts_b200_pair_evolve": (_I, [_VP, C.c_int]),
+    "ts_b200_pair_cross_energies": (_I, [_VP, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "ts_b200_pair_last_error": (C.c_char_p, [_VP]),
+    "ts_b200_pair_destroy": (_I, [_VP]),
     "ts_b200_synchronize": (_I, [_VP]),
     "ts_b200_launch_info": (_I, [_VP, C.POINTER(LaunchShape)]),
     "ts_b200_set_launch": (_I, [_VP, _I, _I, _I, _I]),
@@ -146,9 +153,11 @@ def lib():
     return _lib
 
 
-def check(status, handle=None, batch=None, adjoint=None):
+def check(status, handle=None, batch=None, adjoint=None, pair=None):
     if status != OK:
-        if adjoint:
+        if pair:
+            msg = lib().ts_b200_pair_last_error(pair).decode()
+        elif adjoint:
             msg = lib().ts_b200_adjoint_last_error(adjoint).decode()
         elif batch:
             msg = lib().ts_b200_batch_last_error(batch).decode()

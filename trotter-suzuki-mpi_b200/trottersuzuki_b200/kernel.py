@@ -226,3 +226,51 @@ def launch_count():
 
 def version():
     return lib().ts_b200_version().decode()
+
+
+class Pair:
+    """Two species (two Kernel tiles of the same geometry) evolved together:
+    the reference's two-component kernel and loop (ts_b200_pair_* of
+    include/ts_b200.h).  coupling_ab is g_ab; omega = (omega_r, omega_i) the
+    Rabi coupling.  While paired the tiles step only through the pair."""
+
+    def __init__(self, a, b, coupling_ab, omega_r, omega_i, delta_t):
+        self.a, self.b = a, b
+        self._p = C.c_void_p()
+
+        def raw(k):
+            return k.handle if hasattr(k, "handle") else C.c_void_p(int(k))
+        check(lib().ts_b200_pair_create(raw(a), raw(b), float(coupling_ab), float(omega_r),
+                                        float(omega_i), float(delta_t), C.byref(self._p)),
+              raw(a))
+
+    def _check(self, status):
+        check(status, pair=self._p)
+
+    def rabi(self, var):
+        self._check(lib().ts_b200_pair_rabi(self._p, float(var)))
+
+    def evolve(self, iterations):
+        self._check(lib().ts_b200_pair_evolve(self._p, int(iterations)))
+
+    def cross_energies(self):
+        inter, rabi = C.c_double(), C.c_double()
+        self._check(lib().ts_b200_pair_cross_energies(self._p, C.byref(inter), C.byref(rabi)))
+        return inter.value, rabi.value
+
+    def close(self):
+        if self._p:
+            lib().ts_b200_pair_destroy(self._p)
+            self._p = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
