@@ -1058,6 +1058,136 @@ def run_moving_trap_workload(args, rank, world, local, pg):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------ two-component workload
+# Two species (Hamiltonian2Component) on the headline lattice, real time, FP64:
+# species a the headline Gaussian, species b the same displaced by 1.5 in x;
+# harmonic traps (1, 1.5) and (1.2, 1), g_a = 100, g_b = 80, g_ab = 60,
+# mass_b = 1.2, Rabi coupling omega = 5 + 2i, dt = 1e-4.  One bench step =
+# one evolve(200) of the drop-in two-state Solver.  A species-site-step is
+# one site of one species advanced by one Trotter step.
+TWO_STEPS = 200
+TWO_BYTES = 64  # per species-site-step of the step kernel: psi in + out, table, other species
+
+
+def run_two_component_workload(args, rank, world, local, pg):
+    import torch
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    import trottersuzuki_b200 as ts
+    from trottersuzuki_b200 import launch_count
+    grid = ts.Lattice2D(N_SIDE, LENGTH)
+    info = {"dim_x": grid.dim_x, "dim_y": grid.dim_y, "delta_x": grid.delta_x,
+            "delta_y": grid.delta_y}
+    a0 = initial_state(info)
+    b0 = np.roll(a0, int(round(1.5 / grid.delta_x)), axis=1)
+    sa, sb = ts.State(grid), ts.State(grid)
+    sa.init_state_matrix(a0.real, a0.imag)
+    sb.init_state_matrix(b0.real, b0.imag)
+    pa = ts.HarmonicPotential(grid, OMEGA_X, OMEGA_Y)
+    pb = ts.HarmonicPotential(grid, 1.2, 1.0)
+    ham = ts.Hamiltonian2Component(grid, pa, pb, 1.0, 1.2, G, 60.0, 80.0, 5.0, 2.0)
+    solver = ts.Solver(grid, sa, ham, DT, State2=sb)
+    e_start = solver.get_total_energy()
+    for _ in range(args.warmup):
+        solver.evolve(-TWO_STEPS)
+    cur = torch.cuda.current_stream(device)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    l0 = launch_count()
+    with Clocks(local) as clocks:
+        e0.record(cur)
+        for _ in range(args.steps):
+            solver.evolve(-TWO_STEPS)
+        torch.cuda.synchronize()
+        e1.record(cur)
+        e1.synchronize()
+    launches = launch_count() - l0
+    ms = max_over_ranks(e0.elapsed_time(e1), pg, device)
+    # e2e: evolve(200) with the states copied into both States each call
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(cur)
+    for _ in range(max(1, args.steps // 2)):
+        solver.evolve(TWO_STEPS)
+    torch.cuda.synchronize()
+    t1.record(cur)
+    t1.synchronize()
+    ms_e2e = max_over_ranks(t0.elapsed_time(t1), pg, device)
+    e_end = solver.get_total_energy()
+    n_end = solver.get_squared_norm()
+    if rank != 0:
+        return
+    sites = float(N_SIDE) * N_SIDE
+    value = world * 2 * sites * TWO_STEPS * args.steps / (ms * 1e-3)
+    e2e = world * 2 * sites * TWO_STEPS * max(1, args.steps // 2) / (ms_e2e * 1e-3)
+    peak, peak_kind = measured_peak()
+    # per species-site-step: the step kernel's 64 B plus the Rabi pass (32 B)
+    achieved = (TWO_BYTES + 32) * value / world / 1e9
+    cpu = None
+    if not args.no_cpu_baseline:
+        cpu = two_component_cpu_rate(a0, b0, budget_s=args.ref_budget)
+    line = {
+        "metric": "species-site-steps/s", "value": value, "unit": "species-site-steps/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "two_component_2048", "lattice": f"{N_SIDE}x{N_SIDE}",
+                   "length": LENGTH, "boundary": "closed", "g": [G, 80.0], "g_ab": 60.0,
+                   "mass_b": 1.2, "rabi_omega": [5.0, 2.0], "dt": DT,
+                   "trotter_steps_per_step": TWO_STEPS, "imag_time": False,
+                   "parallelism": f"replicas{world}",
+                   "l2": "inputs larger than L2: 384 MiB moved per Trotter step"},
+        "e2e": {"value": e2e, "unit": "species-site-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 4 * 8 * int(sites),
+                "path": "two-state Solver.evolve(200), both States filled after each call"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                     "algorithmic_bytes_per_species_site_step": TWO_BYTES + 32,
+                     "kernel": "tsb::step_kernel<double, C=2, real, phase 3> x 2 + rabi_kernel"},
+        "energy_drift_rel": abs(e_end - e_start) / abs(e_start),
+        "norm_after": n_end,
+        "cpu_baseline": cpu,
+        "clocks": clocks.summary(),
+        "gpu_launches": launches,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def two_component_cpu_rate(a0, b0, budget_s=12.0):
+    """The reference's own two-state Solver (oracle/_ref) on a bounded sample
+    of the two-component workload, all host threads."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import tsref
+    flavour = "fast" if tsref.available("fast") else ("parity" if tsref.available() else None)
+    if flavour is None:
+        return None
+    threads = os.cpu_count() or 1
+    X = (np.arange(N_SIDE) - N_SIDE / 2 + 0.5) * (LENGTH / N_SIDE)
+    Xg, Yg = np.meshgrid(X, X)
+    Va = 0.5 * (OMEGA_X ** 2 * Xg ** 2 + OMEGA_Y ** 2 * Yg ** 2)
+    Vb = 0.5 * (1.2 ** 2 * Xg ** 2 + Yg ** 2)
+
+    def run(steps):
+        cfg = tsref.make_config(N_SIDE, LENGTH, harmonic=None, coupling=G, delta_t=DT,
+                                segments=((1, False), (steps, False)), omp_threads=threads)
+        _, _, r = tsref.run2(cfg, tsref.Config2(1.2, 80.0, 60.0, 5.0, 2.0), a0, b0, Va, Vb,
+                             flavour=flavour)
+        return r.seg_seconds[1]
+
+    t = run(2)
+    steps = int(max(2, min(200, budget_s / max(t / 2, 1e-6))))
+    secs = run(steps)
+    return {"value": 2 * N_SIDE * N_SIDE * steps / secs, "unit": "species-site-steps/s",
+            "cores": threads, "kind": "reference",
+            "sample": f"{N_SIDE}x{N_SIDE} two species real time, {steps} Trotter steps after "
+                      f"1 warm-up step, reference two-state Solver "
+                      f"({'-Ofast' if flavour == 'fast' else '-O2'} build)"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1071,7 +1201,8 @@ def main():
     ap.add_argument("--no-ref-gpu", action="store_true",
                     help="reference arm: skip timing the reference's CUDA kernel")
     ap.add_argument("--workload", choices=["gpe_imaginary_time_2048", "batch512", "adjoint512",
-                                           "vortex8192", "moving_trap_2048"],
+                                           "vortex8192", "moving_trap_2048",
+                                           "two_component_2048"],
                     default="gpe_imaginary_time_2048")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
@@ -1087,6 +1218,8 @@ def main():
             run_vortex_workload(args, rank, world, local, pg)
         elif args.workload == "moving_trap_2048":
             run_moving_trap_workload(args, rank, world, local, pg)
+        elif args.workload == "two_component_2048":
+            run_two_component_workload(args, rank, world, local, pg)
         else:
             run_b200_arm(args, rank, world, local, pg)
     finally:

@@ -324,6 +324,16 @@ int ts_b200_pair_rabi(ts_b200_pair *p, double var);
  * imaginary time with a Rabi coupling the joint normalisation.  Every step
  * but the last refreshes the halos. */
 int ts_b200_pair_evolve(ts_b200_pair *p, int iterations);
+/* `steps` steps of that loop; with final_steps == 0 none of them is the
+ * call's last (all refresh the halos and take a full Rabi rotation), so a
+ * caller can re-tabulate a time-dependent potential between runs. */
+int ts_b200_pair_steps(ts_b200_pair *p, int steps, int final_steps);
+/* The plug-in protocol's pieces (ITrotterKernel::run_kernel for species
+ * `which`, 0 = a, 1 = b, without the halo refresh, which ts_b200_halo_exchange
+ * on the species' tile does; ITrotterKernel::normalization).  Species b's step
+ * must follow species a's. */
+int ts_b200_pair_step_species(ts_b200_pair *p, int which);
+int ts_b200_pair_normalize(ts_b200_pair *p);
 /* Inter-species and Rabi energies of Solver::calculate_energy_expected_values
  * (src/solver.cpp:340-353,438-439,549-550), as the reference writes them:
  * sum g_ab |a|^4 |b|^4 and 0.5 sum |a|^2 |b|^2 2 Re(conj(a) b omega), each over

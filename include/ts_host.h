@@ -71,12 +71,26 @@ int tsh_hamiltonian_new(void *lattice, void *potential, double mass, double coup
                         double lhy_coupling_a, double angular_velocity, double rot_coord_x,
                         double rot_coord_y, void **out);
 int tsh_hamiltonian_free(void *hamiltonian);
+/* Hamiltonian2Component(grid, potential, potential_b, mass, mass_b, coupling_a,
+ * coupling_ab, coupling_b, omega_r, omega_i, angular_velocity, rot_coord_x,
+ * rot_coord_y) -- src/trottersuzuki.h:455-497 (freed with tsh_hamiltonian_free) */
+int tsh_hamiltonian2_new(void *lattice, void *potential, void *potential_b, double mass,
+                         double mass_b, double coupling_a, double coupling_ab, double coupling_b,
+                         double omega_r, double omega_i, double angular_velocity,
+                         double rot_coord_x, double rot_coord_y, void **out);
 
 /* Solver(grid, state, hamiltonian, delta_t, kernel_type) and its methods
  * -- src/trottersuzuki.h:541-569 */
 int tsh_solver_new(void *lattice, void *state, void *hamiltonian, double delta_t,
                    const char *kernel_type, void **out);
+/* Solver(grid, state1, state2, hamiltonian2, delta_t, kernel_type) --
+ * src/trottersuzuki.h:554-555 */
+int tsh_solver2_new(void *lattice, void *state1, void *state2, void *hamiltonian2,
+                    double delta_t, const char *kernel_type, void **out);
 int tsh_solver_evolve(void *solver, int iterations, int imag_time);
+/* Two components: total, kinetic (1, 2), potential (1, 2), rotational (1, 2),
+ * intra-species (1, 2), inter-species, Rabi, squared norm (1, 2). */
+int tsh_solver_energies2(void *solver, double out[13]);
 /* total, kinetic, potential, rotational, intra-species, Lee-Huang-Yang, squared norm */
 int tsh_solver_energies(void *solver, double out[7]);
 int tsh_solver_set_exp_potential(void *solver, const double *re, const double *im, int length,

@@ -112,3 +112,92 @@ def test_pair_rules():
         k1.set_exp_potential(*O.exp_table(z["Va"], 1e-3, False))
         k1.evolve(5)
         assert np.array_equal(k1.get_state(), ka.get_state())
+
+
+# ------------------------------------------------------- the drop-in Solver
+def _drop_in(name, kernel_type="gpu"):
+    import trottersuzuki_b200 as ts
+    lat, meta, z = load_two(name)
+    N, L, Ny, px, py = meta["lat"]
+    grid = ts.Lattice2D(N, L, Ny, None, periodic_x_axis=px, periodic_y_axis=py)
+    sa, sb = ts.State(grid), ts.State(grid)
+    sa.init_state_matrix(z["psi0_a"].real, z["psi0_a"].imag)
+    sb.init_state_matrix(z["psi0_b"].real, z["psi0_b"].imag)
+    pa, pb = ts.Potential(grid, z["Va"]), ts.Potential(grid, z["Vb"])
+    ham = ts.Hamiltonian2Component(grid, pa, pb, 1.0, meta["mass_b"], meta["g"], meta["g_ab"],
+                                   meta["g_b"], *meta["omega"])
+    solver = ts.Solver(grid, sa, ham, meta["dt"], State2=sb, kernel_type=kernel_type)
+    return meta, z, solver, (sa, sb), (grid, pa, pb, ham)
+
+
+@pytest.mark.parametrize("name", two_names())
+def test_drop_in_two_component_solver(name):
+    meta, z, solver, (sa, sb), keep = _drop_in(name)
+    for it, imag in meta["segments"]:
+        solver.evolve(it, imag)
+    assert np.abs(sa.get_state() - z["psi_a"]).max() <= 1e-10
+    assert np.abs(sb.get_state() - z["psi_b"]).max() <= 1e-10
+    got = [solver.get_total_energy(), solver.get_kinetic_energy(1), solver.get_kinetic_energy(2),
+           solver.get_potential_energy(1), solver.get_potential_energy(2),
+           solver.get_rotational_energy(1), solver.get_rotational_energy(2),
+           solver.get_intra_species_energy(1), solver.get_intra_species_energy(2),
+           solver.get_inter_species_energy(), solver.get_rabi_energy(),
+           solver.get_squared_norm(1), solver.get_squared_norm(2)]
+    assert np.allclose(got, z["energies"], rtol=1e-10, atol=1e-12), (got, z["energies"])
+    assert abs(solver.get_squared_norm() - z["energies"][11] - z["energies"][12]) < 1e-12
+
+
+@pytest.mark.parametrize("kernel_type", ["gpu", "gpu_fp32"])
+def test_kat_mixed_bec(kernel_type):
+    """test/kerneltest.cpp:177-235 through the Python drop-in."""
+    import math
+
+    import trottersuzuki_b200 as ts
+    for imag in (False, True):
+        grid = ts.Lattice2D(250, 100.0)
+        s1 = ts.GaussianState(grid, 1.0)
+        s2 = ts.State(grid)
+        pot = ts.HarmonicPotential(grid, 1.0, 1.0)
+        ham = ts.Hamiltonian2Component(grid, pot, pot, 1.0, 1.0, 0.0, 0.0, 0.0,
+                                       2.0 * math.pi / 10.0)
+        solver = ts.Solver(grid, s1, ham, 1e-3, State2=s2, kernel_type=kernel_type)
+        # the second species starts empty: the initial energy is 0/0 (NaN),
+        # in the reference too, so only the norms are compared
+        n0 = solver.get_squared_norm(1) + solver.get_squared_norm(2)
+        n01, n02 = s1.get_squared_norm(), s2.get_squared_norm()
+        solver.evolve(1000 if imag else 5000, imag)
+        assert math.isfinite(solver.get_total_energy())
+        assert abs(n0 - solver.get_squared_norm()) < 1e-5
+        if imag:
+            assert abs(0.915292 - s1.get_squared_norm()) < 1e-5
+            assert abs(0.084708 - s2.get_squared_norm()) < 1e-5
+        else:
+            assert abs(n01 - s2.get_squared_norm()) < 1e-5
+            assert abs(n02 - s1.get_squared_norm()) < 1e-5
+
+
+@pytest.mark.parametrize("imag", [False, True], ids=["real", "imag"])
+def test_pair_with_an_empty_species_matches_oracle(imag):
+    import math
+
+    from test_oracle_two import empty_species_case
+    from trottersuzuki_b200 import Kernel, Pair
+    lat, a, b, V = empty_species_case()
+    om, dt = 2 * math.pi / 10, 1e-3
+    norms = (O.expectations(lat, a)["norm2"], 0.0) if imag else (0.0, 0.0)
+    p_a = lat.params(dt, imag, norm0=norms[0])
+    p_b = lat.params(dt, imag, norm0=0.0)
+    table = O.exp_table(V, dt, imag)
+    ka, kb = Kernel(desc_from_params(p_a)), Kernel(desc_from_params(p_b))
+    ka.set_state(a)
+    kb.set_state(b)
+    ka.set_exp_potential(*table)
+    kb.set_exp_potential(*table)
+    pair = Pair(ka, kb, 0.0, om, 0.0, dt)
+    pair.rabi(0.5)
+    pair.evolve(150)
+    oa, ob, _ = O.evolve2(lat.params(dt, imag), lat.params(dt, imag), 0.0, om, 0.0, dt, a, b,
+                          table, table, 150, norms, sum(norms))
+    assert np.abs(ka.get_state() - oa).max() <= 1e-10
+    assert np.abs(kb.get_state() - ob).max() <= 1e-10
+    pair.close()

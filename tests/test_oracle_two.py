@@ -77,3 +77,38 @@ def test_rabi_alone_is_unitary_in_real_time():
     n0 = np.abs(a) ** 2 + np.abs(b) ** 2
     assert np.allclose(np.abs(a2) ** 2 + np.abs(b2) ** 2, n0, rtol=1e-13)
     assert np.abs(a2 - a).max() > 1e-3
+
+
+def empty_species_case(n=48, L=20.0):
+    """The reference's mixed-BEC scenario (test/kerneltest.cpp:177-235) on a
+    small lattice: a Gaussian first species, an empty second one, Rabi
+    coupling 2 pi / 10."""
+    lat = O.Lattice(n, L)
+    X, Y = lat.coordinates()
+    a = np.exp(-(X ** 2 + Y ** 2) / 2.0) + 0j
+    a = a / np.sqrt(np.sum(np.abs(a) ** 2) * lat.delta_x * lat.delta_y)
+    b = np.zeros_like(a)
+    V = 0.5 * (X ** 2 + Y ** 2)
+    return lat, a, b, V
+
+
+@pytest.mark.parametrize("imag", [False, True], ids=["real", "imag"])
+def test_oracle_matches_reference_with_an_empty_species(imag):
+    """The species that starts empty is renormalised once the joint
+    normalisation gives it a share (its kept norm starts at 0)."""
+    import math
+
+    import tsref
+    if not tsref.available():
+        pytest.skip("compiled reference not built")
+    lat, a, b, V = empty_species_case()
+    om = 2 * math.pi / 10
+    cfg = tsref.make_config(lat.dim_x, 20.0, harmonic=None, delta_t=1e-3,
+                            segments=((150, imag),), omp_threads=1)
+    ra, rb, res = tsref.run2(cfg, tsref.Config2(1.0, 0.0, 0.0, om, 0.0), a, b, V, V)
+    pa = lat.params(1e-3, imag)
+    norms = (O.expectations(lat, a)["norm2"], 0.0) if imag else (0.0, 0.0)
+    oa, ob, _ = O.evolve2(pa, pa, 0.0, om, 0.0, 1e-3, a, b, O.exp_table(V, 1e-3, imag),
+                          O.exp_table(V, 1e-3, imag), 150, norms, sum(norms))
+    assert np.abs(oa - ra).max() <= 1e-12
+    assert np.abs(ob - rb).max() <= 1e-12

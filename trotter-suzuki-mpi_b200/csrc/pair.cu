@@ -133,11 +133,34 @@ __global__ void __launch_bounds__(kThreads) rabi_kernel(RabiArgs r) {
     block_partials<2>(acc, r.partials);
 }
 
+// Sums of |a|^2 and |b|^2 over the inner region of the current tiles (each
+// with its pending factor), for the joint normalisation on its own.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) pair_norm_kernel(RabiArgs r) {
+    const double fa = r.ta.scal->pending_inv, fb = r.tb.scal->pending_inv;
+    const Cx<T> *pa = reinterpret_cast<const Cx<T> *>(r.ta.psi);
+    const Cx<T> *pb = reinterpret_cast<const Cx<T> *>(r.tb.psi);
+    double acc[2] = {0.0, 0.0};
+    for (int y = r.iy0 + blockIdx.y; y < r.iy1; y += gridDim.y) {
+        for (int x = r.ix0 + blockIdx.x * blockDim.x + threadIdx.x; x < r.ix1;
+             x += gridDim.x * blockDim.x) {
+            const size_t k = (size_t)y * r.P + x;
+            const double re = (double)pa[k].re * fa, im = (double)pa[k].im * fa;
+            const double bre = (double)pb[k].re * fb, bim = (double)pb[k].im * fb;
+            acc[0] += re * re + im * im;
+            acc[1] += bre * bre + bim * bim;
+        }
+    }
+    block_partials<2>(acc, r.partials);
+}
+
 // After the rotation the tiles carry no pending factor; in imaginary time
 // with a Rabi coupling both are normalised together to the total norm and
-// each species keeps its share of it (src/cpukernel.cpp:608-667).
+// each species keeps its share of it (src/cpukernel.cpp:608-667).  keep: the
+// tiles were not rewritten (normalisation alone): their pending factors stay,
+// times the joint one.
 __global__ void rabi_finish_kernel(Scalars *sa, Scalars *sb, const double *partials,
-                                   int normalise, double dxdy, double tot_norm) {
+                                   int normalise, double dxdy, double tot_norm, int keep = 0) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     double s0 = 0.0, s1 = 0.0;
     for (int i = 0; i < kBlocks; ++i) {
@@ -150,8 +173,8 @@ __global__ void rabi_finish_kernel(Scalars *sa, Scalars *sb, const double *parti
         sa->norm_target = s0 / (s0 + s1) * tot_norm;
         sb->norm_target = s1 / (s0 + s1) * tot_norm;
     }
-    sa->pending_inv = f;
-    sb->pending_inv = f;
+    sa->pending_inv = keep ? sa->pending_inv * f : f;
+    sb->pending_inv = keep ? sb->pending_inv * f : f;
 }
 
 struct CrossArgs {
@@ -231,24 +254,11 @@ void join_pair(ts_b200_kernel *k, double cab) {
     }
 }
 
-int launch_rabi(ts_b200_pair *p, double var, bool normalise) {
-    ts_b200_kernel *a = p->a, *b = p->b;
-    // angle of src/cpukernel.cpp:581-606 (omega / 2 as coupling_const[3], [4])
-    const double c3 = 0.5 * p->omega_r, c4 = 0.5 * p->omega_i;
-    const double no = std::sqrt(c3 * c3 + c4 * c4);
-    const double ang = -p->delta_t * var * no;
+RabiArgs tile_args(ts_b200_pair *p) {
+    ts_b200_kernel *a = p->a;
     RabiArgs r{};
-    if (a->imag) {
-        r.cc = std::cosh(ang);
-        r.cs_r = no == 0 ? 0 : c3 / no * std::sinh(ang);
-        r.cs_i = no == 0 ? 0 : c4 / no * std::sinh(ang);
-    } else {
-        r.cc = std::cos(ang);
-        r.cs_r = no == 0 ? 0 : c3 / no * std::sin(ang);
-        r.cs_i = no == 0 ? 0 : c4 / no * std::sin(ang);
-    }
-    r.ta = view(a);
-    r.tb = view(b);
+    r.ta = view(p->a);
+    r.tb = view(p->b);
     r.W = a->W;
     r.H = a->H;
     r.P = a->P;
@@ -258,6 +268,25 @@ int launch_rabi(ts_b200_pair *p, double var, bool normalise) {
     r.iy1 = a->d.inner_y1;
     r.imag = a->imag ? 1 : 0;
     r.partials = p->partials;
+    return r;
+}
+
+int launch_rabi(ts_b200_pair *p, double var, bool normalise) {
+    ts_b200_kernel *a = p->a, *b = p->b;
+    // angle of src/cpukernel.cpp:581-606 (omega / 2 as coupling_const[3], [4])
+    const double c3 = 0.5 * p->omega_r, c4 = 0.5 * p->omega_i;
+    const double no = std::sqrt(c3 * c3 + c4 * c4);
+    const double ang = -p->delta_t * var * no;
+    RabiArgs r = tile_args(p);
+    if (a->imag) {
+        r.cc = std::cosh(ang);
+        r.cs_r = no == 0 ? 0 : c3 / no * std::sinh(ang);
+        r.cs_i = no == 0 ? 0 : c4 / no * std::sinh(ang);
+    } else {
+        r.cc = std::cos(ang);
+        r.cs_r = no == 0 ? 0 : c3 / no * std::sin(ang);
+        r.cs_i = no == 0 ? 0 : c4 / no * std::sin(ang);
+    }
     const dim3 grid(kBlocksX, kBlocksY);
     if (a->fp32) rabi_kernel<float><<<grid, kThreads, 0, a->stream>>>(r);
     else rabi_kernel<double><<<grid, kThreads, 0, a->stream>>>(r);
@@ -268,6 +297,24 @@ int launch_rabi(ts_b200_pair *p, double var, bool normalise) {
     tsbh::g_launches.fetch_add(2, std::memory_order_relaxed);
     return TS_B200_OK;
 }
+
+// One species' step: a with b's current tile, b with a's tile from before
+// a's step (a's input buffer, valid right after a's step).
+int step_species(ts_b200_pair *p, int which, int exchange) {
+    ts_b200_kernel *a = p->a, *b = p->b;
+    if (which == 0) {
+        a->pb = b->psi[b->cur];
+        a->pb_scale = &b->scal->pending_inv;
+        const int s = tsbh::launch_step_tile(a, exchange);
+        return s ? pfail(p, s, "species a: " + a->err) : TS_B200_OK;
+    }
+    b->pb = a->psi[1 - a->cur];
+    b->pb_scale = &a->scal->prev_inv;
+    const int s = tsbh::launch_step_tile(b, exchange);
+    return s ? pfail(p, s, "species b: " + b->err) : TS_B200_OK;
+}
+
+bool has_rabi(const ts_b200_pair *p) { return p->omega_r != 0.0 || p->omega_i != 0.0; }
 
 }  // namespace
 
@@ -320,26 +367,41 @@ int ts_b200_pair_rabi(ts_b200_pair *p, double var) {
     return launch_rabi(p, var, false);
 }
 
-int ts_b200_pair_evolve(ts_b200_pair *p, int iterations) {
-    if (!p || iterations < 0) return TS_B200_INVALID_ARGUMENT;
-    ts_b200_kernel *a = p->a, *b = p->b;
-    const bool rabi = p->omega_r != 0.0 || p->omega_i != 0.0;
-    for (int i = 0; i < iterations; ++i) {
-        const int exchange = i != iterations - 1;
-        a->pb = b->psi[b->cur];
-        a->pb_scale = &b->scal->pending_inv;
-        int s = tsbh::launch_step_tile(a, exchange);
-        if (s) return pfail(p, s, "species a: " + a->err);
-        // species b sees a's tile from before a's step: a's input buffer
-        b->pb = a->psi[1 - a->cur];
-        b->pb_scale = &a->scal->prev_inv;
-        s = tsbh::launch_step_tile(b, exchange);
-        if (s) return pfail(p, s, "species b: " + b->err);
-        if (rabi) {
-            s = launch_rabi(p, i == iterations - 1 ? 0.5 : 1.0, a->imag);
-            if (s) return s;
-        }
+int ts_b200_pair_steps(ts_b200_pair *p, int steps, int final_steps) {
+    if (!p || steps < 0) return TS_B200_INVALID_ARGUMENT;
+    const bool rabi = has_rabi(p);
+    for (int i = 0; i < steps; ++i) {
+        const bool last = final_steps && i == steps - 1;
+        int s = step_species(p, 0, last ? 0 : 1);
+        if (s == TS_B200_OK) s = step_species(p, 1, last ? 0 : 1);
+        if (s == TS_B200_OK && rabi) s = launch_rabi(p, last ? 0.5 : 1.0, p->a->imag);
+        if (s) return s;
     }
+    return TS_B200_OK;
+}
+
+int ts_b200_pair_evolve(ts_b200_pair *p, int iterations) {
+    return ts_b200_pair_steps(p, iterations, 1);
+}
+
+int ts_b200_pair_step_species(ts_b200_pair *p, int which) {
+    if (!p || (which != 0 && which != 1)) return TS_B200_INVALID_ARGUMENT;
+    return step_species(p, which, 0);
+}
+
+int ts_b200_pair_normalize(ts_b200_pair *p) {
+    if (!p) return TS_B200_INVALID_ARGUMENT;
+    ts_b200_kernel *a = p->a;
+    if (!a->imag || !has_rabi(p)) return TS_B200_OK;  // src/cpukernel.cpp:608-609
+    RabiArgs r = tile_args(p);
+    const dim3 grid(kBlocksX, kBlocksY);
+    if (a->fp32) pair_norm_kernel<float><<<grid, kThreads, 0, a->stream>>>(r);
+    else pair_norm_kernel<double><<<grid, kThreads, 0, a->stream>>>(r);
+    PAIR_CHECK(p, cudaGetLastError());
+    rabi_finish_kernel<<<1, 32, 0, a->stream>>>(a->scal, p->b->scal, p->partials, 1,
+                                                a->d.delta_x * a->d.delta_y, p->tot_norm, 1);
+    PAIR_CHECK(p, cudaGetLastError());
+    tsbh::g_launches.fetch_add(2, std::memory_order_relaxed);
     return TS_B200_OK;
 }
 

@@ -1053,8 +1053,11 @@ __global__ void __launch_bounds__(128, V::MIN_BLOCKS) step_kernel(StepArgs<typen
                     // the other species' next step reads this step's input
                     // buffer with the factor that was pending on it
                     a.scal->prev_inv = a.scal->pending_inv;
+                    // the kept norm moves with the joint normalisation: a
+                    // species that started empty is renormalised once it has
+                    // a share (src/cpukernel.cpp:551, norm[i] != 0)
                     const double n0 = a.scal->norm_target;
-                    if (a.scal->renorm && n0 != 0.0) a.scal->pending_inv = 1.0 / sqrt(tot / n0);
+                    if (n0 != 0.0) a.scal->pending_inv = 1.0 / sqrt(tot / n0);
                 } else {
                     if (a.scal->renorm) a.scal->pending_inv = 1.0 / sqrt(tot / a.norm0);
                 }

@@ -54,6 +54,49 @@ private:
     bool imag_time_;
 };
 
+/** Two species evolved together (the reference's two-state CPUBlock,
+ *  src/cpukernel.cpp:274-392,581-667), on a ts_b200_pair of two device tiles.
+ *  The plug-in protocol alternates the species as the reference's kernel
+ *  does: run_kernel / finish_halo_exchange act on the current species and
+ *  wait_for_completion moves to the other one; steps() runs whole steps of
+ *  the pair without the per-call protocol. */
+class B200PairKernel : public ITrotterKernel {
+public:
+    B200PairKernel(Lattice *grid, State *state_a, State *state_b, Hamiltonian2Component *ham,
+                   double **external_pot_real, double **external_pot_imag, double delta_t,
+                   double *norm, bool imag_time, int precision = TS_B200_FP64);
+    ~B200PairKernel();
+
+    void run_kernel_on_halo() {}
+    void run_kernel();
+    void wait_for_completion();
+    void get_sample(size_t dest_stride, size_t x, size_t y, size_t width, size_t height,
+                    double *dest_real, double *dest_imag, double *dest_real2 = 0,
+                    double *dest_imag2 = 0) const;
+    void normalization();
+    void rabi_coupling(double var, double delta_t);
+    void cpy_first_positive_to_first_negative() {}
+    double calculate_squared_norm(bool global = true) const;
+    bool runs_in_place() const { return false; }
+    std::string get_name() const { return "B200 (two components)"; }
+    void update_potential(double *external_pot_real, double *external_pot_imag, int which);
+    void start_halo_exchange() {}
+    void finish_halo_exchange();
+
+    /** n steps of the pair; with final_steps the last one is the evolve()
+     *  call's last (no halo refresh, half Rabi rotation). */
+    void steps(int n, bool final_steps);
+    ts_b200_pair *pair() const { return p_; }
+
+private:
+    void check(int status, const char *what) const;
+    void release();
+    ts_b200_kernel *h_[2] = {nullptr, nullptr};
+    ts_b200_pair *p_ = nullptr;
+    int state_index_ = 0;
+    int dim_x_;
+};
+
 namespace b200 {
 
 struct Expectations {
@@ -72,6 +115,16 @@ ts_b200_energy_result reduce_energies(Lattice *grid, const double *p_real, const
 /** Step descriptor with the constants of the reference's CPUBlock constructor. */
 ts_b200_desc make_desc(Lattice *grid, Hamiltonian *ham, double delta_t, double norm,
                        bool imag_time, int precision);
+/** The same for one species of mass `mass`, g = coupling, g_LHY = lhy. */
+ts_b200_desc make_species_desc(Lattice *grid, Hamiltonian *ham, double delta_t, double norm,
+                               bool imag_time, int precision, double mass, double coupling,
+                               double lhy);
+
+/** Inter-species and Rabi energies of two host tiles (src/solver.cpp:340-353,
+ *  549-550), reduced on the GPU. */
+void reduce_cross_energies(Lattice *grid, const double *a_re, const double *a_im,
+                           const double *b_re, const double *b_im, double coupling_ab,
+                           double omega_r, double omega_i, double *inter, double *rabi);
 
 }  // namespace b200
 

@@ -181,6 +181,16 @@ int tsh_hamiltonian_new(void *lp, void *pp, double mass, double ga, double glhy,
     });
 }
 
+int tsh_hamiltonian2_new(void *lp, void *pp, void *pbp, double mass, double mass_b, double ga,
+                         double gab, double gb, double omega_r, double omega_i, double omega,
+                         double rx, double ry, void **out) {
+    return guard([&] {
+        *out = new Hamiltonian2Component(static_cast<Lattice *>(lp), static_cast<Potential *>(pp),
+                                         static_cast<Potential *>(pbp), mass, mass_b, ga, gab, gb,
+                                         omega_r, omega_i, omega, rx, ry);
+    });
+}
+
 int tsh_hamiltonian_free(void *hp) {
     return guard([&] { delete static_cast<Hamiltonian *>(hp); });
 }
@@ -189,6 +199,34 @@ int tsh_solver_new(void *lp, void *sp, void *hp, double dt, const char *kt, void
     return guard([&] {
         *out = new Solver(static_cast<Lattice *>(lp), static_cast<State *>(sp),
                           static_cast<Hamiltonian *>(hp), dt, kt ? kt : "gpu");
+    });
+}
+
+int tsh_solver2_new(void *lp, void *sp, void *sbp, void *hp, double delta_t,
+                    const char *kernel_type, void **out) {
+    return guard([&] {
+        *out = new Solver(static_cast<Lattice *>(lp), static_cast<State *>(sp),
+                          static_cast<State *>(sbp), static_cast<Hamiltonian2Component *>(hp),
+                          delta_t, kernel_type);
+    });
+}
+
+int tsh_solver_energies2(void *svp, double out[13]) {
+    return guard([&] {
+        Solver *s = static_cast<Solver *>(svp);
+        out[0] = s->get_total_energy();
+        out[1] = s->get_kinetic_energy(1);
+        out[2] = s->get_kinetic_energy(2);
+        out[3] = s->get_potential_energy(1);
+        out[4] = s->get_potential_energy(2);
+        out[5] = s->get_rotational_energy(1);
+        out[6] = s->get_rotational_energy(2);
+        out[7] = s->get_intra_species_energy(1);
+        out[8] = s->get_intra_species_energy(2);
+        out[9] = s->get_inter_species_energy();
+        out[10] = s->get_rabi_energy();
+        out[11] = s->get_squared_norm(1);
+        out[12] = s->get_squared_norm(2);
     });
 }
 

@@ -77,15 +77,13 @@ void Solver::set_exp_potential(double *re, int re_len, double *im, int im_len, i
     memcpy(external_pot_imag[which], im, sizeof(double) * im_len);
     // The reference's CPU kernel reads these arrays in place, so a new table
     // takes effect at the next step; the device kernel holds its own copy.
-    if (kernel != NULL && which == 0)
-        kernel->update_potential(external_pot_real[0], external_pot_imag[0], 0);
+    if (kernel != NULL && (which == 0 || !single_component))
+        kernel->update_potential(external_pot_real[which], external_pot_imag[which], which);
 }
 
 void Solver::init_kernel() {
     delete kernel;
     kernel = NULL;
-    if (!single_component)
-        my_abort("Two-component evolution is not supported by the B200 kernel.");
     int precision;
     if (kernel_type == "gpu" || kernel_type == "b200")
         precision = TS_B200_FP64;
@@ -94,8 +92,14 @@ void Solver::init_kernel() {
     else
         my_abort("Unknown kernel: \"" + kernel_type +
                  "\" (this build provides the B200 kernel: \"gpu\", \"gpu_fp32\")");
-    kernel = new B200Kernel(grid, state, hamiltonian, external_pot_real[0], external_pot_imag[0],
-                            delta_t, norm2[0], imag_time, precision);
+    if (single_component)
+        kernel = new B200Kernel(grid, state, hamiltonian, external_pot_real[0],
+                                external_pot_imag[0], delta_t, norm2[0], imag_time, precision);
+    else
+        kernel = new B200PairKernel(grid, state, state_b,
+                                    static_cast<Hamiltonian2Component *>(hamiltonian),
+                                    external_pot_real, external_pot_imag, delta_t, norm2,
+                                    imag_time, precision);
     kernel_state_current = true;
 }
 
@@ -105,8 +109,13 @@ void Solver::prepare_kernel(bool _imag_time) {
         if (imag_time) {
             initialize_exp_potential(delta_t, 0);
             norm2[0] = state->get_squared_norm();
-        } else if (!is_python) {
-            initialize_exp_potential(delta_t, 0);
+            if (!single_component) {
+                initialize_exp_potential(delta_t, 1);
+                norm2[1] = state_b->get_squared_norm();
+            }
+        } else {
+            if (!is_python) initialize_exp_potential(delta_t, 0);
+            if (!single_component) initialize_exp_potential(delta_t, 1);
         }
         init_kernel();
         has_parameters_changed = false;
@@ -119,6 +128,10 @@ void Solver::evolve(int iterations, bool _imag_time) {
     if (iterations < 0) {
         iterations = -iterations;
         soft_update = true;
+    }
+    if (!single_component) {
+        evolve_two_components(iterations, soft_update);
+        return;
     }
     B200Kernel *bk = static_cast<B200Kernel *>(kernel);
     // Steps are queued in runs; a run is flushed when the potential changes
@@ -145,9 +158,49 @@ void Solver::evolve(int iterations, bool _imag_time) {
     energy_expected_values_updated = false;
 }
 
+// Two components (src/solver.cpp:172-240): a Rabi half step first (every
+// call from C++, only at t = 0 from Python), then the steps of the pair in
+// runs between potential updates, the last one the call's last.
+void Solver::evolve_two_components(int iterations, bool soft_update) {
+    B200PairKernel *pk = static_cast<B200PairKernel *>(kernel);
+    Hamiltonian2Component *h2 = static_cast<Hamiltonian2Component *>(hamiltonian);
+    if (!is_python || current_evolution_time == 0) kernel->rabi_coupling(0.5, delta_t);
+    int pending = 0;
+    for (int i = 0; i < iterations; ++i) {
+        if (i > 0) {
+            const bool ua = hamiltonian->potential->update(current_evolution_time);
+            const bool ub = h2->potential_b->update(current_evolution_time);
+            if ((ua || ub) && pending > 0) {
+                pk->steps(pending, false);
+                pending = 0;
+            }
+            if (ua) {
+                if (!is_python) initialize_exp_potential(delta_t, 0);
+                kernel->update_potential(external_pot_real[0], external_pot_imag[0], 0);
+            }
+            if (ub) {
+                if (!is_python) initialize_exp_potential(delta_t, 1);
+                kernel->update_potential(external_pot_real[1], external_pot_imag[1], 1);
+            }
+        }
+        ++pending;
+        current_evolution_time += delta_t;
+    }
+    pk->steps(pending, true);
+    if (!soft_update) {
+        kernel->get_sample(grid->dim_x, 0, 0, grid->dim_x, grid->dim_y, state->p_real,
+                           state->p_imag, state_b->p_real, state_b->p_imag);
+        state_b->expected_values_updated = false;
+    }
+    state->expected_values_updated = false;
+    energy_expected_values_updated = false;
+}
+
 void Solver::calculate_energy_expected_values(void) {
-    if (!single_component)
-        my_abort("Two-component energies are not supported by the B200 kernel.");
+    if (!single_component) {
+        calculate_energies_two_components();
+        return;
+    }
     std::vector<double> V(size_t(grid->dim_x) * grid->dim_y);
     for (int y = 0; y < grid->dim_y; ++y)
         for (int x = 0; x < grid->dim_x; ++x) {
@@ -173,6 +226,47 @@ void Solver::calculate_energy_expected_values(void) {
     energy_expected_values_updated = true;
 }
 
+// src/solver.cpp:244-564 with two components: each species' terms as for one
+// (its own mass, g, potential), the cross terms from the pair, and the totals
+// of src/solver.cpp:544-558.
+void Solver::calculate_energies_two_components(void) {
+    Hamiltonian2Component *h2 = static_cast<Hamiltonian2Component *>(hamiltonian);
+    const size_t n = size_t(grid->dim_x) * grid->dim_y;
+    std::vector<double> Va(n), Vb(n);
+    for (int y = 0; y < grid->dim_y; ++y)
+        for (int x = 0; x < grid->dim_x; ++x) {
+            Va[size_t(y) * grid->dim_x + x] = h2->potential->get_value(x, y);
+            Vb[size_t(y) * grid->dim_x + x] = h2->potential_b->get_value(x, y);
+        }
+    const ts_b200_energy_result ra =
+        b200::reduce_energies(grid, state->p_real, state->p_imag, Va.data(), h2->mass,
+                              h2->coupling_a, h2->LeeHuangYang_coupling_a, h2->angular_velocity);
+    const ts_b200_energy_result rb =
+        b200::reduce_energies(grid, state_b->p_real, state_b->p_imag, Vb.data(), h2->mass_b,
+                              h2->coupling_b, 0., h2->angular_velocity);
+    b200::reduce_cross_energies(grid, state->p_real, state->p_imag, state_b->p_real,
+                                state_b->p_imag, h2->coupling_ab, h2->omega_r, h2->omega_i,
+                                &inter_species_energy, &rabi_energy);
+    const ts_b200_energy_result *r[2] = {&ra, &rb};
+    for (int c = 0; c < 2; ++c) {
+        norm2[c] = r[c]->norm2;
+        kinetic_energy[c] = r[c]->kinetic;
+        potential_energy[c] = r[c]->potential;
+        rotational_energy[c] = r[c]->rotational;
+        intra_species_energy[c] = r[c]->intra;
+    }
+    LeeHuangYang_energy = ra.lhy;
+    total_energy = kinetic_energy[0] + potential_energy[0] + intra_species_energy[0] +
+                   rotational_energy[0] + kinetic_energy[1] + potential_energy[1] +
+                   intra_species_energy[1] + rotational_energy[1] + inter_species_energy +
+                   rabi_energy;
+    tot_kinetic_energy = kinetic_energy[0] + kinetic_energy[1];
+    tot_potential_energy = potential_energy[0] + potential_energy[1];
+    tot_rotational_energy = rotational_energy[0] + rotational_energy[1];
+    tot_intra_species_energy = intra_species_energy[0] + intra_species_energy[1];
+    energy_expected_values_updated = true;
+}
+
 double Solver::get_total_energy(void) {
     if (!energy_expected_values_updated) calculate_energy_expected_values();
     return total_energy;
@@ -195,7 +289,8 @@ static double pick(size_t which, bool single, double first, double second, doubl
 
 double Solver::get_squared_norm(size_t which) {
     if (!energy_expected_values_updated) calculate_energy_expected_values();
-    return pick(which, single_component, norm2[0], norm2[1], norm2[0]);
+    return pick(which, single_component, norm2[0], norm2[1],
+                single_component ? norm2[0] : norm2[0] + norm2[1]);
 }
 
 double Solver::get_kinetic_energy(size_t which) {
@@ -227,11 +322,15 @@ double Solver::get_LeeHuangYang_energy(void) {
 }
 
 double Solver::get_inter_species_energy(void) {
+    if (!energy_expected_values_updated) calculate_energy_expected_values();
+    if (!single_component) return inter_species_energy;
     cout << "The system has only one component\n";
     return 0;
 }
 
 double Solver::get_rabi_energy(void) {
+    if (!energy_expected_values_updated) calculate_energy_expected_values();
+    if (!single_component) return rabi_energy;
     cout << "The system has only one component\n";
     return 0;
 }

@@ -210,7 +210,7 @@ public:
     Hamiltonian(Lattice *grid, Potential *potential = 0, double mass = 1., double coupling_a = 0.,
                 double LeeHuangYang_coupling_a = 0., double angular_velocity = 0.,
                 double rot_coord_x = 0, double rot_coord_y = 0);
-    ~Hamiltonian();
+    virtual ~Hamiltonian();
 
 protected:
     bool self_init;
@@ -317,6 +317,8 @@ private:
     bool has_parameters_changed;
     bool energy_expected_values_updated;
     void calculate_energy_expected_values(void);
+    void calculate_energies_two_components(void);
+    void evolve_two_components(int iterations, bool soft_update);
     bool is_python;
     bool kernel_state_current;  ///< the kernel's device tile equals *state
 };

@@ -93,6 +93,9 @@ SIGNATURES = {
                                  C.POINTER(_VP)]),
     "ts_b200_pair_rabi": (_I, [_VP, C.c_double]),
     "ts_b200_pair_evolve": (_I, [_VP, C.c_int]),
+    "ts_b200_pair_steps": (_I, [_VP, C.c_int, C.c_int]),
+    "ts_b200_pair_step_species": (_I, [_VP, C.c_int]),
+    "ts_b200_pair_normalize": (_I, [_VP]),
     "ts_b200_pair_cross_energies": (_I, [_VP, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "ts_b200_pair_last_error": (C.c_char_p, [_VP]),
     "ts_b200_pair_destroy": (_I, [_VP]),

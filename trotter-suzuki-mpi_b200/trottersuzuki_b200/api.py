@@ -69,6 +69,9 @@ def host():
             "tsh_hamiltonian_new": (i, [vp, vp, d, d, d, d, d, d, P(vp)]),
             "tsh_hamiltonian_free": (i, [vp]),
             "tsh_solver_new": (i, [vp, vp, vp, d, C.c_char_p, P(vp)]),
+            "tsh_solver2_new": (i, [vp, vp, vp, vp, d, C.c_char_p, P(vp)]),
+            "tsh_solver_energies2": (i, [vp, P(d)]),
+            "tsh_hamiltonian2_new": (i, [vp, vp, vp] + [d] * 10 + [P(vp)]),
             "tsh_solver_evolve": (i, [vp, i, i]),
             "tsh_solver_prepare": (i, [vp, i]),
             "tsh_solver_energies": (i, [vp, P(d)]),
@@ -459,11 +462,28 @@ class Hamiltonian(_Handle):
                        float(angular_velocity), float(rot_coord_x), float(rot_coord_y))
 
 
-class Hamiltonian2Component:
-    """Declared for API compatibility; the B200 kernel evolves one component."""
+class Hamiltonian2Component(Hamiltonian):
+    """Two species (src/trottersuzuki.h:455-497): masses, intra-species
+    couplings g_a and g_b, inter-species g_ab and the Rabi coupling
+    omega = omega_r + i omega_i; potential_b defaults to potential."""
 
-    def __init__(self, *args, **kwargs):
-        raise RuntimeError("Two-component evolution is not supported by the B200 kernel.")
+    def __init__(self, grid, potential=None, potential_b=None, mass=1., mass_b=1.,
+                 coupling_a=0., coupling_ab=0., coupling_b=0., omega_r=0., omega_i=0.,
+                 angular_velocity=0., rot_coord_x=0., rot_coord_y=0.):
+        self.grid = grid
+        self.potential = potential
+        self.potential_b = potential_b if potential_b is not None else potential
+        self.mass, self.mass_b = mass, mass_b
+        self.coupling_a, self.coupling_ab, self.coupling_b = coupling_a, coupling_ab, coupling_b
+        self.omega_r, self.omega_i = omega_r, omega_i
+        self.LeeHuangYang_coupling_a = 0.
+        self.angular_velocity = angular_velocity
+        self._h = _new(host().tsh_hamiltonian2_new, grid._h,
+                       potential._h if potential is not None else None,
+                       potential_b._h if potential_b is not None else None, float(mass),
+                       float(mass_b), float(coupling_a), float(coupling_ab), float(coupling_b),
+                       float(omega_r), float(omega_i), float(angular_velocity),
+                       float(rot_coord_x), float(rot_coord_y))
 
 
 # ------------------------------------------------------------------ solver
@@ -472,18 +492,30 @@ class Solver(_Handle):
 
     def __init__(self, Lattice, State, Hamiltonian, delta_t, Potential=None, State2=None,
                  Potential2=None, kernel_type="gpu"):
-        if State2 is not None:
-            raise RuntimeError("Two-component evolution is not supported by the B200 kernel.")
         self.grid, self.state, self.hamiltonian = Lattice, State, Hamiltonian
+        self.state2 = State2
         self.delta_t = delta_t
         self.potential = Potential if Potential is not None else Hamiltonian.potential
         self.kernel_type = kernel_type
         self.current_evolution_time = 0.0
-        self._h = _new(host().tsh_solver_new, Lattice._h, State._h, Hamiltonian._h,
-                       float(delta_t), kernel_type.encode())
+        if State2 is None:
+            self._h = _new(host().tsh_solver_new, Lattice._h, State._h, Hamiltonian._h,
+                           float(delta_t), kernel_type.encode())
+        else:
+            if not isinstance(Hamiltonian, Hamiltonian2Component):
+                raise RuntimeError("two states need a Hamiltonian2Component")
+            self.potential2 = Potential2 if Potential2 is not None else self.potential
+            self._h = _new(host().tsh_solver2_new, Lattice._h, State._h, State2._h,
+                           Hamiltonian._h, float(delta_t), kernel_type.encode())
 
     def evolve(self, iterations, imag_time=False):
         pot = self.potential
+        if self.state2 is not None:
+            # two components: time-dependent potentials are re-tabulated by the
+            # C++ Solver (src/solver.cpp:186-199)
+            _chk(host().tsh_solver_evolve(self._h, int(iterations), int(bool(imag_time))))
+            self.current_evolution_time += self.delta_t * abs(int(iterations))
+            return
         if pot is None or not getattr(pot, "updated_potential_matrix", False) or imag_time:
             _chk(host().tsh_solver_evolve(self._h, int(iterations), int(bool(imag_time))))
             self.current_evolution_time += self.delta_t * abs(int(iterations))
@@ -557,26 +589,54 @@ class Solver(_Handle):
         _chk(host().tsh_solver_energies(self._h, out))
         return list(out)
 
+    def _energies2(self):
+        out = (C.c_double * 13)()
+        _chk(host().tsh_solver_energies2(self._h, out))
+        return list(out)
+
+    def _pick(self, which, single_index, first):
+        """which: 1 first species, 2 second, 3 total (src/solver.cpp:572-594)."""
+        if self.state2 is None:
+            if which == 2:
+                print("The system has only one component. No input have to be given")
+                return 0.0
+            return self._energies()[single_index]
+        e = self._energies2()
+        a, b = e[first], e[first + 1]
+        return {1: a, 2: b, 3: a + b}.get(int(which), 0.0)
+
     def get_total_energy(self):
-        return self._energies()[0]
+        return self._energies2()[0] if self.state2 is not None else self._energies()[0]
 
     def get_kinetic_energy(self, which=3):
-        return self._energies()[1]
+        return self._pick(which, 1, 1)
 
     def get_potential_energy(self, which=3):
-        return self._energies()[2]
+        return self._pick(which, 2, 3)
 
     def get_rotational_energy(self, which=3):
-        return self._energies()[3]
+        return self._pick(which, 3, 5)
 
     def get_intra_species_energy(self, which=3):
-        return self._energies()[4]
+        return self._pick(which, 4, 7)
 
     def get_LeeHuangYang_energy(self):
-        return self._energies()[5]
+        return 0.0 if self.state2 is not None else self._energies()[5]
+
+    def get_inter_species_energy(self):
+        if self.state2 is None:
+            print("The system has only one component")
+            return 0.0
+        return self._energies2()[9]
+
+    def get_rabi_energy(self):
+        if self.state2 is None:
+            print("The system has only one component")
+            return 0.0
+        return self._energies2()[10]
 
     def get_squared_norm(self, which=3):
-        return self._energies()[6]
+        return self._pick(which, 6, 11)
 
     def kernel_handle(self):
         """The C-ABI handle (ts_b200_kernel*) of the current kernel, or None."""
