@@ -124,6 +124,16 @@ def test_unknown_kernel_type_raises_like_the_reference():
         solver.evolve(1)
 
 
-def test_two_component_is_rejected():
-    with pytest.raises(RuntimeError, match="Two-component"):
-        api.Hamiltonian2Component()
+def test_two_component_host_objects():
+    """Two-state Solver construction (no GPU needed): a Hamiltonian2Component
+    is required, and the CPU kernel type is refused as for one component."""
+    g = api.Lattice2D(16, 4.0)
+    s1, s2 = api.GaussianState(g, 1.0), api.State(g)
+    pot = api.HarmonicPotential(g, 1.0, 1.0)
+    h2 = api.Hamiltonian2Component(g, pot, None, 1.0, 1.2, 2.0, 1.0, 3.0, 0.5, 0.0)
+    assert h2.potential_b is pot and h2.mass_b == 1.2
+    with pytest.raises(RuntimeError, match="Hamiltonian2Component"):
+        api.Solver(g, s1, api.Hamiltonian(g, pot), 1e-3, State2=s2)
+    solver = api.Solver(g, s1, h2, 1e-3, State2=s2, kernel_type="cpu")
+    with pytest.raises(RuntimeError, match="Unknown kernel"):
+        solver.evolve(1)
