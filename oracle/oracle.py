@@ -34,6 +34,7 @@ class Params(C.Structure):
         ("rot_off_x", C.c_int), ("rot_off_y", C.c_int),
         ("delta_x", C.c_double), ("delta_y", C.c_double),
         ("norm0", C.c_double),
+        ("cylindrical", C.c_int), ("kin_radial", C.c_double), ("mirror_sign", C.c_int),
     ]
 
 
@@ -45,6 +46,7 @@ class Geometry(C.Structure):
         ("global_no_halo_dim_x", C.c_int), ("global_no_halo_dim_y", C.c_int),
         ("delta_x", C.c_double), ("delta_y", C.c_double),
         ("length_x", C.c_double), ("length_y", C.c_double),
+        ("cylindrical", C.c_int),
     ]
 
 
@@ -122,7 +124,15 @@ class Lattice:
     """Geometry of a reference Lattice2D / Lattice1D tile (src/model.cpp:32-158)."""
 
     def __init__(self, dim_x, length_x, dim_y=None, length_y=None, periodic_x=False,
-                 periodic_y=False, angular_velocity=0.0, one_d=False):
+                 periodic_y=False, angular_velocity=0.0, one_d=False, cylindrical=False):
+        """cylindrical: the radial axis is x (src/model.cpp:107-158): one more
+        column (r = -dx/2, the mirror of r = dx/2), dx = L / (N + 1 - 0.5),
+        the inner region starting at column 1."""
+        if cylindrical:
+            if periodic_x:
+                raise ValueError("no periodic boundary on the radial axis")
+            dim_x += 1
+        self.cylindrical = bool(cylindrical)
         if one_d:
             dim_y, length_y = 1, 0.0
             self.delta_x = length_x / float(dim_x)
@@ -130,9 +140,10 @@ class Lattice:
             self.halo_x, self.halo_y = 4, 0
             periodic_y = False
         else:
-            dim_y = dim_x if dim_y is None else dim_y
+            dim_y = (dim_x - (1 if cylindrical else 0)) if dim_y is None else dim_y
             length_y = length_x if length_y is None else length_y
-            self.delta_x = length_x / float(dim_x)
+            self.delta_x = (length_x / (float(dim_x) - 0.5) if cylindrical
+                            else length_x / float(dim_x))
             self.delta_y = length_y / float(dim_y)
             self.halo_x = self.halo_y = 4 if angular_velocity == 0.0 else 8
         self.one_d = one_d
@@ -146,6 +157,8 @@ class Lattice:
         else:
             self.start_y, self.end_y, self.inner_start_y, self.inner_end_y = calculate_borders(
                 dim_y, self.halo_y, periodic_y)
+        if cylindrical:
+            self.inner_start_x += 1
         self.dim_x = self.end_x - self.start_x
         self.dim_y = self.end_y - self.start_y
 
@@ -166,12 +179,22 @@ class Lattice:
         g.global_no_halo_dim_y = self.global_no_halo_dim_y
         g.delta_x, g.delta_y = self.delta_x, self.delta_y
         g.length_x, g.length_y = self.length_x, self.length_y
+        g.cylindrical = int(self.cylindrical)
         return g
 
     def coordinates(self):
         """(x, y) arrays of shape (dim_y, dim_x), src/common.cpp:45-65."""
         xi = np.arange(self.dim_x, dtype=np.float64)
         yi = np.arange(self.dim_y, dtype=np.float64)
+        if self.cylindrical:  # src/common.cpp:66-81
+            idx = self.start_x * self.delta_x + xi * self.delta_x - 0.5 * self.delta_x
+            idy = self.start_y * self.delta_y + 0.5 * self.delta_y + yi * self.delta_y
+            y_c = self.global_no_halo_dim_y * self.delta_y * 0.5
+            idy = np.where(idy - y_c < -self.length_y * 0.5, idy + self.length_y, idy)
+            idy = np.where(idy - y_c > self.length_y * 0.5, idy - self.length_y, idy)
+            X = np.broadcast_to(idx[None, :], self.shape)
+            Y = np.broadcast_to((idy - y_c)[:, None], self.shape)
+            return np.ascontiguousarray(X), np.ascontiguousarray(Y)
         idx = self.start_x * self.delta_x + 0.5 * self.delta_x + xi * self.delta_x
         idy = self.start_y * self.delta_y + 0.5 * self.delta_y + yi * self.delta_y
         x_c = self.global_no_halo_dim_x * self.delta_x * 0.5
@@ -184,6 +207,11 @@ class Lattice:
         Y = np.broadcast_to((idy - y_c)[:, None], self.shape)
         return np.ascontiguousarray(X), np.ascontiguousarray(Y)
 
+    def azimuthal(self, angular_momentum, mass=1.0):
+        """l^2 / (2 m r^2) over the tile (src/model.cpp:967-971), cylindrical."""
+        X, _ = self.coordinates()
+        return (angular_momentum * angular_momentum) / (2. * mass * X * X)
+
     def harmonic(self, omega_x, omega_y, mass=1.0, mean_x=0.0, mean_y=0.0):
         """HarmonicPotential::get_value over the tile (src/model.cpp:920-926)."""
         X, Y = self.coordinates()
@@ -192,7 +220,7 @@ class Lattice:
         return 0.5 * mass * (omega_x * omega_x * xr * xr + omega_y * omega_y * yr * yr)
 
     def params(self, delta_t, imag_time=False, mass=1.0, coupling=0.0, lhy=0.0,
-               angular_velocity=0.0, rot_coord=(0.0, 0.0), norm0=0.0):
+               angular_velocity=0.0, rot_coord=(0.0, 0.0), norm0=0.0, angular_momentum=0):
         p = Params()
         p.W, p.H = self.dim_x, self.dim_y
         p.ix0, p.ix1, p.iy0, p.iy1 = self.inner()
@@ -207,6 +235,10 @@ class Lattice:
         p.rot_off_x = int(self.start_x - rcx)
         p.rot_off_y = int(self.start_y - rcy)
         p.norm0 = norm0
+        if self.cylindrical:  # src/cpukernel.cpp:200-210,669-689
+            p.cylindrical = 1
+            p.kin_radial = delta_t / (8. * mass * self.delta_x * self.delta_x)
+            p.mirror_sign = 1 if angular_momentum % 2 == 0 else -1
         return p
 
 

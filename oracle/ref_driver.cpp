@@ -46,6 +46,8 @@ struct tsref_config {
     int omp_threads;             // <= 0: leave OpenMP's default
     int kernel_gpu;              // 1: kernel_type "gpu", the reference's CUDA kernel
                                  // (CC2Kernel, src/gpukernel.cu; libtsref_gpu.so only)
+    int cylindrical;             // 1: coordinate_system "cylindrical" (2D lattices)
+    int angular_momentum;        // of the State (init_kind 0)
 };
 
 struct tsref_result {
@@ -75,7 +77,8 @@ int tsref_geometry(const tsref_config *cfg, tsref_result *res) {
         else
             grid = new Lattice2D(cfg->dim_x, cfg->length_x, cfg->dim_y, cfg->length_y,
                                  cfg->periodic_x != 0, cfg->periodic_y != 0,
-                                 cfg->lattice_angular_velocity);
+                                 cfg->lattice_angular_velocity,
+                                 cfg->cylindrical ? "cylindrical" : "cartesian");
         res->dim_x = grid->dim_x; res->dim_y = grid->dim_y;
         res->halo_x = grid->halo_x; res->halo_y = grid->halo_y;
         res->start_x = grid->start_x; res->start_y = grid->start_y;
@@ -108,7 +111,8 @@ int tsref_run(const tsref_config *cfg, double *psi_re, double *psi_im,
         } else {
             g2 = new Lattice2D(cfg->dim_x, cfg->length_x, cfg->dim_y, cfg->length_y,
                                cfg->periodic_x != 0, cfg->periodic_y != 0,
-                               cfg->lattice_angular_velocity);
+                               cfg->lattice_angular_velocity,
+                               cfg->cylindrical ? "cylindrical" : "cartesian");
             grid = g2;
         }
         const size_t n = size_t(grid->dim_x) * grid->dim_y;
@@ -117,7 +121,7 @@ int tsref_run(const tsref_config *cfg, double *psi_re, double *psi_im,
         if (cfg->init_kind == 0) {
             own_re.assign(psi_re, psi_re + n);
             own_im.assign(psi_im, psi_im + n);
-            state = new State(grid, 0, own_re.data(), own_im.data());
+            state = new State(grid, cfg->angular_momentum, own_re.data(), own_im.data());
         } else if (cfg->init_kind == 1) {
             if (g2) state = new GaussianState(g2, cfg->g_omega_x, cfg->g_omega_y, cfg->g_mean_x,
                                               cfg->g_mean_y, cfg->g_norm, cfg->g_phase);

@@ -143,6 +143,60 @@ static void rotation_cols(const tso_params *p, double *re, double *im) {
     }
 }
 
+/* ---- radial kinetic term (src/cpucylindrical.cpp:4-81) ---------------------
+ * Pairs (i, i+1) of the radial (x) axis with i = start_offset (mod 2), every
+ * row; x = i is the radial index (the tile starts at the axis).  The pair
+ * (0, 1) has its own coupling.  Restated as the reference writes it,
+ * including its choice of hyperbolic functions in real time and circular ones
+ * in imaginary time for the pairs past the first. */
+static void radial_pair(int imag_time, double a, double b, double c, double *re, double *im,
+                        size_t i, size_t j) {
+    double tr = re[i], ti = im[i];
+    if (imag_time) {
+        re[i] = a * tr + b * re[j];
+        im[i] = a * ti + b * im[j];
+        re[j] = a * re[j] + c * tr;
+        im[j] = a * im[j] + c * ti;
+    } else {
+        re[i] = a * tr - b * im[j];
+        im[i] = a * ti + b * re[j];
+        re[j] = a * re[j] - c * ti;
+        im[j] = a * im[j] + c * tr;
+    }
+}
+
+static void radial_sweep(const tso_params *p, int start_offset, double *re, double *im) {
+    const size_t W = (size_t)p->W;
+    int start_i = 0;
+    if (start_offset == 0) {
+        double kr = 2 * p->kin_radial;
+        double a = p->imag_time ? cosh(kr) : cos(kr);
+        double b = p->imag_time ? -sinh(kr) : -sin(kr);
+        for (int y = 0; y < p->H; ++y)
+            radial_pair(p->imag_time, a, b, b, re, im, (size_t)y * W, (size_t)y * W + 1);
+        start_i = 2;
+    }
+    double x = (double)start_i + start_offset;
+    for (int i = start_i + start_offset; i < p->W - 1; i += 2, x += 2) {
+        double kr = p->kin_radial / sqrt(x * x - 0.25);
+        double ratio = sqrt((2 * x + 1) / (2 * x - 1));
+        double sk = p->imag_time ? sin(kr) : sinh(kr);
+        double a = p->imag_time ? cos(kr) : cosh(kr), b = sk * ratio, c = -sk / ratio;
+        for (int y = 0; y < p->H; ++y)
+            radial_pair(p->imag_time, a, b, c, re, im, (size_t)y * W + i, (size_t)y * W + i + 1);
+    }
+}
+
+/* Column 0 (r = -dx/2) mirrors column 1 with the parity of the angular
+ * momentum, after every imaginary-time step (src/cpukernel.cpp:669-689). */
+static void mirror_axis(const tso_params *p, double *re, double *im) {
+    const size_t W = (size_t)p->W;
+    for (int y = 0; y < p->H; ++y) {
+        re[(size_t)y * W] = p->mirror_sign * re[(size_t)y * W + 1];
+        im[(size_t)y * W] = p->mirror_sign * im[(size_t)y * W + 1];
+    }
+}
+
 /* ---- one full step (src/cpukernel.cpp:22-92) ----------------------------- */
 void tso_full_step(const tso_params *p, double *re, double *im, const double *pot_re,
                    const double *pot_im) {
@@ -151,11 +205,19 @@ void tso_full_step(const tso_params *p, double *re, double *im, const double *po
     sweep_horizontal(p, 0, p->aH, p->bH, re, im);
     if (vert) sweep_vertical(p, 1, p->aV, p->bV, re, im);
     sweep_horizontal(p, 1, p->aH, p->bH, re, im);
+    if (p->cylindrical) {
+        radial_sweep(p, 0, re, im);
+        radial_sweep(p, 1, re, im);
+    }
     potential_step(p, pot_re, pot_im, re, im);
     if (p->alpha_x != 0. && p->alpha_y != 0.) {
         rotation_rows(p, re, im);
         rotation_cols(p, re, im);
         rotation_rows(p, re, im);
+    }
+    if (p->cylindrical) {
+        radial_sweep(p, 1, re, im);
+        radial_sweep(p, 0, re, im);
     }
     sweep_horizontal(p, 1, p->aH, p->bH, re, im);
     if (vert) sweep_vertical(p, 1, p->aV, p->bV, re, im);
@@ -221,6 +283,7 @@ void tso_evolve(const tso_params *p, double *re, double *im, const double *pot_r
         tso_full_step(p, re, im, pot_re, pot_im);
         if (i != iterations - 1) tso_halo_exchange(p, re, im);
         renormalise(p, re, im);
+        if (p->cylindrical && p->imag_time) mirror_axis(p, re, im);
     }
 }
 
@@ -489,6 +552,17 @@ void tso_exp_table(int imag_time, double delta_t, const double *V, size_t n, dou
 
 /* ---- coordinates (src/common.cpp:45-65, cartesian) ----------------------- */
 static void coords(const tso_geometry *g, int x_in, int y_in, double *x_out, double *y_out) {
+    if (g->cylindrical) {
+        /* the radial axis x starts at the tile's edge (src/common.cpp:66-81) */
+        double idy = g->start_y * g->delta_y + 0.5 * g->delta_y + y_in * g->delta_y;
+        double idx = g->start_x * g->delta_x + x_in * g->delta_x - 0.5 * g->delta_x;
+        double y_c = g->global_no_halo_dim_y * g->delta_y * 0.5;
+        if (idy - y_c < -g->length_y * 0.5) idy += g->length_y;
+        if (idy - y_c > g->length_y * 0.5) idy -= g->length_y;
+        *x_out = idx;
+        *y_out = idy - y_c;
+        return;
+    }
     double idy = g->start_y * g->delta_y + 0.5 * g->delta_y + y_in * g->delta_y;
     double idx = g->start_x * g->delta_x + 0.5 * g->delta_x + x_in * g->delta_x;
     double x_c = g->global_no_halo_dim_x * g->delta_x * 0.5;
@@ -542,6 +616,7 @@ void tso_energies(const tso_geometry *g, const double *re, const double *im, con
     const double cost_E = -1. / (2. * mass);
     const double c1 = -1. / 12., c2 = 4. / 3., c3 = -2.5;
     const double d1 = 1. / 6., d2 = -1., d3 = 0.5, d4 = 1. / 3.;
+    const int xlim = g->cylindrical ? 3 : 0; /* src/solver.cpp:301 */
     for (int i = g->iy0; i < g->iy1; ++i) {
         for (int j = g->ix0; j < g->ix1; ++j) {
             size_t k = (size_t)i * W + j;
@@ -554,7 +629,7 @@ void tso_energies(const tso_geometry *g, const double *re, const double *im, con
             s_intra += n2 * n2 * 0.5 * g_coupling;
             s_lhy += pow(n2, 2.5) * 0.4 * g_lhy;
             if (((i - g->iy0 >= (ihy == 0) * 2 && i < g->iy1 - (ehy == 0) * 2) || g->H == 1) &&
-                (j - g->ix0 >= (ihx == 0) * 2 && j < g->ix1 - (ehx == 0) * 2)) {
+                (j - g->ix0 >= (ihx == 0) * 2 + xlim && j < g->ix1 - (ehx == 0) * 2)) {
                 cplx r = cload(re, im, k + 1), l = cload(re, im, k - 1);
                 cplx rr = cload(re, im, k + 2), ll = cload(re, im, k - 2);
                 s_n2k += cmul(conjc(c), c).re;
@@ -589,7 +664,7 @@ void tso_energies(const tso_geometry *g, const double *re, const double *im, con
     out->intra = s_intra / s_n2;
     out->lhy = s_lhy / s_n2;
     out->total = out->kinetic + out->potential + out->intra + out->rotational + out->lhy;
-    out->norm2 = s_n2 * (dy * g->length_x / g->global_no_halo_dim_x);
+    out->norm2 = s_n2 * (dy * g->length_x / (g->global_no_halo_dim_x - (g->cylindrical ? 1 : 0)));
 }
 
 /* ---- expectation values (src/model.cpp:385-536, cartesian 2D) ------------- */

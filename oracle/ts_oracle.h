@@ -21,6 +21,9 @@ typedef struct {
     int rot_off_x, rot_off_y;       /* trunc(start - rot_coord) (src/cpukernel.cpp:417) */
     double delta_x, delta_y;
     double norm0;                   /* squared norm kept in imaginary time (src/solver.cpp:155) */
+    int cylindrical;                /* radial axis x (src/cpucylindrical.cpp) */
+    double kin_radial;              /* dt / (8 m dx^2) (src/cpukernel.cpp:200-210) */
+    int mirror_sign;                /* (-1)^l, column 0 = sign * column 1 (src/cpukernel.cpp:669-689) */
 } tso_params;
 
 typedef struct {
@@ -28,6 +31,7 @@ typedef struct {
     int start_x, start_y;
     int global_no_halo_dim_x, global_no_halo_dim_y;
     double delta_x, delta_y, length_x, length_y;
+    int cylindrical;
 } tso_geometry;
 
 typedef struct {

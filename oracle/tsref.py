@@ -37,6 +37,7 @@ class Config(C.Structure):
         ("seg_imag", C.c_int * 8),
         ("omp_threads", C.c_int),
         ("kernel_gpu", C.c_int),
+        ("cylindrical", C.c_int), ("angular_momentum", C.c_int),
     ]
 
 
@@ -106,7 +107,8 @@ def make_config(dim_x, length_x, dim_y=None, length_y=None, periodic_x=False, pe
                 lattice_angular_velocity=None, *, gaussian=None, exponential=None,
                 harmonic=None, mass=1.0, coupling=0.0, lhy_coupling=0.0, angular_velocity=0.0,
                 rot_coord=(0.0, 0.0), force_rotation_periodic=False, delta_t=1e-4,
-                segments=((1, False),), omp_threads=1, kernel_gpu=False):
+                segments=((1, False),), omp_threads=1, kernel_gpu=False, cylindrical=False,
+                angular_momentum=0):
     """Build a Config.  dim_y == 0 selects a 1D lattice.
 
     gaussian = (omega_x, omega_y, mean_x, mean_y, norm, phase) -> GaussianState;
@@ -153,6 +155,8 @@ def make_config(dim_x, length_x, dim_y=None, length_y=None, periodic_x=False, pe
         c.seg_imag[i] = int(bool(imag))
     c.omp_threads = omp_threads
     c.kernel_gpu = int(bool(kernel_gpu))
+    c.cylindrical = int(bool(cylindrical))
+    c.angular_momentum = int(angular_momentum)
     return c
 
 

@@ -9,7 +9,9 @@ own; these fixtures pin both the oracle restatement and the B200 kernel.
 
     python tests/golden/gen_golden.py        (needs oracle/_ref, i.e. the reference sources)
 
-Two-component cases (Hamiltonian2Component, the two-state Solver) go to two/.
+Two-component cases (Hamiltonian2Component, the two-state Solver) go to two/,
+cylindrical lattices (the radial kinetic term, the azimuthal potential, the
+mirrored axis column) to cyl/.
 """
 import json
 import os
@@ -111,6 +113,45 @@ def main2():
         print(f"{name}: tile {pa.shape}, E = {res.total_energy:.15g}")
 
 
+# Cylindrical lattices (files under cyl/): the radial axis is x; tiles at most
+# 128 columns wide (one cache block of the reference).  lattice (N, L, Ny, Ly,
+# periodic_y), angular momentum l, g, evolve segments.
+CASES_CYL = {
+    "cyl_real_l0": dict(lat=(60, 10.0, 48, 8.0, False), l=0, g=2.0, dt=1e-3,
+                        segments=[(25, False)]),
+    "cyl_imag_l1": dict(lat=(60, 10.0, 48, 8.0, False), l=1, g=1.0, dt=1e-3,
+                        segments=[(30, True)]),
+    "cyl_real_l2_two_calls": dict(lat=(50, 8.0, 40, 6.0, False), l=2, g=0.0, dt=1e-3,
+                                  segments=[(10, False), (7, False)]),
+    "cyl_periodic_y_imag": dict(lat=(40, 8.0, 36, 6.0, True), l=0, g=3.0, dt=1e-3,
+                                segments=[(20, True)]),
+}
+
+
+def main_cyl():
+    os.makedirs(os.path.join(HERE, "cyl"), exist_ok=True)
+    for i, (name, case) in enumerate(sorted(CASES_CYL.items())):
+        N, L, Ny, Ly, py = case["lat"]
+        lat = O.Lattice(N, L, Ny, Ly, False, py, cylindrical=True)
+        rng = np.random.default_rng(3000 + i)
+        X, Y = lat.coordinates()
+        psi0 = (X ** case["l"]) * np.exp(-(X ** 2 + (Y - 0.3) ** 2) / 2.0) * np.exp(0.2j * Y)
+        psi0 = psi0 * (1 + 0.02 * rng.uniform(-1, 1, lat.shape))
+        V = 0.5 * (X ** 2 + 1.3 * Y ** 2) + 0.1 * rng.uniform(-1, 1, lat.shape)
+        cfg = tsref.make_config(N, L, Ny, Ly, False, py, 0.0, harmonic=None, coupling=case["g"],
+                                delta_t=case["dt"], segments=case["segments"], omp_threads=1,
+                                cylindrical=True, angular_momentum=case["l"])
+        psi, res = tsref.run(cfg, psi0, V)
+        meta = dict(case, name=name)
+        np.savez_compressed(
+            os.path.join(HERE, "cyl", name + ".npz"), psi0=psi0, V=V, psi=psi,
+            energies=np.array([res.total_energy, res.kinetic_energy, res.potential_energy,
+                               res.rotational_energy, res.intra_energy, res.lhy_energy,
+                               res.squared_norm]),
+            meta=json.dumps(meta))
+        print(f"{name}: tile {psi.shape}, E = {res.total_energy:.15g}")
+
+
 def main():
     if not tsref.available():
         raise SystemExit("oracle/_ref/libtsref.so is missing: run oracle/build_ref.sh first")
@@ -134,6 +175,7 @@ def main():
             meta=json.dumps(meta))
         print(f"{name}: tile {psi.shape}, E = {res.total_energy:.15g}")
     main2()
+    main_cyl()
 
 
 if __name__ == "__main__":
