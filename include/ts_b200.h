@@ -70,6 +70,11 @@ typedef struct {
     double delta_x, delta_y;
     double norm0;                    /* imaginary time: squared norm kept after each step;
                                         0 disables the renormalisation (as the reference) */
+    int32_t cylindrical;             /* radial axis x (Lattice::coordinate_system
+                                        "cylindrical"): the radial kinetic term and, in
+                                        imaginary time, column 0 mirroring column 1 */
+    int32_t angular_momentum;        /* State::angular_momentum: parity of that mirror */
+    double kin_radial;               /* dt / (8 m dx^2) (kin_radial[0]) */
 } ts_b200_desc;
 
 typedef struct ts_b200_kernel ts_b200_kernel;

@@ -20,6 +20,9 @@ def desc_from_params(p, precision=_capi.FP64):
     d.rot_offset_x, d.rot_offset_y = float(p.rot_off_x), float(p.rot_off_y)
     d.delta_x, d.delta_y = p.delta_x, p.delta_y
     d.norm0 = p.norm0
+    d.cylindrical = p.cylindrical
+    d.kin_radial = p.kin_radial
+    d.angular_momentum = 0 if p.mirror_sign >= 0 else 1  # only its parity enters
     return d
 
 

@@ -217,8 +217,8 @@ int ts_b200_adjoint_create(const ts_b200_desc *d, double delta_t, int steps, int
     *out = nullptr;
     if (!d || steps < 1 || checkpoint_every < 0 || !(delta_t > 0.0)) return TS_B200_INVALID_ARGUMENT;
     if (d->imag_time || d->precision != TS_B200_FP64 || d->periodic_x || d->periodic_y ||
-        (d->alpha_x != 0.0 && d->alpha_y != 0.0))
-        return TS_B200_UNSUPPORTED;  // real time, FP64, closed boundaries, no rotating frame
+        (d->alpha_x != 0.0 && d->alpha_y != 0.0) || d->cylindrical)
+        return TS_B200_UNSUPPORTED;  // real time, FP64, closed cartesian tile, no rotating frame
     if (checkpoint_every == 0 && (d->coupling != 0.0 || d->lhy_coupling != 0.0))
         return TS_B200_INVALID_ARGUMENT;  // inverse steps need the linear step
     ts_b200_adjoint *a = new (std::nothrow) ts_b200_adjoint();

@@ -483,8 +483,8 @@ int ts_b200_batch_create(ts_b200_kernel *const *kernels, int n, ts_b200_batch **
             if (kernels[j] == t) return TS_B200_INVALID_ARGUMENT;  // a tile appears once
         if (t->fp32 != k0->fp32 || t->imag != k0->imag || t->device != k0->device)
             return TS_B200_INVALID_ARGUMENT;
-        // batched strips carry no rotating frame and no second species
-        if (t->rot || t->pair_mode) return TS_B200_UNSUPPORTED;
+        // batched strips carry no rotating frame, second species or radial term
+        if (t->rot || t->pair_mode || t->cyl) return TS_B200_UNSUPPORTED;
         phase = std::max(phase, t->phase);
     }
     ts_b200_batch *b = new (std::nothrow) ts_b200_batch();

@@ -41,6 +41,8 @@ struct ts_b200_kernel {
     int device = 0;
     // two components (pair.cu): the tile is one species of a ts_b200_pair;
     // pb / pb_scale / cab are the other species' tile for the next step
+    bool cyl = false;        // cylindrical lattice (radial axis x)
+    void *rad = nullptr;     // per column: radial pair (a, b), (c, 0) in the tile's precision
     bool pair_mode = false;
     int phase_alone = 0;  // phase outside the pair
     const void *pb = nullptr;

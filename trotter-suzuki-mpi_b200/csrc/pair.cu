@@ -329,7 +329,8 @@ int ts_b200_pair_create(ts_b200_kernel *a, ts_b200_kernel *b, double coupling_ab
     // no rotating frame (the reference's Hamiltonian2Component leaves the
     // rotation centre unset) and no Lee-Huang-Yang term (absent from the
     // reference's two-component phase)
-    if (a->rot || b->rot || a->d.lhy_coupling != 0.0 || b->d.lhy_coupling != 0.0)
+    if (a->rot || b->rot || a->d.lhy_coupling != 0.0 || b->d.lhy_coupling != 0.0 || a->cyl ||
+        b->cyl)
         return TS_B200_UNSUPPORTED;
     ts_b200_pair *p = new (std::nothrow) ts_b200_pair;
     if (!p) return TS_B200_OUT_OF_MEMORY;

@@ -86,6 +86,10 @@ struct StepArgs {
     const void *pb;
     const double *pb_scale;
     T cab;
+    // cylindrical: per tile column x, the radial pair (x, x+1) as (a, b, c, 0)
+    // (a - 1 in delta form); the sign of the mirrored axis column
+    const void *rad;
+    T mirror_sign;
 };
 
 // ---------------------------------------------------------------- PTX helpers
@@ -307,6 +311,24 @@ __device__ __forceinline__ void hsweep_lane(Cx<T> (&w)[2], T ai, T bi, T al, T b
     }
 }
 
+// Radial kinetic sweep (src/cpucylindrical.cpp:4-81) on one row, 2 cells per
+// lane: the pair (x, x+1) with x = PAR (mod 2) updates its first cell with
+// (a, b) and its second with (a, c); (a0, b0) and (a1, b1) are the
+// coefficients of this lane's cells 0 and 1 for the sweep's parity.
+template <bool IMAG, int PAR, typename T>
+__device__ __forceinline__ void rsweep_lane(Cx<T> (&w)[2], T a0, T b0, T a1, T b1) {
+    if (PAR == 0) {
+        const Cx<T> p = w[0], q = w[1];
+        w[0] = kin<IMAG>(p, q, a0, b0);
+        w[1] = kin<IMAG>(q, p, a1, b1);
+    } else {
+        const Cx<T> right = shfl_down1(w[0]);
+        const Cx<T> left = shfl_up1(w[1]);
+        w[0] = kin<IMAG>(w[0], left, a0, b0);
+        w[1] = kin<IMAG>(w[1], right, a1, b1);
+    }
+}
+
 // The same for C cells per lane: (pa[i], pb[i]) for the pair (i, i+1) inside
 // the lane, (al, bl) / (ar, br) for the pairs with the neighbour lanes.
 template <bool IMAG, int PAR, int C, typename T>
@@ -520,18 +542,22 @@ __device__ __forceinline__ void potential_row(Cx<T> (&w)[C], const TabT *tab, T 
 
 
 // Compile-time description of a kernel variant.
-// PHASE: 0 no nonlinear phase, 1 g|psi|^2 only, 2 with the Lee-Huang-Yang term,
-// 3 g|psi|^2 + g_ab|psi_b|^2 (one component of a two-component system).
+// PHASE & 3: 0 no nonlinear phase, 1 g|psi|^2 only, 2 with the Lee-Huang-Yang
+// term, 3 g|psi|^2 + g_ab|psi_b|^2 (one component of a two-component system);
+// PHASE & 4: cylindrical lattice (radial kinetic sweeps, mirrored axis column).
 template <typename T_, int C_, bool IMAG_, bool ROT_, int PHASE_>
 struct Variant {
     using T = T_;
     static constexpr int C = C_;
     static constexpr bool IMAG = IMAG_;
     static constexpr bool ROT = ROT_;
-    static constexpr bool PHASE = PHASE_ != 0;
-    static constexpr bool LHY = PHASE_ == 2;
-    static constexpr bool PB = PHASE_ == 3;
-    static constexpr int HX = ROT_ ? 8 : 4;
+    static constexpr bool PHASE = (PHASE_ & 3) != 0;
+    static constexpr bool LHY = (PHASE_ & 3) == 2;
+    static constexpr bool PB = (PHASE_ & 3) == 3;
+    static constexpr bool CYL = (PHASE_ & 4) != 0;
+    // recomputed halo columns: one per horizontal pair sweep of the step
+    // (4 kinetic; 4 more rotation row sweeps or radial sweeps)
+    static constexpr int HX = (ROT_ || (PHASE_ & 4)) ? 8 : 4;
     static constexpr int HY = ROT_ ? 6 : 4;
     // Register window (rows); the body is unrolled over two windows so that
     // the parity of every row index is a compile-time constant.
@@ -594,6 +620,8 @@ struct Walk {
     T inv;
     T aH, bH, aV, bV, ca, caa;  // step constants, read from the parameters once
     T pbs, cab;                 // PB: factor of the other species' tile, g_ab * dt
+    T rca[2][2], rcb[2][2];     // CYL: radial (a, b_self) of cell [i] for parity [p]
+    T msign;                    // CYL, imaginary time: mirror sign on the lane of column 0
     T hpa[C - 1], hpb[C - 1];        // LANE_COEF: this lane's pairs (i, i+1)
     T hal, hbl, har, hbr;            //   and its pairs with the neighbour lanes
 
@@ -690,6 +718,10 @@ __device__ __forceinline__ void walk_row(Walk<V> &w, const StepArgs<typename V::
     if (!GUARD || (r - 2 >= ra && r - 2 < rb)) {
         const int u = r - 2;
         hsw<V, ((K + 1) & 1), EDGE>(w, WS(2));
+        if constexpr (V::CYL) {
+            rsweep_lane<IMAG, 0>(WS(2), w.rca[0][0], w.rcb[0][0], w.rca[0][1], w.rcb[0][1]);
+            rsweep_lane<IMAG, 1>(WS(2), w.rca[1][0], w.rcb[1][0], w.rca[1][1], w.rcb[1][1]);
+        }
         const int q = w.tslot;
         const TabT *tp =
             reinterpret_cast<const TabT *>(w.ring + q * V::SLOT + V::PSI_BYTES) + C * w.lane;
@@ -706,6 +738,10 @@ __device__ __forceinline__ void walk_row(Walk<V> &w, const StepArgs<typename V::
             rrow<IMAG, C, 0, EDGE>(WS(2), ab.re, ab.im, w.m);
             rrow<IMAG, C, 1, EDGE>(WS(2), ab.re, ab.im, w.m);
         } else {
+            if constexpr (V::CYL) {
+                rsweep_lane<IMAG, 1>(WS(2), w.rca[1][0], w.rcb[1][0], w.rca[1][1], w.rcb[1][1]);
+                rsweep_lane<IMAG, 0>(WS(2), w.rca[0][0], w.rcb[0][0], w.rca[0][1], w.rcb[0][1]);
+            }
             hsw<V, ((K + 1) & 1), EDGE>(w, WS(2));
         }
         __syncwarp();
@@ -751,6 +787,14 @@ __device__ __forceinline__ void walk_row(Walk<V> &w, const StepArgs<typename V::
         if (u >= w.oy0 && u < w.oy1) {
             Cx<T> *orow = reinterpret_cast<Cx<T> *>(a.psi_out) + (size_t)u * a.P + w.xl;
             const bool norm_row = IMAG && u >= a.iy0 && u < a.iy1;
+            if constexpr (V::CYL && IMAG) {
+                // column 0 mirrors column 1 (src/cpukernel.cpp:669-689); msign is
+                // 0 on every other lane
+                if (w.msign != T(0)) {
+                    WS(NWIN - 1)[0].re = w.msign * WS(NWIN - 1)[1].re;
+                    WS(NWIN - 1)[0].im = w.msign * WS(NWIN - 1)[1].im;
+                }
+            }
 #pragma unroll
             for (int i = 0; i < C; ++i) {
                 const Cx<T> v = WS(NWIN - 1)[i];
@@ -928,6 +972,27 @@ __device__ __forceinline__ void run_task(Walk<V> &w, const StepArgs<typename V::
 #pragma unroll
         for (int i = 0; i < C; ++i)
             w.colab[i] = reinterpret_cast<const Cx<T> *>(a.col_ab)[w.present[i] ? w.xl + i : 0];
+    }
+    if constexpr (V::CYL) {
+        // pair starting at column x: valid when x >= 0 and x + 1 < W
+        const T one = DeltaForm<T>::value ? T(0) : T(1);
+        const Cx<T> *rad = reinterpret_cast<const Cx<T> *>(a.rad);  // (a, b), (c, 0) per column
+        auto pair_ok = [&](int x) { return x >= 0 && x + 1 < a.W; };
+        const int x0 = w.xl;
+        // parity 0: cells 0, 1 pair with each other (pair at x0)
+        const bool p0 = pair_ok(x0);
+        w.rca[0][0] = p0 ? rad[2 * x0].re : one;
+        w.rcb[0][0] = p0 ? rad[2 * x0].im : T(0);
+        w.rca[0][1] = w.rca[0][0];
+        w.rcb[0][1] = p0 ? rad[2 * x0 + 1].re : T(0);
+        // parity 1: cell 0 is the second cell of the pair at x0 - 1, cell 1 the
+        // first of the pair at x0 + 1
+        const bool pl = pair_ok(x0 - 1), pr = pair_ok(x0 + 1);
+        w.rca[1][0] = pl ? rad[2 * (x0 - 1)].re : one;
+        w.rcb[1][0] = pl ? rad[2 * (x0 - 1) + 1].re : T(0);
+        w.rca[1][1] = pr ? rad[2 * (x0 + 1)].re : one;
+        w.rcb[1][1] = pr ? rad[2 * (x0 + 1)].im : T(0);
+        w.msign = (V::IMAG && x0 == 0) ? a.mirror_sign : T(0);
     }
 #pragma unroll
     for (int j = 0; j < NWIN; ++j)

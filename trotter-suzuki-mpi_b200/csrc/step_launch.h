@@ -45,14 +45,22 @@ cudaError_t launch_phase(int phase, const StepArgs<T> &a, int warps, size_t smem
     if constexpr (C == 2 && !ROT) {
         if (phase == 3)
             return launch_step_variant<Variant<T, C, IMAG, ROT, 3>>(a, warps, smem, blocks, st, bps);
+        if (phase == 4)
+            return launch_step_variant<Variant<T, C, IMAG, ROT, 4>>(a, warps, smem, blocks, st, bps);
+        if (phase == 5)
+            return launch_step_variant<Variant<T, C, IMAG, ROT, 5>>(a, warps, smem, blocks, st, bps);
+        if (phase == 6)
+            return launch_step_variant<Variant<T, C, IMAG, ROT, 6>>(a, warps, smem, blocks, st, bps);
     }
+    if (phase > 3) return cudaErrorInvalidValue;
     if (phase == 2) return launch_step_variant<Variant<T, C, IMAG, ROT, 2>>(a, warps, smem, blocks, st, bps);
     if (phase == 1) return launch_step_variant<Variant<T, C, IMAG, ROT, 1>>(a, warps, smem, blocks, st, bps);
     return launch_step_variant<Variant<T, C, IMAG, ROT, 0>>(a, warps, smem, blocks, st, bps);
 }
 
 // phase: 0 none, 1 g|psi|^2, 2 g|psi|^2 + Lee-Huang-Yang, 3 two components
-// (g|psi|^2 + g_ab|psi_b|^2; 2 cells per lane, no rotating frame).
+// (g|psi|^2 + g_ab|psi_b|^2; 2 cells per lane, no rotating frame); 4-6: 0-2 on
+// a cylindrical lattice (2 cells per lane, no rotating frame).
 template <typename T, bool IMAG>
 cudaError_t launch_step_imag_t(int C, bool rot, int phase, const StepArgs<T> &a, int warps,
                                size_t smem, int blocks, cudaStream_t st, int *bps) {

@@ -312,14 +312,28 @@ struct RedArgs {
     int start_x, start_y, gnx, gny;
     double Lx, Ly;
     double mass, g, glhy, omega;
+    int cyl;           // cylindrical lattice: radial coordinates, energy region from column 3
     double *partials;  // gridDim.x * RED_MAX_TERMS
     double *out;       // RED_MAX_TERMS
     unsigned int *ticket;
 };
 
-// Cartesian cell-centre coordinates (src/common.cpp:45-65).
+// Cell-centre coordinates (src/common.cpp:45-81): cartesian, or on a
+// cylindrical lattice the radial x from the tile's edge, r = -dx/2 at column 0.
 __device__ __forceinline__ void cell_coords(const RedArgs &a, int xi, int yi, double *xo,
                                             double *yo) {
+    if (a.cyl) {
+        double idy = __dadd_rn(__dadd_rn(__dmul_rn(a.start_y, a.dy), __dmul_rn(0.5, a.dy)),
+                               __dmul_rn(yi, a.dy));
+        const double idx = __dsub_rn(__dadd_rn(__dmul_rn(a.start_x, a.dx), __dmul_rn(xi, a.dx)),
+                                     __dmul_rn(0.5, a.dx));
+        const double y_c = __dmul_rn(__dmul_rn(a.gny, a.dy), 0.5);
+        if (idy - y_c < -a.Ly * 0.5) idy = __dadd_rn(idy, a.Ly);
+        if (idy - y_c > a.Ly * 0.5) idy = __dsub_rn(idy, a.Ly);
+        *xo = idx;
+        *yo = __dsub_rn(idy, y_c);
+        return;
+    }
     double idy = __dadd_rn(__dadd_rn(__dmul_rn(a.start_y, a.dy), __dmul_rn(0.5, a.dy)),
                            __dmul_rn(yi, a.dy));
     double idx = __dadd_rn(__dadd_rn(__dmul_rn(a.start_x, a.dx), __dmul_rn(0.5, a.dx)),
@@ -409,8 +423,10 @@ __global__ void __launch_bounds__(RED_THREADS) energy_kernel(RedArgs a) {
         acc[3] += n2 * a.V[(size_t)i * a.W + j];
         acc[5] += n2 * n2 * 0.5 * a.g;
         if (a.glhy != 0.0) acc[6] += pow(n2, 2.5) * 0.4 * a.glhy;
+        // src/solver.cpp:301,358-361: on a cylindrical lattice the kinetic
+        // region starts 3 columns further from the axis
         if (((i - a.iy0 >= (ihy == 0) * 2 && i < a.iy1 - (ehy == 0) * 2) || a.H == 1) &&
-            (j - a.ix0 >= (ihx == 0) * 2 && j < a.ix1 - (ehx == 0) * 2)) {
+            (j - a.ix0 >= (ihx == 0) * 2 + (a.cyl ? 3 : 0) && j < a.ix1 - (ehx == 0) * 2)) {
             const Cx<double> r = ldc<T>(a, s, j + 1, i), l = ldc<T>(a, s, j - 1, i);
             const Cx<double> rr = ldc<T>(a, s, j + 2, i), ll = ldc<T>(a, s, j - 2, i);
             acc[1] += n2;
@@ -571,7 +587,7 @@ int min_ring(const ts_b200_kernel *) { return 4; }
 // task per warp: every SM then holds the same number of tasks (the launch
 // time is that of the most loaded SM).
 int balanced_segments(const ts_b200_kernel *k, int blocks_per_sm, int warps) {
-    const int hx = k->rot ? 8 : 4;
+    const int hx = (k->rot || k->cyl) ? 8 : 4;  // Variant::HX
     const int wo = 32 * k->C - 2 * hx;
     const int strips = div_up(k->W, wo);
     const long rw = (long)blocks_per_sm * k->num_sms * warps;
@@ -592,7 +608,7 @@ void auto_segments(ts_b200_kernel *k) {
 }
 
 void geometry(const ts_b200_kernel *k, int *strips, int *segs, int *blocks, size_t *smem) {
-    const int hx = k->rot ? 8 : 4;
+    const int hx = (k->rot || k->cyl) ? 8 : 4;  // Variant::HX
     const int wo = 32 * k->C - 2 * hx;
     *strips = div_up(k->W, wo);
     *segs = div_up(k->H, k->seg_h);
@@ -670,6 +686,8 @@ void tsbh::fill_step_constants(const ts_b200_kernel *k, StepArgs<T> &a) {
     a.pb = k->pb;
     a.pb_scale = k->pb_scale;
     a.cab = (T)k->cab;
+    a.rad = k->rad;
+    a.mirror_sign = (T)(k->d.angular_momentum % 2 == 0 ? 1 : -1);
 }
 template void tsbh::fill_step_constants<double>(const ts_b200_kernel *, StepArgs<double> &);
 template void tsbh::fill_step_constants<float>(const ts_b200_kernel *, StepArgs<float> &);
@@ -781,6 +799,7 @@ void fill_red_args(ts_b200_kernel *k, RedArgs &a) {
     a.partials = k->red_partials;
     a.out = k->red_out;
     a.ticket = k->red_ticket;
+    a.cyl = k->cyl ? 1 : 0;
 }
 
 int red_blocks(const ts_b200_kernel *k) {
@@ -792,6 +811,44 @@ int read_red(ts_b200_kernel *k, double *host, int nterms) {
     TSB_CHECK(k, cudaMemcpyAsync(host, k->red_out, nterms * sizeof(double), cudaMemcpyDeviceToHost,
                                  k->stream));
     TSB_CHECK(k, cudaStreamSynchronize(k->stream));
+    return TS_B200_OK;
+}
+
+// Radial pair coefficients per tile column x (the pair (x, x+1); the tile
+// starts at the axis), computed on the host with the C library as
+// src/cpucylindrical.cpp:11-35 (real time) and :50-74 (imaginary time) do,
+// including their choice of circular functions for the first pair in real time
+// and hyperbolic ones past it (and the other way round in imaginary time).
+// Stored as (a, b), (c, 0); a - 1 in float (delta form).
+template <typename T>
+int upload_radial(ts_b200_kernel *k) {
+    const int W = k->W;
+    Cx<T> *tab = new (std::nothrow) Cx<T>[2 * (size_t)W];
+    if (!tab) return fail(k, TS_B200_OUT_OF_MEMORY, "host allocation for the radial table");
+    const double kin = k->d.kin_radial;
+    for (int x = 0; x < W; ++x) {
+        double a, am1, b, c;
+        if (x == 0) {
+            const double kr = 2 * kin;
+            a = k->imag ? std::cosh(kr) : std::cos(kr);
+            am1 = k->imag ? cosh_m1(kr) : cos_m1(kr);
+            b = c = k->imag ? -std::sinh(kr) : -std::sin(kr);
+        } else {
+            const double xd = (double)x;
+            const double kr = kin / std::sqrt(xd * xd - 0.25);
+            const double ratio = std::sqrt((2 * xd + 1) / (2 * xd - 1));
+            const double sk = k->imag ? std::sin(kr) : std::sinh(kr);
+            a = k->imag ? std::cos(kr) : std::cosh(kr);
+            am1 = k->imag ? cos_m1(kr) : cosh_m1(kr);
+            b = sk * ratio;
+            c = -sk / ratio;
+        }
+        tab[2 * x] = Cx<T>{(T)(sizeof(T) == 4 ? am1 : a), (T)b};
+        tab[2 * x + 1] = Cx<T>{(T)c, T(0)};
+    }
+    cudaError_t e = cudaMemcpy(k->rad, tab, sizeof(Cx<T>) * 2 * (size_t)W, cudaMemcpyHostToDevice);
+    delete[] tab;
+    if (e != cudaSuccess) return cuda_fail(k, e, "radial table upload");
     return TS_B200_OK;
 }
 
@@ -909,6 +966,10 @@ int ts_b200_create(const ts_b200_desc *d, ts_b200_kernel **out) {
     if ((long)d->dim_x * d->dim_y > (1L << 31) - 1) return TS_B200_UNSUPPORTED;
     if (d->periodic_x && d->dim_x < 2 * d->halo_x) return TS_B200_INVALID_ARGUMENT;
     if (d->periodic_y && d->dim_y < 2 * d->halo_y) return TS_B200_INVALID_ARGUMENT;
+    // cylindrical: the radial axis is not periodic, and the rotating frame is
+    // not combined with it here
+    if (d->cylindrical && (d->periodic_x || (d->alpha_x != 0.0 && d->alpha_y != 0.0)))
+        return TS_B200_UNSUPPORTED;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return TS_B200_NO_DEVICE;
     ts_b200_kernel *k = new (std::nothrow) ts_b200_kernel();
@@ -921,6 +982,8 @@ int ts_b200_create(const ts_b200_desc *d, ts_b200_kernel **out) {
     k->imag = d->imag_time != 0;
     k->rot = d->alpha_x != 0.0 && d->alpha_y != 0.0;
     k->phase = d->lhy_coupling != 0.0 ? 2 : (d->coupling != 0.0 ? 1 : 0);
+    k->cyl = d->cylindrical != 0;
+    if (k->cyl) k->phase |= 4;
     k->cell = k->fp32 ? 8 : 16;
     k->tab_cell = k->imag ? k->cell / 2 : k->cell;
     int dev = 0;
@@ -947,6 +1010,7 @@ int ts_b200_create(const ts_b200_desc *d, ts_b200_kernel **out) {
         alloc(&k->col_ab, (size_t)k->W * (k->fp32 ? 8 : 16));
     }
     if (k->fp32 && !k->imag) alloc((void **)&k->kin_sched, (size_t)kSchedLen * sizeof(float4));
+    if (k->cyl) alloc(&k->rad, (size_t)k->W * 2 * k->cell);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&k->own_stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
         int s = cuda_fail(nullptr, e, "allocation");
@@ -972,6 +1036,13 @@ int ts_b200_create(const ts_b200_desc *d, ts_b200_kernel **out) {
             return s;
         }
     }
+    if (k->cyl) {
+        int s = k->fp32 ? upload_radial<float>(k) : upload_radial<double>(k);
+        if (s != TS_B200_OK) {
+            ts_b200_destroy(k);
+            return s;
+        }
+    }
     if (k->kin_sched) {
         int s = upload_kinetic_schedule(k);
         if (s != TS_B200_OK) {
@@ -990,7 +1061,7 @@ int ts_b200_destroy(ts_b200_kernel *k) {
     if (k->stream && k->stream != k->own_stream) cudaStreamSynchronize(k->stream);
     void *bufs[] = {k->psi[0], k->psi[1], k->tab, k->row_ab, k->col_ab, k->partials, k->scal,
                     k->staging, k->vtab, k->red_partials, k->red_out, k->red_ticket,
-                    k->kin_sched};
+                    k->kin_sched, k->rad};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (k->own_stream) cudaStreamDestroy(k->own_stream);
@@ -1266,7 +1337,8 @@ int ts_b200_energies(ts_b200_kernel *k, const double *potential, const ts_b200_e
     out->intra = s[5] / s[0];
     out->lhy = s[6] / s[0];
     out->total = out->kinetic + out->potential + out->intra + out->rotational + out->lhy;
-    out->norm2 = s[0] * (k->d.delta_y * p->length_x / p->global_no_halo_dim_x);
+    out->norm2 = s[0] * (k->d.delta_y * p->length_x /
+                         (p->global_no_halo_dim_x - (k->cyl ? 1 : 0)));
     return TS_B200_OK;
 }
 
@@ -1326,6 +1398,7 @@ int ts_b200_set_launch(ts_b200_kernel *k, int C, int seg_h, int warps, int ring)
     if (C != 0 && C != 2 && C != 4) return TS_B200_INVALID_ARGUMENT;
     if (C == 4 && k->rot) return fail(k, TS_B200_UNSUPPORTED, "rotation kernels use 2 cells per lane");
     if (C == 4 && k->pair_mode) return fail(k, TS_B200_UNSUPPORTED, "pair kernels use 2 cells per lane");
+    if (C == 4 && k->cyl) return fail(k, TS_B200_UNSUPPORTED, "cylindrical kernels use 2 cells per lane");
     if (warps != 0 && warps != 1 && warps != 2 && warps != 4) return TS_B200_INVALID_ARGUMENT;
     if (ring != 0 && (ring < min_ring(k) || ring > 16))
         return fail(k, TS_B200_INVALID_ARGUMENT, "ring depth out of range for this variant");

@@ -34,6 +34,8 @@ class Desc(C.Structure):
         ("rot_offset_x", C.c_double), ("rot_offset_y", C.c_double),
         ("delta_x", C.c_double), ("delta_y", C.c_double),
         ("norm0", C.c_double),
+        ("cylindrical", C.c_int32), ("angular_momentum", C.c_int32),
+        ("kin_radial", C.c_double),
     ]
 
 
