@@ -38,12 +38,21 @@ int tsh_lattice2d_new(int dim_x, double length_x, int dim_y, double length_y, in
                       int periodic_y, double angular_velocity, void **out);
 /* Lattice1D(dim, length, periodic_x, "cartesian") -- src/trottersuzuki.h:74 */
 int tsh_lattice1d_new(int dim, double length, int periodic_x, void **out);
+/* The same with Lattice::coordinate_system ("cartesian" or "cylindrical",
+ * src/model.cpp:32-158). */
+int tsh_lattice2d_new_cs(int dim_x, double length_x, int dim_y, double length_y, int periodic_x,
+                         int periodic_y, double angular_velocity, const char *coordinate_system,
+                         void **out);
+int tsh_lattice1d_new_cs(int dim_x, double length_x, int periodic_x,
+                         const char *coordinate_system, void **out);
 int tsh_lattice_info_get(void *lattice, tsh_lattice_info *out);
 int tsh_lattice_free(void *lattice);
 
 /* State(grid) (zero), GaussianState, ExponentialState, SinusoidState
  * -- src/trottersuzuki.h:138,209-336 */
 int tsh_state_new(void *lattice, void **out);
+/* State(grid, angular_momentum) (src/trottersuzuki.h:138) */
+int tsh_state_new_l(void *lattice, int angular_momentum, void **out);
 int tsh_gaussian_state_new(void *lattice, double omega_x, double omega_y, double mean_x,
                            double mean_y, double norm, double phase, void **out);
 int tsh_exponential_state_new(void *lattice, int n_x, int n_y, double norm, double phase,

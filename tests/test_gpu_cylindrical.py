@@ -91,3 +91,23 @@ def test_cylindrical_rejects_rotation_and_radial_periodicity():
     d.alpha_x = d.alpha_y = 0.1
     with pytest.raises(B200Error):
         Kernel(d)
+
+
+@pytest.mark.parametrize("name", cyl_names())
+def test_drop_in_cylindrical_solver(name):
+    """Lattice2D(..., coordinate_system="cylindrical"), State(grid, l) and the
+    Solver: the azimuthal term enters the table and the energies."""
+    import trottersuzuki_b200 as ts
+    lat, meta, z = load_cyl(name)
+    N, L, Ny, Ly, py = meta["lat"]
+    grid = ts.Lattice2D(N, L, Ny, Ly, periodic_y_axis=py, coordinate_system="cylindrical")
+    state = ts.State(grid, meta["l"])
+    state.init_state_matrix(z["psi0"].real, z["psi0"].imag)
+    pot = ts.Potential(grid, z["V"])
+    ham = ts.Hamiltonian(grid, pot, 1.0, meta["g"])
+    solver = ts.Solver(grid, state, ham, meta["dt"])
+    for it, imag in meta["segments"]:
+        solver.evolve(it, imag)
+    assert np.abs(state.get_state() - z["psi"]).max() <= 1e-10
+    got = solver._energies()
+    assert np.allclose(got, z["energies"], rtol=1e-10, atol=1e-12), (got, z["energies"])

@@ -65,3 +65,20 @@ def test_cylindrical_geometry():
     assert lat.inner()[0] == 1
     X, _ = lat.coordinates()
     assert X[0, 0] == -0.5 * lat.delta_x and X[0, 1] == 0.5 * lat.delta_x
+
+
+def test_host_cylindrical_lattice_matches_oracle_geometry():
+    """The drop-in Lattice2D / Lattice1D with coordinate_system="cylindrical"
+    (no GPU needed) against the oracle's restatement of src/model.cpp:32-158."""
+    import trottersuzuki_b200 as ts
+    for args in ((60, 10.0, 48, 8.0, False), (40, 8.0, 36, 6.0, True)):
+        N, L, Ny, Ly, py = args
+        g = ts.Lattice2D(N, L, Ny, Ly, periodic_y_axis=py, coordinate_system="cylindrical")
+        lat = O.Lattice(N, L, Ny, Ly, False, py, cylindrical=True)
+        assert (g.dim_y, g.dim_x) == lat.shape
+        assert g.delta_x == lat.delta_x and g.delta_y == lat.delta_y
+        assert g.inner_start_x - g.start_x == lat.inner()[0]
+        X, Y = lat.coordinates()
+        assert ts.map_lattice_to_coordinate_space(g, 0, 3) == (X[3, 0], Y[3, 0])
+    g1 = ts.Lattice1D(50, 6.0, coordinate_system="cylindrical")
+    assert g1.dim_x == 51 and g1.delta_x == 6.0 / 50.5

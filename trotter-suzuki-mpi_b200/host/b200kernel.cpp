@@ -8,15 +8,14 @@
 namespace b200 {
 
 ts_b200_desc make_desc(Lattice *g, Hamiltonian *ham, double dt, double norm, bool imag,
-                       int precision) {
+                       int precision, int angular_momentum) {
     return make_species_desc(g, ham, dt, norm, imag, precision, ham->mass, ham->coupling_a,
-                             ham->LeeHuangYang_coupling_a);
+                             ham->LeeHuangYang_coupling_a, angular_momentum);
 }
 
 ts_b200_desc make_species_desc(Lattice *g, Hamiltonian *ham, double dt, double norm, bool imag,
-                               int precision, double mass, double coupling, double lhy) {
-    if (g->coordinate_system != "cartesian")
-        my_abort("The B200 kernel supports cartesian coordinates only.");
+                               int precision, double mass, double coupling, double lhy,
+                               int angular_momentum) {
     ts_b200_desc d = {};
     d.dim_x = g->dim_x;
     d.dim_y = g->dim_y;
@@ -54,6 +53,12 @@ ts_b200_desc make_species_desc(Lattice *g, Hamiltonian *ham, double dt, double n
     d.delta_x = g->delta_x;
     d.delta_y = g->delta_y;
     d.norm0 = imag ? norm : 0.0;
+    if (g->coordinate_system == "cylindrical") {
+        // src/cpukernel.cpp:200-210 (kin_radial) and :669-689 (the mirror's parity)
+        d.cylindrical = 1;
+        d.kin_radial = dt / (8. * mass * g->delta_x * g->delta_x);
+        d.angular_momentum = angular_momentum;
+    }
     return d;
 }
 
@@ -85,6 +90,8 @@ struct ScratchTile {
         d.a_h = d.a_v = 1.0;
         d.delta_x = g->delta_x;
         d.delta_y = g->delta_y;
+        // the reductions' coordinates, energy region and norm follow the lattice
+        d.cylindrical = g->coordinate_system == "cylindrical" ? 1 : 0;
         int s = ts_b200_create(&d, &h);
         if (s) fail(s, nullptr, "creating a device tile");
         s = ts_b200_set_state(h, re, im, g->dim_x);
@@ -150,7 +157,8 @@ void reduce_cross_energies(Lattice *g, const double *a_re, const double *a_im, c
 B200Kernel::B200Kernel(Lattice *grid, State *state, Hamiltonian *ham, double *pot_re,
                        double *pot_im, double dt, double norm, bool imag, int precision)
     : h_(nullptr), dim_x_(grid->dim_x), dim_y_(grid->dim_y), imag_time_(imag) {
-    ts_b200_desc d = b200::make_desc(grid, ham, dt, norm, imag, precision);
+    ts_b200_desc d =
+        b200::make_desc(grid, ham, dt, norm, imag, precision, state->angular_momentum);
     int s = ts_b200_create(&d, &h_);
     if (s) b200::fail(s, nullptr, "B200Kernel: creating the device tile");
     s = ts_b200_set_state(h_, state->p_real, state->p_imag, grid->dim_x);

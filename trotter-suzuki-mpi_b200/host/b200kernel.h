@@ -114,11 +114,11 @@ ts_b200_energy_result reduce_energies(Lattice *grid, const double *p_real, const
 
 /** Step descriptor with the constants of the reference's CPUBlock constructor. */
 ts_b200_desc make_desc(Lattice *grid, Hamiltonian *ham, double delta_t, double norm,
-                       bool imag_time, int precision);
+                       bool imag_time, int precision, int angular_momentum = 0);
 /** The same for one species of mass `mass`, g = coupling, g_LHY = lhy. */
 ts_b200_desc make_species_desc(Lattice *grid, Hamiltonian *ham, double delta_t, double norm,
                                bool imag_time, int precision, double mass, double coupling,
-                               double lhy);
+                               double lhy, int angular_momentum = 0);
 
 /** Inter-species and Rabi energies of two host tiles (src/solver.cpp:340-353,
  *  549-550), reduced on the GPU. */

@@ -52,6 +52,15 @@ int tsh_lattice1d_new(int n, double l, int px, void **out) {
     return guard([&] { *out = new Lattice1D(n, l, px != 0); });
 }
 
+int tsh_lattice2d_new_cs(int nx, double lx, int ny, double ly, int px, int py, double omega,
+                         const char *cs, void **out) {
+    return guard([&] { *out = new Lattice2D(nx, lx, ny, ly, px != 0, py != 0, omega, cs); });
+}
+
+int tsh_lattice1d_new_cs(int n, double l, int px, const char *cs, void **out) {
+    return guard([&] { *out = new Lattice1D(n, l, px != 0, cs); });
+}
+
 int tsh_lattice_info_get(void *lp, tsh_lattice_info *o) {
     return guard([&] {
         Lattice *g = static_cast<Lattice *>(lp);
@@ -91,6 +100,10 @@ static Lattice2D *as2d(void *lp) {
 
 int tsh_state_new(void *lp, void **out) {
     return guard([&] { *out = new State(static_cast<Lattice *>(lp)); });
+}
+
+int tsh_state_new_l(void *lp, int angular_momentum, void **out) {
+    return guard([&] { *out = new State(static_cast<Lattice *>(lp), angular_momentum); });
 }
 
 int tsh_gaussian_state_new(void *lp, double wx, double wy, double mx, double my, double norm,

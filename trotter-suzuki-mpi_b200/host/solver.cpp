@@ -61,9 +61,15 @@ Solver::~Solver() {
 void Solver::initialize_exp_potential(double dt, int which) {
     Potential *pot = which == 0 ? hamiltonian->potential
                                 : static_cast<Hamiltonian2Component *>(hamiltonian)->potential_b;
+    const bool cyl = grid->coordinate_system == "cylindrical";
     for (int y = 0; y < grid->dim_y; ++y)
         for (int x = 0; x < grid->dim_x; ++x) {
-            const double v = pot->get_value(x, y);
+            double v = pot->get_value(x, y);
+            // the centrifugal term l^2 / (2 m r^2) (src/solver.cpp:85-96)
+            if (cyl)
+                v += which == 0 ? hamiltonian->azimuthal_potential(x, state->angular_momentum)
+                                : static_cast<Hamiltonian2Component *>(hamiltonian)
+                                      ->azimuthal_potential_b(x, state_b->angular_momentum);
             const complex<double> e = imag_time ? exp(complex<double>(-dt * v, 0.))
                                                 : exp(complex<double>(0., -dt * v));
             external_pot_real[which][size_t(y) * grid->dim_x + x] = real(e);

@@ -53,6 +53,9 @@ def host():
             "tsh_last_error": (C.c_char_p, []),
             "tsh_lattice2d_new": (i, [i, d, i, d, i, i, d, P(vp)]),
             "tsh_lattice1d_new": (i, [i, d, i, P(vp)]),
+            "tsh_lattice2d_new_cs": (i, [i, d, i, d, i, i, d, C.c_char_p, P(vp)]),
+            "tsh_lattice1d_new_cs": (i, [i, d, i, C.c_char_p, P(vp)]),
+            "tsh_state_new_l": (i, [vp, i, P(vp)]),
             "tsh_lattice_info_get": (i, [vp, P(_Info)]),
             "tsh_lattice_free": (i, [vp]),
             "tsh_state_new": (i, [vp, P(vp)]),
@@ -136,10 +139,8 @@ class Lattice(_Handle):
 
 class Lattice1D(Lattice):
     def __init__(self, dim_x, length_x, periodic_x_axis=False, coordinate_system="cartesian"):
-        if coordinate_system != "cartesian":
-            raise RuntimeError("The B200 kernel supports cartesian coordinates only.")
-        self._h = _new(host().tsh_lattice1d_new, int(dim_x), float(length_x),
-                       int(bool(periodic_x_axis)))
+        self._h = _new(host().tsh_lattice1d_new_cs, int(dim_x), float(length_x),
+                       int(bool(periodic_x_axis)), coordinate_system.encode())
         self.coordinate_system = coordinate_system
         self._load()
 
@@ -147,19 +148,26 @@ class Lattice1D(Lattice):
 class Lattice2D(Lattice):
     def __init__(self, dim_x, length_x, dim_y=None, length_y=None, periodic_x_axis=False,
                  periodic_y_axis=False, angular_velocity=0., coordinate_system="cartesian"):
-        if coordinate_system != "cartesian":
-            raise RuntimeError("The B200 kernel supports cartesian coordinates only.")
         dim_y = dim_x if dim_y is None else dim_y
         length_y = length_x if length_y is None else length_y
-        self._h = _new(host().tsh_lattice2d_new, int(dim_x), float(length_x), int(dim_y),
+        self._h = _new(host().tsh_lattice2d_new_cs, int(dim_x), float(length_x), int(dim_y),
                        float(length_y), int(bool(periodic_x_axis)), int(bool(periodic_y_axis)),
-                       float(angular_velocity))
+                       float(angular_velocity), coordinate_system.encode())
         self.coordinate_system = coordinate_system
         self._load()
 
 
 def map_lattice_to_coordinate_space(grid, x, y=0):
-    """Cell-centre coordinates of tile cell (x, y) (src/common.cpp:45-65)."""
+    """Cell-centre coordinates of tile cell (x, y) (src/common.cpp:45-81); on a
+    cylindrical lattice x is the radius, -dx/2 at column 0."""
+    if getattr(grid, "coordinate_system", "cartesian") == "cylindrical":
+        idy = grid.start_y * grid.delta_y + 0.5 * grid.delta_y + y * grid.delta_y
+        y_c = grid.global_no_halo_dim_y * grid.delta_y * 0.5
+        if idy - y_c < -grid.length_y * 0.5:
+            idy += grid.length_y
+        if idy - y_c > grid.length_y * 0.5:
+            idy -= grid.length_y
+        return grid.start_x * grid.delta_x + x * grid.delta_x - 0.5 * grid.delta_x, idy - y_c
     idx = grid.start_x * grid.delta_x + 0.5 * grid.delta_x + x * grid.delta_x
     x_c = grid.global_no_halo_dim_x * grid.delta_x * 0.5
     if idx - x_c < -grid.length_x * 0.5:
@@ -212,7 +220,7 @@ class State(_Handle):
     def __init__(self, grid, angular_momentum=0):
         self.grid = grid
         self.angular_momentum = angular_momentum
-        self._h = _new(host().tsh_state_new, grid._h)
+        self._h = _new(host().tsh_state_new_l, grid._h, int(angular_momentum))
 
     def _arrays(self):
         re = C.POINTER(C.c_double)()
