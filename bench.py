@@ -1188,6 +1188,82 @@ def two_component_cpu_rate(a0, b0, budget_s=12.0):
                       f"({'-Ofast' if flavour == 'fast' else '-O2'} build)"}
 
 
+# ------------------------------------------------------ cylindrical workload
+# A vortex ground state on a cylindrical (r, z) lattice: 2048 radial x 2048
+# axial cells over r in [0, 12), z in [-12, 12), angular momentum l = 1,
+# harmonic trap (1, 1.5), g = 100, imaginary time, dt = 1e-4, FP64; initial
+# state r exp(-(r^2 + z^2) / 8) times (1 + 0.01 u).  One bench step = one
+# evolve(200); the radial sweeps and the mirrored axis column run inside the
+# fused step.
+CYL_STEPS = 200
+CYL_L = 1
+
+
+def run_cylindrical_workload(args, rank, world, local, pg):
+    import torch
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    import trottersuzuki_b200 as ts
+    from trottersuzuki_b200 import launch_count
+    from trottersuzuki_b200.api import _coordinate_grid
+    grid = ts.Lattice2D(N_SIDE, LENGTH / 2, N_SIDE, LENGTH, coordinate_system="cylindrical")
+    R, Z = _coordinate_grid(grid)
+    rng = np.random.Generator(np.random.PCG64(SEED))
+    psi0 = (R * np.exp(-(R * R + Z * Z) / 8.0) *
+            (1 + 0.01 * rng.uniform(-1, 1, R.shape))).astype(np.complex128)
+    state = ts.State(grid, CYL_L)
+    state.init_state_matrix(psi0.real, psi0.imag)
+    pot = ts.HarmonicPotential(grid, OMEGA_X, OMEGA_Y)
+    ham = ts.Hamiltonian(grid, pot, 1.0, G)
+    solver = ts.Solver(grid, state, ham, DT)
+    for _ in range(args.warmup):
+        solver.evolve(-CYL_STEPS, True)
+    cur = torch.cuda.current_stream(device)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    l0 = launch_count()
+    with Clocks(local) as clocks:
+        e0.record(cur)
+        for _ in range(args.steps):
+            solver.evolve(-CYL_STEPS, True)
+        torch.cuda.synchronize()
+        e1.record(cur)
+        e1.synchronize()
+    launches = launch_count() - l0
+    ms = max_over_ranks(e0.elapsed_time(e1), pg, device)
+    solver.evolve(0, True)
+    energy = solver.get_total_energy()
+    if rank != 0:
+        return
+    sites = float(grid.dim_x) * grid.dim_y
+    value = world * sites * CYL_STEPS * args.steps / (ms * 1e-3)
+    peak, peak_kind = measured_peak()
+    achieved = BYTES_PER_SITE_STEP["fp64"] * value / world / 1e9
+    line = {
+        "metric": "site-steps/s", "value": value, "unit": "site-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "cylindrical_vortex_2048",
+                   "lattice": f"{grid.dim_x}x{grid.dim_y} (r, z)",
+                   "length_r": LENGTH / 2, "length_z": LENGTH, "angular_momentum": CYL_L,
+                   "g": G, "omega_rz": [OMEGA_X, OMEGA_Y], "dt": DT, "imag_time": True,
+                   "trotter_steps_per_step": CYL_STEPS, "parallelism": f"replicas{world}",
+                   "l2": "inputs larger than L2: 160 MiB moved per Trotter step"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                     "algorithmic_bytes_per_site_step": BYTES_PER_SITE_STEP["fp64"],
+                     "kernel": "tsb::step_kernel<double, C=2, imaginary, cylindrical, GPE>"},
+        "energy_after": energy,
+        "clocks": clocks.summary(),
+        "gpu_launches": launches,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1202,7 +1278,7 @@ def main():
                     help="reference arm: skip timing the reference's CUDA kernel")
     ap.add_argument("--workload", choices=["gpe_imaginary_time_2048", "batch512", "adjoint512",
                                            "vortex8192", "moving_trap_2048",
-                                           "two_component_2048"],
+                                           "two_component_2048", "cylindrical_vortex_2048"],
                     default="gpe_imaginary_time_2048")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
@@ -1220,6 +1296,8 @@ def main():
             run_moving_trap_workload(args, rank, world, local, pg)
         elif args.workload == "two_component_2048":
             run_two_component_workload(args, rank, world, local, pg)
+        elif args.workload == "cylindrical_vortex_2048":
+            run_cylindrical_workload(args, rank, world, local, pg)
         else:
             run_b200_arm(args, rank, world, local, pg)
     finally:
