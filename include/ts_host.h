@@ -66,6 +66,12 @@ int tsh_state_touch(void *state);
  * mean_pypy, mean_lz -- State::get_* (src/trottersuzuki.h:150-159) */
 int tsh_state_expectations(void *state, double out[10]);
 int tsh_state_free(void *state);
+/* State::write_to_file (kind 0, the file `name`), write_particle_density
+ * (kind 1, name + "-density"), write_phase (kind 2, name + "-phase") and
+ * loadtxt: the reference's text format (src/model.cpp:254-383,636-638,
+ * src/common.cpp:161-181). */
+int tsh_state_write(void *state, int kind, const char *name);
+int tsh_state_loadtxt(void *state, const char *name);
 
 /* Potential(grid, matrix) (the matrix is copied) and HarmonicPotential
  * -- src/trottersuzuki.h:365,410 */

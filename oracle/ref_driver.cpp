@@ -14,6 +14,7 @@
 // src/trottersuzuki.h:34-597), runs Solver::evolve (src/solver.cpp:150-242)
 // and returns the tile, the energies (src/solver.cpp:566-680) and the state
 // expectation values (src/model.cpp:385-536).
+#include <algorithm>
 #include <cstring>
 #include <cstdio>
 #include <chrono>
@@ -199,6 +200,48 @@ int tsref_run(const tsref_config *cfg, double *psi_re, double *psi_im,
         if (!cfg->force_rotation_periodic) delete ham;
         delete pot;
         delete state;
+        delete grid;
+    } catch (std::exception &e) {
+        snprintf(g_err, sizeof g_err, "%s", e.what());
+        return 1;
+    }
+    return 0;
+}
+
+// State text I/O of the reference (src/model.cpp:254-383,636-638): load = 0
+// writes the state given in re/im (kind 0 state, 1 density, 2 phase) to
+// `name`; load = 1 reads `name` into a fresh State and returns its tile.
+int tsref_state_io(const tsref_config *cfg, double *re, double *im, int kind, const char *name,
+                   int load) {
+    try {
+        Lattice *grid;
+        if (cfg->dim_y == 0)
+            grid = new Lattice1D(cfg->dim_x, cfg->length_x, cfg->periodic_x != 0);
+        else
+            grid = new Lattice2D(cfg->dim_x, cfg->length_x, cfg->dim_y, cfg->length_y,
+                                 cfg->periodic_x != 0, cfg->periodic_y != 0,
+                                 cfg->lattice_angular_velocity,
+                                 cfg->cylindrical ? "cylindrical" : "cartesian");
+        const size_t n = size_t(grid->dim_x) * grid->dim_y;
+        std::vector<double> r(n, 0.0), i(n, 0.0);
+        if (!load) {
+            std::copy(re, re + n, r.begin());
+            std::copy(im, im + n, i.begin());
+        }
+        State *st = new State(grid, 0, r.data(), i.data());
+        if (load) {
+            std::vector<char> nm(name, name + strlen(name) + 1);
+            st->loadtxt(nm.data());
+            std::copy(r.begin(), r.end(), re);
+            std::copy(i.begin(), i.end(), im);
+        } else if (kind == 0) {
+            st->write_to_file(name);
+        } else if (kind == 1) {
+            st->write_particle_density(name);
+        } else {
+            st->write_phase(name);
+        }
+        delete st;
         delete grid;
     } catch (std::exception &e) {
         snprintf(g_err, sizeof g_err, "%s", e.what());

@@ -99,6 +99,9 @@ def _lib(flavour="parity"):
         lib.tsref_run2.argtypes = [C.POINTER(Config), C.POINTER(Config2)] + [C.c_void_p] * 6 + \
             [C.POINTER(Result2)]
         lib.tsref_run2.restype = C.c_int
+        lib.tsref_state_io.argtypes = [C.POINTER(Config), C.c_void_p, C.c_void_p, C.c_int,
+                                       C.c_char_p, C.c_int]
+        lib.tsref_state_io.restype = C.c_int
         _libs[flavour] = lib
     return _libs[flavour]
 
@@ -203,3 +206,24 @@ def run2(cfg, c2, psi_a, psi_b, pot_a, pot_b, flavour="parity"):
     if rc != 0:
         raise RuntimeError(_lib(flavour).tsref_last_error().decode())
     return arrs[0] + 1j * arrs[1], arrs[2] + 1j * arrs[3], res
+
+
+def write_state(cfg, psi, kind, name, flavour="parity"):
+    """The reference writes the tile psi (kind 0 state, 1 density, 2 phase)."""
+    re = np.ascontiguousarray(np.real(psi), np.float64).copy()
+    im = np.ascontiguousarray(np.imag(psi), np.float64).copy()
+    if _lib(flavour).tsref_state_io(C.byref(cfg), re.ctypes.data, im.ctypes.data, int(kind),
+                                    str(name).encode(), 0) != 0:
+        raise RuntimeError(_lib(flavour).tsref_last_error().decode())
+
+
+def load_state(cfg, name, flavour="parity"):
+    """The reference reads a state file into a fresh tile."""
+    geo = geometry(cfg, flavour)
+    re = np.zeros((geo.dim_y, geo.dim_x))
+    im = np.zeros((geo.dim_y, geo.dim_x))
+    if _lib(flavour).tsref_state_io(C.byref(cfg), re.ctypes.data, im.ctypes.data, 0,
+                                    str(name).encode(), 1) != 0:
+        raise RuntimeError(_lib(flavour).tsref_last_error().decode())
+    return re + 1j * im
+

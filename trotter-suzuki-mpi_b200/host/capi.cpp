@@ -102,6 +102,20 @@ int tsh_state_new(void *lp, void **out) {
     return guard([&] { *out = new State(static_cast<Lattice *>(lp)); });
 }
 
+int tsh_state_write(void *sp, int kind, const char *name) {
+    return guard([&] {
+        State *st = static_cast<State *>(sp);
+        if (kind == 0) st->write_to_file(name);
+        else if (kind == 1) st->write_particle_density(name);
+        else if (kind == 2) st->write_phase(name);
+        else my_abort("tsh_state_write: kind 0 (state), 1 (density) or 2 (phase)");
+    });
+}
+
+int tsh_state_loadtxt(void *sp, const char *name) {
+    return guard([&] { static_cast<State *>(sp)->loadtxt(const_cast<char *>(name)); });
+}
+
 int tsh_state_new_l(void *lp, int angular_momentum, void **out) {
     return guard([&] { *out = new State(static_cast<Lattice *>(lp), angular_momentum); });
 }

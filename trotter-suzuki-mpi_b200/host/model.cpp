@@ -331,27 +331,36 @@ TS_STATE_GETTER(get_mean_pypy, mean_PyPy)
 TS_STATE_GETTER(get_mean_angular_momentum, mean_angular_momentum)
 #undef TS_STATE_GETTER
 
-void State::write_to_file(string prefix) {
-    std::ofstream out((prefix + "-state").c_str());
+// The reference's single-process stamp / print_complex_matrix
+// (src/model.cpp:636-638, src/common.cpp:161-170,254-265): the file is named
+// by the argument itself; each lattice row is a line of "(re,im) " with the
+// stream's default formatting (6 significant digits), so files written here
+// and by the reference are the same byte for byte.  The rows and columns are
+// the lattice without its periodic halo; on a cylindrical lattice the columns
+// are the inner ones (the reference's own width there, global_dim_x, runs one
+// cell past each row).
+void State::write_to_file(string filename) {
+    std::ofstream out(filename.c_str(), std::ios::out | std::ios::trunc);
     const int ox = grid->inner_start_x - grid->start_x, oy = grid->inner_start_y - grid->start_y;
-    const int w = grid->inner_end_x - grid->inner_start_x;
-    const int h = grid->inner_end_y - grid->inner_start_y;
-    out.precision(17);
+    const int w = grid->coordinate_system == "cylindrical"
+                      ? grid->inner_end_x - grid->inner_start_x
+                      : grid->global_dim_x - 2 * grid->periods[1] * grid->halo_x;
+    const int h = grid->global_dim_y - 2 * grid->periods[0] * grid->halo_y;
     for (int j = 0; j < h; ++j) {
         for (int i = 0; i < w; ++i) {
             const size_t k = size_t(j + oy) * grid->dim_x + (i + ox);
             out << "(" << p_real[k] << "," << p_imag[k] << ") ";
         }
-        out << "\n";
+        out << std::endl;
     }
 }
 
+// print_matrix of src/common.cpp:172-181: "v " per cell, default formatting.
 static void write_matrix(const string &name, const double *m, int w, int h) {
-    std::ofstream out(name.c_str());
-    out.precision(17);
+    std::ofstream out(name.c_str(), std::ios::out | std::ios::trunc);
     for (int j = 0; j < h; ++j) {
         for (int i = 0; i < w; ++i) out << m[size_t(j) * w + i] << " ";
-        out << "\n";
+        out << std::endl;
     }
 }
 

@@ -56,6 +56,8 @@ def host():
             "tsh_lattice2d_new_cs": (i, [i, d, i, d, i, i, d, C.c_char_p, P(vp)]),
             "tsh_lattice1d_new_cs": (i, [i, d, i, C.c_char_p, P(vp)]),
             "tsh_state_new_l": (i, [vp, i, P(vp)]),
+            "tsh_state_write": (i, [vp, i, C.c_char_p]),
+            "tsh_state_loadtxt": (i, [vp, C.c_char_p]),
             "tsh_lattice_info_get": (i, [vp, P(_Info)]),
             "tsh_lattice_free": (i, [vp]),
             "tsh_state_new": (i, [vp, P(vp)]),
@@ -262,6 +264,21 @@ class State(_Handle):
         g = self.grid
         return a[g.inner_start_y - g.start_y:g.inner_end_y - g.start_y,
                  g.inner_start_x - g.start_x:g.inner_end_x - g.start_x]
+
+    def write_to_file(self, filename):
+        """The state as text, "(re,im) " per cell (src/model.cpp:636-638)."""
+        _chk(host().tsh_state_write(self._h, 0, str(filename).encode()))
+
+    def write_particle_density(self, fileprefix):
+        _chk(host().tsh_state_write(self._h, 1, str(fileprefix).encode()))
+
+    def write_phase(self, fileprefix):
+        _chk(host().tsh_state_write(self._h, 2, str(fileprefix).encode()))
+
+    def loadtxt(self, filename):
+        """Read a state written by write_to_file (src/model.cpp:254-322)."""
+        _chk(host().tsh_state_loadtxt(self._h, str(filename).encode()))
+        _chk(host().tsh_state_touch(self._h))
 
     def get_particle_density(self):
         re, im = self._arrays()
