@@ -203,6 +203,19 @@ int ts_b200_set_potential_device(ts_b200_kernel *k, const double *potential, siz
 int ts_b200_evolve_potentials(ts_b200_kernel *k, const double *potentials, size_t pitch,
                               size_t slab, int count, double delta_t, int exchange);
 
+/* One lattice split across ranks in slabs of rows (the reference's MPI
+ * tiles, src/common.cpp:83-102, and their halo exchange,
+ * src/cpukernel.cpp:691-747): the current buffer's rows [row0, row0 + nrows)
+ * as one device span of `bytes` (rows are contiguous, pitch included), for
+ * sending the edge rows and receiving the halo rows; the device address of
+ * the squared norm of the tile's inner region after the last step (times
+ * dx dy, before renormalisation), to be summed over the ranks; and the
+ * imaginary-time renormalisation from that sum (device pointer), which
+ * replaces the one the step took from the tile alone. */
+int ts_b200_rows(ts_b200_kernel *k, int row0, int nrows, void **ptr, size_t *bytes);
+int ts_b200_last_norm(ts_b200_kernel *k, double **device_ptr);
+int ts_b200_renormalize_from(ts_b200_kernel *k, const double *total_norm);
+
 /* Queue all work of this handle on `stream` (a cudaStream_t); NULL restores
  * the handle's own stream. */
 int ts_b200_set_stream(ts_b200_kernel *k, void *stream);

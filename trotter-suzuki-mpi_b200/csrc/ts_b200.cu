@@ -926,6 +926,13 @@ int upload_kinetic_schedule(ts_b200_kernel *k) {
 
 int grid_for(size_t n) { return (int)std::max<size_t>(1, std::min<size_t>((n + 255) / 256, 8192)); }
 
+// The pending factor from a norm summed over several tiles (one lattice
+// split across ranks): src/cpukernel.cpp:537-562 with the MPI_Allgather sum.
+__global__ void renorm_from_kernel(Scalars *scal, const double *total, double norm0) {
+    if (threadIdx.x == 0 && blockIdx.x == 0 && scal->renorm)
+        scal->pending_inv = 1.0 / sqrt(*total / norm0);
+}
+
 // A tile that is one species of a pair steps only through the pair.
 int reject_pair_mode(ts_b200_kernel *k) {
     return fail(k, TS_B200_UNSUPPORTED, "the tile is one component of a pair: step the pair");
@@ -1189,6 +1196,29 @@ int ts_b200_evolve_potentials(ts_b200_kernel *k, const double *potentials, size_
         const int s = launch_step(k, exchange);
         if (s) return s;
     }
+    return TS_B200_OK;
+}
+
+int ts_b200_rows(ts_b200_kernel *k, int row0, int nrows, void **ptr, size_t *bytes) {
+    if (!k || !ptr || !bytes || row0 < 0 || nrows < 0 || row0 + nrows > k->H)
+        return TS_B200_INVALID_ARGUMENT;
+    *ptr = static_cast<unsigned char *>(k->psi[k->cur]) + (size_t)row0 * k->P * k->cell;
+    *bytes = (size_t)nrows * k->P * k->cell;
+    return TS_B200_OK;
+}
+
+int ts_b200_last_norm(ts_b200_kernel *k, double **device_ptr) {
+    if (!k || !device_ptr) return TS_B200_INVALID_ARGUMENT;
+    *device_ptr = &k->scal->last_norm;
+    return TS_B200_OK;
+}
+
+int ts_b200_renormalize_from(ts_b200_kernel *k, const double *total_norm) {
+    if (!k || !total_norm) return TS_B200_INVALID_ARGUMENT;
+    if (!k->imag) return TS_B200_OK;
+    renorm_from_kernel<<<1, 32, 0, k->stream>>>(k->scal, total_norm, k->d.norm0);
+    TSB_CHECK(k, cudaGetLastError());
+    g_launches.fetch_add(1, std::memory_order_relaxed);
     return TS_B200_OK;
 }
 
