@@ -16,6 +16,7 @@ struct ts_b200_kernel {
     int W = 0, H = 0, P = 0;
     bool fp32 = false, imag = false, rot = false;
     int phase = 0;  // 0 none, 1 g|psi|^2, 2 with Lee-Huang-Yang, 3 one component of a pair
+                    // (7: the same with the Rabi rotation applied at load), | 4 cylindrical
     size_t cell = 0, tab_cell = 0;
     void *psi[2] = {nullptr, nullptr};
     int cur = 0;
@@ -48,6 +49,9 @@ struct ts_b200_kernel {
     const void *pb = nullptr;
     const double *pb_scale = nullptr;
     double cab = 0.0;
+    // phase 7: cos (minus 1 in single precision), the other cell's factor in
+    // this species' rotation (re, im), this cell's factor in the other's
+    double rabi[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     std::string err;
 };
 

@@ -378,6 +378,34 @@ int step_species(ts_b200_pair *p, int which, int exchange) {
 
 bool has_rabi(const ts_b200_pair *p) { return p->omega_r != 0.0 || p->omega_i != 0.0; }
 
+void set_phase(ts_b200_kernel *k, int phase) {
+    if (k->phase == phase) return;
+    k->phase = phase;
+    k->resident_blocks = 0;  // occupancy of the other variant
+}
+
+// Constants of the full (var = 1) real-time rotation as each species' loads
+// apply it (phase 7): a' = cc a + i cs b, b' = cc b + i conj(cs) a with
+// cs = (omega / |omega|) sin(angle) (src/cpucartesian.cpp:264-290).
+void set_folded_rotation(ts_b200_pair *p) {
+    const double c3 = 0.5 * p->omega_r, c4 = 0.5 * p->omega_i;
+    const double no = std::sqrt(c3 * c3 + c4 * c4);
+    const double ang = -p->delta_t * no;
+    const double sn = std::sin(ang), h = std::sin(0.5 * ang);
+    const double cs_r = c3 / no * sn, cs_i = c4 / no * sn;
+    const double sa[2] = {-cs_i, cs_r};  // factor of b in a'
+    const double sb[2] = {cs_i, cs_r};   // factor of a in b'
+    for (int w = 0; w < 2; ++w) {
+        ts_b200_kernel *k = w == 0 ? p->a : p->b;
+        const double *self = w == 0 ? sa : sb, *other = w == 0 ? sb : sa;
+        k->rabi[0] = k->fp32 ? -2.0 * h * h : std::cos(ang);
+        k->rabi[1] = self[0];
+        k->rabi[2] = self[1];
+        k->rabi[3] = other[0];
+        k->rabi[4] = other[1];
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -437,14 +465,28 @@ int ts_b200_pair_rabi(ts_b200_pair *p, double var) {
 int ts_b200_pair_steps(ts_b200_pair *p, int steps, int final_steps) {
     if (!p || steps < 0) return TS_B200_INVALID_ARGUMENT;
     const bool rabi = has_rabi(p);
-    for (int i = 0; i < steps; ++i) {
+    // In real time the rotation after step i (never the call's last) is
+    // applied by step i + 1 as it loads both species' rows (phase 7): the
+    // rotation is pointwise and both steps load the pair of cells it mixes,
+    // so no pass over the tiles is left for it.  The rotation after the
+    // call's last step is a pass of its own, and so is every rotation in
+    // imaginary time, where the joint normalisation follows it.
+    const bool fold = rabi && !p->a->imag;
+    if (fold) set_folded_rotation(p);
+    int s = TS_B200_OK;
+    for (int i = 0; i < steps && s == TS_B200_OK; ++i) {
         const bool last = final_steps && i == steps - 1;
-        int s = step_species(p, 0, last ? 0 : 1);
+        const int phase = fold && i > 0 ? 7 : 3;
+        set_phase(p->a, phase);
+        set_phase(p->b, phase);
+        s = step_species(p, 0, last ? 0 : 1);
         if (s == TS_B200_OK) s = step_species(p, 1, last ? 0 : 1);
-        if (s == TS_B200_OK && rabi) s = launch_rabi(p, last ? 0.5 : 1.0, p->a->imag);
-        if (s) return s;
+        if (s == TS_B200_OK && rabi && (!fold || i == steps - 1))
+            s = launch_rabi(p, last ? 0.5 : 1.0, p->a->imag);
     }
-    return TS_B200_OK;
+    set_phase(p->a, 3);
+    set_phase(p->b, 3);
+    return s;
 }
 
 int ts_b200_pair_evolve(ts_b200_pair *p, int iterations) {

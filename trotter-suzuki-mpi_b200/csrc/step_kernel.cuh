@@ -86,6 +86,11 @@ struct StepArgs {
     const void *pb;
     const double *pb_scale;
     T cab;
+    // two components in real time, phase bit 8: the Rabi rotation that
+    // follows the previous step, applied to (own, other) as the rows arrive:
+    // cos (minus 1 in delta form), the complex factor of the other species'
+    // cell in the own cell's rotation and that of the own cell in the other's
+    T rabi_cc, rabi_sr, rabi_si, rabi_or, rabi_oi;
     // cylindrical: per tile column x, the radial pair (x, x+1) as (a, b, c, 0)
     // (a - 1 in delta form); the sign of the mirrored axis column
     const void *rad;
@@ -484,23 +489,31 @@ __device__ __forceinline__ void st_cx_global(Cx<T> *p, Cx<T> v) {
     *reinterpret_cast<typename Vec2T<T>::type *>(p) = o;
 }
 
+// Rabi rotation of one cell (src/cpucartesian.cpp:264-290, real time):
+// cc * self + (sr + i si) * other, cc - 1 in delta form.
+template <typename T>
+__device__ __forceinline__ Cx<T> rabi_cell(Cx<T> self, Cx<T> other, T cc, T sr, T si) {
+    Cx<T> r;
+    r.re = lin(cc, self.re, fma_t(sr, other.re, -mul_t(si, other.im)));
+    r.im = lin(cc, self.im, fma_t(sr, other.im, mul_t(si, other.re)));
+    return r;
+}
+
 // Potential, GPE and LHY phase on one row (src/cpucartesian.cpp:96-106,130-134).
 // |psi|^2 is taken before the table multiply, as the reference does.
 // PB (two components): the phase adds g_ab dt |psi_b|^2, psi_b the other
-// species' cell (row `pb`, times `pbs`) at the start of this step
+// species' cell at the start of this step (`ub`, already scaled)
 // (src/cpucartesian.cpp:73-92,113-126).
 template <bool IMAG, bool PHASE, bool LHY, bool PB, int C, typename T, typename TabT>
 __device__ __forceinline__ void potential_row(Cx<T> (&w)[C], const TabT *tab, T ca, T caa,
-                                              const Cx<T> *pb = nullptr, T pbs = T(1),
-                                              T cab = T(0)) {
+                                              const Cx<T> (*ub)[C] = nullptr, T cab = T(0)) {
 #pragma unroll
     for (int i = 0; i < C; ++i) {
         Cx<T> v = w[i];
         T thb = T(0);
         if (PB) {
-            const Cx<T> u = ld_cx_shared(pb + i);
-            const T ur = mul_t(u.re, pbs), ui = mul_t(u.im, pbs);
-            thb = mul_t(cab, fma_t(ur, ur, mul_t(ui, ui)));
+            const Cx<T> u = (*ub)[i];
+            thb = mul_t(cab, fma_t(u.re, u.re, mul_t(u.im, u.im)));
         }
         if (IMAG) {
             const T pr = reinterpret_cast<const T *>(tab)[i];
@@ -544,7 +557,9 @@ __device__ __forceinline__ void potential_row(Cx<T> (&w)[C], const TabT *tab, T 
 // Compile-time description of a kernel variant.
 // PHASE & 3: 0 no nonlinear phase, 1 g|psi|^2 only, 2 with the Lee-Huang-Yang
 // term, 3 g|psi|^2 + g_ab|psi_b|^2 (one component of a two-component system);
-// PHASE & 4: cylindrical lattice (radial kinetic sweeps, mirrored axis column).
+// PHASE & 4: cylindrical lattice (radial kinetic sweeps, mirrored axis column);
+// PHASE & 8 (with 3, real time): the Rabi rotation of the previous step
+// applied to both species' cells as they are loaded.
 template <typename T_, int C_, bool IMAG_, bool ROT_, int PHASE_>
 struct Variant {
     using T = T_;
@@ -555,6 +570,8 @@ struct Variant {
     static constexpr bool LHY = (PHASE_ & 3) == 2;
     static constexpr bool PB = (PHASE_ & 3) == 3;
     static constexpr bool CYL = (PHASE_ & 4) != 0;
+    static constexpr bool RABI = (PHASE_ & 8) != 0;
+    static_assert(!RABI || (PB && !IMAG_ && !CYL), "Rabi loads: two components, real time");
     // recomputed halo columns: one per horizontal pair sweep of the step
     // (4 kinetic; 4 more rotation row sweeps or radial sweeps)
     static constexpr int HX = (ROT_ || (PHASE_ & 4)) ? 8 : 4;
@@ -620,6 +637,7 @@ struct Walk {
     T inv;
     T aH, bH, aV, bV, ca, caa;  // step constants, read from the parameters once
     T pbs, cab;                 // PB: factor of the other species' tile, g_ab * dt
+    T rcc, rsr, rsi, ror, roi;  // RABI: rotation of the own and of the other cell
     T rca[2][2], rcb[2][2];     // CYL: radial (a, b_self) of cell [i] for parity [p]
     T msign;                    // CYL, imaginary time: mirror sign on the lane of column 0
     T hpa[C - 1], hpb[C - 1];        // LANE_COEF: this lane's pairs (i, i+1)
@@ -701,6 +719,15 @@ __device__ __forceinline__ void walk_row(Walk<V> &w, const StepArgs<typename V::
 #pragma unroll
         for (int i = 0; i < C; ++i) {
             Cx<T> v = ld_cx_shared(sp + i);
+            if constexpr (V::RABI) {
+                const Cx<T> *bp = reinterpret_cast<const Cx<T> *>(w.ring + q * V::SLOT +
+                                                                  V::PSI_BYTES + V::TAB_BYTES) +
+                                  C * w.lane;
+                Cx<T> u = ld_cx_shared(bp + i);
+                u.re = mul_t(u.re, w.pbs);
+                u.im = mul_t(u.im, w.pbs);
+                v = rabi_cell(v, u, w.rcc, w.rsr, w.rsi);
+            }
             if (IMAG) {
                 v.re = v.re * w.inv;
                 v.im = v.im * w.inv;
@@ -729,7 +756,21 @@ __device__ __forceinline__ void walk_row(Walk<V> &w, const StepArgs<typename V::
             const Cx<T> *bp = reinterpret_cast<const Cx<T> *>(w.ring + q * V::SLOT +
                                                               V::PSI_BYTES + V::TAB_BYTES) +
                               C * w.lane;
-            potential_row<IMAG, PHASE, false, true, C>(WS(2), tp, w.ca, w.caa, bp, w.pbs, w.cab);
+            Cx<T> ub[C];
+#pragma unroll
+            for (int i = 0; i < C; ++i) {
+                Cx<T> u = ld_cx_shared(bp + i);
+                u.re = mul_t(u.re, w.pbs);
+                u.im = mul_t(u.im, w.pbs);
+                if constexpr (V::RABI) {
+                    // the other species rotated from the cells this row started from
+                    const Cx<T> o = ld_cx_shared(
+                        reinterpret_cast<const Cx<T> *>(w.ring + q * V::SLOT) + C * w.lane + i);
+                    u = rabi_cell(u, o, w.rcc, w.ror, w.roi);
+                }
+                ub[i] = u;
+            }
+            potential_row<IMAG, PHASE, false, true, C>(WS(2), tp, w.ca, w.caa, &ub, w.cab);
         } else {
             potential_row<IMAG, PHASE, V::LHY, false, C>(WS(2), tp, w.ca, w.caa);
         }
@@ -896,6 +937,13 @@ __device__ __forceinline__ void bind_args(Walk<V> &w, const StepArgs<typename V:
     if constexpr (V::PB) {
         w.pbs = (T)__ldcg(a.pb_scale);
         w.cab = a.cab;
+    }
+    if constexpr (V::RABI) {
+        w.rcc = a.rabi_cc;
+        w.rsr = a.rabi_sr;
+        w.rsi = a.rabi_si;
+        w.ror = a.rabi_or;
+        w.roi = a.rabi_oi;
     }
     w.gpsi_pitch = (size_t)a.P * sizeof(Cx<T>);
     w.gtab_pitch = (size_t)a.P * sizeof(typename V::TabT);

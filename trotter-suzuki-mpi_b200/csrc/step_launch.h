@@ -51,6 +51,11 @@ cudaError_t launch_phase(int phase, const StepArgs<T> &a, int warps, size_t smem
             return launch_step_variant<Variant<T, C, IMAG, ROT, 5>>(a, warps, smem, blocks, st, bps);
         if (phase == 6)
             return launch_step_variant<Variant<T, C, IMAG, ROT, 6>>(a, warps, smem, blocks, st, bps);
+        if constexpr (!IMAG) {
+            if (phase == 7)
+                return launch_step_variant<Variant<T, C, IMAG, ROT, 11>>(a, warps, smem, blocks,
+                                                                         st, bps);
+        }
     }
     if (phase > 3) return cudaErrorInvalidValue;
     if (phase == 2) return launch_step_variant<Variant<T, C, IMAG, ROT, 2>>(a, warps, smem, blocks, st, bps);
@@ -60,7 +65,8 @@ cudaError_t launch_phase(int phase, const StepArgs<T> &a, int warps, size_t smem
 
 // phase: 0 none, 1 g|psi|^2, 2 g|psi|^2 + Lee-Huang-Yang, 3 two components
 // (g|psi|^2 + g_ab|psi_b|^2; 2 cells per lane, no rotating frame); 4-6: 0-2 on
-// a cylindrical lattice (2 cells per lane, no rotating frame).
+// a cylindrical lattice (2 cells per lane, no rotating frame); 7: 3 in real
+// time with the previous step's Rabi rotation applied as the rows are loaded.
 template <typename T, bool IMAG>
 cudaError_t launch_step_imag_t(int C, bool rot, int phase, const StepArgs<T> &a, int warps,
                                size_t smem, int blocks, cudaStream_t st, int *bps) {

@@ -617,7 +617,8 @@ void geometry(const ts_b200_kernel *k, int *strips, int *segs, int *blocks, size
     if (k->resident_blocks > 0) *blocks = std::min(*blocks, k->resident_blocks);
     // per warp: ring slots + one mbarrier per ring slot
     *smem = (size_t)k->warps *
-            (k->ring * slot_bytes(k->C, k->fp32, k->imag, k->phase == 3) + 8 * k->ring);
+            (k->ring * slot_bytes(k->C, k->fp32, k->imag, k->phase == 3 || k->phase == 7) +
+             8 * k->ring);
 }
 
 template <typename T>
@@ -686,6 +687,11 @@ void tsbh::fill_step_constants(const ts_b200_kernel *k, StepArgs<T> &a) {
     a.pb = k->pb;
     a.pb_scale = k->pb_scale;
     a.cab = (T)k->cab;
+    a.rabi_cc = (T)k->rabi[0];
+    a.rabi_sr = (T)k->rabi[1];
+    a.rabi_si = (T)k->rabi[2];
+    a.rabi_or = (T)k->rabi[3];
+    a.rabi_oi = (T)k->rabi[4];
     a.rad = k->rad;
     a.mirror_sign = (T)(k->d.angular_momentum % 2 == 0 ? 1 : -1);
 }
