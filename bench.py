@@ -77,11 +77,11 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def committed_traffic():
-    """DRAM bytes (read + write) per step-kernel launch on this workload, from
-    the committed ncu summary (a line `dram_bytes_per_launch: <int>`), if any."""
+def committed_traffic(summary="step_kernel_gpe_imag_2048.md"):
+    """DRAM bytes (read + write) per step-kernel launch on a workload, from
+    its committed ncu summary (a line `dram_bytes_per_launch: <int>`), if any."""
     import re
-    path = os.path.join(REPO, "profiles", "step_kernel_gpe_imag_2048.md")
+    path = os.path.join(REPO, "profiles", summary)
     try:
         with open(path) as f:
             m = re.search(r"^dram_bytes_per_launch:\s*(\d+)", f.read(), re.M)
@@ -1148,7 +1148,8 @@ def run_two_component_workload(args, rank, world, local, pg):
                 "d2h_bytes_per_step": 4 * 8 * int(sites),
                 "path": "two-state Solver.evolve(200), both States filled after each call"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                     "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": committed_traffic("step_kernel_two_component_2048.md"),
                      "algorithmic_bytes_per_species_site_step": two_bytes,
                      "kernel": "tsb::step_kernel<double, C=2, real, two components, "
                                "Rabi rotation at load> x 2 per Trotter step"},
@@ -1258,7 +1259,8 @@ def run_cylindrical_workload(args, rank, world, local, pg):
                    "trotter_steps_per_step": CYL_STEPS, "parallelism": f"replicas{world}",
                    "l2": "inputs larger than L2: 160 MiB moved per Trotter step"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                     "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": committed_traffic("step_kernel_cylindrical_2048.md"),
                      "algorithmic_bytes_per_site_step": BYTES_PER_SITE_STEP["fp64"],
                      "kernel": "tsb::step_kernel<double, C=2, imaginary, cylindrical, GPE>"},
         "energy_after": energy,
