@@ -200,6 +200,34 @@ __device__ __forceinline__ Cx<T> kin(Cx<T> s, Cx<T> p, T a, T b) {
     return r;
 }
 
+// Single precision: both components in packed pairs (FMUL2 / FFMA2 / FADD2
+// of sm_100) with the same roundings as the scalar form above.  In real time
+// the partner enters crossed (re <- im), so the two fused multiply-adds stay
+// scalar: a packed one would need the partner's halves swapped first.
+template <>
+__device__ __forceinline__ Cx<float> kin<true, float>(Cx<float> s, Cx<float> p, float a, float b) {
+    const float2 s2 = make_float2(s.re, s.im);
+    const float2 t = __fmul2_rn(make_float2(b, b), make_float2(p.re, p.im));
+    const float2 r = __fadd2_rn(s2, __ffma2_rn(make_float2(a, a), s2, t));
+    return Cx<float>{r.x, r.y};
+}
+template <>
+__device__ __forceinline__ Cx<float> kin<false, float>(Cx<float> s, Cx<float> p, float a, float b) {
+    const float2 t = __fmul2_rn(make_float2(b, b), make_float2(p.re, p.im));
+    const float2 u = make_float2(__fmaf_rn(a, s.re, -t.y), __fmaf_rn(a, s.im, t.x));
+    const float2 r = __fadd2_rn(make_float2(s.re, s.im), u);
+    return Cx<float>{r.x, r.y};
+}
+
+// v * f for a real factor f (both components, one packed multiply in single precision).
+__device__ __forceinline__ Cx<double> scale_cx(Cx<double> v, double f) {
+    return Cx<double>{mul_t(f, v.re), mul_t(f, v.im)};
+}
+__device__ __forceinline__ Cx<float> scale_cx(Cx<float> v, float f) {
+    const float2 r = __fmul2_rn(make_float2(f, f), make_float2(v.re, v.im));
+    return Cx<float>{r.x, r.y};
+}
+
 // Rotation pair (src/cpucartesian.cpp:149-153 real, :210-214 imaginary):
 // `first` is the lower-index cell of the pair, `second` the higher one.
 template <bool IMAG, typename T>
@@ -522,12 +550,9 @@ __device__ __forceinline__ void potential_row(Cx<T> (&w)[C], const TabT *tab, T 
                 T th = mul_t(ca, n2);
                 if (LHY) th = fma_t(caa, mul_t(n2, sqrt_t(n2)), th);
                 if (PB) th = th + thb;
-                const T t = mul_t(phase_expneg(th), pr);
-                v.re = mul_t(t, v.re);
-                v.im = mul_t(t, v.im);
+                v = scale_cx(v, mul_t(phase_expneg(th), pr));
             } else {
-                v.re = mul_t(pr, v.re);
-                v.im = mul_t(pr, v.im);
+                v = scale_cx(v, pr);
             }
         } else {
             const Cx<T> e = reinterpret_cast<const Cx<T> *>(tab)[i];
@@ -539,15 +564,11 @@ __device__ __forceinline__ void potential_row(Cx<T> (&w)[C], const TabT *tab, T 
                 if (PB) th = th + thb;
                 phase_sincos(th, &s, &c);
             }
-            // the table holds (cos, sin) of -dt V; in delta form (cos - 1, sin)
-            T t = v.re;
-            v.re = lin(e.re, t, -mul_t(e.im, v.im));
-            v.im = lin(e.re, v.im, mul_t(e.im, t));
-            if (PHASE) {
-                t = v.re;
-                v.re = lin(c, t, mul_t(s, v.im));
-                v.im = lin(c, v.im, -mul_t(s, t));
-            }
+            // the table holds (cos, sin) of -dt V; in delta form (cos - 1, sin):
+            // v (cos + i sin), the kinetic pair's form with the cell as its own
+            // partner; the phase multiplies by (c - i s)
+            v = kin<false>(v, v, e.re, e.im);
+            if (PHASE) v = kin<false>(v, v, c, -s);
         }
         w[i] = v;
     }
@@ -724,14 +745,9 @@ __device__ __forceinline__ void walk_row(Walk<V> &w, const StepArgs<typename V::
                                                                   V::PSI_BYTES + V::TAB_BYTES) +
                                   C * w.lane;
                 Cx<T> u = ld_cx_shared(bp + i);
-                u.re = mul_t(u.re, w.pbs);
-                u.im = mul_t(u.im, w.pbs);
-                v = rabi_cell(v, u, w.rcc, w.rsr, w.rsi);
+                v = rabi_cell(v, scale_cx(u, w.pbs), w.rcc, w.rsr, w.rsi);
             }
-            if (IMAG) {
-                v.re = v.re * w.inv;
-                v.im = v.im * w.inv;
-            }
+            if (IMAG) v = scale_cx(v, w.inv);
             WS(0)[i] = (!EDGE || w.present[i]) ? v : Cx<T>{T(0), T(0)};
         }
     }
@@ -759,9 +775,7 @@ __device__ __forceinline__ void walk_row(Walk<V> &w, const StepArgs<typename V::
             Cx<T> ub[C];
 #pragma unroll
             for (int i = 0; i < C; ++i) {
-                Cx<T> u = ld_cx_shared(bp + i);
-                u.re = mul_t(u.re, w.pbs);
-                u.im = mul_t(u.im, w.pbs);
+                Cx<T> u = scale_cx(ld_cx_shared(bp + i), w.pbs);
                 if constexpr (V::RABI) {
                     // the other species rotated from the cells this row started from
                     const Cx<T> o = ld_cx_shared(
