@@ -185,38 +185,44 @@ __device__ __forceinline__ T lin(T a, T z, T p) {
     return fma_t(a, z, p);
 }
 
-// Kinetic pair (src/cpucartesian.cpp:8-11 real time, :29-32 imaginary time);
-// the update is symmetric, so each cell is updated from (self, partner).
-template <bool IMAG, typename T>
-__device__ __forceinline__ Cx<T> kin(Cx<T> s, Cx<T> p, T a, T b) {
-    Cx<T> r;
-    if (IMAG) {
-        r.re = lin(a, s.re, mul_t(b, p.re));
-        r.im = lin(a, s.im, mul_t(b, p.im));
-    } else {
-        r.re = lin(a, s.re, -mul_t(b, p.im));
-        r.im = lin(a, s.im, mul_t(b, p.re));
-    }
-    return r;
+// The two pair forms, for a coefficient pair (a, b) and a cell s with its
+// partner p:
+//   direct: s + (a s + b p) per component (a s + b p without delta form),
+//   cross:  the same with b p replaced by i b p (re <- -b p.im, im <- b p.re).
+template <typename T>
+__device__ __forceinline__ Cx<T> pair_direct(Cx<T> s, Cx<T> p, T a, T b) {
+    return Cx<T>{lin(a, s.re, mul_t(b, p.re)), lin(a, s.im, mul_t(b, p.im))};
 }
-
+template <typename T>
+__device__ __forceinline__ Cx<T> pair_cross(Cx<T> s, Cx<T> p, T a, T b) {
+    return Cx<T>{lin(a, s.re, -mul_t(b, p.im)), lin(a, s.im, mul_t(b, p.re))};
+}
 // Single precision: both components in packed pairs (FMUL2 / FFMA2 / FADD2
-// of sm_100) with the same roundings as the scalar form above.  In real time
-// the partner enters crossed (re <- im), so the two fused multiply-adds stay
-// scalar: a packed one would need the partner's halves swapped first.
+// of sm_100) with the same roundings as the scalar forms.  In the cross form
+// the partner enters with its halves swapped, so its two fused multiply-adds
+// stay scalar: a packed one would need the swap first.
 template <>
-__device__ __forceinline__ Cx<float> kin<true, float>(Cx<float> s, Cx<float> p, float a, float b) {
+__device__ __forceinline__ Cx<float> pair_direct<float>(Cx<float> s, Cx<float> p, float a,
+                                                        float b) {
     const float2 s2 = make_float2(s.re, s.im);
     const float2 t = __fmul2_rn(make_float2(b, b), make_float2(p.re, p.im));
     const float2 r = __fadd2_rn(s2, __ffma2_rn(make_float2(a, a), s2, t));
     return Cx<float>{r.x, r.y};
 }
 template <>
-__device__ __forceinline__ Cx<float> kin<false, float>(Cx<float> s, Cx<float> p, float a, float b) {
+__device__ __forceinline__ Cx<float> pair_cross<float>(Cx<float> s, Cx<float> p, float a,
+                                                       float b) {
     const float2 t = __fmul2_rn(make_float2(b, b), make_float2(p.re, p.im));
     const float2 u = make_float2(__fmaf_rn(a, s.re, -t.y), __fmaf_rn(a, s.im, t.x));
     const float2 r = __fadd2_rn(make_float2(s.re, s.im), u);
     return Cx<float>{r.x, r.y};
+}
+
+// Kinetic pair (src/cpucartesian.cpp:8-11 real time, :29-32 imaginary time);
+// the update is symmetric, so each cell is updated from (self, partner).
+template <bool IMAG, typename T>
+__device__ __forceinline__ Cx<T> kin(Cx<T> s, Cx<T> p, T a, T b) {
+    return IMAG ? pair_direct(s, p, a, b) : pair_cross(s, p, a, b);
 }
 
 // v * f for a real factor f (both components, one packed multiply in single precision).
@@ -230,30 +236,15 @@ __device__ __forceinline__ Cx<float> scale_cx(Cx<float> v, float f) {
 
 // Rotation pair (src/cpucartesian.cpp:149-153 real, :210-214 imaginary):
 // `first` is the lower-index cell of the pair, `second` the higher one.
+// (-b) x is -(b x) exactly, so signs move onto the coefficient.
 template <bool IMAG, typename T>
 __device__ __forceinline__ Cx<T> rot_first(Cx<T> f, Cx<T> s, T a, T b) {
-    Cx<T> r;
-    if (IMAG) {
-        r.re = lin(a, f.re, mul_t(b, s.im));
-        r.im = lin(a, f.im, -mul_t(b, s.re));
-    } else {
-        r.re = lin(a, f.re, mul_t(b, s.re));
-        r.im = lin(a, f.im, mul_t(b, s.im));
-    }
-    return r;
+    return IMAG ? pair_cross(f, s, a, -b) : pair_direct(f, s, a, b);
 }
 
 template <bool IMAG, typename T>
 __device__ __forceinline__ Cx<T> rot_second(Cx<T> s, Cx<T> f, T a, T b) {
-    Cx<T> r;
-    if (IMAG) {
-        r.re = lin(a, s.re, -mul_t(b, f.im));
-        r.im = lin(a, s.im, mul_t(b, f.re));
-    } else {
-        r.re = lin(a, s.re, -mul_t(b, f.re));
-        r.im = lin(a, s.im, -mul_t(b, f.im));
-    }
-    return r;
+    return IMAG ? pair_cross(s, f, a, b) : pair_direct(s, f, a, -b);
 }
 
 template <typename T>
@@ -444,22 +435,26 @@ __device__ __forceinline__ float sqrt_t(float x) { return sqrtf(x); }
 // (Horner's rule) leave a remainder below 1e-19, i.e. well under half an ulp
 // of double; larger arguments take the CUDA math library.
 // Returns sin(th) and cos(th) (cos(th) - 1 in delta form).
+// Below 1/32 the series apply (the comparison is exact in either precision).
+__device__ __forceinline__ bool phase_small(double th) { return fabs(th) < 0.03125; }
+__device__ __forceinline__ bool phase_small(float th) { return fabsf(th) < 0.03125f; }
+
 template <typename T>
 __device__ __forceinline__ void phase_sincos(T th, T *s, T *c) {
     // warp-uniform choice: the library path only if some lane needs it
-    if (!__any_sync(0xffffffffu, !(fabs((double)th) < 0.03125))) {
+    if (!__any_sync(0xffffffffu, !phase_small(th))) {
         const T t = th * th;
         T pc = T(-2.7557319223985893e-07);            // -1/10!
         pc = fma_t(pc, t, T(2.4801587301587302e-05));  //  1/8!
         pc = fma_t(pc, t, T(-1.3888888888888889e-03)); // -1/6!
         pc = fma_t(pc, t, T(4.1666666666666664e-02));  //  1/4!
         pc = fma_t(pc, t, T(-0.5));                    // -1/2!
-        *c = DeltaForm<T>::value ? mul_t(pc, t) : fma_t(pc, t, T(1));
         T ps = T(-2.5052108385441720e-08);             // -1/11!
         ps = fma_t(ps, t, T(2.7557319223985888e-06));  //  1/9!
         ps = fma_t(ps, t, T(-1.9841269841269841e-04)); // -1/7!
         ps = fma_t(ps, t, T(8.3333333333333332e-03));  //  1/5!
         ps = fma_t(ps, t, T(-1.6666666666666666e-01)); // -1/3!
+        *c = DeltaForm<T>::value ? mul_t(pc, t) : fma_t(pc, t, T(1));
         *s = fma_t(mul_t(ps, t), th, th);
     } else {
         sincos_t(th, s, c);
@@ -474,7 +469,7 @@ __device__ __forceinline__ void phase_sincos(T th, T *s, T *c) {
 // exp(-th) for the imaginary-time nonlinear factor (same truncation rule).
 template <typename T>
 __device__ __forceinline__ T phase_expneg(T th) {
-    if (!__any_sync(0xffffffffu, !(fabs((double)th) < 0.03125))) {
+    if (!__any_sync(0xffffffffu, !phase_small(th))) {
         const T x = -th;
         T p = T(2.4801587301587302e-05);             // 1/8!
         p = fma_t(p, x, T(1.9841269841269841e-04)); // 1/7!
@@ -487,6 +482,22 @@ __device__ __forceinline__ T phase_expneg(T th) {
         return fma_t(p, x, T(1));
     }
     return exp_t(-th);
+}
+
+// exp(-th0), exp(-th1) of two single-precision cells: the series of both in
+// one packed pair, each cell with the roundings of phase_expneg.
+__device__ __forceinline__ float2 phase_expneg2(float th0, float th1) {
+    if (!__any_sync(0xffffffffu, !(phase_small(th0) && phase_small(th1)))) {
+        const float2 x = make_float2(-th0, -th1);
+        constexpr double k[8] = {1.9841269841269841e-04, 1.3888888888888889e-03,
+                                 8.3333333333333332e-03, 4.1666666666666664e-02,
+                                 1.6666666666666666e-01, 0.5, 1.0, 1.0};
+        float2 p = make_float2(float(2.4801587301587302e-05), float(2.4801587301587302e-05));
+#pragma unroll
+        for (int j = 0; j < 8; ++j) p = __ffma2_rn(p, x, make_float2(float(k[j]), float(k[j])));
+        return p;
+    }
+    return make_float2(phase_expneg(th0), phase_expneg(th1));
 }
 
 template <typename T>
@@ -535,6 +546,30 @@ __device__ __forceinline__ Cx<T> rabi_cell(Cx<T> self, Cx<T> other, T cc, T sr, 
 template <bool IMAG, bool PHASE, bool LHY, bool PB, int C, typename T, typename TabT>
 __device__ __forceinline__ void potential_row(Cx<T> (&w)[C], const TabT *tab, T ca, T caa,
                                               const Cx<T> (*ub)[C] = nullptr, T cab = T(0)) {
+    if constexpr (IMAG && PHASE && std::is_same<T, float>::value && C % 2 == 0) {
+        // single precision: the factors of two cells at a time in packed pairs
+        T th[C];
+#pragma unroll
+        for (int i = 0; i < C; ++i) {
+            const Cx<T> v = w[i];
+            const T n2 = fma_t(v.re, v.re, mul_t(v.im, v.im));
+            th[i] = mul_t(ca, n2);
+            if (LHY) th[i] = fma_t(caa, mul_t(n2, sqrt_t(n2)), th[i]);
+            if (PB) {
+                const Cx<T> u = (*ub)[i];
+                th[i] = th[i] + mul_t(cab, fma_t(u.re, u.re, mul_t(u.im, u.im)));
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < C; i += 2) {
+            const float2 pr = make_float2(reinterpret_cast<const T *>(tab)[i],
+                                          reinterpret_cast<const T *>(tab)[i + 1]);
+            const float2 f = __fmul2_rn(phase_expneg2(th[i], th[i + 1]), pr);
+            w[i] = scale_cx(w[i], f.x);
+            w[i + 1] = scale_cx(w[i + 1], f.y);
+        }
+        return;
+    }
 #pragma unroll
     for (int i = 0; i < C; ++i) {
         Cx<T> v = w[i];
