@@ -222,11 +222,13 @@ int ts_b200_set_stream(ts_b200_kernel *k, void *stream);
 int ts_b200_synchronize(ts_b200_kernel *k);
 
 /* Geometry of the fused step launch chosen for this tile (for reporting):
- * cells per lane, rows per segment, warps per block, ring depth, tasks. */
+ * cells per lane, rows per segment, warps per block, ring depth, tasks, and
+ * the row walk (0 checked, 1 look-ahead). */
 typedef struct {
     int32_t cells_per_lane, segment_rows, warps_per_block, ring_depth;
     int32_t strips, segments, blocks, threads;
     int64_t smem_bytes;
+    int32_t walk, reserved;
 } ts_b200_launch_shape;
 
 int ts_b200_launch_info(const ts_b200_kernel *k, ts_b200_launch_shape *out);
@@ -235,6 +237,13 @@ int ts_b200_launch_info(const ts_b200_kernel *k, ts_b200_launch_shape *out);
  * current choice.  Only shapes this build instantiates are accepted. */
 int ts_b200_set_launch(ts_b200_kernel *k, int cells_per_lane, int segment_rows, int warps_per_block,
                        int ring_depth);
+
+/* Row walk of the fused step (no counterpart in the reference; both walks
+ * perform the same operations per cell): 1 (default) the look-ahead walk,
+ * which single-component cartesian tiles without a rotating frame use, with
+ * even segments, ring depth 6 and 4 or 8 warps per block; 0 the checked walk
+ * of every variant.  Variants without a look-ahead walk ignore the choice. */
+int ts_b200_set_walk(ts_b200_kernel *k, int walk);
 
 /* ---- Batched evolution (no counterpart in the reference, which evolves one
  * lattice per Solver; the batch replaces a loop of per-tile evolve() calls).

@@ -11,13 +11,25 @@
 #                                                 binary runnable on another host CPU)
 #   libtsref_gpu.so   nvcc -DCUDA -O2, sm_100a    adds the reference's CUDA kernel
 #
-# Usage: oracle/build_ref.sh [reference_root]   (default /root/reference)
+# Usage: oracle/build_ref.sh [--optional] [reference_root]
+#   reference_root defaults to $TS_REFERENCE_ROOT, else /root/reference (where
+#   the reference is mounted read-only beside this repository); with
+#   --optional a missing source tree is not an error (nothing is built).
 set -eu
-REF=${1:-/root/reference}
+OPTIONAL=0
+if [ "${1:-}" = "--optional" ]; then
+    OPTIONAL=1
+    shift
+fi
+REF=${1:-${TS_REFERENCE_ROOT:-/root/reference}}
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT="$HERE/_ref"
 SRC="$REF/src"
 if [ ! -f "$SRC/cpukernel.cpp" ]; then
+    if [ "$OPTIONAL" = 1 ]; then
+        echo "reference sources not found under $SRC: oracle/_ref not rebuilt"
+        exit 0
+    fi
     echo "reference sources not found under $SRC" >&2
     exit 1
 fi

@@ -93,6 +93,9 @@ def lib():
         L.tso_adjoint_real.argtypes = [C.POINTER(Params), dp, dp, C.c_double, dp, dp, C.c_int,
                                        dp, dp, dp, dp, dp]
         L.tso_adjoint_real.restype = C.c_int
+        L.tso_adjoint_imag.argtypes = [C.POINTER(Params), dp, C.c_double, dp, dp, C.c_int,
+                                       dp, dp, dp, dp, dp]
+        L.tso_adjoint_imag.restype = C.c_int
         L.tso_full_step2.argtypes = [C.POINTER(Params), C.c_double, dp, dp, dp, dp, dp, dp]
         L.tso_rabi.argtypes = [C.POINTER(Params), C.c_double, C.c_double, C.c_double,
                                C.c_double, dp, dp, dp, dp]
@@ -377,4 +380,25 @@ def adjoint_real(p, tab_re, tab_im, delta_t, psi0, steps, lam_t):
                                 li.ctypes.data, gv.ctypes.data, gr.ctypes.data, gi.ctypes.data)
     if rc != 0:
         raise RuntimeError(f"tso_adjoint_real: status {rc}")
+    return gv, gr + 1j * gi
+
+
+def adjoint_imag(p, tab_re, delta_t, psi0, steps, lam_t):
+    """Reverse mode of `steps` closed imaginary-time steps with renormalisation
+    to norm0 = N(psi0) (CPU FP64 check of the B200 imaginary-time adjoint;
+    oracle/ts_oracle.c tso_adjoint_imag).  lam_t = dL/dre + i dL/dim at psi(T);
+    returns (dL/dV, dL/dpsi0)."""
+    shape = (p.H, p.W)
+    a = lambda z: np.ascontiguousarray(z, np.float64)
+    r0, i0 = a(np.real(psi0)), a(np.imag(psi0))
+    lr, li = a(np.real(lam_t)), a(np.imag(lam_t))
+    tr = a(tab_re)
+    gv = np.zeros(shape)
+    gr = np.zeros(shape)
+    gi = np.zeros(shape)
+    rc = lib().tso_adjoint_imag(C.byref(p), tr.ctypes.data, float(delta_t), r0.ctypes.data,
+                                i0.ctypes.data, int(steps), lr.ctypes.data, li.ctypes.data,
+                                gv.ctypes.data, gr.ctypes.data, gi.ctypes.data)
+    if rc != 0:
+        raise RuntimeError(f"tso_adjoint_imag: status {rc}")
     return gv, gr + 1j * gi

@@ -513,6 +513,110 @@ int tso_adjoint_real(const tso_params *p, const double *pot_re, const double *po
     return 0;
 }
 
+/* ---- reverse mode of the imaginary-time evolution (closed tile) ----------
+ * Not a restatement of the reference (it has no derivatives): the transpose
+ * of tso_evolve in imaginary time, the CPU FP64 check of the B200 imaginary-
+ * time adjoint.  Forward: norm0 = N(psi_0) (the State's norm when the
+ * imaginary-time evolution starts, src/solver.cpp:155), then per step
+ *     phi_{k+1} = S(psi_k),  psi_{k+1} = c_{k+1} phi_{k+1},
+ *     c = sqrt(norm0 / N(phi))                      (src/cpukernel.cpp:551-562)
+ * with N(x) = dA sum |x|^2 over the tile.  Reverse, from Lambda = dL/dpsi_T:
+ *   - normalisation of step k's output: kappa_k = Re<Lambda, psi_k>,
+ *         Lambda <- c_k (Lambda - (dA / norm0) kappa_k psi_k);
+ *   - the step: every imaginary-time pair matrix [[a, b], [b, a]] is
+ *     symmetric, so the transposed sweeps are the sweeps themselves, in
+ *     reverse order; the potential stage psi' = f E x (E = exp(-V dt),
+ *     f = exp(-theta(|x|^2)), theta = g|x|^2 + g_lhy|x|^3, g and g_lhy
+ *     already times dt) has the transpose
+ *         lambda = f E (lambda' - 2 theta' s x),  s = Re(conj(lambda') x),
+ *         dL/dV += -dt f E s,                 theta' = g + 1.5 g_lhy |x|;
+ *   - norm0 depends on psi_0: dL/dpsi_0 += (dA / norm0) sum_{k>=1} kappa_k psi_0.
+ * All forward states are stored (small tiles). */
+static void adjoint_potential_imag(const tso_params *p, const double *pot_re, double dt,
+                                   const double *xr, const double *xi, double *lr, double *li,
+                                   double *grad_v) {
+    const size_t n = (size_t)p->W * p->H;
+    for (size_t k = 0; k < n; ++k) {
+        double n2 = xr[k] * xr[k] + xi[k] * xi[k];
+        double r = sqrt(n2);
+        double th = p->coupling * n2 + p->lhy_coupling * n2 * r;
+        double dth = p->coupling + 1.5 * p->lhy_coupling * r;
+        double fe = exp(-th) * pot_re[k];
+        double sdot = lr[k] * xr[k] + li[k] * xi[k];
+        grad_v[k] += -dt * fe * sdot;
+        lr[k] = fe * (lr[k] - 2. * dth * sdot * xr[k]);
+        li[k] = fe * (li[k] - 2. * dth * sdot * xi[k]);
+    }
+}
+
+int tso_adjoint_imag(const tso_params *p, const double *pot_re, double dt, const double *psi0_re,
+                     const double *psi0_im, int steps, const double *lam_re, const double *lam_im,
+                     double *grad_v, double *grad_re, double *grad_im) {
+    const size_t n = (size_t)p->W * p->H;
+    const int vert = p->H > 1;
+    if (!p->imag_time || p->periodic_x || p->periodic_y || (p->alpha_x != 0. && p->alpha_y != 0.) ||
+        p->cylindrical)
+        return 1;
+    const double dA = p->delta_x * p->delta_y;
+    /* states psi_0 .. psi_T (normalised) and factors c_1 .. c_T */
+    double *states = (double *)malloc(sizeof(double) * 2 * n * (size_t)(steps + 1));
+    double *cs = (double *)malloc(sizeof(double) * (size_t)(steps + 1));
+    double *xr = (double *)malloc(sizeof(double) * n), *xi = (double *)malloc(sizeof(double) * n);
+    if (!states || !cs || !xr || !xi) {
+        free(states); free(cs); free(xr); free(xi);
+        return 2;
+    }
+    memcpy(states, psi0_re, sizeof(double) * n);
+    memcpy(states + n, psi0_im, sizeof(double) * n);
+    const double norm0 = tso_squared_norm(p, psi0_re, psi0_im);
+    cs[0] = 1.;
+    for (int s = 1; s <= steps; ++s) {
+        double *pr = states + 2 * n * (size_t)(s - 1), *nr = states + 2 * n * (size_t)s;
+        memcpy(nr, pr, sizeof(double) * 2 * n);
+        tso_full_step(p, nr, nr + n, pot_re, NULL);
+        double f = sqrt(tso_squared_norm(p, nr, nr + n) / norm0);
+        for (size_t k = 0; k < n; ++k) {
+            nr[k] /= f;
+            nr[n + k] /= f;
+        }
+        cs[s] = 1. / f;
+    }
+    memcpy(grad_re, lam_re, sizeof(double) * n);
+    memcpy(grad_im, lam_im, sizeof(double) * n);
+    memset(grad_v, 0, sizeof(double) * n);
+    double kappa_sum = 0.;
+    for (int s = steps; s >= 1; --s) {
+        const double *pr = states + 2 * n * (size_t)s, *pi = pr + n;
+        double kappa = 0.;
+        for (size_t k = 0; k < n; ++k) kappa += grad_re[k] * pr[k] + grad_im[k] * pi[k];
+        kappa_sum += kappa;
+        const double m = dA / norm0 * kappa;
+        for (size_t k = 0; k < n; ++k) {
+            grad_re[k] = cs[s] * (grad_re[k] - m * pr[k]);
+            grad_im[k] = cs[s] * (grad_im[k] - m * pi[k]);
+        }
+        memcpy(xr, states + 2 * n * (size_t)(s - 1), sizeof(double) * n);
+        memcpy(xi, states + 2 * n * (size_t)(s - 1) + n, sizeof(double) * n);
+        forward_half(p, xr, xi);  /* x: the potential stage's input */
+        if (vert) sweep_vertical(p, 0, p->aV, p->bV, grad_re, grad_im);
+        sweep_horizontal(p, 0, p->aH, p->bH, grad_re, grad_im);
+        if (vert) sweep_vertical(p, 1, p->aV, p->bV, grad_re, grad_im);
+        sweep_horizontal(p, 1, p->aH, p->bH, grad_re, grad_im);
+        adjoint_potential_imag(p, pot_re, dt, xr, xi, grad_re, grad_im, grad_v);
+        sweep_horizontal(p, 1, p->aH, p->bH, grad_re, grad_im);
+        if (vert) sweep_vertical(p, 1, p->aV, p->bV, grad_re, grad_im);
+        sweep_horizontal(p, 0, p->aH, p->bH, grad_re, grad_im);
+        if (vert) sweep_vertical(p, 0, p->aV, p->bV, grad_re, grad_im);
+    }
+    const double m0 = dA / norm0 * kappa_sum;
+    for (size_t k = 0; k < n; ++k) {
+        grad_re[k] += m0 * psi0_re[k];
+        grad_im[k] += m0 * psi0_im[k];
+    }
+    free(states); free(cs); free(xr); free(xi);
+    return 0;
+}
+
 /* ---- step constants (src/cpukernel.cpp:185-217) and table (src/solver.cpp:74-109) */
 void tso_init_constants(tso_params *p, double delta_t, double mass, double g, double g_lhy,
                         double omega, double delta_x, double delta_y) {

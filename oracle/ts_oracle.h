@@ -59,6 +59,14 @@ int tso_adjoint_real(const tso_params *p, const double *pot_re, const double *po
                      const double *lam_re, const double *lam_im, double *grad_v,
                      double *grad_re, double *grad_im);
 
+/* Reverse mode of `steps` imaginary-time steps on a closed tile, with the
+ * renormalisation after every step to norm0 = N(psi_0) (test check of the
+ * B200 imaginary-time adjoint; not in the reference): from lambda =
+ * dL/dpsi(T) to dL/dV and dL/dpsi0 (the table is exp(-V dt), pot_re). */
+int tso_adjoint_imag(const tso_params *p, const double *pot_re, double dt, const double *psi0_re,
+                     const double *psi0_im, int steps, const double *lam_re, const double *lam_im,
+                     double *grad_v, double *grad_re, double *grad_im);
+
 void tso_evolve(const tso_params *p, double *re, double *im, const double *pot_re,
                 const double *pot_im, int iterations);
 /* Two components: one component's step with the other's density (pb) in

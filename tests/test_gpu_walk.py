@@ -1,0 +1,123 @@
+"""The look-ahead row walk of the fused step against the oracle and against
+the checked walk.
+
+Both walks perform the same operations per cell (the same pair forms,
+potential row and fused multiply-adds), so in real time they agree bit for
+bit, whatever the launch shape; in imaginary time the squared norm is summed
+over a different grid of blocks, so the renormalisation factor may differ in
+its last bits (1e-13).  The oracle bar is the FP64 parity bar, 1e-10.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from helpers import desc_from_params, seeded_case
+
+pytestmark = pytest.mark.gpu
+
+TOL_PSI = 1e-10
+
+
+def _oracle(lat, psi0, V, dt, imag, g, lhy, steps):
+    n0 = O.expectations(lat, psi0)["norm2"] if imag else 0.0
+    p = lat.params(dt, imag, 1.0, g, lhy, 0.0, norm0=n0)
+    tr, ti = O.exp_table(V, dt, imag)
+    return p, tr, ti, O.evolve(p, psi0, tr, ti, steps)
+
+
+def _gpu(p, psi0, tr, ti, steps, walk, launch=None, precision=0, split=None):
+    from trottersuzuki_b200 import Kernel
+    with Kernel(desc_from_params(p, precision)) as k:
+        k.set_walk(walk)
+        if launch:
+            k.set_launch(**launch)
+        shape = k.launch_shape()
+        k.set_state(psi0)
+        k.set_exp_potential(tr, ti)
+        for s in (split or [steps]):
+            k.evolve(s)
+        return k.get_state(), shape
+
+
+# name, N, L, Ny, periodic, g, lhy, imag, steps
+CASES = [
+    ("closed_real", 64, 10.0, None, (False, False), 0.0, 0.0, False, 20),
+    ("gpe_lhy_real", 64, 10.0, None, (False, False), 5.0, 0.3, False, 20),
+    ("gpe_imag", 64, 10.0, None, (False, False), 5.0, 0.0, True, 20),
+    ("ragged", 61, 10.0, 47, (False, False), 1.0, 0.0, False, 20),
+    ("periodic", 64, 10.0, None, (True, True), 2.0, 0.0, False, 20),
+    ("periodic_x_imag", 64, 10.0, None, (True, False), 2.0, 0.0, True, 12),
+    ("periodic_odd", 63, 10.0, 45, (True, True), 1.0, 0.0, False, 12),
+    ("tall", 40, 10.0, 700, (False, False), 1.0, 0.0, False, 8),
+    ("wide_imag_periodic", 530, 20.0, 96, (True, True), 4.0, 0.2, True, 6),
+    ("tiny", 3, 1.0, 2, (False, False), 1.0, 0.0, False, 5),
+    ("one_row", 50, 5.0, 1, (False, False), 1.0, 0.0, False, 5),
+    ("short_rows", 200, 10.0, 9, (False, False), 1.0, 0.0, True, 7),
+]
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
+def test_look_ahead_walk_matches_oracle_and_checked_walk(case):
+    _, N, L, Ny, per, g, lhy, imag, steps = case
+    lat, psi0, V = seeded_case(N, L, Ny, per)
+    p, tr, ti, ref = _oracle(lat, psi0, V, 1e-3, imag, g, lhy, steps)
+    got, shape = _gpu(p, psi0, tr, ti, steps, walk=1)
+    assert shape["walk"] == 1
+    assert np.abs(got - ref).max() <= TOL_PSI
+    old, shape0 = _gpu(p, psi0, tr, ti, steps, walk=0)
+    assert shape0["walk"] == 0
+    if imag:
+        assert np.abs(got - old).max() <= 1e-13 * np.abs(old).max()
+    else:
+        assert np.array_equal(got, old)
+
+
+@pytest.mark.parametrize("launch", [
+    dict(cells_per_lane=2, segment_rows=16),
+    dict(cells_per_lane=4, segment_rows=40),
+    dict(cells_per_lane=2, segment_rows=7, warps_per_block=1),
+    dict(cells_per_lane=4, segment_rows=256, warps_per_block=8),
+    dict(cells_per_lane=2, segment_rows=2, warps_per_block=8),
+    dict(cells_per_lane=2, segment_rows=300, warps_per_block=2),
+])
+@pytest.mark.parametrize("imag", [False, True], ids=["real", "imag"])
+def test_look_ahead_walk_launch_shapes(launch, imag):
+    """Any strip/segment cut of the look-ahead walk gives the checked walk's
+    bits (real time) and the oracle's result at the parity bar."""
+    lat, psi0, V = seeded_case(333, 12.0, 290, (False, False))
+    p, tr, ti, ref = _oracle(lat, psi0, V, 1e-3, imag, 3.0, 0.0, 9)
+    got, shape = _gpu(p, psi0, tr, ti, 9, walk=1, launch=launch, split=[4, 5])
+    assert shape["walk"] == 1 and shape["segment_rows"] % 2 == 0
+    assert np.abs(got - ref).max() <= TOL_PSI
+    if not imag:
+        old, _ = _gpu(p, psi0, tr, ti, 9, walk=0, split=[4, 5])
+        assert np.array_equal(got, old)
+
+
+@pytest.mark.parametrize("imag", [False, True], ids=["real", "imag"])
+@pytest.mark.parametrize("cells", [2, 4])
+def test_look_ahead_walk_fp32(imag, cells):
+    """FP32 storage through the look-ahead walk: the checked walk's bits in
+    real time (the same float arithmetic per cell), the FP32 bar against the
+    FP64 oracle."""
+    from trottersuzuki_b200 import _capi
+    lat, psi0, V = seeded_case(257, 12.0, 203, (False, False))
+    p, tr, ti, ref = _oracle(lat, psi0, V, 1e-3, imag, 3.0, 0.0, 15)
+    launch = dict(cells_per_lane=cells, segment_rows=24)
+    got, shape = _gpu(p, psi0, tr, ti, 15, walk=1, launch=launch, precision=_capi.FP32)
+    assert shape["walk"] == 1
+    assert np.abs(got - ref).max() <= 2e-5 * np.abs(ref).max()
+    old, _ = _gpu(p, psi0, tr, ti, 15, walk=0, launch=launch, precision=_capi.FP32)
+    if imag:
+        assert np.abs(got - old).max() <= 1e-6 * np.abs(old).max()
+    else:
+        assert np.array_equal(got, old)
+
+
+def test_rotating_frame_keeps_the_checked_walk():
+    from trottersuzuki_b200 import Kernel
+    lat, psi0, V = seeded_case(64, 10.0, None, (False, False), omega=0.7)
+    p = lat.params(1e-3, False, 1.0, 1.0, 0.0, 0.7)
+    with Kernel(desc_from_params(p)) as k:
+        k.set_walk(1)
+        assert k.launch_shape()["walk"] == 0

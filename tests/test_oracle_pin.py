@@ -163,3 +163,45 @@ def test_cpu_adjoint_matches_finite_differences(g, lhy):
     ys, xs = zip(*sites)
     for col, adj in ((0, gv[ys, xs]), (1, gp.real[ys, xs]), (2, gp.imag[ys, xs])):
         assert np.abs(adj - fd[:, col]).max() <= 1e-6 * np.abs(fd[:, col]).max()
+
+
+@pytest.mark.parametrize("g,lhy", [(0.0, 0.0), (3.0, 0.0), (3.0, 0.8)])
+def test_cpu_imag_adjoint_matches_finite_differences(g, lhy):
+    """The CPU FP64 imaginary-time adjoint (renormalisation after every step
+    to the initial norm) against central differences of the oracle's
+    imaginary-time evolution, for L = sum_{x>0} |psi(T)|^2 dA; the initial
+    norm moves with psi0 as in Solver::evolve (src/solver.cpp:155)."""
+    lat = O.Lattice(24, 6.0, 20, None)
+    rng = np.random.default_rng(2)
+    X, _ = lat.coordinates()
+    psi0 = (O.gaussian(lat, 1.0, 1.0, -0.5, 0.3) * (1 + 0.3 * rng.uniform(-1, 1, lat.shape))
+            * np.exp(0.7j * X))
+    V = lat.harmonic(1.0, 1.0) + 0.2 * rng.uniform(-1, 1, lat.shape)
+    dt, steps = 1e-2, 30
+    dA = lat.delta_x * lat.delta_y
+    mask = X > 0
+
+    def loss(Vh, ph):
+        n0 = O.expectations(lat, ph)["norm2"]
+        p = lat.params(dt, True, 1.0, g, lhy, 0.0, norm0=n0)
+        tr, ti = O.exp_table(Vh, dt, True)
+        psi = O.evolve(p, ph, tr, ti, steps)
+        return float((np.abs(psi) ** 2 * mask).sum() * dA), psi
+
+    _, psi_t = loss(V, psi0)
+    p = lat.params(dt, True, 1.0, g, lhy, 0.0, norm0=O.expectations(lat, psi0)["norm2"])
+    tr, _ = O.exp_table(V, dt, True)
+    gv, gp = O.adjoint_imag(p, tr, dt, psi0, steps, 2 * dA * mask * psi_t)
+    h = 1e-5
+    sites = [(10, 12), (5, 3), (15, 20), (9, 8), (3, 17)]
+    fd = []
+    for y, x in sites:
+        e = np.zeros_like(V)
+        e[y, x] = h
+        fd.append(((loss(V + e, psi0)[0] - loss(V - e, psi0)[0]) / (2 * h),
+                   (loss(V, psi0 + e)[0] - loss(V, psi0 - e)[0]) / (2 * h),
+                   (loss(V, psi0 + 1j * e)[0] - loss(V, psi0 - 1j * e)[0]) / (2 * h)))
+    fd = np.array(fd)
+    ys, xs = zip(*sites)
+    for col, adj in ((0, gv[ys, xs]), (1, gp.real[ys, xs]), (2, gp.imag[ys, xs])):
+        assert np.abs(adj - fd[:, col]).max() <= 1e-6 * np.abs(fd[:, col]).max()

@@ -584,6 +584,8 @@ int ts_b200_batch_launch_info(ts_b200_batch *b, ts_b200_launch_shape *out) {
     out->blocks = std::max(1, std::min(b->resident_blocks, div_up(b->n_tasks, b->shape.warps)));
     out->threads = 32 * b->shape.warps;
     out->smem_bytes = (int64_t)batch_smem(b, b->shape.warps);
+    out->walk = 0;
+    out->reserved = 0;
     return TS_B200_OK;
 }
 

@@ -35,6 +35,7 @@ struct ts_b200_kernel {
     int C = 2, seg_h = 64, warps = 4, ring = 4;
     int resident_blocks = 0;  // blocks of the current launch shape resident on the GPU (0: unknown)
     bool auto_seg = true;     // pick the segment height from the resident grid
+    bool walk2 = true;        // look-ahead walk (walk2.cuh) where the variant has one
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
     float4 *kin_sched = nullptr;  // FP32 real time: per-step kinetic coefficients
@@ -84,5 +85,9 @@ void fill_step_constants(const ts_b200_kernel *k, tsb::StepArgs<T> &a);
 // One fused step of the tile from device buffer `in` to `out` (tile layout,
 // row pitch k->P), on the tile's stream; the tile's own buffers are untouched.
 int launch_step_buffers(ts_b200_kernel *k, const void *in, void *out);
+
+// Imaginary time: the squared norm every step restores (a launch parameter of
+// the step, so a captured evolve graph is dropped when it changes).
+int set_norm0(ts_b200_kernel *k, double norm0);
 
 }  // namespace tsbh

@@ -1,0 +1,11 @@
+// Look-ahead walk variants: float, real time.
+#include "step2_launch.h"
+
+namespace tsb {
+
+cudaError_t launch_step2_f32_real(int C, int phase, const StepArgs<float> &a, int warps,
+                                  size_t smem, int blocks, cudaStream_t st, int *bps) {
+    return launch_step2_t<float, false>(C, phase, a, warps, smem, blocks, st, bps);
+}
+
+}  // namespace tsb

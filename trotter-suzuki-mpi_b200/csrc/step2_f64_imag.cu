@@ -1,0 +1,11 @@
+// Look-ahead walk variants: double, imaginary time.
+#include "step2_launch.h"
+
+namespace tsb {
+
+cudaError_t launch_step2_f64_imag(int C, int phase, const StepArgs<double> &a, int warps,
+                                  size_t smem, int blocks, cudaStream_t st, int *bps) {
+    return launch_step2_t<double, true>(C, phase, a, warps, smem, blocks, st, bps);
+}
+
+}  // namespace tsb

@@ -513,21 +513,29 @@ __global__ void __launch_bounds__(RED_THREADS) expect_kernel(RedArgs a) {
 // --------------------------------------------------------- step dispatch
 // The step variants are instantiated in step_f64_real.cu, step_f64_imag.cu,
 // step_f32_real.cu and step_f32_imag.cu (compiled in parallel).
+// w2: the look-ahead walk (walk2.cuh), else the checked walk (step_kernel.cuh)
 template <typename T>
-cudaError_t dispatch_step(int C, bool imag, bool rot, int phase, const StepArgs<T> &a, int warps,
-                          size_t smem, int blocks, cudaStream_t st, int *bps);
+cudaError_t dispatch_step(int C, bool imag, bool rot, int phase, bool w2, const StepArgs<T> &a,
+                          int warps, size_t smem, int blocks, cudaStream_t st, int *bps);
 
 template <>
-cudaError_t dispatch_step<double>(int C, bool imag, bool rot, int phase,
+cudaError_t dispatch_step<double>(int C, bool imag, bool rot, int phase, bool w2,
                                   const StepArgs<double> &a, int warps, size_t smem, int blocks,
                                   cudaStream_t st, int *bps) {
+    if (w2)
+        return imag ? tsb::launch_step2_f64_imag(C, phase, a, warps, smem, blocks, st, bps)
+                    : tsb::launch_step2_f64_real(C, phase, a, warps, smem, blocks, st, bps);
     return imag ? tsb::launch_step_f64_imag(C, rot, phase, a, warps, smem, blocks, st, bps)
                 : tsb::launch_step_f64_real(C, rot, phase, a, warps, smem, blocks, st, bps);
 }
 
 template <>
-cudaError_t dispatch_step<float>(int C, bool imag, bool rot, int phase, const StepArgs<float> &a,
-                                 int warps, size_t smem, int blocks, cudaStream_t st, int *bps) {
+cudaError_t dispatch_step<float>(int C, bool imag, bool rot, int phase, bool w2,
+                                 const StepArgs<float> &a, int warps, size_t smem, int blocks,
+                                 cudaStream_t st, int *bps) {
+    if (w2)
+        return imag ? tsb::launch_step2_f32_imag(C, phase, a, warps, smem, blocks, st, bps)
+                    : tsb::launch_step2_f32_real(C, phase, a, warps, smem, blocks, st, bps);
     return imag ? tsb::launch_step_f32_imag(C, rot, phase, a, warps, smem, blocks, st, bps)
                 : tsb::launch_step_f32_real(C, rot, phase, a, warps, smem, blocks, st, bps);
 }
@@ -581,6 +589,14 @@ void choose_launch(ts_b200_kernel *k) {
 // three rows plus at least one in flight.
 int min_ring(const ts_b200_kernel *) { return 4; }
 
+// The look-ahead walk covers single-component cartesian tiles without a
+// rotating frame (phases 0-2); the other variants take the checked walk.
+bool use_walk2(const ts_b200_kernel *k) { return k->walk2 && !k->rot && !k->cyl && k->phase <= 2; }
+
+// Rows per segment as launched: the look-ahead walk needs even segments
+// (compile-time row parities).
+int eff_seg(const ts_b200_kernel *k) { return use_walk2(k) ? (k->seg_h + 1) & ~1 : k->seg_h; }
+
 // One round of tasks over the resident warps: as many row segments per strip
 // as there are resident warps per strip.
 // Rows per segment for a grid of `blocks_per_sm` blocks on every SM, one
@@ -592,7 +608,8 @@ int balanced_segments(const ts_b200_kernel *k, int blocks_per_sm, int warps) {
     const int strips = div_up(k->W, wo);
     const long rw = (long)blocks_per_sm * k->num_sms * warps;
     const int per_strip = (int)std::max(1L, rw / std::max(1, strips));
-    return std::max(8, div_up(k->H, per_strip));
+    const int seg = std::max(8, div_up(k->H, per_strip));
+    return use_walk2(k) ? (seg + 1) & ~1 : seg;
 }
 
 // Default: 4 blocks of 4 warps per SM (fewer, taller tasks than a grid
@@ -611,10 +628,16 @@ void geometry(const ts_b200_kernel *k, int *strips, int *segs, int *blocks, size
     const int hx = (k->rot || k->cyl) ? 8 : 4;  // Variant::HX
     const int wo = 32 * k->C - 2 * hx;
     *strips = div_up(k->W, wo);
-    *segs = div_up(k->H, k->seg_h);
+    *segs = div_up(k->H, eff_seg(k));
     const int tasks = *strips * *segs;
     *blocks = div_up(tasks, k->warps);
     if (k->resident_blocks > 0) *blocks = std::min(*blocks, k->resident_blocks);
+    if (use_walk2(k)) {
+        // per warp: 6 ring slots, the vertical pair coefficients, 6 mbarriers
+        *smem = (size_t)k->warps * (6 * slot_bytes(k->C, k->fp32, k->imag) +
+                                    tsb::w2_vlen(eff_seg(k)) * 2 * (k->fp32 ? 4 : 8) + 6 * 8);
+        return;
+    }
     // per warp: ring slots + one mbarrier per ring slot
     *smem = (size_t)k->warps *
             (k->ring * slot_bytes(k->C, k->fp32, k->imag, k->phase == 3 || k->phase == 7) +
@@ -711,8 +734,8 @@ int launch_step_buffers_t(ts_b200_kernel *k, const void *in, void *out, bool dry
         geometry(k, &strips, &segs, &blocks, &smem);
         StepArgs<T> a0{};
         int bps = 0;
-        cudaError_t e = dispatch_step<T>(k->C, k->imag, k->rot, k->phase, a0, k->warps, smem, 0,
-                                         k->stream, &bps);
+        cudaError_t e = dispatch_step<T>(k->C, k->imag, k->rot, k->phase, use_walk2(k), a0,
+                                         k->warps, smem, 0, k->stream, &bps);
         if (e != cudaSuccess) return cuda_fail(k, e, "step kernel configuration");
         if (bps < 1) return fail(k, TS_B200_UNSUPPORTED, "step kernel does not fit on an SM");
         k->resident_blocks = bps * k->num_sms;
@@ -733,11 +756,11 @@ int launch_step_buffers_t(ts_b200_kernel *k, const void *in, void *out, bool dry
     tsbh::fill_step_constants(k, a);
     a.n_strips = strips;
     a.n_segs = segs;
-    a.seg_h = k->seg_h;
-    a.ring = k->ring;
+    a.seg_h = eff_seg(k);
+    a.ring = use_walk2(k) ? 6 : k->ring;
     a.partials = k->partials;
-    cudaError_t e = dispatch_step<T>(k->C, k->imag, k->rot, k->phase, a, k->warps, smem, blocks,
-                                     k->stream, nullptr);
+    cudaError_t e = dispatch_step<T>(k->C, k->imag, k->rot, k->phase, use_walk2(k), a, k->warps,
+                                     smem, blocks, k->stream, nullptr);
     if (e != cudaSuccess) return cuda_fail(k, e, "step kernel launch");
     if (!dry) g_launches.fetch_add(1, std::memory_order_relaxed);
     return TS_B200_OK;
@@ -762,6 +785,15 @@ int launch_step(ts_b200_kernel *k, int exchange, bool dry = false) {
 }  // namespace
 
 int tsbh::launch_step_tile(ts_b200_kernel *k, int exchange) { return launch_step(k, exchange); }
+
+int tsbh::set_norm0(ts_b200_kernel *k, double norm0) {
+    if (!k->imag || !(norm0 > 0.0)) return fail(k, TS_B200_INVALID_ARGUMENT, "norm0");
+    if (k->d.norm0 != norm0) {
+        k->d.norm0 = norm0;
+        drop_graph(k);
+    }
+    return TS_B200_OK;
+}
 
 int tsbh::launch_step_buffers(ts_b200_kernel *k, const void *in, void *out) {
     return k->fp32 ? launch_step_buffers_t<float>(k, in, out, false)
@@ -1418,9 +1450,10 @@ int ts_b200_launch_info(const ts_b200_kernel *k, ts_b200_launch_shape *out) {
     size_t smem;
     geometry(k, &strips, &segs, &blocks, &smem);
     out->cells_per_lane = k->C;
-    out->segment_rows = k->seg_h;
+    out->segment_rows = eff_seg(k);
     out->warps_per_block = k->warps;
-    out->ring_depth = k->ring;
+    out->ring_depth = use_walk2(k) ? 6 : k->ring;
+    out->walk = use_walk2(k) ? 1 : 0;
     out->strips = strips;
     out->segments = segs;
     out->blocks = blocks;
@@ -1435,7 +1468,10 @@ int ts_b200_set_launch(ts_b200_kernel *k, int C, int seg_h, int warps, int ring)
     if (C == 4 && k->rot) return fail(k, TS_B200_UNSUPPORTED, "rotation kernels use 2 cells per lane");
     if (C == 4 && k->pair_mode) return fail(k, TS_B200_UNSUPPORTED, "pair kernels use 2 cells per lane");
     if (C == 4 && k->cyl) return fail(k, TS_B200_UNSUPPORTED, "cylindrical kernels use 2 cells per lane");
-    if (warps != 0 && warps != 1 && warps != 2 && warps != 4) return TS_B200_INVALID_ARGUMENT;
+    if (warps != 0 && warps != 1 && warps != 2 && warps != 4 && warps != 8)
+        return TS_B200_INVALID_ARGUMENT;
+    if (warps == 8 && !use_walk2(k))
+        return fail(k, TS_B200_UNSUPPORTED, "8 warps per block need the look-ahead walk");
     if (ring != 0 && (ring < min_ring(k) || ring > 16))
         return fail(k, TS_B200_INVALID_ARGUMENT, "ring depth out of range for this variant");
     if (seg_h < 0) return TS_B200_INVALID_ARGUMENT;
@@ -1451,6 +1487,16 @@ int ts_b200_set_launch(ts_b200_kernel *k, int C, int seg_h, int warps, int ring)
     size_t smem;
     geometry(k, &strips, &segs, &blocks, &smem);
     if (smem > 227 * 1024) return fail(k, TS_B200_INVALID_ARGUMENT, "ring does not fit in shared memory");
+    drop_graph(k);
+    return TS_B200_OK;
+}
+
+int ts_b200_set_walk(ts_b200_kernel *k, int walk) {
+    if (!k || (walk != 0 && walk != 1)) return TS_B200_INVALID_ARGUMENT;
+    if (k->walk2 == (walk == 1)) return TS_B200_OK;
+    k->walk2 = walk == 1;
+    if (!use_walk2(k) && k->warps > 4) k->warps = 4;
+    k->resident_blocks = 0;
     drop_graph(k);
     return TS_B200_OK;
 }

@@ -1,0 +1,518 @@
+// Streamed step without per-stage row checks ("look-ahead walk").
+//
+// Same work decomposition as step_kernel (a warp walks one strip of 32 x C
+// columns down a segment of rows, keeping a register window of rows and
+// running every stage of V0 H0 V1 H1 P H1 V1 H0 V0 one row behind the
+// previous one), arranged so that the row body carries no row checks:
+//
+//   * The walk of a segment with output rows [oy0, oy1) visits the rows
+//     oy0 - 4 .. oy1 + 3 (the 4 vertical sweeps spoil one row per sweep at
+//     each end of the walk, so these halo rows absorb everything that happens
+//     beyond them).  Rows of the walk outside the tile are not copied: their
+//     ring slot keeps an older row (finite values), which only ever meets a
+//     tile row through a vertical pair across the tile edge, and those pairs
+//     carry the identity (1, 0) from a per-warp table of pair coefficients
+//     (src/cpucartesian.cpp:4-70 skips them: closed boundary).  Every other
+//     stage needs no check at all.
+//   * The walk stores row c - 4 in the iteration that loads row c; with the
+//     4 halo rows below the segment the last stored row is finished in the
+//     iteration of the last loaded row, so there is no drain.
+//   * Ring slots and window rows are compile-time indices: the body is
+//     unrolled over 6 rows, which is the ring depth and the window height
+//     (the window holds the row being loaded one iteration ahead plus rows
+//     c .. c-4), and even, so row parities are compile-time as well.  The
+//     mbarriers are re-initialised for every task, so their phases are
+//     compile-time up to one bit per chunk.
+//   * Loads run one row ahead: the iteration of row c waits for row c + 1
+//     and moves it to registers while the stages of row c run, so the
+//     shared-memory latency is off the stage chain.
+//
+// Variants: single component, no rotating frame, cartesian (phases 0-2), 2 or
+// 4 cells per lane, both precisions and time modes.  The arithmetic of each
+// cell is that of step_kernel (the same pair forms, potential row and
+// reductions), so both give the same bits.
+#pragma once
+#include "step_kernel.cuh"
+#include "walk2_shape.h"
+
+namespace tsb {
+
+template <class V>
+struct W2Shape {
+    static constexpr int C = V::C;
+    static constexpr int NW = 6;      // window rows
+    static constexpr int D = 6;       // ring slots per warp
+    static constexpr int UNROLL = 6;  // rows per unrolled chunk
+    static constexpr int HX = 4, HY = 4;
+    static constexpr int SW = 32 * C, WO = SW - 2 * HX;
+    static constexpr int SLOT = V::PSI_BYTES + V::TAB_BYTES;
+    // vertical pair coefficients: entry j is the pair (u - 1, u) with
+    // u = ra + j - VPAD; the first stages of a walk read up to VPAD entries
+    // before the first row
+    static constexpr int VPAD = 4;
+    static_assert(!V::ROT && !V::PB && !V::CYL, "look-ahead walk: plain variants only");
+    static_assert(D == UNROLL && NW == UNROLL && UNROLL % 2 == 0, "compile-time slots and parities");
+};
+
+
+__device__ __forceinline__ void mbar_inval(uint64_t *bar) {
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+template <class V>
+struct Walk2 {
+    using T = typename V::T;
+    using TabT = typename V::TabT;
+    using S = W2Shape<V>;
+    static constexpr int C = V::C;
+
+    Cx<T> win[S::NW][C];
+    T hpa[C - 1], hpb[C - 1];  // this lane's horizontal pairs (i, i+1)
+    T hal, hbl, har, hbr;      // and its pairs with the neighbour lanes
+    bool out_col[C], norm_col[C], all_out;
+    int ra, nit, lane;
+    int n_lo, n_hi;  // iterations whose stored row is in the norm region
+    const unsigned char *gpsi, *gtab;  // row 0 of the strip's first copied column
+    size_t gpsi_pitch, gtab_pitch;
+    uint32_t psi_off, psi_bytes, tab_off, tab_bytes;
+    int H;
+    unsigned char *ring;
+    Cx<T> *vco;
+    uint64_t *bars;
+    Cx<T> *orow;  // row oy0 - 8 of the output at this lane's first column (moved per row)
+    size_t opitch;  // output row pitch in cells
+    double nacc;
+    bool failed;
+    int fail_idx;  // walk index whose wait gave up
+    T inv;
+    T aH, bH, aV, bV, ca, caa;
+
+    // copy row index `tp` of the walk into slot q, or complete the slot's
+    // phase without data for rows outside the tile or past the walk
+    __device__ __forceinline__ void issue(int tp, int q) {
+        if (lane == 0) {
+            const int row = ra + tp;
+            unsigned char *sb = ring + q * S::SLOT;
+            if (tp < nit && row >= 0 && row < H) {
+                mbar_expect_tx(&bars[q], psi_bytes + tab_bytes);
+                bulk_g2s(sb + psi_off, gpsi + (size_t)row * gpsi_pitch, psi_bytes, &bars[q]);
+                bulk_g2s(sb + V::PSI_BYTES + tab_off, gtab + (size_t)row * gtab_pitch, tab_bytes,
+                         &bars[q]);
+            } else {
+                mbar_arrive(&bars[q]);
+            }
+        }
+    }
+};
+
+// Cells of this lane from a ring slot row (vector loads of 16 bytes).
+template <typename T, int C>
+__device__ __forceinline__ void load_row_cells(const unsigned char *p, Cx<T> (&v)[C]) {
+    if constexpr (sizeof(T) == 4 && C % 2 == 0) {
+#pragma unroll
+        for (int i = 0; i < C; i += 2) {
+            const float4 q = reinterpret_cast<const float4 *>(p)[i / 2];
+            v[i] = Cx<T>{q.x, q.y};
+            v[i + 1] = Cx<T>{q.z, q.w};
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < C; ++i) v[i] = ld_cx_shared(reinterpret_cast<const Cx<T> *>(p) + i);
+    }
+}
+
+// Table values of this lane from a ring slot row.
+template <typename TabT, int C>
+__device__ __forceinline__ void load_tab_cells(const unsigned char *p, TabT (&v)[C]) {
+    constexpr int BYTES = C * (int)sizeof(TabT);
+    if constexpr (BYTES % 16 == 0) {
+        uint4 *d = reinterpret_cast<uint4 *>(v);
+#pragma unroll
+        for (int i = 0; i < BYTES / 16; ++i) d[i] = reinterpret_cast<const uint4 *>(p)[i];
+    } else if constexpr (BYTES % 8 == 0) {
+        uint2 *d = reinterpret_cast<uint2 *>(v);
+#pragma unroll
+        for (int i = 0; i < BYTES / 8; ++i) d[i] = reinterpret_cast<const uint2 *>(p)[i];
+    } else {
+#pragma unroll
+        for (int i = 0; i < C; ++i) v[i] = reinterpret_cast<const TabT *>(p)[i];
+    }
+}
+
+template <typename T, int C>
+__device__ __forceinline__ void store_row_cells(Cx<T> *o, const Cx<T> (&v)[C], const bool (&in)[C],
+                                                bool all) {
+    if constexpr (sizeof(T) == 4 && C % 2 == 0) {
+        if (all) {
+#pragma unroll
+            for (int i = 0; i < C; i += 2)
+                reinterpret_cast<float4 *>(o)[i / 2] =
+                    make_float4(v[i].re, v[i].im, v[i + 1].re, v[i + 1].im);
+            return;
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < C; ++i)
+        if (in[i]) st_cx_global(o + i, v[i]);
+}
+
+// One iteration: current row c = ra + t (t = base + K, base a multiple of 6).
+template <class V, int K>
+__device__ __forceinline__ void w2_row(Walk2<V> &w, int t, uint32_t ph) {
+    using T = typename V::T;
+    using TabT = typename V::TabT;
+    using S = W2Shape<V>;
+    constexpr int C = V::C;
+    constexpr bool IMAG = V::IMAG, PHASE = V::PHASE;
+    // row c - j lives in win[(K - j) mod 6]
+#define W2S(j) w.win[((K) - (j) + 2 * S::NW) % S::NW]
+    // ---- look-ahead: wait for row c + 1 and move it to the window
+    {
+        constexpr int q = (K + 1) % S::D;
+        const uint32_t par = (K + 1 < S::D) ? ph : (ph ^ 1u);
+        if (!mbar_wait_bounded(&w.bars[q], par)) {
+            w.failed = true;
+            w.fail_idx = t + 1;
+            return;
+        }
+        Cx<T> v[C];
+        load_row_cells<T, C>(w.ring + q * S::SLOT + C * (int)sizeof(Cx<T>) * w.lane, v);
+#pragma unroll
+        for (int i = 0; i < C; ++i) W2S(-1)[i] = IMAG ? scale_cx(v[i], w.inv) : v[i];
+    }
+    const Cx<T> *vc = w.vco + t + S::VPAD;
+    // ---- S1: V0 on rows (c-1, c)
+    {
+        const Cx<T> cv = vc[0];
+        vsweep<IMAG, C, ((K + 1) & 1)>(W2S(1), W2S(0), cv.re, cv.im);
+    }
+    // ---- S2: H0 on row c-1
+    hsweep_lanes<IMAG, ((K + 1) & 1), C>(W2S(1), w.hpa, w.hpb, w.hal, w.hbl, w.har, w.hbr);
+    // ---- S3: V1 on rows (c-2, c-1)
+    {
+        const Cx<T> cv = vc[-1];
+        vsweep<IMAG, C, ((K + 1) & 1)>(W2S(2), W2S(1), cv.re, cv.im);
+    }
+    // ---- S4: H1, P, H1 on row c-2 (table of row c-2 from its slot)
+    {
+        constexpr int q = (K + S::D - 2) % S::D;
+        hsweep_lanes<IMAG, ((K + 1) & 1), C>(W2S(2), w.hpa, w.hpb, w.hal, w.hbl, w.har, w.hbr);
+        alignas(16) TabT tv[C];
+        load_tab_cells<TabT, C>(w.ring + q * S::SLOT + V::PSI_BYTES + C * (int)sizeof(TabT) * w.lane,
+                                tv);
+        potential_row<IMAG, PHASE, V::LHY, false, C>(W2S(2), tv, w.ca, w.caa);
+        hsweep_lanes<IMAG, ((K + 1) & 1), C>(W2S(2), w.hpa, w.hpb, w.hal, w.hbl, w.har, w.hbr);
+    }
+    // ---- S5: V1 on rows (c-3, c-2)
+    {
+        const Cx<T> cv = vc[-2];
+        vsweep<IMAG, C, ((K) & 1)>(W2S(3), W2S(2), cv.re, cv.im);
+    }
+    // ---- S6: H0 on row c-3
+    hsweep_lanes<IMAG, ((K + 1) & 1), C>(W2S(3), w.hpa, w.hpb, w.hal, w.hbl, w.har, w.hbr);
+    // ---- S7: V0 on rows (c-4, c-3)
+    {
+        const Cx<T> cv = vc[-3];
+        vsweep<IMAG, C, ((K) & 1)>(W2S(4), W2S(3), cv.re, cv.im);
+    }
+    // ---- row c-4 is finished: store it (the first 8 rows of a walk are halo)
+    if (t >= 8) {
+        store_row_cells<T, C>(w.orow, W2S(4), w.out_col, w.all_out);
+        if (IMAG && t >= w.n_lo && t < w.n_hi) {
+#pragma unroll
+            for (int i = 0; i < C; ++i) {
+                const Cx<T> v = W2S(4)[i];
+                if (w.norm_col[i])
+                    w.nacc += (double)v.re * (double)v.re + (double)v.im * (double)v.im;
+            }
+        }
+    }
+    w.orow += w.opitch;
+    // ---- the slot of row c-2 is free: copy row c+4 into it
+    {
+        constexpr int q = (K + S::D - 2) % S::D;
+        __syncwarp();
+        if (w.lane == 0) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        w.issue(t + 4, q);
+    }
+#undef W2S
+}
+
+template <class V, int K>
+__device__ __forceinline__ bool w2_rows(Walk2<V> &w, int base, uint32_t ph) {
+    if constexpr (K < W2Shape<V>::UNROLL) {
+        const int t = base + K;
+        if (t >= w.nit) return false;
+        w2_row<V, K>(w, t, ph);
+        if (w.failed) return false;
+        return w2_rows<V, K + 1>(w, base, ph);
+    }
+    return true;
+}
+
+// One task: strip x segment, interior strips first.
+template <class V>
+__device__ __forceinline__ void w2_task(Walk2<V> &w, const StepArgs<typename V::T> &a, int task) {
+    using T = typename V::T;
+    using TabT = typename V::TabT;
+    using S = W2Shape<V>;
+    constexpr int C = V::C;
+    const int lane = w.lane;
+    int strip, seg;
+    {
+        const int n_int = a.n_strips > 2 ? (a.n_strips - 2) * a.n_segs : 0;
+        if (task < n_int) {
+            strip = 1 + task % (a.n_strips - 2);
+            seg = task / (a.n_strips - 2);
+        } else {
+            const int e = task - n_int;
+            const int n_edge_strips = a.n_strips > 2 ? 2 : a.n_strips;
+            const int es = e % n_edge_strips;
+            strip = (a.n_strips > 2 && es == 1) ? a.n_strips - 1 : es;
+            seg = e / n_edge_strips;
+        }
+    }
+    const int ox0 = strip * S::WO, ox1 = min(ox0 + S::WO, a.W);
+    const int c0 = ox0 - S::HX;
+    const int oy0 = seg * a.seg_h, oy1 = min(oy0 + a.seg_h, a.H);
+    w.ra = oy0 - S::HY;
+    w.nit = (oy1 - oy0) + 2 * S::HY;
+    w.n_lo = a.iy0 - oy0 + 8;
+    w.n_hi = a.iy1 - oy0 + 8;
+    const int cs = max(c0, 0);
+    const int ce = min(c0 + S::SW, a.P);
+    w.psi_off = (uint32_t)(cs - c0) * sizeof(Cx<T>);
+    w.psi_bytes = (uint32_t)(ce - cs) * sizeof(Cx<T>);
+    w.tab_off = (uint32_t)(cs - c0) * sizeof(TabT);
+    w.tab_bytes = (uint32_t)(ce - cs) * sizeof(TabT);
+    w.gpsi = reinterpret_cast<const unsigned char *>(a.psi_in) + (size_t)cs * sizeof(Cx<T>);
+    w.gtab = reinterpret_cast<const unsigned char *>(a.pot) + (size_t)cs * sizeof(TabT);
+    const int xl = c0 + C * lane;
+    bool present[C];
+    w.all_out = true;
+#pragma unroll
+    for (int i = 0; i < C; ++i) {
+        const int x = xl + i;
+        present[i] = x >= 0 && x < a.W;
+        w.out_col[i] = x >= ox0 && x < ox1;
+        w.norm_col[i] = w.out_col[i] && x >= a.ix0 && x < a.ix1;
+        w.all_out = w.all_out && w.out_col[i];
+    }
+    {
+        const T one = DeltaForm<T>::value ? T(0) : T(1);
+#pragma unroll
+        for (int i = 0; i + 1 < C; ++i) {
+            const bool p = present[i] && present[i + 1];
+            w.hpa[i] = p ? w.aH : one;
+            w.hpb[i] = p ? w.bH : T(0);
+        }
+        const bool pl = lane > 0 && present[0] && xl - 1 >= 0;
+        const bool pr = lane < 31 && present[C - 1] && xl + C < a.W;
+        w.hal = pl ? w.aH : one;
+        w.hbl = pl ? w.bH : T(0);
+        w.har = pr ? w.aH : one;
+        w.hbr = pr ? w.bH : T(0);
+        // vertical pairs (u - 1, u): the identity unless both rows are in the tile
+        const int vl = w2_vlen(a.seg_h);
+        for (int j = lane; j < vl; j += 32) {
+            const int u = w.ra + j - S::VPAD;
+            const bool ok = u >= 1 && u < a.H;
+            w.vco[j] = ok ? Cx<T>{w.aV, w.bV} : Cx<T>{one, T(0)};
+        }
+    }
+    w.orow = reinterpret_cast<Cx<T> *>(a.psi_out) + (ptrdiff_t)(oy0 - 8) * a.P + xl;
+    __syncwarp();  // the previous task's reads of the ring are done
+    if (c0 < 0 || c0 + S::SW > a.P) {
+        // cells of the strip outside the tile read as 0 (copies do not cover them)
+        uint32_t *ring32 = reinterpret_cast<uint32_t *>(w.ring);
+        for (int i = lane; i < S::D * S::SLOT / 4; i += 32) {
+            const uint32_t off = (uint32_t)(i * 4) % (uint32_t)S::SLOT;
+            bool copied;
+            if (off < (uint32_t)V::PSI_BYTES) {
+                copied = off >= w.psi_off && off < w.psi_off + w.psi_bytes;
+            } else {
+                const uint32_t tt = off - (uint32_t)V::PSI_BYTES;
+                copied = tt >= w.tab_off && tt < w.tab_off + w.tab_bytes;
+            }
+            if (!copied) ring32[i] = 0u;
+        }
+    }
+    __syncwarp();
+    if (lane == 0) {
+        // fresh barriers: every slot starts at phase 0 for this task
+#pragma unroll
+        for (int q = 0; q < S::D; ++q) {
+            mbar_inval(&w.bars[q]);
+            mbar_init(&w.bars[q], 1);
+        }
+        fence_mbar_init();
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < S::D - 2; ++q) w.issue(q, q);
+    // row 0 of the walk
+    if (!mbar_wait_bounded(&w.bars[0], 0u)) {
+        w.failed = true;
+        w.fail_idx = 0;
+    } else {
+        Cx<T> v[C];
+        load_row_cells<T, C>(w.ring + C * (int)sizeof(Cx<T>) * lane, v);
+#pragma unroll
+        for (int i = 0; i < C; ++i) w.win[0][i] = V::IMAG ? scale_cx(v[i], w.inv) : v[i];
+        for (int base = 0; !w.failed; base += S::UNROLL) {
+            const uint32_t ph = (uint32_t)(base / S::UNROLL) & 1u;
+            if (!w2_rows<V, 0>(w, base, ph)) break;
+        }
+    }
+    if (w.failed) {
+        if (lane == 0) atomicExch(&a.scal->error, 1);
+        // let the copies still in flight land before the block can exit:
+        // indices [0, 4) were issued before the walk and index t + 4 by each
+        // completed iteration t; the wait for index fail_idx gave up
+        const int issued_to = max(S::D - 2, w.fail_idx + 3);
+        for (int j = w.fail_idx; j < issued_to; ++j)
+            (void)mbar_wait_bounded(&w.bars[j % S::D], (uint32_t)(j / S::D) & 1u, 100000000ull);
+    }
+}
+
+// The end of a step launch, shared with step_kernel: in FP32 real time the
+// last block advances the coefficient schedule; in imaginary time the block
+// partials of the squared norm are summed in a fixed order by the last block,
+// which sets the renormalisation factor the next step applies.
+template <class V>
+__device__ __forceinline__ void w2_finish(const StepArgs<typename V::T> &a, double nacc, int warps,
+                                          int warp, int lane) {
+    if constexpr (!V::IMAG && DeltaForm<typename V::T>::value) {
+        if (a.kin_sched) {
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                __threadfence();
+                if (atomicAdd(&a.scal->ticket, 1u) == gridDim.x - 1) {
+                    a.scal->step += 1u;
+                    a.scal->ticket = 0u;
+                    __threadfence();
+                }
+            }
+        }
+    }
+    if constexpr (V::IMAG) {
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) nacc += __shfl_xor_sync(0xffffffffu, nacc, off);
+        __shared__ double s_warp[32];
+        __shared__ unsigned int s_last;
+        __shared__ double red[256];
+        if (lane == 0) s_warp[warp] = nacc;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double b = 0.0;
+            for (int i = 0; i < warps; ++i) b += s_warp[i];
+            a.partials[blockIdx.x] = b;
+            __threadfence();
+            const unsigned int t = atomicAdd(&a.scal->ticket, 1u);
+            s_last = (t == gridDim.x - 1) ? 1u : 0u;
+        }
+        __syncthreads();
+        if (s_last) {
+            __threadfence();
+            const int nb = gridDim.x;
+            double acc[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) acc[j] = 0.0;
+            for (int base = threadIdx.x; base < nb; base += 8 * (int)blockDim.x) {
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const int t = base + j * (int)blockDim.x;
+                    if (t < nb) acc[j] += __ldcg(&a.partials[t]);
+                }
+            }
+            red[threadIdx.x] =
+                ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
+            __syncthreads();
+            for (int h = blockDim.x >> 1; h > 0; h >>= 1) {
+                if ((int)threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+                __syncthreads();
+            }
+            if (threadIdx.x == 0) {
+                const double tot = red[0] * a.dxdy;
+                a.scal->last_norm = tot;
+                if (a.scal->renorm) a.scal->pending_inv = 1.0 / sqrt(tot / a.norm0);
+                a.scal->ticket = 0u;
+            }
+        }
+    }
+}
+
+// Blocks of 4 or 8 warps (the block partial reduction assumes a power of two
+// threads, at most 256); each warp loops over the tasks
+// t = warp_global, warp_global + total_warps, ...
+template <class V>
+__global__ void __launch_bounds__(256, 1) step2_kernel(StepArgs<typename V::T> a) {
+    using T = typename V::T;
+    using S = W2Shape<V>;
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int warps = blockDim.x >> 5;
+    const int warp = __shfl_sync(0xffffffffu, (int)(threadIdx.x >> 5), 0);
+    const int lane = threadIdx.x & 31;
+    const int n_tasks = a.n_strips * a.n_segs;
+    const int vl = w2_vlen(a.seg_h);
+
+    Walk2<V> w;
+    w.lane = lane;
+    w.nacc = 0.0;
+    w.failed = false;
+    w.H = a.H;
+    w.ring = smem + (size_t)warp * S::D * S::SLOT;
+    w.vco = reinterpret_cast<Cx<T> *>(smem + (size_t)warps * S::D * S::SLOT) + (size_t)warp * vl;
+    w.bars = reinterpret_cast<uint64_t *>(smem + (size_t)warps * S::D * S::SLOT +
+                                          (size_t)warps * vl * sizeof(Cx<T>)) +
+             warp * S::D;
+    w.opitch = (size_t)a.P;
+    {
+        uint4 *z = reinterpret_cast<uint4 *>(w.ring);
+        for (int i = lane; i < S::D * S::SLOT / 16; i += 32) z[i] = make_uint4(0u, 0u, 0u, 0u);
+    }
+    if (lane == 0) {
+        for (int q = 0; q < S::D; ++q) mbar_init(&w.bars[q], 1);
+        fence_mbar_init();
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncwarp();
+    // finite window contents before the first task (the first rows of every
+    // walk meet whatever the window holds only in halo rows)
+#pragma unroll
+    for (int j = 0; j < S::NW; ++j)
+#pragma unroll
+        for (int i = 0; i < V::C; ++i) w.win[j][i] = Cx<T>{T(0), T(0)};
+    // step constants
+    w.inv = V::IMAG ? (T)a.scal->pending_inv : T(1);
+    w.aH = a.aH;
+    w.bH = a.bH;
+    w.aV = a.aV;
+    w.bV = a.bV;
+    if constexpr (DeltaForm<T>::value && !V::IMAG) {
+        if (a.kin_sched) {
+            const unsigned int step = __ldcg(&a.scal->step);
+            const float4 c = __ldg(&a.kin_sched[step % (unsigned int)a.sched_len]);
+            w.aH = c.x;
+            w.bH = c.y;
+            w.aV = c.z;
+            w.bV = c.w;
+        }
+    }
+    w.ca = a.ca;
+    w.caa = a.caa;
+    w.gpsi_pitch = (size_t)a.P * sizeof(Cx<T>);
+    w.gtab_pitch = (size_t)a.P * sizeof(typename V::TabT);
+
+    for (int task = blockIdx.x * warps + warp; task < n_tasks && !w.failed;
+         task += gridDim.x * warps)
+        w2_task(w, a, task);
+
+    w2_finish<V>(a, w.nacc, warps, warp, lane);
+}
+
+}  // namespace tsb

@@ -17,9 +17,13 @@
  *    rotation coordinates are the extended tile coordinates, as the
  *    reference's formulas give them.
  *  - Energies, norms and expectation values are reduced on the GPU in FP64.
- *  - Two-component systems (Hamiltonian2Component), cylindrical coordinates
- *    and BesselState are declared for source compatibility but the B200
- *    kernel rejects them at Solver construction.
+ *  - Two-component systems (Hamiltonian2Component, the two-state Solver, Rabi
+ *    coupling) and cylindrical lattices run on the B200 kernel
+ *    (B200PairKernel, the cylindrical step variants).  Not supported, as on
+ *    the reference's own GPU path: two components with a rotating frame or the
+ *    Lee-Huang-Yang term, and cylindrical lattices with a rotating frame.
+ *    BesselState is not provided (cylindrical states come from
+ *    init_state_matrix).
  */
 #ifndef TS_B200_TROTTERSUZUKI_H
 #define TS_B200_TROTTERSUZUKI_H

@@ -66,6 +66,7 @@ class LaunchShape(C.Structure):
         ("warps_per_block", C.c_int32), ("ring_depth", C.c_int32),
         ("strips", C.c_int32), ("segments", C.c_int32), ("blocks", C.c_int32),
         ("threads", C.c_int32), ("smem_bytes", C.c_int64),
+        ("walk", C.c_int32), ("reserved", C.c_int32),
     ]
 
 
@@ -108,6 +109,7 @@ SIGNATURES = {
     "ts_b200_launch_info": (_I, [_VP, C.POINTER(LaunchShape)]),
     "ts_b200_set_launch": (_I, [_VP, _I, _I, _I, _I]),
     "ts_b200_autotune": (_I, [_VP, _I]),
+    "ts_b200_set_walk": (_I, [_VP, _I]),
     "ts_b200_batch_create": (_I, [C.POINTER(_VP), _I, C.POINTER(_VP)]),
     "ts_b200_batch_destroy": (None, [_VP]),
     "ts_b200_batch_size": (_I, [_VP]),

@@ -28,11 +28,28 @@ def _stale(obj, deps):
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+def _includes(path, seen=None):
+    """Files under csrc/ and include/ that `path` includes, recursively."""
+    seen = set() if seen is None else seen
+    try:
+        text = open(path).read()
+    except OSError:
+        return seen
+    for line in text.splitlines():
+        line = line.strip()
+        if line.startswith("#include \""):
+            name = line.split('"')[1]
+            for d in (CSRC, INCLUDE):
+                f = os.path.join(d, name)
+                if os.path.exists(f) and f not in seen:
+                    seen.add(f)
+                    _includes(f, seen)
+    return seen
+
+
 def _compile(src, extra):
     obj = os.path.join(BUILD, os.path.basename(src) + ".o")
-    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
-    headers.append(os.path.join(INCLUDE, "ts_b200.h"))
-    if _stale(obj, [src] + headers):
+    if _stale(obj, [src] + sorted(_includes(src))):
         cmd = [NVCC] + ARCH + FLAGS + extra + ["-c", src, "-o", obj + ".tmp"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:

@@ -153,6 +153,10 @@ class Kernel:
         self._check(lib().ts_b200_set_launch(self._h, cells_per_lane, segment_rows,
                                              warps_per_block, ring_depth))
 
+    def set_walk(self, walk):
+        """1: look-ahead row walk (default where the variant has one), 0: checked walk."""
+        self._check(lib().ts_b200_set_walk(self._h, int(walk)))
+
 
 class Batch:
     """Many tiles advanced together, one persistent launch per Trotter step.
