@@ -333,10 +333,11 @@ def run_b200_arm(args, rank, world, local, pg):
     shape = _capi.LaunchShape()
     L.ts_b200_launch_info(handle, C.byref(shape))
 
-    # energies of the final FP64 state (for the FP32 comparison)
+    # energies and tile of the final FP64 state (for the FP32 comparison)
     solver.evolve(0, True)  # copies the tile back (get_sample)
     e64 = solver.get_total_energy()
     n64 = solver.get_squared_norm()
+    psi64 = state.get_state()
 
     # ---- e2e: through the C ABI with pinned host buffers, every step copies
     # the state in (H2D) and the result out (D2H)
@@ -392,12 +393,48 @@ def run_b200_arm(args, rank, world, local, pg):
         solver32.evolve(0, True)
         e32 = solver32.get_total_energy()
         n32 = solver32.get_squared_norm()
+        d = state.get_state() - psi64
         v32 = world * site_steps / (ms32 * 1e-3)
         fp32 = {"value": v32, "unit": "site-steps/s", "speedup_vs_fp64": v32 / value,
                 "rel_energy_err_vs_fp64": abs(e32 - e64) / abs(e64),
                 "rel_norm_err_vs_fp64": abs(n32 - n64) / abs(n64),
+                "rel_psi_l2_err_vs_fp64": float(np.linalg.norm(d) / np.linalg.norm(psi64)),
+                "max_abs_psi_err_vs_fp64": float(np.abs(d).max()),
+                "trotter_steps_compared": (args.warmup + args.steps) * TROTTER_PER_STEP + 1,
                 "bytes_per_site_step": BYTES_PER_SITE_STEP["fp32"]}
         del solver32
+
+    # ---- the metric's other two parts, on their own configurations: FP64
+    # against FP32 storage on the precision configuration (8192^2 periodic
+    # rotating-frame GPE, 5000 steps) and the adjoint/forward cost with its
+    # finite-difference check (512^2 real time, 3000 steps)
+    precision = adjoint = None
+    if not args.no_configs:
+        torch.cuda.empty_cache()
+        vres, vclk, _ = vortex_leg(args, local, pg, device, stream, conditioning=False)
+        precision = {
+            "config": vortex_config(),
+            "fp64": {k: vres["fp64"][k] for k in ("value", "us_per_launch", "roofline", "energy",
+                                                   "norm", "launch")},
+            "fp32_store": dict({k: vres["fp32"][k] for k in ("value", "us_per_launch",
+                                                             "roofline", "energy", "norm",
+                                                             "launch")},
+                               speedup_vs_fp64=vres["fp32"]["value"] / vres["fp64"]["value"]),
+            "fp32_vs_fp64_errors": vres["errors_fp32"],
+            "clocks": vclk,
+        }
+        torch.cuda.empty_cache()
+        aout, aclk, _ = adjoint_leg(args, local, device, stream)
+        adjoint = {
+            "config": {"workload": "adjoint512", "lattice": f"{ADJ_N}x{ADJ_N}",
+                       "length": ADJ_LENGTH, "dt": ADJ_DT, "trotter_steps": ADJ_STEPS,
+                       "boundary": "closed", "loss": "sum_{x>0} |psi(T)|^2 dx dy"},
+            "runs": {k: {kk: v[kk] for kk in ("adjoint_over_forward", "forward_ms", "adjoint_ms",
+                                              "fd_rel_err", "fd_sites", "checkpoint_every", "g",
+                                              "imag_time")}
+                     for k, v in aout.items()},
+            "clocks": aclk,
+        }
 
     if rank != 0:
         return
@@ -438,6 +475,8 @@ def run_b200_arm(args, rank, world, local, pg):
                         "pinned host buffers"},
         "roofline": roofline,
         "fp32_store": fp32,
+        "precision_config": precision,
+        "adjoint_config": adjoint,
         "cpu_baseline": cpu,
         "clocks": clk,
         "gpu_launches": launches,
@@ -685,24 +724,30 @@ def adjoint_setup(n=ADJ_N, seed=ADJ_SEED):
     return V, psi0.astype(np.complex128), mask, dx, sites
 
 
-def run_adjoint_workload(args, rank, world, local, pg):
+# (label, g, checkpoint interval, imaginary time)
+ADJ_CASES = (("linear_inverse_steps", 0.0, 0, False), ("gpe_g50_checkpoint100", 50.0, 100, False),
+             ("imag_gpe_g50_checkpoint100", 50.0, 100, True))
+
+
+def adjoint_leg(args, local, device, stream, cases=ADJ_CASES, n_sites=ADJ_SITES):
+    """Forward and adjoint runs of the differentiation configuration, timed on
+    the device, with central finite differences of the B200 forward pass at
+    `n_sites` seeded sites."""
     import torch
-    torch.cuda.set_device(local)
-    device = torch.device("cuda", local)
     import trottersuzuki_b200 as ts
     from trottersuzuki_b200 import launch_count
     from trottersuzuki_b200.adjoint import AdjointEngine
     V, psi0, mask, dx, sites = adjoint_setup()
+    sites = sites[:n_sites]
     dA = dx * dx
-    stream = torch.cuda.Stream(device=device)
     m = torch.tensor(mask, device=device)
     out = {}
     clk = None
     launches = 0
-    for label, g, every in (("linear_inverse_steps", 0.0, 0), ("gpe_g50_checkpoint100", 50.0, 100)):
+    for label, g, every, imag in cases:
         grid = ts.Lattice2D(ADJ_N, ADJ_LENGTH)
         ham = ts.Hamiltonian(grid, None, 1.0, g)
-        desc = ts.make_desc(grid, ham, ADJ_DT)
+        desc = ts.make_desc(grid, ham, ADJ_DT, imag_time=imag, norm=1.0 if imag else 0.0)
         eng = AdjointEngine(desc, ADJ_DT, ADJ_STEPS, every)
         with torch.cuda.stream(stream):
             Vt = torch.tensor(V, dtype=torch.float64, device=device)
@@ -768,8 +813,17 @@ def run_adjoint_workload(args, rank, world, local, pg):
             "fd_rel_err": {"dL_dV": rel(gv[ys, xs], fd_v), "dL_dre_psi0": rel(gp.real[ys, xs], fd_r),
                            "dL_dim_psi0": rel(gp.imag[ys, xs], fd_i)},
             "fd_sites": len(sites), "fd_step": {"V": hv, "psi0": hp},
-            "checkpoint_every": every, "g": g}
+            "checkpoint_every": every, "g": g, "imag_time": imag}
         eng.close()
+    return out, clk, launches
+
+
+def run_adjoint_workload(args, rank, world, local, pg):
+    import torch
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    stream = torch.cuda.Stream(device=device)
+    out, clk, launches = adjoint_leg(args, local, device, stream)
     if rank != 0:
         return
     lin = out["linear_inverse_steps"]
@@ -817,44 +871,55 @@ VORTEX_BYTES = {"fp64": 48, "fp32": 24}
 
 
 def vortex_initial(grid):
+    """Thomas-Fermi profile times 8 windings, evaluated with torch in FP64 on
+    the current device (the 8192^2 tile is 1 GiB; numpy would take ~20 s)."""
+    import torch
     from trottersuzuki_b200.api import _coordinate_grid
     X, Y = _coordinate_grid(grid)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    x = torch.tensor(np.ascontiguousarray(X[0, :]), dtype=torch.float64, device=dev)[None, :]
+    y = torch.tensor(np.ascontiguousarray(Y[:, 0]), dtype=torch.float64, device=dev)[:, None]
     rng = np.random.Generator(np.random.PCG64(VORTEX_SEED))
     r = 10.0 * np.sqrt(rng.uniform(0.0, 1.0, 8))
     phi = rng.uniform(0.0, 2.0 * math.pi, 8)
     centres = np.stack([r * np.cos(phi), r * np.sin(phi)], axis=1)
     mu = math.sqrt(VORTEX_G / math.pi)
-    dens = np.maximum(0.0, (mu - 0.5 * (X * X + Y * Y)) / VORTEX_G)
-    psi = np.sqrt(dens).astype(np.complex128)
+    dens = torch.clamp((mu - 0.5 * (x * x + y * y)) / VORTEX_G, min=0.0)
+    theta = torch.zeros_like(dens)
     for cx, cy in centres:
-        psi *= np.exp(1j * np.arctan2(Y - cy, X - cx))
-    return psi, centres
+        theta += torch.atan2(y - float(cy), x - float(cx))
+    amp = torch.sqrt(dens)
+    re = (amp * torch.cos(theta)).cpu().numpy()
+    im = (amp * torch.sin(theta)).cpu().numpy()
+    del x, y, dens, theta, amp
+    return re, im, centres
 
 
-def run_vortex_workload(args, rank, world, local, pg):
+def vortex_leg(args, local, pg, device, stream, conditioning=True, steps=VORTEX_STEPS):
+    """The precision configuration: FP64 and FP32-storage runs of `steps`
+    Trotter steps from the same psi0 (and, with `conditioning`, FP64 from psi0
+    rounded to float), timed on the device; errors of FP32 against FP64."""
     import torch
-    torch.cuda.set_device(local)
-    device = torch.device("cuda", local)
     import trottersuzuki_b200 as ts
     from trottersuzuki_b200 import _capi, launch_count
     L = _capi.lib()
-    stream = torch.cuda.Stream(device=device)
     res = {}
     clk = None
     launches = 0
     psi64 = None
-    # fp64: the oracle run; fp32: FP32 storage; fp64_from_fp32_psi0: FP64 from
-    # psi0 rounded to float (the conditioning of the configuration: how much
-    # an initial perturbation of FP32 rounding size grows by time T)
-    for kernel_type, prec in (("gpu", "fp64"), ("gpu_fp32", "fp32"),
-                              ("gpu", "fp64_from_fp32_psi0")):
+    inner = None
+    runs = [("gpu", "fp64"), ("gpu_fp32", "fp32")]
+    if conditioning:
+        runs.append(("gpu", "fp64_from_fp32_psi0"))
+    for kernel_type, prec in runs:
         grid = ts.Lattice2D(VORTEX_N, VORTEX_LENGTH, periodic_x_axis=True, periodic_y_axis=True,
                             angular_velocity=VORTEX_OMEGA)
         state = ts.State(grid)
-        psi0, centres = vortex_initial(grid)
+        re0, im0, centres = vortex_initial(grid)
         if prec == "fp64_from_fp32_psi0":
-            psi0 = psi0.astype(np.complex64).astype(np.complex128)
-        state.init_state_matrix(psi0.real, psi0.imag)
+            re0 = re0.astype(np.float32).astype(np.float64)
+            im0 = im0.astype(np.float32).astype(np.float64)
+        state.init_state_matrix(re0, im0)
         pot = ts.HarmonicPotential(grid, 1.0, 1.0)
         ham = ts.Hamiltonian(grid, pot, 1.0, VORTEX_G, 0.0, VORTEX_OMEGA)
         solver = ts.Solver(grid, state, ham, VORTEX_DT, kernel_type=kernel_type)
@@ -862,7 +927,8 @@ def run_vortex_workload(args, rank, world, local, pg):
         # warm-up steps, then the state is reset and the kernel rebuilt from it
         solver.evolve(-args.warmup)
         torch.cuda.synchronize()
-        state.init_state_matrix(psi0.real, psi0.imag)
+        state.init_state_matrix(re0, im0)
+        del re0, im0
         solver.update_parameters()
         solver.evolve(0)
         h = solver.kernel_handle()
@@ -873,19 +939,29 @@ def run_vortex_workload(args, rank, world, local, pg):
         l0 = launch_count()
         with Clocks(local) as clocks:
             ev0.record(stream)
-            solver.evolve(-VORTEX_STEPS)
+            solver.evolve(-steps)
             ev1.record(stream)
             ev1.synchronize()
         ms = max_over_ranks(ev0.elapsed_time(ev1), pg, device)
         if prec == "fp64":
             clk = clocks.summary()
             launches = launch_count() - l0
+        shape = _capi.LaunchShape()
+        L.ts_b200_launch_info(C.c_void_p(h), C.byref(shape))
         solver.evolve(0)  # copies the tile back
         psi = np.array(state.p_real) + 1j * np.array(state.p_imag)
         sh = VORTEX_N * VORTEX_N
-        res[prec] = {"value": world * sh * VORTEX_STEPS / (ms * 1e-3), "ms": ms,
+        peak, peak_kind = measured_peak()
+        bpl = VORTEX_BYTES["fp32" if prec == "fp32" else "fp64"] * sh
+        ach = bpl / (ms / steps * 1e-3) / 1e9
+        res[prec] = {"value": pg_world(pg) * sh * steps / (ms * 1e-3), "ms": ms,
+                     "us_per_launch": ms / steps * 1e3,
                      "energy": solver.get_total_energy(), "norm": solver.get_squared_norm(),
-                     "initial_energy": e0_energy}
+                     "initial_energy": e0_energy,
+                     "roofline": {"achieved": ach, "peak": peak, "unit": "GB/s",
+                                  "frac": ach / peak, "peak_kind": peak_kind,
+                                  "algorithmic_bytes_per_launch": bpl},
+                     "launch": {k: getattr(shape, k) for k, _ in _capi.LaunchShape._fields_}}
         if prec == "fp64":
             psi64 = psi
             inner = (slice(grid.inner_start_y - grid.start_y, grid.inner_end_y - grid.start_y),
@@ -899,31 +975,47 @@ def run_vortex_workload(args, rank, world, local, pg):
                 "norm_rel": abs(res[prec]["norm"] - res["fp64"]["norm"]) / abs(res["fp64"]["norm"]),
                 "energy_rel": abs(res[prec]["energy"] - res["fp64"]["energy"]) /
                               abs(res["fp64"]["energy"])}
-        del solver, ham, pot, state, grid
+        del solver, ham, pot, state, grid, psi
         torch.cuda.synchronize()
+    return res, clk, launches
+
+
+def pg_world(pg):
+    import torch.distributed as dist
+    return dist.get_world_size() if pg else 1
+
+
+def vortex_config(steps=VORTEX_STEPS):
+    return {"workload": "vortex8192_precision", "lattice": f"{VORTEX_N}x{VORTEX_N}",
+            "length": VORTEX_LENGTH, "boundary": "periodic", "g": VORTEX_G,
+            "omega_rot": VORTEX_OMEGA, "dt": VORTEX_DT, "trotter_steps": steps,
+            "initial": "Thomas-Fermi x 8 windings (radius 10)", "seed": VORTEX_SEED}
+
+
+def run_vortex_workload(args, rank, world, local, pg):
+    import torch
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    stream = torch.cuda.Stream(device=device)
+    res, clk, launches = vortex_leg(args, local, pg, device, stream, conditioning=True)
     if rank != 0:
         return
-    peak, peak_kind = measured_peak()
-    ms_launch = res["fp64"]["ms"] / VORTEX_STEPS
-    achieved = VORTEX_BYTES["fp64"] * VORTEX_N * VORTEX_N / (ms_launch * 1e-3) / 1e9
+    r64 = res["fp64"]["roofline"]
     line = {
         "metric": "site-steps/s", "value": res["fp64"]["value"], "unit": "site-steps/s",
         "n_gpus": world, "steps": 1, "warmup": args.warmup,
         "ms_per_step": res["fp64"]["ms"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "vortex8192_precision", "lattice": f"{VORTEX_N}x{VORTEX_N}",
-                   "length": VORTEX_LENGTH, "boundary": "periodic", "g": VORTEX_G,
-                   "omega_rot": VORTEX_OMEGA, "dt": VORTEX_DT, "trotter_steps": VORTEX_STEPS,
-                   "initial": "Thomas-Fermi x 8 windings (radius 10)", "seed": VORTEX_SEED,
-                   "parallelism": f"replicas{world}",
-                   "l2": "inputs larger than L2: 3 GiB moved per Trotter step in FP64"},
+        "config": dict(vortex_config(), parallelism=f"replicas{world}",
+                       l2="inputs larger than L2: 3 GiB moved per Trotter step in FP64"),
         "fp64": res["fp64"],
         "fp32_store": dict(res["fp32"], speedup_vs_fp64=res["fp32"]["value"] / res["fp64"]["value"]),
         "fp32_vs_fp64_errors": res["errors_fp32"],
         "fp64_from_fp32_rounded_psi0_vs_fp64": res["errors_fp64_from_fp32_psi0"],
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
-                     "algorithmic_bytes_per_launch": VORTEX_BYTES["fp64"] * VORTEX_N * VORTEX_N,
+        "roofline": {"bound": "hbm", "achieved": r64["achieved"], "peak": r64["peak"],
+                     "unit": "GB/s", "frac": r64["frac"], "peak_kind": r64["peak_kind"],
+                     "traffic": None,
+                     "algorithmic_bytes_per_launch": r64["algorithmic_bytes_per_launch"],
                      "kernel": "tsb::step_kernel<double, C=2, real, rotating frame, GPE> + halo"},
         "clocks": clk,
         "gpu_launches": launches,
@@ -1280,6 +1372,8 @@ def main():
                     help="seconds of reference CPU work per sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32", action="store_true")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the precision (8192^2) and adjoint (512^2) legs of the default run")
     ap.add_argument("--no-ref-gpu", action="store_true",
                     help="reference arm: skip timing the reference's CUDA kernel")
     ap.add_argument("--workload", choices=["gpe_imaginary_time_2048", "batch512", "adjoint512",

@@ -223,7 +223,7 @@ int ts_b200_synchronize(ts_b200_kernel *k);
 
 /* Geometry of the fused step launch chosen for this tile (for reporting):
  * cells per lane, rows per segment, warps per block, ring depth, tasks, and
- * the row walk (0 checked, 1 look-ahead). */
+ * the row walk (0 checked; 1 or 2: look-ahead, rows per iteration). */
 typedef struct {
     int32_t cells_per_lane, segment_rows, warps_per_block, ring_depth;
     int32_t strips, segments, blocks, threads;
@@ -238,12 +238,23 @@ int ts_b200_launch_info(const ts_b200_kernel *k, ts_b200_launch_shape *out);
 int ts_b200_set_launch(ts_b200_kernel *k, int cells_per_lane, int segment_rows, int warps_per_block,
                        int ring_depth);
 
-/* Row walk of the fused step (no counterpart in the reference; both walks
- * perform the same operations per cell): 1 (default) the look-ahead walk,
+/* Row walk of the fused step (no counterpart in the reference; every walk
+ * performs the same operations per cell): 2 (default) the look-ahead walk,
  * which single-component cartesian tiles without a rotating frame use, with
- * even segments, ring depth 6 and 4 or 8 warps per block; 0 the checked walk
- * of every variant.  Variants without a look-ahead walk ignore the choice. */
+ * even segments, a ring of 6 rows, 4 or 8 warps per block and two rows per
+ * iteration (one mbarrier per row pair; with 4 cells per lane one row); 1 the
+ * same walk with one row per iteration; 0 the checked walk of every variant.  Variants without a
+ * look-ahead walk ignore the choice.  ts_b200_launch_info reports the rows per
+ * iteration in use (0 for the checked walk). */
 int ts_b200_set_walk(ts_b200_kernel *k, int walk);
+
+/* The look-ahead walk launches each fused step with a programmatic
+ * dependency on the previous kernel of the stream (on = 1, the default): the
+ * step's blocks are scheduled as the previous step's blocks retire and set up
+ * their shared memory, then wait for the previous kernel to complete before
+ * they read the tile.  on = 0 launches each step after the previous kernel
+ * has completed.  No counterpart in the reference. */
+int ts_b200_set_overlap(ts_b200_kernel *k, int on);
 
 /* ---- Batched evolution (no counterpart in the reference, which evolves one
  * lattice per Solver; the batch replaces a loop of per-tile evolve() calls).
@@ -372,9 +383,10 @@ int ts_b200_pair_destroy(ts_b200_pair *p);
 
 /* Autotuner for this tile: times `trial_steps` steps for each balanced launch
  * shape (rows per segment such that every SM holds the same number of
- * blocks, for 1 .. the resident blocks per SM, 4 or 2 warps per block) and
- * for segments of 32, 64 and 128 rows taken by the persistent warps in turn,
- * and keeps the fastest.  The trials read the current state and write the other
+ * blocks, for 1 .. the resident blocks per SM, 4 or 2 warps per block; 4 or 8
+ * with the look-ahead walk, each with and without programmatic dependent
+ * launch) and for segments of 32, 64 and 128 rows taken by the persistent
+ * warps in turn, and keeps the fastest.  The trials read the current state and write the other
  * buffer, the scalars a step updates are restored: the state is unchanged.
  * Synchronises the tile's stream.  No counterpart in the reference. */
 int ts_b200_autotune(ts_b200_kernel *k, int trial_steps);

@@ -80,7 +80,8 @@ class Result2(C.Structure):
 _libs = {}
 
 
-_NAMES = {"parity": "libtsref.so", "fast": "libtsref_fast.so", "gpu": "libtsref_gpu.so"}
+_NAMES = {"parity": "libtsref.so", "fast": "libtsref_fast.so", "gpu": "libtsref_gpu.so",
+          "b200": "libtsref_b200.so"}
 
 
 def available(flavour="parity"):

@@ -56,13 +56,14 @@ CASES = [
 ]
 
 
+@pytest.mark.parametrize("walk", [1, 2])
 @pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
-def test_look_ahead_walk_matches_oracle_and_checked_walk(case):
+def test_look_ahead_walk_matches_oracle_and_checked_walk(case, walk):
     _, N, L, Ny, per, g, lhy, imag, steps = case
     lat, psi0, V = seeded_case(N, L, Ny, per)
     p, tr, ti, ref = _oracle(lat, psi0, V, 1e-3, imag, g, lhy, steps)
-    got, shape = _gpu(p, psi0, tr, ti, steps, walk=1)
-    assert shape["walk"] == 1
+    got, shape = _gpu(p, psi0, tr, ti, steps, walk=walk)
+    assert shape["walk"] == walk
     assert np.abs(got - ref).max() <= TOL_PSI
     old, shape0 = _gpu(p, psi0, tr, ti, steps, walk=0)
     assert shape0["walk"] == 0
@@ -81,13 +82,15 @@ def test_look_ahead_walk_matches_oracle_and_checked_walk(case):
     dict(cells_per_lane=2, segment_rows=300, warps_per_block=2),
 ])
 @pytest.mark.parametrize("imag", [False, True], ids=["real", "imag"])
-def test_look_ahead_walk_launch_shapes(launch, imag):
+@pytest.mark.parametrize("walk", [1, 2])
+def test_look_ahead_walk_launch_shapes(launch, imag, walk):
     """Any strip/segment cut of the look-ahead walk gives the checked walk's
     bits (real time) and the oracle's result at the parity bar."""
     lat, psi0, V = seeded_case(333, 12.0, 290, (False, False))
     p, tr, ti, ref = _oracle(lat, psi0, V, 1e-3, imag, 3.0, 0.0, 9)
-    got, shape = _gpu(p, psi0, tr, ti, 9, walk=1, launch=launch, split=[4, 5])
-    assert shape["walk"] == 1 and shape["segment_rows"] % 2 == 0
+    got, shape = _gpu(p, psi0, tr, ti, 9, walk=walk, launch=launch, split=[4, 5])
+    rows = walk if launch["cells_per_lane"] == 2 else 1
+    assert shape["walk"] == rows and shape["segment_rows"] % 2 == 0
     assert np.abs(got - ref).max() <= TOL_PSI
     if not imag:
         old, _ = _gpu(p, psi0, tr, ti, 9, walk=0, split=[4, 5])
@@ -95,8 +98,8 @@ def test_look_ahead_walk_launch_shapes(launch, imag):
 
 
 @pytest.mark.parametrize("imag", [False, True], ids=["real", "imag"])
-@pytest.mark.parametrize("cells", [2, 4])
-def test_look_ahead_walk_fp32(imag, cells):
+@pytest.mark.parametrize("cells,walk", [(2, 1), (2, 2), (4, 1)])
+def test_look_ahead_walk_fp32(imag, cells, walk):
     """FP32 storage through the look-ahead walk: the checked walk's bits in
     real time (the same float arithmetic per cell), the FP32 bar against the
     FP64 oracle."""
@@ -104,8 +107,8 @@ def test_look_ahead_walk_fp32(imag, cells):
     lat, psi0, V = seeded_case(257, 12.0, 203, (False, False))
     p, tr, ti, ref = _oracle(lat, psi0, V, 1e-3, imag, 3.0, 0.0, 15)
     launch = dict(cells_per_lane=cells, segment_rows=24)
-    got, shape = _gpu(p, psi0, tr, ti, 15, walk=1, launch=launch, precision=_capi.FP32)
-    assert shape["walk"] == 1
+    got, shape = _gpu(p, psi0, tr, ti, 15, walk=walk, launch=launch, precision=_capi.FP32)
+    assert shape["walk"] == walk
     assert np.abs(got - ref).max() <= 2e-5 * np.abs(ref).max()
     old, _ = _gpu(p, psi0, tr, ti, 15, walk=0, launch=launch, precision=_capi.FP32)
     if imag:

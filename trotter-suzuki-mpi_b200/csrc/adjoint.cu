@@ -9,6 +9,12 @@
 // reverse pass recomputes each segment's states from its checkpoint (forward
 // step kernel into a segment buffer) and runs the adjoint steps over them in
 // reverse.
+// IMAGINARY mode (imaginary time, checkpoints): as CHECKPOINT, with the
+// renormalisation after every step: the forward pass takes norm0 = N(psi_0)
+// (read back once per forward: it is a launch parameter of the step), each
+// checkpoint keeps its tile with the pending factor c, the recomputation
+// records every step's factor, and the reverse pass of each step also reads
+// the next state for the transposed renormalisation.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -38,6 +44,14 @@ struct ts_b200_adjoint {
     int *error = nullptr;
     int seg_h = 32, warps = 2, ring = 4, blocks = 0;
     bool forward_done = false;
+    // imaginary time: factors c of the checkpoints and of a segment's states,
+    // the projection coefficients mu (ping-pong), the running sum of the
+    // inner products, block partials and ticket of the reductions; norm0
+    bool imag = false;
+    double *ckpt_c = nullptr, *seg_c = nullptr, *mu = nullptr, *ksum = nullptr;
+    double *partials = nullptr;
+    unsigned int *ticket = nullptr;
+    double norm0 = 0.0;
     void *state0 = nullptr;           // a segment's first state (graph-fixed address)
     cudaGraphExec_t inv_graph = nullptr;  // kInvGraphSteps inverse adjoint steps
     cudaGraphExec_t seg_graph = nullptr;  // one full checkpoint segment
@@ -65,6 +79,70 @@ int acuda(ts_b200_adjoint *a, cudaError_t e, const char *what) {
         if (e_ != cudaSuccess) return acuda(a, e_, #call);   \
     } while (0)
 
+// exp(-V dt) per cell (imaginary time, real table, src/solver.cpp:74-109);
+// padding columns [W, P) get 0.
+__global__ void table_imag_from_potential_kernel(const double *V, int W, int H, int P, double dt,
+                                                 double *tab) {
+    const size_t n = (size_t)P * H;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const int y = (int)(i / P), x = (int)(i % P);
+        tab[i] = x < W ? exp(-V[(size_t)y * W + x] * dt) : 0.0;
+    }
+}
+
+// Re<Lambda, c phi> over the tile (W x H, pitch P; Lambda of pitch W) with c
+// the pending factor of phi: block sums, then the last block adds them in a
+// fixed order and writes mu = scale * sum and the running sum (= the sum).
+__global__ void adj_dot_kernel(const Cx<double> *lam, const Cx<double> *phi, const double *c,
+                               int W, int H, int P, double scale, double *partials,
+                               unsigned int *ticket, double *mu, double *ksum) {
+    double s = 0.0;
+    const size_t n = (size_t)W * H;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const size_t y = i / W, x = i % W;
+        const Cx<double> l = lam[i], f = phi[y * P + x];
+        s = __fma_rn(l.re, f.re, __fma_rn(l.im, f.im, s));
+    }
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    __shared__ double sw[8];
+    __shared__ unsigned int last;
+    if ((threadIdx.x & 31) == 0) sw[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double b = 0.0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) b += sw[i];
+        partials[blockIdx.x] = b;
+        __threadfence();
+        last = (atomicAdd(ticket, 1u) == gridDim.x - 1) ? 1u : 0u;
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        double tot = 0.0;
+        for (int i = 0; i < (int)gridDim.x; ++i) tot += __ldcg(&partials[i]);
+        tot *= *c;
+        *mu = scale * tot;
+        *ksum = tot;
+        *ticket = 0u;
+    }
+}
+
+// dL/dpsi_0 = Lambda_0 + (dA / norm0) (sum of Re<Lambda_k, psi_k>, k >= 1) psi_0:
+// the gradient through norm0 = N(psi_0).  Output of pitch W.
+__global__ void adj_grad_psi0_kernel(const Cx<double> *lam, const Cx<double> *psi0, int W, int H,
+                                     int P, double scale, const double *ksum, Cx<double> *out) {
+    const double m = scale * *ksum;
+    const size_t n = (size_t)W * H;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const size_t y = i / W, x = i % W;
+        const Cx<double> l = lam[y * P + x], p = psi0[y * P + x];
+        out[i] = Cx<double>{__fma_rn(m, p.re, l.re), __fma_rn(m, p.im, l.im)};
+    }
+}
+
 // exp(-i V dt) per cell (the reference tabulates it with std::exp(complex),
 // src/solver.cpp:74-109); padding columns [W, P) get 0.
 __global__ void table_from_potential_kernel(const double *V, int W, int H, int P, double dt,
@@ -90,12 +168,13 @@ void *ckpt_at(ts_b200_adjoint *a, int j) {
     return static_cast<unsigned char *>(a->ckpt) + (size_t)j * state_bytes(a);
 }
 
-void *seg_at(ts_b200_adjoint *a, int j) {  // recomputed state j (1 .. every-1)
+void *seg_at(ts_b200_adjoint *a, int j) {  // recomputed state j (1 .. every-1; .. every imag)
     return static_cast<unsigned char *>(a->seg) + (size_t)(j - 1) * state_bytes(a);
 }
 
 size_t adj_smem(const ts_b200_adjoint *a) {
-    return (size_t)a->warps * (a->ring * AdjVariant<0, 0>::SLOT + 8 * a->ring);
+    const int slot = a->imag ? AdjVariant<2, 0>::SLOT : AdjVariant<0, 0>::SLOT;
+    return (size_t)a->warps * (a->ring * slot + 8 * a->ring);
 }
 
 template <class A>
@@ -121,6 +200,11 @@ cudaError_t launch_adj_variant(ts_b200_adjoint *a, const AdjArgs &args, int bloc
 cudaError_t launch_adj(ts_b200_adjoint *a, int mode, int phase, const AdjArgs &args, int blocks,
                        int *bps) {
     if (mode == 0) return launch_adj_variant<AdjVariant<0, 0>>(a, args, blocks, bps);
+    if (mode == 2) {
+        if (phase == 2) return launch_adj_variant<AdjVariant<2, 2>>(a, args, blocks, bps);
+        if (phase == 1) return launch_adj_variant<AdjVariant<2, 1>>(a, args, blocks, bps);
+        return launch_adj_variant<AdjVariant<2, 0>>(a, args, blocks, bps);
+    }
     if (phase == 2) return launch_adj_variant<AdjVariant<1, 2>>(a, args, blocks, bps);
     if (phase == 1) return launch_adj_variant<AdjVariant<1, 1>>(a, args, blocks, bps);
     return launch_adj_variant<AdjVariant<1, 0>>(a, args, blocks, bps);
@@ -146,7 +230,36 @@ AdjArgs adj_args(ts_b200_adjoint *a) {
     x.ca = d.coupling;
     x.caa = d.lhy_coupling;
     x.dt = a->dt;
+    x.partials = a->partials;
+    x.ticket = a->ticket;
+    x.kappa_sum = a->ksum;
+    x.mu_scale = a->imag ? a->k->d.delta_x * a->k->d.delta_y / a->norm0 : 0.0;
     return x;
+}
+
+// One reverse imaginary-time step: psi_k = c_k phi_k (phi_k at psi_k_in, c_k
+// at *c_k), Lambda_{k+1} and psi_{k+1} (phi at psn, c at *c_n); mu_{k+1} in,
+// mu_k out; `accumulate` adds Re<Lambda_k, psi_k> to the running sum.
+int adj_step_imag(ts_b200_adjoint *a, const void *psi_k_in, const double *c_k, const void *psn,
+                  const double *c_n, const void *lam_in, void *lam_out, const double *mu_in,
+                  double *mu_out, bool accumulate) {
+    AdjArgs x = adj_args(a);
+    x.psi_in = psi_k_in;
+    x.psi_out = nullptr;
+    x.lam_in = lam_in;
+    x.lam_out = lam_out;
+    x.psn_in = psn;
+    x.c_in = c_k;
+    x.c_next = c_n;
+    x.mu_next = mu_in;
+    x.mu_out = mu_out;
+    x.accumulate = accumulate ? 1 : 0;
+    const int tasks = x.n_strips * x.n_segs;
+    const int blocks = std::max(1, std::min(a->blocks, div_up(tasks, a->warps)));
+    cudaError_t e = launch_adj(a, 2, a->k->phase, x, blocks, nullptr);
+    if (e != cudaSuccess) return acuda(a, e, "adjoint kernel launch");
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    return TS_B200_OK;
 }
 
 int adj_step(ts_b200_adjoint *a, int mode, const void *psi_in, void *psi_out, const void *lam_in,
@@ -191,6 +304,34 @@ int capture(ts_b200_adjoint *a, cudaGraphExec_t *exec, F body) {
     return TS_B200_OK;
 }
 
+// Imaginary time: recompute states 1 .. len of the segment from a->state0
+// (factor seg_c[0]), each step's factor into seg_c[i], then len reverse steps
+// (lambda ping-pongs from lam[l], mu from mu[l]); `first` is the global index
+// of the segment's first step (the step 0 pass adds nothing to the sum).
+int segment_pass_imag(ts_b200_adjoint *a, int len, int l, int first) {
+    ts_b200_kernel *k = a->k;
+    int s = TS_B200_OK;
+    cudaError_t e = cudaMemcpyAsync(&k->scal->pending_inv, &a->seg_c[0], sizeof(double),
+                                    cudaMemcpyDeviceToDevice, k->stream);
+    if (e != cudaSuccess) return acuda(a, e, "segment factor");
+    for (int i = 1; i <= len && s == TS_B200_OK; ++i) {
+        s = tile_status(a, tsbh::launch_step_buffers(k, i == 1 ? a->state0 : seg_at(a, i - 1),
+                                                     seg_at(a, i)));
+        if (s == TS_B200_OK) {
+            e = cudaMemcpyAsync(&a->seg_c[i], &k->scal->pending_inv, sizeof(double),
+                                cudaMemcpyDeviceToDevice, k->stream);
+            if (e != cudaSuccess) return acuda(a, e, "segment factor");
+        }
+    }
+    for (int i = len - 1; i >= 0 && s == TS_B200_OK; --i) {
+        const void *psi_n = i == 0 ? a->state0 : seg_at(a, i);
+        s = adj_step_imag(a, psi_n, &a->seg_c[i], seg_at(a, i + 1), &a->seg_c[i + 1], a->lam[l],
+                          a->lam[l ^ 1], &a->mu[l], &a->mu[l ^ 1], first + i > 0);
+        l ^= 1;
+    }
+    return s;
+}
+
 // Reverse pass of one checkpoint segment of `len` steps starting from the
 // state in a->state0: recompute states 1 .. len-1, then len adjoint steps
 // (lambda ping-pongs from lam[l]).
@@ -216,14 +357,16 @@ int ts_b200_adjoint_create(const ts_b200_desc *d, double delta_t, int steps, int
     if (!out) return TS_B200_INVALID_ARGUMENT;
     *out = nullptr;
     if (!d || steps < 1 || checkpoint_every < 0 || !(delta_t > 0.0)) return TS_B200_INVALID_ARGUMENT;
-    if (d->imag_time || d->precision != TS_B200_FP64 || d->periodic_x || d->periodic_y ||
+    if (d->precision != TS_B200_FP64 || d->periodic_x || d->periodic_y ||
         (d->alpha_x != 0.0 && d->alpha_y != 0.0) || d->cylindrical)
-        return TS_B200_UNSUPPORTED;  // real time, FP64, closed cartesian tile, no rotating frame
-    if (checkpoint_every == 0 && (d->coupling != 0.0 || d->lhy_coupling != 0.0))
-        return TS_B200_INVALID_ARGUMENT;  // inverse steps need the linear step
+        return TS_B200_UNSUPPORTED;  // FP64, closed cartesian tile, no rotating frame
+    if (checkpoint_every == 0 && (d->coupling != 0.0 || d->lhy_coupling != 0.0 || d->imag_time))
+        return TS_B200_INVALID_ARGUMENT;  // inverse steps need the linear unitary step
     ts_b200_adjoint *a = new (std::nothrow) ts_b200_adjoint();
     if (!a) return TS_B200_OUT_OF_MEMORY;
-    int s = ts_b200_create(d, &a->k);
+    ts_b200_desc dd = *d;
+    if (dd.imag_time) dd.norm0 = 1.0;  // renormalised; the forward pass sets N(psi_0)
+    int s = ts_b200_create(&dd, &a->k);
     if (s) {
         delete a;
         return s;
@@ -231,6 +374,7 @@ int ts_b200_adjoint_create(const ts_b200_desc *d, double delta_t, int steps, int
     a->dt = delta_t;
     a->steps = steps;
     a->every = checkpoint_every;
+    a->imag = d->imag_time != 0;
     a->W = a->k->W;
     a->H = a->k->H;
     a->P = a->k->P;
@@ -247,13 +391,22 @@ int ts_b200_adjoint_create(const ts_b200_desc *d, double delta_t, int steps, int
     if (a->every > 0) {
         a->n_ckpt = (steps + a->every - 1) / a->every;  // states at 0, every, 2 every, ...
         alloc(&a->ckpt, sb * a->n_ckpt);
-        if (a->every > 1) alloc(&a->seg, sb * (a->every - 1));
+        // imaginary time also recomputes the next segment's first state
+        const int nseg = a->imag ? a->every : a->every - 1;
+        if (nseg > 0) alloc(&a->seg, sb * nseg);
         alloc(&a->state0, sb);
+    }
+    if (a->imag) {
+        alloc(reinterpret_cast<void **>(&a->ckpt_c), sizeof(double) * a->n_ckpt);
+        alloc(reinterpret_cast<void **>(&a->seg_c), sizeof(double) * (a->every + 1));
+        alloc(reinterpret_cast<void **>(&a->mu), sizeof(double) * 2);
+        alloc(reinterpret_cast<void **>(&a->ksum), sizeof(double));
+        alloc(reinterpret_cast<void **>(&a->ticket), sizeof(unsigned int));
     }
     if (e == cudaSuccess) {
         int bps = 0;
         AdjArgs x{};
-        e = launch_adj(a, a->every > 0 ? 1 : 0, a->k->phase, x, 0, &bps);
+        e = launch_adj(a, a->imag ? 2 : (a->every > 0 ? 1 : 0), a->k->phase, x, 0, &bps);
         if (e == cudaSuccess && bps < 1) e = cudaErrorInvalidConfiguration;
         a->blocks = bps * a->k->num_sms;
         // one round of tasks over the resident warps (the tile is often small)
@@ -261,6 +414,9 @@ int ts_b200_adjoint_create(const ts_b200_desc *d, double delta_t, int steps, int
         const int per_strip = std::max(1, a->blocks * a->warps / strips);
         a->seg_h = std::max(8, div_up(a->H, per_strip));
         a->seg_h += a->seg_h & 1;
+        // block partials of the reductions (adjoint steps and the dot kernel)
+        if (a->imag) alloc(reinterpret_cast<void **>(&a->partials),
+                           sizeof(double) * std::max(a->blocks, 1024));
     }
     if (e != cudaSuccess) {
         const int st = e == cudaErrorMemoryAllocation ? TS_B200_OUT_OF_MEMORY : TS_B200_CUDA_ERROR;
@@ -281,6 +437,12 @@ void ts_b200_adjoint_destroy(ts_b200_adjoint *a) {
     cudaFree(a->seg);
     cudaFree(a->error);
     cudaFree(a->state0);
+    cudaFree(a->ckpt_c);
+    cudaFree(a->seg_c);
+    cudaFree(a->mu);
+    cudaFree(a->ksum);
+    cudaFree(a->partials);
+    cudaFree(a->ticket);
     if (a->inv_graph) cudaGraphExecDestroy(a->inv_graph);
     if (a->seg_graph) cudaGraphExecDestroy(a->seg_graph);
     ts_b200_destroy(a->k);
@@ -298,16 +460,41 @@ int ts_b200_adjoint_forward(ts_b200_adjoint *a, const double *potential, const v
     ts_b200_kernel *k = a->k;
     const size_t n = (size_t)a->P * a->H;
     const int grid = (int)std::min<size_t>((n + 255) / 256, 4096);
-    table_from_potential_kernel<<<grid, 256, 0, k->stream>>>(
-        potential, a->W, a->H, a->P, a->dt, static_cast<Cx<double> *>(k->tab));
+    if (a->imag)
+        table_imag_from_potential_kernel<<<grid, 256, 0, k->stream>>>(
+            potential, a->W, a->H, a->P, a->dt, static_cast<double *>(k->tab));
+    else
+        table_from_potential_kernel<<<grid, 256, 0, k->stream>>>(
+            potential, a->W, a->H, a->P, a->dt, static_cast<Cx<double> *>(k->tab));
     TSBA_CHECK(a, cudaGetLastError());
     g_launches.fetch_add(1, std::memory_order_relaxed);
     int s = tile_status(a, ts_b200_set_state_device(k, psi0, (size_t)a->W));
     if (s) return s;
+    if (a->imag) {
+        // norm0 = N(psi_0), the norm every step restores (src/solver.cpp:155);
+        // a launch parameter of the step, so the graphs follow a new value
+        double n0 = 0.0;
+        s = tile_status(a, ts_b200_squared_norm(k, &n0));
+        if (s) return s;
+        if (!(n0 > 0.0)) return afail(a, TS_B200_INVALID_ARGUMENT, "psi0 has zero norm");
+        if (n0 != a->norm0) {
+            a->norm0 = n0;
+            s = tile_status(a, tsbh::set_norm0(k, n0));
+            if (s) return s;
+            if (a->seg_graph) {
+                cudaGraphExecDestroy(a->seg_graph);
+                a->seg_graph = nullptr;
+            }
+        }
+    }
     if (a->every > 0) {
         for (int j = 0; j < a->n_ckpt; ++j) {
             TSBA_CHECK(a, cudaMemcpyAsync(ckpt_at(a, j), k->psi[k->cur], state_bytes(a),
                                           cudaMemcpyDeviceToDevice, k->stream));
+            if (a->imag)
+                TSBA_CHECK(a, cudaMemcpyAsync(&a->ckpt_c[j], &k->scal->pending_inv,
+                                              sizeof(double), cudaMemcpyDeviceToDevice,
+                                              k->stream));
             const int len = std::min(a->every, a->steps - j * a->every);
             s = tile_status(a, ts_b200_evolve(k, len));
             if (s) return s;
@@ -332,6 +519,60 @@ int ts_b200_adjoint_backward(ts_b200_adjoint *a, const void *grad_psi_t, double 
     TSBA_CHECK(a, cudaMemsetAsync(a->gv, 0, (size_t)a->P * a->H * sizeof(double), k->stream));
     int l = 0;
     int s = TS_B200_OK;
+    if (a->imag) {
+        // mu_T and the running sum from Re<Lambda_T, psi_T>, psi_T = c_T phi_T
+        TSBA_CHECK(a, cudaMemsetAsync(a->ticket, 0, sizeof(unsigned int), k->stream));
+        const double scale = k->d.delta_x * k->d.delta_y / a->norm0;
+        adj_dot_kernel<<<std::min(1024, div_up((long)a->W * a->H, 256)), 256, 0, k->stream>>>(
+            static_cast<const Cx<double> *>(grad_psi_t), static_cast<const Cx<double> *>(k->psi[k->cur]),
+            &k->scal->pending_inv, a->W, a->H, a->P, scale, a->partials, a->ticket, &a->mu[0],
+            a->ksum);
+        TSBA_CHECK(a, cudaGetLastError());
+        g_launches.fetch_add(1, std::memory_order_relaxed);
+        for (int j = a->n_ckpt - 1; j >= 0 && s == TS_B200_OK; --j) {
+            const int len = std::min(a->every, a->steps - j * a->every);
+            TSBA_CHECK(a, cudaMemcpyAsync(a->state0, ckpt_at(a, j), state_bytes(a),
+                                          cudaMemcpyDeviceToDevice, k->stream));
+            TSBA_CHECK(a, cudaMemcpyAsync(&a->seg_c[0], &a->ckpt_c[j], sizeof(double),
+                                          cudaMemcpyDeviceToDevice, k->stream));
+            if (len == a->every && (len & 1) == 0 && j > 0) {
+                // full segments of an even length leave lambda and mu in [l]
+                if (!a->seg_graph) {
+                    s = capture(a, &a->seg_graph, [&] { return segment_pass_imag(a, len, 0, 1); });
+                    if (s) return s;
+                }
+                if (l != 0) {  // the graph starts from lam[0], mu[0]
+                    TSBA_CHECK(a, cudaMemcpyAsync(a->lam[0], a->lam[1], state_bytes(a),
+                                                  cudaMemcpyDeviceToDevice, k->stream));
+                    TSBA_CHECK(a, cudaMemcpyAsync(&a->mu[0], &a->mu[1], sizeof(double),
+                                                  cudaMemcpyDeviceToDevice, k->stream));
+                    l = 0;
+                }
+                TSBA_CHECK(a, cudaGraphLaunch(a->seg_graph, k->stream));
+                g_launches.fetch_add(2 * len, std::memory_order_relaxed);
+            } else {
+                s = segment_pass_imag(a, len, l, j * a->every);
+                if (len & 1) l ^= 1;
+            }
+        }
+        if (s) return s;
+        a->forward_done = false;
+        if (grad_potential)
+            TSBA_CHECK(a, cudaMemcpy2DAsync(grad_potential, a->W * sizeof(double), a->gv,
+                                            a->P * sizeof(double), a->W * sizeof(double), a->H,
+                                            cudaMemcpyDeviceToDevice, k->stream));
+        if (grad_psi0) {
+            // psi_0 is checkpoint 0 (factor 1: a state set from outside)
+            adj_grad_psi0_kernel<<<std::min(1024, div_up((long)a->W * a->H, 256)), 256, 0,
+                                   k->stream>>>(
+                static_cast<const Cx<double> *>(a->lam[l]),
+                static_cast<const Cx<double> *>(ckpt_at(a, 0)), a->W, a->H, a->P, scale, a->ksum,
+                static_cast<Cx<double> *>(grad_psi0));
+            TSBA_CHECK(a, cudaGetLastError());
+            g_launches.fetch_add(1, std::memory_order_relaxed);
+        }
+        return TS_B200_OK;
+    }
     if (a->every == 0) {
         // ping-pong from (psi[cur], lam[0]); runs of kInvGraphSteps replayed
         int c = k->cur;  // psi(T)

@@ -25,10 +25,34 @@
 //    the transposed stages on lambda, mapping (psi_n, lambda_{n+1}) to
 //    lambda_n.
 //
+// IMAGINARY (imaginary time, checkpoints): the forward step is
+// phi_{k+1} = S(psi_k), psi_{k+1} = c_{k+1} phi_{k+1} with
+// c = sqrt(norm0 / N(phi)) (src/cpukernel.cpp:551-562), N(x) = dA sum |x|^2.
+// Every imaginary-time pair matrix [[a, b], [b, a]] (src/cpucartesian.cpp:
+// 25-44,59-70) is symmetric, so the transposed sweeps are the sweeps
+// themselves; the potential stage psi' = f E x (E = exp(-V dt) from the real
+// table, f = exp(-theta(|x|^2)), src/cpucartesian.cpp:128-136) has
+//     lambda = f E (lambda' - 2 theta' s x),  s = Re(conj(lambda') x),
+//     dL/dV += -dt f E s.
+// The pass of step k reads psi_k (stored phi_k with its factor c_k) and the
+// adjoint Lambda_{k+1} = dL/dpsi_{k+1}; it applies the transpose of the
+// renormalisation as the rows arrive,
+//     lambda = c_{k+1} (Lambda_{k+1} - mu_{k+1} psi_{k+1}),
+//     mu_{k+1} = (dA / norm0) Re<Lambda_{k+1}, psi_{k+1}>,
+// which needs psi_{k+1} (stored phi_{k+1}, factor c_{k+1}) as a third field.
+// The pass also produces mu_k for the next pass: Re<Lambda_k, psi_k> with
+// Lambda_k = J^T lambda equals Re<K_2^T lambda, J_P chi> summed over the
+// cells (J = K_2 J_P K_1, K_1 the stages before the potential, K_2 those
+// after, chi = K_1 psi_k), and both factors are in registers at the
+// potential stage: J_P chi = f E (1 - 2 theta' |chi|^2) chi.  The owned cells
+// add it to a per-lane sum, the blocks' sums meet in a fixed order in the
+// last block to finish, which writes mu_k (and adds the sum to the running
+// total the gradient of the initial norm needs).
+//
 // The walk is the forward kernel's (column strips of 32 lanes x 2 cells,
 // a 5-row register window per field, rows streamed through a shared-memory
-// ring by bulk copies); each ring slot holds a row of psi, lambda, the table
-// and dL/dV.
+// ring by bulk copies); each ring slot holds a row of psi, lambda, (in
+// imaginary time) psi_{k+1}, the table and dL/dV.
 #pragma once
 #include "step_kernel.cuh"
 
@@ -46,17 +70,33 @@ struct AdjArgs {
     int n_strips, n_segs, seg_h, ring;
     double aH, bH, aV, bV;
     double ca, caa, dt;  // g dt, g_LHY dt, dt
+    // IMAGINARY: psi_{k+1} (stored phi_{k+1}), the factors c_k, c_{k+1}, the
+    // projection coefficient mu_{k+1} in, mu_k out, the running sum of the
+    // inner products (added to when `accumulate`), dA / norm0, and the
+    // per-block partials with the ticket of the last block
+    const void *psn_in;
+    const double *c_in, *c_next, *mu_next;
+    double *mu_out, *kappa_sum;
+    double *partials;
+    unsigned int *ticket;
+    double mu_scale;
+    int accumulate;
 };
 
 template <int MODE_, int PHASE_>
 struct AdjVariant {
-    static constexpr int MODE = MODE_;  // 0 INVERSE, 1 CHECKPOINT
+    static constexpr int MODE = MODE_;  // 0 INVERSE, 1 CHECKPOINT, 2 IMAGINARY
     static constexpr int PHASE = PHASE_;
+    static constexpr bool IMAG = MODE_ == 2;
     static constexpr int C = 2, NWIN = 5, HX = 4, HY = 4, UNROLL = 10, OUT_LAG = 4;
     static constexpr int SW = 64, WO = SW - 2 * HX;
     static constexpr int ROW = SW * 16;             // bytes of one Cx<double> row
-    static constexpr int GV_OFF = 3 * ROW;          // slot: psi | lambda | table | dL/dV
-    static constexpr int SLOT = 3 * ROW + SW * 8;
+    // slot: psi | lambda | [psi_{k+1}] | table | dL/dV
+    static constexpr int PSN_OFF = 2 * ROW;
+    static constexpr int TAB_OFF = IMAG ? 3 * ROW : 2 * ROW;
+    static constexpr int TAB_CELL = IMAG ? 8 : 16;  // real table in imaginary time
+    static constexpr int GV_OFF = TAB_OFF + SW * TAB_CELL;
+    static constexpr int SLOT = GV_OFF + SW * 8;
 };
 
 struct AdjWalk {
@@ -66,6 +106,9 @@ struct AdjWalk {
     int lslot, tslot, issued_to, loaded_to;
     uint32_t phase_bits;
     const unsigned char *gpsi, *glam, *gtab, *ggv;  // row 0, column cs
+    const unsigned char *gpsn;                      // IMAGINARY: psi_{k+1}
+    double cin, cnext, m2;  // IMAGINARY: c_k, c_{k+1}, mu_{k+1} c_{k+1}
+    double kacc;            // IMAGINARY: this lane's part of Re<Lambda_k, psi_k>
     size_t pitch16, pitch8;
     uint32_t off16, bytes16, off8, bytes8;
     unsigned char *ring;
@@ -77,20 +120,30 @@ struct AdjWalk {
     template <class A>
     __device__ __forceinline__ void issue(int row, int q) {
         unsigned char *sb = ring + q * A::SLOT;
-        mbar_expect_tx(&bars[q], 3 * bytes16 + bytes8);
-        bulk_g2s(sb + off16, gpsi + (size_t)row * pitch16, bytes16, &bars[q]);
-        bulk_g2s(sb + A::ROW + off16, glam + (size_t)row * pitch16, bytes16, &bars[q]);
-        bulk_g2s(sb + 2 * A::ROW + off16, gtab + (size_t)row * pitch16, bytes16, &bars[q]);
-        bulk_g2s(sb + A::GV_OFF + off8, ggv + (size_t)row * pitch8, bytes8, &bars[q]);
+        if constexpr (A::IMAG) {
+            mbar_expect_tx(&bars[q], 3 * bytes16 + 2 * bytes8);
+            bulk_g2s(sb + off16, gpsi + (size_t)row * pitch16, bytes16, &bars[q]);
+            bulk_g2s(sb + A::ROW + off16, glam + (size_t)row * pitch16, bytes16, &bars[q]);
+            bulk_g2s(sb + A::PSN_OFF + off16, gpsn + (size_t)row * pitch16, bytes16, &bars[q]);
+            bulk_g2s(sb + A::TAB_OFF + off8, gtab + (size_t)row * pitch8, bytes8, &bars[q]);
+            bulk_g2s(sb + A::GV_OFF + off8, ggv + (size_t)row * pitch8, bytes8, &bars[q]);
+        } else {
+            mbar_expect_tx(&bars[q], 3 * bytes16 + bytes8);
+            bulk_g2s(sb + off16, gpsi + (size_t)row * pitch16, bytes16, &bars[q]);
+            bulk_g2s(sb + A::ROW + off16, glam + (size_t)row * pitch16, bytes16, &bars[q]);
+            bulk_g2s(sb + A::TAB_OFF + off16, gtab + (size_t)row * pitch16, bytes16, &bars[q]);
+            bulk_g2s(sb + A::GV_OFF + off8, ggv + (size_t)row * pitch8, bytes8, &bars[q]);
+        }
     }
     __device__ __forceinline__ int next(int q) const { return q + 1 == D ? 0 : q + 1; }
 };
 
-// Horizontal sweep; NEG: the transposed (inverse) rotation.
-template <int PAR, bool NEG>
+// Horizontal sweep; NEG: the transposed (inverse) rotation; IM: the
+// imaginary-time pair matrix (symmetric: its own transpose).
+template <int PAR, bool NEG, bool IM = false>
 __device__ __forceinline__ void adj_h(AdjWalk &w, Cx<double> (&row)[2]) {
     const double s = NEG ? -1.0 : 1.0;
-    hsweep_lane<false, PAR>(row, w.hai, s * w.hbi, w.hal, s * w.hbl, w.har, s * w.hbr);
+    hsweep_lane<IM, PAR>(row, w.hai, s * w.hbi, w.hal, s * w.hbl, w.har, s * w.hbr);
 }
 
 // Potential stage of row u (both fields at this point of the pipeline).
@@ -98,10 +151,40 @@ template <class A>
 __device__ __forceinline__ void adj_potential(AdjWalk &w, const AdjArgs &a, Cx<double> (&ps)[2],
                                               Cx<double> (&la)[2], int q, int u) {
     const unsigned char *sb = w.ring + q * A::SLOT;
-    const Cx<double> *tp = reinterpret_cast<const Cx<double> *>(sb + 2 * A::ROW) + 2 * w.lane;
     const double *gp = reinterpret_cast<const double *>(sb + A::GV_OFF) + 2 * w.lane;
     const bool out_row = u >= w.oy0 && u < w.oy1;
     double *grow = a.gv + (size_t)u * a.P + w.xl;
+    if constexpr (A::IMAG) {
+        const double *ep = reinterpret_cast<const double *>(sb + A::TAB_OFF) + 2 * w.lane;
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            // psi is chi (the stage's input), lambda is at the stage's output
+            const Cx<double> x = ps[i];
+            const Cx<double> l = la[i];
+            const double n2 = __fma_rn(x.re, x.re, __dmul_rn(x.im, x.im));
+            double th = 0.0, dth = 0.0;
+            if (A::PHASE) {
+                th = __dmul_rn(a.ca, n2);
+                dth = a.ca;
+                if (A::PHASE == 2) {
+                    const double r = sqrt(n2);
+                    th = __fma_rn(a.caa, __dmul_rn(n2, r), th);
+                    dth = __fma_rn(1.5 * a.caa, r, dth);
+                }
+            }
+            const double fe = A::PHASE ? __dmul_rn(phase_expneg(th), ep[i]) : ep[i];
+            const double sd = __fma_rn(l.re, x.re, __dmul_rn(l.im, x.im));
+            const double k2 = 2.0 * dth * sd;
+            if (out_row && w.out_col[i]) {
+                grow[i] = __fma_rn(-a.dt, __dmul_rn(fe, sd), gp[i]);
+                w.kacc = __fma_rn(__dmul_rn(fe, __fma_rn(-2.0 * dth, n2, 1.0)), sd, w.kacc);
+            }
+            la[i].re = __dmul_rn(fe, __fma_rn(-k2, x.re, l.re));
+            la[i].im = __dmul_rn(fe, __fma_rn(-k2, x.im, l.im));
+        }
+        return;
+    }
+    const Cx<double> *tp = reinterpret_cast<const Cx<double> *>(sb + A::TAB_OFF) + 2 * w.lane;
 #pragma unroll
     for (int i = 0; i < 2; ++i) {
         const Cx<double> e = ld_cx_shared(tp + i);
@@ -153,12 +236,16 @@ template <class A, int K, bool GUARD>
 __device__ __forceinline__ void adj_row(AdjWalk &w, const AdjArgs &a, int r) {
     constexpr int NWIN = 5;
     constexpr bool INV = A::MODE == 0;
+    constexpr bool IM = A::IMAG;
 #define PS(j) w.ps[((K) - (j) + 2 * NWIN) % NWIN]
 #define LA(j) w.la[((K) - (j) + 2 * NWIN) % NWIN]
     const int ra = w.ra, rb = w.rb;
     const double aV = w.aVv, bV = w.bVv;
-    // psi: inverse rotations (INVERSE) or forward ones (CHECKPOINT)
+    // psi: inverse rotations (INVERSE) or forward ones (CHECKPOINT, IMAGINARY);
+    // lambda: the transposed stages (b -> -b in real time, the same in
+    // imaginary time)
     const double bVp = INV ? -bV : bV;
+    const double bVl = IM ? bV : -bV;
 
     if (!GUARD || (r >= ra && r < rb)) {
         const int q = w.lslot;
@@ -177,30 +264,42 @@ __device__ __forceinline__ void adj_row(AdjWalk &w, const AdjArgs &a, int r) {
             PS(0)[i] = ld_cx_shared(sp + i);
             LA(0)[i] = ld_cx_shared(sl + i);
         }
+        if constexpr (A::IMAG) {
+            // psi_k = c_k phi_k; lambda = c_{k+1} (Lambda - mu c_{k+1} phi_{k+1})
+            const Cx<double> *sn =
+                reinterpret_cast<const Cx<double> *>(sb + A::PSN_OFF) + 2 * w.lane;
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+                const Cx<double> n = ld_cx_shared(sn + i);
+                PS(0)[i] = scale_cx(PS(0)[i], w.cin);
+                LA(0)[i].re = __dmul_rn(w.cnext, __fma_rn(-w.m2, n.re, LA(0)[i].re));
+                LA(0)[i].im = __dmul_rn(w.cnext, __fma_rn(-w.m2, n.im, LA(0)[i].im));
+            }
+        }
     }
     // S1: V0 on rows (r-1, r)
     if (!GUARD || (r - 1 >= ra && r < rb)) {
-        vsweep<false, 2, ((K + 1) & 1)>(PS(1), PS(0), aV, bVp);
-        vsweep<false, 2, ((K + 1) & 1)>(LA(1), LA(0), aV, -bV);
+        vsweep<IM, 2, ((K + 1) & 1)>(PS(1), PS(0), aV, bVp);
+        vsweep<IM, 2, ((K + 1) & 1)>(LA(1), LA(0), aV, bVl);
     }
     // S2: H0 on row r-1
     if (!GUARD || (r - 1 >= ra && r - 1 < rb)) {
-        adj_h<((K + 1) & 1), INV>(w, PS(1));
-        adj_h<((K + 1) & 1), true>(w, LA(1));
+        adj_h<((K + 1) & 1), INV, IM>(w, PS(1));
+        adj_h<((K + 1) & 1), !IM, IM>(w, LA(1));
     }
     // S3: V1 on rows (r-2, r-1)
     if (!GUARD || (r - 2 >= ra && r - 1 < rb)) {
-        vsweep<false, 2, ((K + 1) & 1)>(PS(2), PS(1), aV, bVp);
-        vsweep<false, 2, ((K + 1) & 1)>(LA(2), LA(1), aV, -bV);
+        vsweep<IM, 2, ((K + 1) & 1)>(PS(2), PS(1), aV, bVp);
+        vsweep<IM, 2, ((K + 1) & 1)>(LA(2), LA(1), aV, bVl);
     }
     // S4: H1, potential, H1 on row r-2; refill its slot
     if (!GUARD || (r - 2 >= ra && r - 2 < rb)) {
         const int u = r - 2;
-        adj_h<((K + 1) & 1), INV>(w, PS(2));
-        adj_h<((K + 1) & 1), true>(w, LA(2));
+        adj_h<((K + 1) & 1), INV, IM>(w, PS(2));
+        adj_h<((K + 1) & 1), !IM, IM>(w, LA(2));
         const int q = w.tslot;
         adj_potential<A>(w, a, PS(2), LA(2), q, u);
-        adj_h<((K + 1) & 1), true>(w, LA(2));
+        adj_h<((K + 1) & 1), !IM, IM>(w, LA(2));
         if (INV) adj_h<((K + 1) & 1), true>(w, PS(2));
         __syncwarp();
         if (u + w.D < rb) {
@@ -214,17 +313,17 @@ __device__ __forceinline__ void adj_row(AdjWalk &w, const AdjArgs &a, int r) {
     }
     // S5: V1 on rows (r-3, r-2)
     if (!GUARD || (r - 3 >= ra && r - 2 < rb)) {
-        vsweep<false, 2, ((K) & 1)>(LA(3), LA(2), aV, -bV);
+        vsweep<IM, 2, ((K) & 1)>(LA(3), LA(2), aV, bVl);
         if (INV) vsweep<false, 2, ((K) & 1)>(PS(3), PS(2), aV, -bV);
     }
     // S6: H0 on row r-3
     if (!GUARD || (r - 3 >= ra && r - 3 < rb)) {
-        adj_h<((K + 1) & 1), true>(w, LA(3));
+        adj_h<((K + 1) & 1), !IM, IM>(w, LA(3));
         if (INV) adj_h<((K + 1) & 1), true>(w, PS(3));
     }
     // S7: V0 on rows (r-4, r-3)
     if (!GUARD || (r - 4 >= ra && r - 3 < rb)) {
-        vsweep<false, 2, ((K) & 1)>(LA(4), LA(3), aV, -bV);
+        vsweep<IM, 2, ((K) & 1)>(LA(4), LA(3), aV, bVl);
         if (INV) vsweep<false, 2, ((K) & 1)>(PS(4), PS(3), aV, -bV);
     }
     // store the finished row r - 4
@@ -276,6 +375,12 @@ __global__ void __launch_bounds__(64, 6) adjoint_kernel(AdjArgs a) {
     w.phase_bits = 0u;
     w.pitch16 = (size_t)a.P * 16;
     w.pitch8 = (size_t)a.P * 8;
+    w.kacc = 0.0;
+    if constexpr (A::IMAG) {
+        w.cin = *a.c_in;
+        w.cnext = *a.c_next;
+        w.m2 = *a.mu_next * w.cnext;
+    }
     {
         uint4 *z = reinterpret_cast<uint4 *>(w.ring);
         const int n16 = D * A::SLOT / 16;
@@ -305,7 +410,8 @@ __global__ void __launch_bounds__(64, 6) adjoint_kernel(AdjArgs a) {
         w.bytes8 = (uint32_t)(ce - cs) * 8u;
         w.gpsi = reinterpret_cast<const unsigned char *>(a.psi_in) + (size_t)cs * 16;
         w.glam = reinterpret_cast<const unsigned char *>(a.lam_in) + (size_t)cs * 16;
-        w.gtab = reinterpret_cast<const unsigned char *>(a.pot) + (size_t)cs * 16;
+        w.gtab = reinterpret_cast<const unsigned char *>(a.pot) + (size_t)cs * A::TAB_CELL;
+        if constexpr (A::IMAG) w.gpsn = reinterpret_cast<const unsigned char *>(a.psn_in) + (size_t)cs * 16;
         w.ggv = reinterpret_cast<const unsigned char *>(a.gv) + (size_t)cs * 8;
         w.xl = c0 + 2 * lane;
         bool present[2];
@@ -343,9 +449,13 @@ __global__ void __launch_bounds__(64, 6) adjoint_kernel(AdjArgs a) {
             for (int i = lane; i < words; i += 32) {
                 const uint32_t off = (uint32_t)(i * 4) % (uint32_t)A::SLOT;
                 bool copied;
-                if (off < (uint32_t)A::GV_OFF) {
+                if (off < (uint32_t)A::TAB_OFF) {
                     const uint32_t t = off % (uint32_t)A::ROW;
                     copied = t >= w.off16 && t < w.off16 + w.bytes16;
+                } else if (off < (uint32_t)A::GV_OFF) {
+                    const uint32_t t = off - (uint32_t)A::TAB_OFF;
+                    copied = A::TAB_CELL == 16 ? (t >= w.off16 && t < w.off16 + w.bytes16)
+                                               : (t >= w.off8 && t < w.off8 + w.bytes8);
                 } else {
                     const uint32_t t = off - (uint32_t)A::GV_OFF;
                     copied = t >= w.off8 && t < w.off8 + w.bytes8;
@@ -369,6 +479,33 @@ __global__ void __launch_bounds__(64, 6) adjoint_kernel(AdjArgs a) {
                 w.phase_bits ^= 1u << q;
                 q = w.next(q);
             }
+        }
+    }
+    if constexpr (A::IMAG) {
+        // Re<Lambda_k, psi_k>: lanes, warps of the block, then the blocks in
+        // a fixed order by the last block to finish
+        double v = w.kacc;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+        __shared__ double s_warp[32];
+        __shared__ unsigned int s_last;
+        if (lane == 0) s_warp[warp] = v;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double b = 0.0;
+            for (int i = 0; i < warps; ++i) b += s_warp[i];
+            a.partials[blockIdx.x] = b;
+            __threadfence();
+            s_last = (atomicAdd(a.ticket, 1u) == gridDim.x - 1) ? 1u : 0u;
+        }
+        __syncthreads();
+        if (s_last && threadIdx.x == 0) {
+            __threadfence();
+            double tot = 0.0;
+            for (int i = 0; i < (int)gridDim.x; ++i) tot += __ldcg(&a.partials[i]);
+            *a.mu_out = a.mu_scale * tot;
+            if (a.accumulate) *a.kappa_sum += tot;
+            *a.ticket = 0u;
         }
     }
 }

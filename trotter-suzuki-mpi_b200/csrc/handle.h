@@ -35,7 +35,9 @@ struct ts_b200_kernel {
     int C = 2, seg_h = 64, warps = 4, ring = 4;
     int resident_blocks = 0;  // blocks of the current launch shape resident on the GPU (0: unknown)
     bool auto_seg = true;     // pick the segment height from the resident grid
-    bool walk2 = true;        // look-ahead walk (walk2.cuh) where the variant has one
+    bool overlap = true;      // look-ahead walk: programmatic dependent launch of each step
+    int walk2 = 2;            // rows per iteration of the look-ahead walk (walk2.cuh) where
+                              // the variant has one; 0: the checked walk
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
     float4 *kin_sched = nullptr;  // FP32 real time: per-step kinetic coefficients

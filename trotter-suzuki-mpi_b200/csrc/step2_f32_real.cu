@@ -3,9 +3,9 @@
 
 namespace tsb {
 
-cudaError_t launch_step2_f32_real(int C, int phase, const StepArgs<float> &a, int warps,
-                                  size_t smem, int blocks, cudaStream_t st, int *bps) {
-    return launch_step2_t<float, false>(C, phase, a, warps, smem, blocks, st, bps);
+cudaError_t launch_step2_f32_real(int C, int R, int phase, const StepArgs<float> &a, int warps,
+                                  size_t smem, int blocks, cudaStream_t st, int *bps, bool pdl) {
+    return launch_step2_t<float, false>(C, R, phase, a, warps, smem, blocks, st, bps, pdl);
 }
 
 }  // namespace tsb

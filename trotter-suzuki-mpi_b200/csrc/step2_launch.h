@@ -1,15 +1,17 @@
 // Launch templates of the look-ahead walk (walk2.cuh); one translation unit
 // per precision and time mode (step2_f{64,32}_{real,imag}.cu).
 #pragma once
-#include "step_launch.h"
+#include "step2_decl.h"
 #include "walk2.cuh"
 
 namespace tsb {
 
-template <class V>
+// pdl: launch with a programmatic dependency on the stream's previous kernel
+// (the set-up of this step overlaps the end of the previous one)
+template <class V, int R = 1>
 cudaError_t launch_step2_variant(const StepArgs<typename V::T> &a, int warps, size_t smem,
-                                 int blocks, cudaStream_t st, int *blocks_per_sm) {
-    auto fn = step2_kernel<V>;
+                                 int blocks, cudaStream_t st, int *blocks_per_sm, bool pdl) {
+    auto fn = step2_kernel<V, R>;
     static int configured_smem = -1;
     if ((int)smem > configured_smem) {
         cudaError_t e =
@@ -22,21 +24,38 @@ cudaError_t launch_step2_variant(const StepArgs<typename V::T> &a, int warps, si
         if (e != cudaSuccess) return e;
     }
     if (blocks == 0) return cudaSuccess;
-    fn<<<blocks, warps * 32, smem, st>>>(a);
-    return cudaGetLastError();
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)blocks);
+    cfg.blockDim = dim3((unsigned)(warps * 32));
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, fn, a);
 }
 
+// R: rows per iteration of the walk (2: cells per lane 2 only)
 template <typename T, bool IMAG>
-cudaError_t launch_step2_t(int C, int phase, const StepArgs<T> &a, int warps, size_t smem,
-                           int blocks, cudaStream_t st, int *bps) {
+cudaError_t launch_step2_t(int C, int R, int phase, const StepArgs<T> &a, int warps, size_t smem,
+                           int blocks, cudaStream_t st, int *bps, bool pdl) {
+    if (C == 2 && R == 2) {
+        if (phase == 0) return launch_step2_variant<Variant<T, 2, IMAG, false, 0>, 2>(a, warps, smem, blocks, st, bps, pdl);
+        if (phase == 1) return launch_step2_variant<Variant<T, 2, IMAG, false, 1>, 2>(a, warps, smem, blocks, st, bps, pdl);
+        if (phase == 2) return launch_step2_variant<Variant<T, 2, IMAG, false, 2>, 2>(a, warps, smem, blocks, st, bps, pdl);
+        return cudaErrorInvalidValue;
+    }
+    if (R != 1) return cudaErrorInvalidValue;
     if (C == 2) {
-        if (phase == 0) return launch_step2_variant<Variant<T, 2, IMAG, false, 0>>(a, warps, smem, blocks, st, bps);
-        if (phase == 1) return launch_step2_variant<Variant<T, 2, IMAG, false, 1>>(a, warps, smem, blocks, st, bps);
-        if (phase == 2) return launch_step2_variant<Variant<T, 2, IMAG, false, 2>>(a, warps, smem, blocks, st, bps);
+        if (phase == 0) return launch_step2_variant<Variant<T, 2, IMAG, false, 0>>(a, warps, smem, blocks, st, bps, pdl);
+        if (phase == 1) return launch_step2_variant<Variant<T, 2, IMAG, false, 1>>(a, warps, smem, blocks, st, bps, pdl);
+        if (phase == 2) return launch_step2_variant<Variant<T, 2, IMAG, false, 2>>(a, warps, smem, blocks, st, bps, pdl);
     } else if (C == 4) {
-        if (phase == 0) return launch_step2_variant<Variant<T, 4, IMAG, false, 0>>(a, warps, smem, blocks, st, bps);
-        if (phase == 1) return launch_step2_variant<Variant<T, 4, IMAG, false, 1>>(a, warps, smem, blocks, st, bps);
-        if (phase == 2) return launch_step2_variant<Variant<T, 4, IMAG, false, 2>>(a, warps, smem, blocks, st, bps);
+        if (phase == 0) return launch_step2_variant<Variant<T, 4, IMAG, false, 0>>(a, warps, smem, blocks, st, bps, pdl);
+        if (phase == 1) return launch_step2_variant<Variant<T, 4, IMAG, false, 1>>(a, warps, smem, blocks, st, bps, pdl);
+        if (phase == 2) return launch_step2_variant<Variant<T, 4, IMAG, false, 2>>(a, warps, smem, blocks, st, bps, pdl);
     }
     return cudaErrorInvalidValue;
 }

@@ -430,19 +430,43 @@ __device__ __forceinline__ double sqrt_t(double x) { return sqrt(x); }
 __device__ __forceinline__ float sqrt_t(float x) { return sqrtf(x); }
 
 // Phase factors of the GPE / LHY term for small arguments.  The nonlinear
-// phase g*dt*|psi|^2 is far below 1/32 in practice, where the Maclaurin
-// series of cos, sin and exp truncated after the x^10 / x^11 / x^8 terms
-// (Horner's rule) leave a remainder below 1e-19, i.e. well under half an ulp
-// of double; larger arguments take the CUDA math library.
-// Returns sin(th) and cos(th) (cos(th) - 1 in delta form).
-// Below 1/32 the series apply (the comparison is exact in either precision).
+// phase g*dt*|psi|^2 is far below 1/32 in practice, where truncated Maclaurin
+// series of cos, sin and exp (Horner's rule) leave a remainder well under half
+// an ulp; larger arguments take the CUDA math library.  Two tiers, chosen for
+// the whole warp:
+//   |th| < 2^-8: double cos / sin to the t^3 terms (t = th^2), exp to x^6
+//                (remainders below 3e-21); float cos / sin to t^2, exp to x^4
+//                (below 1e-14);
+//   |th| < 1/32: cos / sin to t^5, exp to x^8 (remainders below 1e-19).
+// Returns sin(th) and cos(th) (cos(th) - 1 in delta form).  The comparisons
+// are exact in either precision.
+__device__ __forceinline__ bool phase_tiny(double th) { return fabs(th) < 0.00390625; }
+__device__ __forceinline__ bool phase_tiny(float th) { return fabsf(th) < 0.00390625f; }
 __device__ __forceinline__ bool phase_small(double th) { return fabs(th) < 0.03125; }
 __device__ __forceinline__ bool phase_small(float th) { return fabsf(th) < 0.03125f; }
 
 template <typename T>
 __device__ __forceinline__ void phase_sincos(T th, T *s, T *c) {
-    // warp-uniform choice: the library path only if some lane needs it
-    if (!__any_sync(0xffffffffu, !phase_small(th))) {
+    constexpr bool F = std::is_same<T, float>::value;
+    // warp-uniform choice: the shorter series if every lane allows it, the
+    // library path only if some lane needs it
+    if (!__any_sync(0xffffffffu, !phase_tiny(th))) {
+        const T t = th * th;
+        T pc, ps;
+        if (F) {
+            pc = fma_t(T(4.1666666666666664e-02), t, T(-0.5));              // 1/4!, -1/2!
+            ps = fma_t(T(8.3333333333333332e-03), t, T(-1.6666666666666666e-01));  // 1/5!, -1/3!
+        } else {
+            pc = T(-1.3888888888888889e-03);               // -1/6!
+            pc = fma_t(pc, t, T(4.1666666666666664e-02));  //  1/4!
+            pc = fma_t(pc, t, T(-0.5));                    // -1/2!
+            ps = T(-1.9841269841269841e-04);               // -1/7!
+            ps = fma_t(ps, t, T(8.3333333333333332e-03));  //  1/5!
+            ps = fma_t(ps, t, T(-1.6666666666666666e-01)); // -1/3!
+        }
+        *c = DeltaForm<T>::value ? mul_t(pc, t) : fma_t(pc, t, T(1));
+        *s = fma_t(mul_t(ps, t), th, th);
+    } else if (!__any_sync(0xffffffffu, !phase_small(th))) {
         const T t = th * th;
         T pc = T(-2.7557319223985893e-07);            // -1/10!
         pc = fma_t(pc, t, T(2.4801587301587302e-05));  //  1/8!
@@ -466,9 +490,25 @@ __device__ __forceinline__ void phase_sincos(T th, T *s, T *c) {
     }
 }
 
-// exp(-th) for the imaginary-time nonlinear factor (same truncation rule).
+// exp(-th) for the imaginary-time nonlinear factor (same tiers).
 template <typename T>
 __device__ __forceinline__ T phase_expneg(T th) {
+    constexpr bool F = std::is_same<T, float>::value;
+    if (!__any_sync(0xffffffffu, !phase_tiny(th))) {
+        const T x = -th;
+        T p;
+        if (F) {
+            p = fma_t(T(4.1666666666666664e-02), x, T(1.6666666666666666e-01));  // 1/4!, 1/3!
+        } else {
+            p = T(1.3888888888888889e-03);               // 1/6!
+            p = fma_t(p, x, T(8.3333333333333332e-03));  // 1/5!
+            p = fma_t(p, x, T(4.1666666666666664e-02));  // 1/4!
+            p = fma_t(p, x, T(1.6666666666666666e-01));  // 1/3!
+        }
+        p = fma_t(p, x, T(0.5));  // 1/2!
+        p = fma_t(p, x, T(1));
+        return fma_t(p, x, T(1));
+    }
     if (!__any_sync(0xffffffffu, !phase_small(th))) {
         const T x = -th;
         T p = T(2.4801587301587302e-05);             // 1/8!
@@ -487,6 +527,14 @@ __device__ __forceinline__ T phase_expneg(T th) {
 // exp(-th0), exp(-th1) of two single-precision cells: the series of both in
 // one packed pair, each cell with the roundings of phase_expneg.
 __device__ __forceinline__ float2 phase_expneg2(float th0, float th1) {
+    if (!__any_sync(0xffffffffu, !(phase_tiny(th0) && phase_tiny(th1)))) {
+        const float2 x = make_float2(-th0, -th1);
+        constexpr double k[4] = {1.6666666666666666e-01, 0.5, 1.0, 1.0};
+        float2 p = make_float2(float(4.1666666666666664e-02), float(4.1666666666666664e-02));
+#pragma unroll
+        for (int j = 0; j < 4; ++j) p = __ffma2_rn(p, x, make_float2(float(k[j]), float(k[j])));
+        return p;
+    }
     if (!__any_sync(0xffffffffu, !(phase_small(th0) && phase_small(th1)))) {
         const float2 x = make_float2(-th0, -th1);
         constexpr double k[8] = {1.9841269841269841e-04, 1.3888888888888889e-03,

@@ -3,7 +3,6 @@
 #include <cuda_runtime.h>
 
 #include "step_kernel.cuh"
-#include "walk2_shape.h"
 
 namespace tsb {
 
@@ -17,16 +16,6 @@ cudaError_t launch_step_f32_real(int C, bool rot, int phase, const StepArgs<floa
                                  size_t smem, int blocks, cudaStream_t st, int *blocks_per_sm);
 cudaError_t launch_step_f32_imag(int C, bool rot, int phase, const StepArgs<float> &a, int warps,
                                  size_t smem, int blocks, cudaStream_t st, int *blocks_per_sm);
-
-// The look-ahead walk (walk2.cuh): phases 0-2, no rotating frame, cartesian.
-cudaError_t launch_step2_f64_real(int C, int phase, const StepArgs<double> &a, int warps,
-                                  size_t smem, int blocks, cudaStream_t st, int *blocks_per_sm);
-cudaError_t launch_step2_f64_imag(int C, int phase, const StepArgs<double> &a, int warps,
-                                  size_t smem, int blocks, cudaStream_t st, int *blocks_per_sm);
-cudaError_t launch_step2_f32_real(int C, int phase, const StepArgs<float> &a, int warps,
-                                  size_t smem, int blocks, cudaStream_t st, int *blocks_per_sm);
-cudaError_t launch_step2_f32_imag(int C, int phase, const StepArgs<float> &a, int warps,
-                                  size_t smem, int blocks, cudaStream_t st, int *blocks_per_sm);
 
 template <class V>
 cudaError_t launch_step_variant(const StepArgs<typename V::T> &a, int warps, size_t smem,

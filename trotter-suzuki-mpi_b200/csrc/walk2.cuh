@@ -26,6 +26,10 @@
 //   * Loads run one row ahead: the iteration of row c waits for row c + 1
 //     and moves it to registers while the stages of row c run, so the
 //     shared-memory latency is off the stage chain.
+//   * Or (R = 2) two rows per iteration: one ring slot and one mbarrier per
+//     pair of rows, and the stages of both rows in one basic block, where
+//     the second row's chain of stages runs one stage behind the first's
+//     (row c + 1's V0 needs only row c's V0), so the two chains overlap.
 //
 // Variants: single component, no rotating frame, cartesian (phases 0-2), 2 or
 // 4 cells per lane, both precisions and time modes.  The arithmetic of each
@@ -37,21 +41,25 @@
 
 namespace tsb {
 
-template <class V>
+template <class V, int R_ = 1>
 struct W2Shape {
     static constexpr int C = V::C;
-    static constexpr int NW = 6;      // window rows
-    static constexpr int D = 6;       // ring slots per warp
-    static constexpr int UNROLL = 6;  // rows per unrolled chunk
+    static constexpr int R = R_;        // rows per iteration (and per ring slot)
+    static constexpr int NW = 6;        // window rows
+    static constexpr int D = 6 / R_;    // ring slots per warp
+    static constexpr int UNROLL = 6;    // rows per unrolled chunk
     static constexpr int HX = 4, HY = 4;
     static constexpr int SW = 32 * C, WO = SW - 2 * HX;
-    static constexpr int SLOT = V::PSI_BYTES + V::TAB_BYTES;
+    static constexpr int ROWB = V::PSI_BYTES + V::TAB_BYTES;  // one row of psi and table
+    static constexpr int SLOT = R_ * ROWB;
     // vertical pair coefficients: entry j is the pair (u - 1, u) with
     // u = ra + j - VPAD; the first stages of a walk read up to VPAD entries
     // before the first row
     static constexpr int VPAD = 4;
     static_assert(!V::ROT && !V::PB && !V::CYL, "look-ahead walk: plain variants only");
-    static_assert(D == UNROLL && NW == UNROLL && UNROLL % 2 == 0, "compile-time slots and parities");
+    static_assert(R_ == 1 || R_ == 2, "one or two rows per iteration");
+    static_assert(D * R == UNROLL && NW == UNROLL && UNROLL % 2 == 0,
+                  "compile-time slots and parities");
 };
 
 
@@ -62,11 +70,11 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
-template <class V>
+template <class V, int R = 1>
 struct Walk2 {
     using T = typename V::T;
     using TabT = typename V::TabT;
-    using S = W2Shape<V>;
+    using S = W2Shape<V, R>;
     static constexpr int C = V::C;
 
     Cx<T> win[S::NW][C];
@@ -86,24 +94,52 @@ struct Walk2 {
     size_t opitch;  // output row pitch in cells
     double nacc;
     bool failed;
-    int fail_idx;  // walk index whose wait gave up
+    int fail_idx;  // ring slot index (rows R * fail_idx ..) whose wait gave up
     T inv;
     T aH, bH, aV, bV, ca, caa;
 
-    // copy row index `tp` of the walk into slot q, or complete the slot's
-    // phase without data for rows outside the tile or past the walk
-    __device__ __forceinline__ void issue(int tp, int q) {
-        if (lane == 0) {
-            const int row = ra + tp;
-            unsigned char *sb = ring + q * S::SLOT;
-            if (tp < nit && row >= 0 && row < H) {
-                mbar_expect_tx(&bars[q], psi_bytes + tab_bytes);
-                bulk_g2s(sb + psi_off, gpsi + (size_t)row * gpsi_pitch, psi_bytes, &bars[q]);
-                bulk_g2s(sb + V::PSI_BYTES + tab_off, gtab + (size_t)row * gtab_pitch, tab_bytes,
-                         &bars[q]);
-            } else {
-                mbar_arrive(&bars[q]);
-            }
+    // copy the rows of slot index `si` of the walk (rows R si .. R si + R - 1)
+    // into ring slot q; rows outside the tile or past the walk are not
+    // copied, and a slot without any row completes its phase by a plain
+    // arrive.  Lane 0 issues, through predicates (no divergent branch in the
+    // row body).
+    __device__ __forceinline__ void issue(int si, int q) {
+        const uint32_t sb = smem_u32(ring + q * S::SLOT);
+        const uint32_t bar = smem_u32(&bars[q]);
+        const uint32_t rowbytes = psi_bytes + tab_bytes;
+        uint32_t p[2], n = 0;
+        const unsigned char *src_psi[2], *src_tab[2];
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+            const int tp = R * si + k, row = ra + tp;
+            const bool real = tp < nit && row >= 0 && row < H;
+            p[k] = (lane == 0 && real) ? 1u : 0u;
+            n += real ? 1u : 0u;
+            const int rr = real ? row : 0;
+            src_psi[k] = gpsi + (size_t)rr * gpsi_pitch;
+            src_tab[k] = gtab + (size_t)rr * gtab_pitch;
+        }
+        const uint32_t pc = (lane == 0 && n > 0) ? 1u : 0u;
+        const uint32_t pa = (lane == 0 && n == 0) ? 1u : 0u;
+        asm volatile(
+            "{\n\t.reg .pred pc, pa;\n\t"
+            "setp.ne.u32 pc, %0, 0;\n\t"
+            "setp.ne.u32 pa, %1, 0;\n\t"
+            "@pc mbarrier.arrive.expect_tx.shared::cta.b64 _, [%2], %3;\n\t"
+            "@pa mbarrier.arrive.shared::cta.b64 _, [%2];\n\t}" ::"r"(pc),
+            "r"(pa), "r"(bar), "r"(n * rowbytes)
+            : "memory");
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+            const uint32_t rb = sb + (uint32_t)(k * S::ROWB);
+            asm volatile(
+                "{\n\t.reg .pred p;\n\t"
+                "setp.ne.u32 p, %0, 0;\n\t"
+                "@p cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%1], [%2], %3, [%4];\n\t"
+                "@p cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%5], [%6], %7, [%4];\n\t}" ::"r"(p[k]),
+                "r"(rb + psi_off), "l"(src_psi[k]), "r"(psi_bytes), "r"(bar),
+                "r"(rb + (uint32_t)V::PSI_BYTES + tab_off), "l"(src_tab[k]), "r"(tab_bytes)
+                : "memory");
         }
     }
 };
@@ -159,30 +195,18 @@ __device__ __forceinline__ void store_row_cells(Cx<T> *o, const Cx<T> (&v)[C], c
         if (in[i]) st_cx_global(o + i, v[i]);
 }
 
-// One iteration: current row c = ra + t (t = base + K, base a multiple of 6).
-template <class V, int K>
-__device__ __forceinline__ void w2_row(Walk2<V> &w, int t, uint32_t ph) {
+// The stages of current row c = ra + t (t = base + K, base a multiple of 6):
+// V0 H0 V1 (H1 P H1) V1 H0 V0 one row behind each other, then the store of
+// the finished row c - 4.
+template <class V, int R, int K>
+__device__ __forceinline__ void w2_stages(Walk2<V, R> &w, int t) {
     using T = typename V::T;
     using TabT = typename V::TabT;
-    using S = W2Shape<V>;
+    using S = W2Shape<V, R>;
     constexpr int C = V::C;
     constexpr bool IMAG = V::IMAG, PHASE = V::PHASE;
     // row c - j lives in win[(K - j) mod 6]
 #define W2S(j) w.win[((K) - (j) + 2 * S::NW) % S::NW]
-    // ---- look-ahead: wait for row c + 1 and move it to the window
-    {
-        constexpr int q = (K + 1) % S::D;
-        const uint32_t par = (K + 1 < S::D) ? ph : (ph ^ 1u);
-        if (!mbar_wait_bounded(&w.bars[q], par)) {
-            w.failed = true;
-            w.fail_idx = t + 1;
-            return;
-        }
-        Cx<T> v[C];
-        load_row_cells<T, C>(w.ring + q * S::SLOT + C * (int)sizeof(Cx<T>) * w.lane, v);
-#pragma unroll
-        for (int i = 0; i < C; ++i) W2S(-1)[i] = IMAG ? scale_cx(v[i], w.inv) : v[i];
-    }
     const Cx<T> *vc = w.vco + t + S::VPAD;
     // ---- S1: V0 on rows (c-1, c)
     {
@@ -196,12 +220,14 @@ __device__ __forceinline__ void w2_row(Walk2<V> &w, int t, uint32_t ph) {
         const Cx<T> cv = vc[-1];
         vsweep<IMAG, C, ((K + 1) & 1)>(W2S(2), W2S(1), cv.re, cv.im);
     }
-    // ---- S4: H1, P, H1 on row c-2 (table of row c-2 from its slot)
+    // ---- S4: H1, P, H1 on row c-2 (its table from its ring slot)
     {
-        constexpr int q = (K + S::D - 2) % S::D;
+        constexpr int RT = (K + S::UNROLL - 2) % S::UNROLL;  // row c-2 within the chunk
+        constexpr int q = RT / R, pos = RT % R;
         hsweep_lanes<IMAG, ((K + 1) & 1), C>(W2S(2), w.hpa, w.hpb, w.hal, w.hbl, w.har, w.hbr);
         alignas(16) TabT tv[C];
-        load_tab_cells<TabT, C>(w.ring + q * S::SLOT + V::PSI_BYTES + C * (int)sizeof(TabT) * w.lane,
+        load_tab_cells<TabT, C>(w.ring + q * S::SLOT + pos * S::ROWB + V::PSI_BYTES +
+                                    C * (int)sizeof(TabT) * w.lane,
                                 tv);
         potential_row<IMAG, PHASE, V::LHY, false, C>(W2S(2), tv, w.ca, w.caa);
         hsweep_lanes<IMAG, ((K + 1) & 1), C>(W2S(2), w.hpa, w.hpb, w.hal, w.hbl, w.har, w.hbr);
@@ -218,8 +244,9 @@ __device__ __forceinline__ void w2_row(Walk2<V> &w, int t, uint32_t ph) {
         const Cx<T> cv = vc[-3];
         vsweep<IMAG, C, ((K) & 1)>(W2S(4), W2S(3), cv.re, cv.im);
     }
-    // ---- row c-4 is finished: store it (the first 8 rows of a walk are halo)
-    if (t >= 8) {
+    // ---- row c-4 is finished: store it (the first 8 rows of a walk are halo;
+    // with two rows per iteration the second row can lie past the walk)
+    if (t >= 8 && (R == 1 || t < w.nit)) {
         store_row_cells<T, C>(w.orow, W2S(4), w.out_col, w.all_out);
         if (IMAG && t >= w.n_lo && t < w.n_hi) {
 #pragma unroll
@@ -231,34 +258,84 @@ __device__ __forceinline__ void w2_row(Walk2<V> &w, int t, uint32_t ph) {
         }
     }
     w.orow += w.opitch;
-    // ---- the slot of row c-2 is free: copy row c+4 into it
-    {
-        constexpr int q = (K + S::D - 2) % S::D;
+#undef W2S
+}
+
+// This lane's cells of row `pos` of ring slot q into window row `dst`.
+template <class V, int R>
+__device__ __forceinline__ void w2_load(Walk2<V, R> &w, int q, int pos,
+                                        Cx<typename V::T> (&dst)[V::C]) {
+    using T = typename V::T;
+    using S = W2Shape<V, R>;
+    constexpr int C = V::C;
+    Cx<T> v[C];
+    load_row_cells<T, C>(w.ring + q * S::SLOT + pos * S::ROWB + C * (int)sizeof(Cx<T>) * w.lane, v);
+#pragma unroll
+    for (int i = 0; i < C; ++i) dst[i] = V::IMAG ? scale_cx(v[i], w.inv) : v[i];
+}
+
+// One iteration (row t = base + K with R = 1; rows t, t + 1 with R = 2, K
+// even); ph is the chunk's mbarrier parity.
+template <class V, int R, int K>
+__device__ __forceinline__ void w2_iter(Walk2<V, R> &w, int t, uint32_t ph) {
+    using S = W2Shape<V, R>;
+#define W2S(j) w.win[((K) - (j) + 2 * S::NW) % S::NW]
+    if constexpr (R == 1) {
+        // look-ahead: wait for row t + 1 and move it to the window
+        constexpr int q = (K + 1) % S::D;
+        const uint32_t par = (K + 1 < S::D) ? ph : (ph ^ 1u);
+        if (!mbar_wait_bounded(&w.bars[q], par)) {
+            w.failed = true;
+            w.fail_idx = t + 1;
+            return;
+        }
+        w2_load(w, q, 0, W2S(-1));
+        w2_stages<V, R, K>(w, t);
+        // the slot of row t-2 is free: copy row t + 4 into it
+        constexpr int qi = (K + S::D - 2) % S::D;
         __syncwarp();
-        if (w.lane == 0) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        w.issue(t + 4, q);
+        // the slot's generic-proxy reads happen-before the bulk copy refills it
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        w.issue(t + 4, qi);
+    } else {
+        // rows t and t + 1 arrive together in slot K / 2
+        constexpr int q = K / 2;
+        if (!mbar_wait_bounded(&w.bars[q], ph)) {
+            w.failed = true;
+            w.fail_idx = t / 2;
+            return;
+        }
+        w2_load(w, q, 0, W2S(0));
+        w2_load(w, q, 1, W2S(-1));
+        w2_stages<V, R, K>(w, t);
+        w2_stages<V, R, K + 1>(w, t + 1);
+        // the slot of rows t-2, t-1 is free: copy rows t + 4, t + 5 into it
+        constexpr int qi = (q + 2) % S::D;
+        __syncwarp();
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        w.issue(t / 2 + 2, qi);
     }
 #undef W2S
 }
 
-template <class V, int K>
-__device__ __forceinline__ bool w2_rows(Walk2<V> &w, int base, uint32_t ph) {
-    if constexpr (K < W2Shape<V>::UNROLL) {
+template <class V, int R, int K>
+__device__ __forceinline__ bool w2_rows(Walk2<V, R> &w, int base, uint32_t ph) {
+    if constexpr (K < W2Shape<V, R>::UNROLL) {
         const int t = base + K;
         if (t >= w.nit) return false;
-        w2_row<V, K>(w, t, ph);
+        w2_iter<V, R, K>(w, t, ph);
         if (w.failed) return false;
-        return w2_rows<V, K + 1>(w, base, ph);
+        return w2_rows<V, R, K + R>(w, base, ph);
     }
     return true;
 }
 
 // One task: strip x segment, interior strips first.
-template <class V>
-__device__ __forceinline__ void w2_task(Walk2<V> &w, const StepArgs<typename V::T> &a, int task) {
+template <class V, int R>
+__device__ __forceinline__ void w2_task(Walk2<V, R> &w, const StepArgs<typename V::T> &a, int task) {
     using T = typename V::T;
     using TabT = typename V::TabT;
-    using S = W2Shape<V>;
+    using S = W2Shape<V, R>;
     constexpr int C = V::C;
     const int lane = w.lane;
     int strip, seg;
@@ -329,7 +406,7 @@ __device__ __forceinline__ void w2_task(Walk2<V> &w, const StepArgs<typename V::
         // cells of the strip outside the tile read as 0 (copies do not cover them)
         uint32_t *ring32 = reinterpret_cast<uint32_t *>(w.ring);
         for (int i = lane; i < S::D * S::SLOT / 4; i += 32) {
-            const uint32_t off = (uint32_t)(i * 4) % (uint32_t)S::SLOT;
+            const uint32_t off = (uint32_t)(i * 4) % (uint32_t)S::ROWB;
             bool copied;
             if (off < (uint32_t)V::PSI_BYTES) {
                 copied = off >= w.psi_off && off < w.psi_off + w.psi_bytes;
@@ -352,28 +429,35 @@ __device__ __forceinline__ void w2_task(Walk2<V> &w, const StepArgs<typename V::
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
     __syncwarp();
+    // the first 4 rows of the walk (slots 0 .. 3, or row pairs 0 .. 1)
+    constexpr int PRE = 4 / R;
 #pragma unroll
-    for (int q = 0; q < S::D - 2; ++q) w.issue(q, q);
-    // row 0 of the walk
-    if (!mbar_wait_bounded(&w.bars[0], 0u)) {
-        w.failed = true;
-        w.fail_idx = 0;
-    } else {
-        Cx<T> v[C];
-        load_row_cells<T, C>(w.ring + C * (int)sizeof(Cx<T>) * lane, v);
-#pragma unroll
-        for (int i = 0; i < C; ++i) w.win[0][i] = V::IMAG ? scale_cx(v[i], w.inv) : v[i];
+    for (int q = 0; q < PRE; ++q) w.issue(q, q);
+    bool ok = true;
+    if constexpr (R == 1) {
+        // row 0 of the walk; the iterations load one row ahead
+        ok = mbar_wait_bounded(&w.bars[0], 0u);
+        if (!ok) {
+            w.failed = true;
+            w.fail_idx = 0;
+        } else {
+            w2_load(w, 0, 0, w.win[0]);
+        }
+    }
+    if (ok) {
         for (int base = 0; !w.failed; base += S::UNROLL) {
             const uint32_t ph = (uint32_t)(base / S::UNROLL) & 1u;
-            if (!w2_rows<V, 0>(w, base, ph)) break;
+            if (!w2_rows<V, R, 0>(w, base, ph)) break;
         }
     }
     if (w.failed) {
         if (lane == 0) atomicExch(&a.scal->error, 1);
         // let the copies still in flight land before the block can exit:
-        // indices [0, 4) were issued before the walk and index t + 4 by each
-        // completed iteration t; the wait for index fail_idx gave up
-        const int issued_to = max(S::D - 2, w.fail_idx + 3);
+        // slots [0, PRE) were issued before the walk and one more by each
+        // completed iteration (R = 1: iteration t waits for row t + 1 and
+        // issues row t + 4; R = 2: iteration k waits for pair k and issues
+        // pair k + 2); the wait for slot index fail_idx gave up
+        const int issued_to = R == 1 ? max(PRE, w.fail_idx + 3) : max(PRE, w.fail_idx + 2);
         for (int j = w.fail_idx; j < issued_to; ++j)
             (void)mbar_wait_bounded(&w.bars[j % S::D], (uint32_t)(j / S::D) & 1u, 100000000ull);
     }
@@ -404,7 +488,7 @@ __device__ __forceinline__ void w2_finish(const StepArgs<typename V::T> &a, doub
         for (int off = 16; off > 0; off >>= 1) nacc += __shfl_xor_sync(0xffffffffu, nacc, off);
         __shared__ double s_warp[32];
         __shared__ unsigned int s_last;
-        __shared__ double red[256];
+        __shared__ double red[32];
         if (lane == 0) s_warp[warp] = nacc;
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -417,6 +501,9 @@ __device__ __forceinline__ void w2_finish(const StepArgs<typename V::T> &a, doub
         }
         __syncthreads();
         if (s_last) {
+            // the block partials in a fixed order: thread i adds partials i,
+            // i + threads, ... (all loads in flight), the warps fold their
+            // lanes by shuffles, thread 0 adds the warps in order
             __threadfence();
             const int nb = gridDim.x;
             double acc[8];
@@ -429,15 +516,16 @@ __device__ __forceinline__ void w2_finish(const StepArgs<typename V::T> &a, doub
                     if (t < nb) acc[j] += __ldcg(&a.partials[t]);
                 }
             }
-            red[threadIdx.x] =
+            double v =
                 ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+            if (lane == 0) red[warp] = v;
             __syncthreads();
-            for (int h = blockDim.x >> 1; h > 0; h >>= 1) {
-                if ((int)threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
-                __syncthreads();
-            }
             if (threadIdx.x == 0) {
-                const double tot = red[0] * a.dxdy;
+                double t = 0.0;
+                for (int i = 0; i < warps; ++i) t += red[i];
+                const double tot = t * a.dxdy;
                 a.scal->last_norm = tot;
                 if (a.scal->renorm) a.scal->pending_inv = 1.0 / sqrt(tot / a.norm0);
                 a.scal->ticket = 0u;
@@ -449,18 +537,25 @@ __device__ __forceinline__ void w2_finish(const StepArgs<typename V::T> &a, doub
 // Blocks of 4 or 8 warps (the block partial reduction assumes a power of two
 // threads, at most 256); each warp loops over the tasks
 // t = warp_global, warp_global + total_warps, ...
-template <class V>
-__global__ void __launch_bounds__(256, 1) step2_kernel(StepArgs<typename V::T> a) {
+// Register budget: 2 cells per lane fit 128 registers, so 16 warps of the
+// default 4-warp blocks stay resident per SM; 4 cells per lane take up to 255.
+template <class V, int R>
+__global__ void __launch_bounds__(256, V::C == 2 ? 2 : 1) step2_kernel(StepArgs<typename V::T> a) {
     using T = typename V::T;
-    using S = W2Shape<V>;
+    using S = W2Shape<V, R>;
     extern __shared__ __align__(128) unsigned char smem[];
+    // the next step's blocks may be scheduled as this step's blocks retire
+    // (programmatic dependent launch): their set-up below overlaps this
+    // step's tail, and they wait for this step's completion before reading
+    // its output
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     const int warps = blockDim.x >> 5;
     const int warp = __shfl_sync(0xffffffffu, (int)(threadIdx.x >> 5), 0);
     const int lane = threadIdx.x & 31;
     const int n_tasks = a.n_strips * a.n_segs;
     const int vl = w2_vlen(a.seg_h);
 
-    Walk2<V> w;
+    Walk2<V, R> w;
     w.lane = lane;
     w.nacc = 0.0;
     w.failed = false;
@@ -470,7 +565,6 @@ __global__ void __launch_bounds__(256, 1) step2_kernel(StepArgs<typename V::T> a
     w.bars = reinterpret_cast<uint64_t *>(smem + (size_t)warps * S::D * S::SLOT +
                                           (size_t)warps * vl * sizeof(Cx<T>)) +
              warp * S::D;
-    w.opitch = (size_t)a.P;
     {
         uint4 *z = reinterpret_cast<uint4 *>(w.ring);
         for (int i = lane; i < S::D * S::SLOT / 16; i += 32) z[i] = make_uint4(0u, 0u, 0u, 0u);
@@ -487,6 +581,10 @@ __global__ void __launch_bounds__(256, 1) step2_kernel(StepArgs<typename V::T> a
     for (int j = 0; j < S::NW; ++j)
 #pragma unroll
         for (int i = 0; i < V::C; ++i) w.win[j][i] = Cx<T>{T(0), T(0)};
+    // everything below reads what the previous step wrote (the tile, the
+    // renormalisation factor, the schedule's step): wait for its completion
+    // (immediate without a programmatic dependency)
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     // step constants
     w.inv = V::IMAG ? (T)a.scal->pending_inv : T(1);
     w.aH = a.aH;
@@ -505,6 +603,7 @@ __global__ void __launch_bounds__(256, 1) step2_kernel(StepArgs<typename V::T> a
     }
     w.ca = a.ca;
     w.caa = a.caa;
+    w.opitch = (size_t)a.P;
     w.gpsi_pitch = (size_t)a.P * sizeof(Cx<T>);
     w.gtab_pitch = (size_t)a.P * sizeof(typename V::TabT);
 

@@ -110,6 +110,7 @@ SIGNATURES = {
     "ts_b200_set_launch": (_I, [_VP, _I, _I, _I, _I]),
     "ts_b200_autotune": (_I, [_VP, _I]),
     "ts_b200_set_walk": (_I, [_VP, _I]),
+    "ts_b200_set_overlap": (_I, [_VP, _I]),
     "ts_b200_batch_create": (_I, [C.POINTER(_VP), _I, C.POINTER(_VP)]),
     "ts_b200_batch_destroy": (None, [_VP]),
     "ts_b200_batch_size": (_I, [_VP]),

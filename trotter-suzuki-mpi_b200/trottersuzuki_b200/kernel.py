@@ -154,7 +154,8 @@ class Kernel:
                                              warps_per_block, ring_depth))
 
     def set_walk(self, walk):
-        """1: look-ahead row walk (default where the variant has one), 0: checked walk."""
+        """2: look-ahead row walk, two rows per iteration (default where the variant
+        has one), 1: the same with one row per iteration, 0: checked walk."""
         self._check(lib().ts_b200_set_walk(self._h, int(walk)))
 
 
