@@ -449,7 +449,8 @@ def run_b200_arm(args, rank, world, local, pg):
                 "frac": achieved / peak if achieved else None, "peak_kind": peak_kind,
                 "traffic": traffic,
                 "algorithmic_bytes_per_launch": bytes_per_launch,
-                "kernel": "tsb::step_kernel<double, C=2, imaginary, no rotation, GPE>"}
+                "kernel": "tsb::step2_kernel<double, C=2, imaginary, GPE, 2 rows per iteration> "
+                          "(look-ahead walk)"}
 
     cpu = None
     if not args.no_cpu_baseline:

@@ -98,6 +98,25 @@ def test_look_ahead_walk_launch_shapes(launch, imag, walk):
 
 
 @pytest.mark.parametrize("imag", [False, True], ids=["real", "imag"])
+@pytest.mark.parametrize("walk", [1, 2])
+@pytest.mark.parametrize("seg", [10, 12, 14])
+def test_many_segments_odd_height(imag, walk, seg):
+    """Many segments on 301 rows with a short last segment (segment rows 10:
+    31 segments, the last of 1 row; 12: 26 segments, the last of 1 row; 14:
+    22 segments, the last of 7 rows), ragged columns (233 = 4 x 56 + 9): the
+    checked walk's bits in real time, the oracle's result always."""
+    lat, psi0, V = seeded_case(233, 12.0, 301, (False, False))
+    p, tr, ti, ref = _oracle(lat, psi0, V, 1e-3, imag, 3.0, 0.2, 7)
+    got, shape = _gpu(p, psi0, tr, ti, 7, walk=walk,
+                      launch=dict(cells_per_lane=2, segment_rows=seg), split=[3, 4])
+    assert shape["segments"] == -(-301 // seg)
+    assert np.abs(got - ref).max() <= TOL_PSI
+    if not imag:
+        old, _ = _gpu(p, psi0, tr, ti, 7, walk=0, split=[3, 4])
+        assert np.array_equal(got, old)
+
+
+@pytest.mark.parametrize("imag", [False, True], ids=["real", "imag"])
 @pytest.mark.parametrize("cells,walk", [(2, 1), (2, 2), (4, 1)])
 def test_look_ahead_walk_fp32(imag, cells, walk):
     """FP32 storage through the look-ahead walk: the checked walk's bits in

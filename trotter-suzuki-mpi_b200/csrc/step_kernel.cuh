@@ -435,8 +435,9 @@ __device__ __forceinline__ float sqrt_t(float x) { return sqrtf(x); }
 // an ulp; larger arguments take the CUDA math library.  Two tiers, chosen for
 // the whole warp:
 //   |th| < 2^-8: double cos / sin to the t^3 terms (t = th^2), exp to x^6
-//                (remainders below 3e-21); float cos / sin to t^2, exp to x^4
-//                (below 1e-14);
+//                (remainders below 3e-21; Estrin's scheme, a shorter
+//                dependency chain than Horner's); float cos / sin to t^2,
+//                exp to x^4 (below 1e-14);
 //   |th| < 1/32: cos / sin to t^5, exp to x^8 (remainders below 1e-19).
 // Returns sin(th) and cos(th) (cos(th) - 1 in delta form).  The comparisons
 // are exact in either precision.
@@ -452,20 +453,23 @@ __device__ __forceinline__ void phase_sincos(T th, T *s, T *c) {
     // library path only if some lane needs it
     if (!__any_sync(0xffffffffu, !phase_tiny(th))) {
         const T t = th * th;
-        T pc, ps;
         if (F) {
-            pc = fma_t(T(4.1666666666666664e-02), t, T(-0.5));              // 1/4!, -1/2!
-            ps = fma_t(T(8.3333333333333332e-03), t, T(-1.6666666666666666e-01));  // 1/5!, -1/3!
+            const T pc = fma_t(T(4.1666666666666664e-02), t, T(-0.5));               // 1/4!, -1/2!
+            const T ps = fma_t(T(8.3333333333333332e-03), t, T(-1.6666666666666666e-01));  // 1/5!, -1/3!
+            *c = DeltaForm<T>::value ? mul_t(pc, t) : fma_t(pc, t, T(1));
+            *s = fma_t(mul_t(ps, t), th, th);
         } else {
-            pc = T(-1.3888888888888889e-03);               // -1/6!
-            pc = fma_t(pc, t, T(4.1666666666666664e-02));  //  1/4!
-            pc = fma_t(pc, t, T(-0.5));                    // -1/2!
-            ps = T(-1.9841269841269841e-04);               // -1/7!
-            ps = fma_t(ps, t, T(8.3333333333333332e-03));  //  1/5!
-            ps = fma_t(ps, t, T(-1.6666666666666666e-01)); // -1/3!
+            // Estrin's scheme (two levels instead of Horner's three):
+            // cos = (1 - t/2!) + t^2 (1/4! - t/6!),
+            // sin = th + (th t) ((-1/3! + t/5!) - t^2/7!)
+            const T t2 = mul_t(t, t);
+            const T c0 = fma_t(t, T(-0.5), T(1));
+            const T c1 = fma_t(t, T(-1.3888888888888889e-03), T(4.1666666666666664e-02));
+            const T s0 = fma_t(t, T(8.3333333333333332e-03), T(-1.6666666666666666e-01));
+            const T ps = fma_t(t2, T(-1.9841269841269841e-04), s0);
+            *c = fma_t(c1, t2, c0);
+            *s = fma_t(mul_t(th, t), ps, th);
         }
-        *c = DeltaForm<T>::value ? mul_t(pc, t) : fma_t(pc, t, T(1));
-        *s = fma_t(mul_t(ps, t), th, th);
     } else if (!__any_sync(0xffffffffu, !phase_small(th))) {
         const T t = th * th;
         T pc = T(-2.7557319223985893e-07);            // -1/10!
@@ -496,18 +500,22 @@ __device__ __forceinline__ T phase_expneg(T th) {
     constexpr bool F = std::is_same<T, float>::value;
     if (!__any_sync(0xffffffffu, !phase_tiny(th))) {
         const T x = -th;
-        T p;
         if (F) {
-            p = fma_t(T(4.1666666666666664e-02), x, T(1.6666666666666666e-01));  // 1/4!, 1/3!
-        } else {
-            p = T(1.3888888888888889e-03);               // 1/6!
-            p = fma_t(p, x, T(8.3333333333333332e-03));  // 1/5!
-            p = fma_t(p, x, T(4.1666666666666664e-02));  // 1/4!
-            p = fma_t(p, x, T(1.6666666666666666e-01));  // 1/3!
+            T p = fma_t(T(4.1666666666666664e-02), x, T(1.6666666666666666e-01));  // 1/4!, 1/3!
+            p = fma_t(p, x, T(0.5));  // 1/2!
+            p = fma_t(p, x, T(1));
+            return fma_t(p, x, T(1));
         }
-        p = fma_t(p, x, T(0.5));  // 1/2!
-        p = fma_t(p, x, T(1));
-        return fma_t(p, x, T(1));
+        // Estrin's scheme (three levels instead of Horner's seven):
+        // (1 + x + x^2/2! + x^3/3!) + x^4 (1/4! + x/5! + x^2/6!)
+        const T x2 = mul_t(x, x);
+        const T x4 = mul_t(x2, x2);
+        const T a0 = x + T(1);
+        const T a1 = fma_t(x, T(1.6666666666666666e-01), T(0.5));
+        const T b0 = fma_t(x, T(8.3333333333333332e-03), T(4.1666666666666664e-02));
+        const T lo = fma_t(a1, x2, a0);
+        const T hi = fma_t(x2, T(1.3888888888888889e-03), b0);
+        return fma_t(hi, x4, lo);
     }
     if (!__any_sync(0xffffffffu, !phase_small(th))) {
         const T x = -th;

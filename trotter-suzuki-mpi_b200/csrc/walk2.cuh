@@ -330,7 +330,11 @@ __device__ __forceinline__ bool w2_rows(Walk2<V, R> &w, int base, uint32_t ph) {
     return true;
 }
 
-// One task: strip x segment, interior strips first.
+// One task: strip x segment.  The first and last strips come first: their
+// tasks start with extra set-up (clearing the ring bytes outside the tile),
+// and the lowest task indices go to the blocks the SMs schedule first (the
+// warp scheduler favours older blocks; tasks in the youngest blocks of an SM
+// start and finish last).
 template <class V, int R>
 __device__ __forceinline__ void w2_task(Walk2<V, R> &w, const StepArgs<typename V::T> &a, int task) {
     using T = typename V::T;
@@ -340,16 +344,16 @@ __device__ __forceinline__ void w2_task(Walk2<V, R> &w, const StepArgs<typename 
     const int lane = w.lane;
     int strip, seg;
     {
-        const int n_int = a.n_strips > 2 ? (a.n_strips - 2) * a.n_segs : 0;
-        if (task < n_int) {
-            strip = 1 + task % (a.n_strips - 2);
-            seg = task / (a.n_strips - 2);
-        } else {
-            const int e = task - n_int;
-            const int n_edge_strips = a.n_strips > 2 ? 2 : a.n_strips;
-            const int es = e % n_edge_strips;
+        const int n_edge_strips = a.n_strips > 2 ? 2 : a.n_strips;
+        const int n_edge = n_edge_strips * a.n_segs;
+        if (task < n_edge) {
+            const int es = task % n_edge_strips;
             strip = (a.n_strips > 2 && es == 1) ? a.n_strips - 1 : es;
-            seg = e / n_edge_strips;
+            seg = task / n_edge_strips;
+        } else {
+            const int e = task - n_edge;
+            strip = 1 + e % (a.n_strips - 2);
+            seg = e / (a.n_strips - 2);
         }
     }
     const int ox0 = strip * S::WO, ox1 = min(ox0 + S::WO, a.W);
