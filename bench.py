@@ -408,7 +408,7 @@ def run_b200_arm(args, rank, world, local, pg):
     # against FP32 storage on the precision configuration (8192^2 periodic
     # rotating-frame GPE, 5000 steps) and the adjoint/forward cost with its
     # finite-difference check (512^2 real time, 3000 steps)
-    precision = adjoint = None
+    precision = adjoint = slab = None
     if not args.no_configs:
         torch.cuda.empty_cache()
         vres, vclk, _ = vortex_leg(args, local, pg, device, stream, conditioning=False)
@@ -435,6 +435,12 @@ def run_b200_arm(args, rank, world, local, pg):
                      for k, v in aout.items()},
             "clocks": aclk,
         }
+        # the precision configuration's lattice as one lattice in slabs of
+        # rows over the ranks (strong scaling; at N = 1 one slab that is its
+        # own neighbour across the periodic wrap)
+        torch.cuda.empty_cache()
+        sres, sclk, _ = slab_leg(args, rank, world, local, pg, device)
+        slab = dict(sres, config=slab_config(), clocks=sclk)
 
     if rank != 0:
         return
@@ -478,6 +484,7 @@ def run_b200_arm(args, rank, world, local, pg):
         "fp32_store": fp32,
         "precision_config": precision,
         "adjoint_config": adjoint,
+        "slab_config": slab,
         "cpu_baseline": cpu,
         "clocks": clk,
         "gpu_launches": launches,
@@ -993,6 +1000,155 @@ def vortex_config(steps=VORTEX_STEPS):
             "initial": "Thomas-Fermi x 8 windings (radius 10)", "seed": VORTEX_SEED}
 
 
+# ------------------------------------------------------------- slab workload
+# The precision workload's lattice (8192^2, periodic, rotating frame, FP64
+# real time) as ONE lattice split into slabs of rows: one slab per rank over
+# NCCL (strong scaling: the whole job does the same work at every N), or
+# several slabs on the one GPU of a process (--slabs-per-gpu), exchanged by
+# device copies.  Each slab steps as its edge bands and its interior on two
+# streams; the halo rows move while the interior runs.
+SLAB_STEPS = 200      # Trotter steps per bench step
+SLAB_BYTES = 48       # FP64 real time, rotating frame: psi in + out + complex table
+
+
+def slab_tiles(rank, world, per_gpu, precision):
+    """This rank's slab kernels of the 8192^2 vortex lattice (state and
+    potential table from the same psi0 and trap as the precision workload)."""
+    import torch
+    import trottersuzuki_b200 as ts
+    from trottersuzuki_b200 import Kernel
+    from trottersuzuki_b200.api import _coordinate_grid
+    from trottersuzuki_b200.slab import SlabLayout
+    grid = ts.Lattice2D(VORTEX_N, VORTEX_LENGTH, periodic_x_axis=True, periodic_y_axis=True,
+                        angular_velocity=VORTEX_OMEGA)
+    pot = ts.HarmonicPotential(grid, 1.0, 1.0)
+    ham = ts.Hamiltonian(grid, pot, 1.0, VORTEX_G, 0.0, VORTEX_OMEGA)
+    whole = ts.make_desc(grid, ham, VORTEX_DT, False, 0.0, precision)
+    re0, im0, _ = vortex_initial(grid)
+    X, Y = _coordinate_grid(grid)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    x = torch.tensor(np.ascontiguousarray(X[0, :]), dtype=torch.float64, device=dev)[None, :]
+    ys = np.ascontiguousarray(Y[:, 0])
+    n_slabs = world * per_gpu
+    kernels, layouts = [], []
+    for j in range(per_gpu):
+        r = rank * per_gpu + j
+        lay = SlabLayout(VORTEX_N, whole.halo_y, True, r, n_slabs)
+        d = type(whole).from_buffer_copy(whole)
+        d.dim_y = lay.rows
+        d.inner_y0, d.inner_y1 = lay.inner_rows()
+        d.periodic_y = 0
+        d.rot_offset_y = whole.rot_offset_y + lay.start + whole.halo_y
+        rows = slice(lay.start + whole.halo_y, lay.end + whole.halo_y)
+        k = Kernel(d)
+        k.set_state(re0[rows] + 1j * im0[rows])
+        y = torch.tensor(ys[rows], dtype=torch.float64, device=dev)[:, None]
+        V = (0.5 * (x * x + y * y)).contiguous()
+        torch.cuda.synchronize()
+        k.set_potential_device(V.data_ptr(), V.shape[1], VORTEX_DT)
+        k.synchronize()
+        del V, y
+        kernels.append(k)
+        layouts.append(lay)
+    del re0, im0, X, Y
+    return kernels, layouts
+
+
+def slab_leg(args, rank, world, local, pg, device, per_gpu=1, split=True, steps=SLAB_STEPS):
+    """Strong scaling of one lattice: value = lattice site-steps per second of
+    the whole job (the slowest rank's device time)."""
+    import torch
+    from trottersuzuki_b200 import _capi, launch_count
+    from trottersuzuki_b200.slab import NativeSlabs
+    if world > 1 and per_gpu != 1:
+        raise ValueError("several slabs per GPU only in a one-process run")
+    kernels, layouts = slab_tiles(rank, world, per_gpu, _capi.FP64)
+    stream = torch.cuda.Stream(device=device)
+    for k in kernels:
+        k.set_stream(stream.cuda_stream)
+    if per_gpu > 1:
+        slabs = NativeSlabs.local(kernels, layouts)
+        transport = f"{per_gpu} slabs on one GPU, device copies"
+    else:
+        import torch.distributed as dist
+        slabs = NativeSlabs.nccl(kernels[0], layouts[0], dist if pg else None)
+        transport = "NCCL send/recv between ranks" if world > 1 else \
+            "NCCL send/recv of the one slab with itself across the periodic wrap"
+    slabs.set_split(split)
+    edge, inner, is_split, per_step = slabs.plan(0)
+    for _ in range(args.warmup):
+        slabs.evolve(20)
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    l0 = launch_count()
+    with Clocks(local) as clocks:
+        e0.record(stream)
+        for _ in range(args.steps):
+            slabs.evolve(steps)
+        e1.record(stream)
+        e1.synchronize()
+    launches = launch_count() - l0
+    ms = max_over_ranks(e0.elapsed_time(e1), pg, device)
+    norm = sum(k.squared_norm() for k in kernels)
+    if pg:
+        t = torch.tensor([norm], dtype=torch.float64, device=device)
+        pg.all_reduce(t)
+        norm = float(t.item())
+    total = VORTEX_N * VORTEX_N * steps * args.steps
+    rows_here = sum(lay.inner_end - lay.inner_start for lay in layouts)
+    per_gpu_bytes = SLAB_BYTES * VORTEX_N * rows_here * steps * args.steps
+    peak, peak_kind = measured_peak()
+    ach = per_gpu_bytes / (ms * 1e-3) / 1e9
+    slabs.close()
+    for k in kernels:
+        k.close()
+    return {"value": total / (ms * 1e-3), "unit": "site-steps/s", "ms": ms,
+            "us_per_trotter_step": ms / (steps * args.steps) * 1e3,
+            "slabs": world * per_gpu, "slabs_per_gpu": per_gpu, "split": bool(is_split),
+            "edge_windows": edge, "interior_window": list(inner),
+            "kernel_launches_per_step": per_step, "transport": transport,
+            "squared_norm_after": norm,
+            "roofline": {"achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                         "peak_kind": peak_kind, "algorithmic_bytes_per_site": SLAB_BYTES,
+                         "note": "this rank's inner rows; halo rows recomputed by both "
+                                 "neighbours are not counted"}}, clocks.summary(), launches
+
+
+def slab_config(steps=SLAB_STEPS):
+    return dict(vortex_config(steps), workload="vortex8192_slabs", precision="fp64",
+                split="rows, one slab per rank")
+
+
+def run_slab_workload(args, rank, world, local, pg):
+    import torch
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    res, clk, launches = slab_leg(args, rank, world, local, pg, device,
+                                  per_gpu=args.slabs_per_gpu, split=not args.no_split)
+    if rank != 0:
+        return
+    r = res["roofline"]
+    line = {
+        "metric": "site-steps/s", "value": res["value"], "unit": "site-steps/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": res["ms"] / args.steps, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": dict(slab_config(), parallelism=f"slabs{res['slabs']}",
+                       l2="inputs larger than L2: 3 GiB moved per Trotter step in FP64"),
+        "slab": res,
+        "roofline": {"bound": "hbm", "achieved": r["achieved"], "peak": r["peak"],
+                     "unit": "GB/s", "frac": r["frac"], "peak_kind": r["peak_kind"],
+                     "traffic": None, "kernel": "tsb::step_kernel<double, C=2, real, rotating "
+                                                "frame, GPE>, edge bands + interior"},
+        "clocks": clk,
+        "gpu_launches": launches,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_vortex_workload(args, rank, world, local, pg):
     import torch
     torch.cuda.set_device(local)
@@ -1377,6 +1533,13 @@ def main():
                     help="skip the precision (8192^2) and adjoint (512^2) legs of the default run")
     ap.add_argument("--no-ref-gpu", action="store_true",
                     help="reference arm: skip timing the reference's CUDA kernel")
+    ap.add_argument("--split", choices=["none", "slab"], default="none",
+                    help="slab: the 8192^2 vortex lattice as one lattice in slabs of rows "
+                         "over the ranks (strong scaling)")
+    ap.add_argument("--slabs-per-gpu", type=int, default=1,
+                    help="--split slab in one process: this many slabs on its GPU")
+    ap.add_argument("--no-split", action="store_true",
+                    help="--split slab: one launch per slab step (no edge/interior overlap)")
     ap.add_argument("--workload", choices=["gpe_imaginary_time_2048", "batch512", "adjoint512",
                                            "vortex8192", "moving_trap_2048",
                                            "two_component_2048", "cylindrical_vortex_2048"],
@@ -1387,6 +1550,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference_arm(args, rank, world, pg)
+        elif args.split == "slab":
+            run_slab_workload(args, rank, world, local, pg)
         elif args.workload == "batch512":
             run_batch_workload(args, rank, world, local, pg)
         elif args.workload == "adjoint512":

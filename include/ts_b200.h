@@ -216,6 +216,76 @@ int ts_b200_rows(ts_b200_kernel *k, int row0, int nrows, void **ptr, size_t *byt
 int ts_b200_last_norm(ts_b200_kernel *k, double **device_ptr);
 int ts_b200_renormalize_from(ts_b200_kernel *k, const double *total_norm);
 
+/* ---- Slabs driven natively: the same lattice split, with the exchange and
+ * the joint norm issued on the tiles' streams (no host step per step),
+ * replayed from CUDA graphs, and each step run as its edge bands (the rows
+ * the neighbours need) and its interior (which reads no halo row) on two
+ * streams, so that the exchange overlaps the interior: the reference's
+ * halo-first step, src/solver.cpp:202-210 with src/cpukernel.cpp:691-747
+ * (run_kernel_on_halo, start_halo_exchange, run_kernel,
+ * finish_halo_exchange).  A slab tile is closed in y (periodic_y = 0): inner
+ * rows [inner_y0, inner_y1), halo_y rows above it when it has an upper
+ * neighbour (inner_y0 = halo_y, else 0) and below it when it has a lower one
+ * (dim_y - inner_y1 = halo_y, else inner_y1 = dim_y); periodic x is kept on
+ * the tile.  Imaginary-time tiles carry the whole lattice's norm0. */
+typedef struct ts_b200_slabs ts_b200_slabs;
+
+/* A slab's neighbours: up (smaller rows) and down; a tile index of the group
+ * (slabs of one process) or a rank of the communicator (NCCL); -1 none.  The
+ * *_wraps flags mark a link across the lattice's periodic wrap, whose
+ * messages the last step of an evolve call leaves out (src/solver.cpp:
+ * 203-209, where a single tile skips its periodic halo copy). */
+typedef struct {
+    int32_t up, down;
+    int32_t up_wraps, down_wraps;
+} ts_b200_slab_link;
+
+/* Row windows of a slab's split step (host only, no device needed): out[0..3]
+ * the edge windows [a0, a1) and [b0, b1) (b0 = b1 = 0 for one), out[4..5] the
+ * interior, out[6] 1 when the step splits (a neighbour and an interior of
+ * at least 2 reach + 2 rows), out[7] 0.  reach: rows a segment's walk reads
+ * past its output rows (4; 6 in a rotating frame), at most halo. */
+int ts_b200_slab_windows(int rows, int inner_y0, int inner_y1, int halo, int reach, int has_up,
+                         int has_down, int32_t out[8]);
+
+/* The messages of a slab's step (host only): up to 4 entries of
+ * (peer, first tile row of the h-row span, tag, 1 send / 0 receive) in the
+ * order both ends post them, as src/cpukernel.cpp:717-747: the last h inner
+ * rows go down into the lower neighbour's top halo (tag 1), the first h
+ * inner rows up into the upper neighbour's bottom halo (tag 2).  final: the
+ * last step of an evolve call (links across the wrap left out).  Returns the
+ * number of entries (negative: invalid arguments). */
+int ts_b200_slab_messages(int inner_y0, int inner_y1, int halo, const ts_b200_slab_link *link,
+                          int final, int32_t out[16]);
+
+/* Slabs of one process on one GPU (their exchange by device copies). */
+int ts_b200_slabs_create_local(ts_b200_slabs **out, ts_b200_kernel *const *tiles,
+                               const ts_b200_slab_link *links, int n_tiles);
+
+/* One slab per process, the exchange and the norm sum over NCCL (loaded at
+ * run time: the libnccl.so.2 already in the process, else the loader's).
+ * Rank 0 draws the id with ts_b200_nccl_unique_id and the ranks share it;
+ * creation is collective over the nranks ranks. */
+int ts_b200_nccl_unique_id(void *id, size_t bytes);
+int ts_b200_slabs_create_nccl(ts_b200_slabs **out, ts_b200_kernel *tile,
+                              const ts_b200_slab_link *link, const void *nccl_id, size_t id_bytes,
+                              int nranks, int rank);
+
+/* 1 (default): split steps where a slab allows; 0: one launch per step. */
+int ts_b200_slabs_set_split(ts_b200_slabs *s, int on);
+
+/* The plan of tile `tile`: out[0..6] as ts_b200_slab_windows (as used),
+ * out[7] the group's kernel launches per step. */
+int ts_b200_slabs_plan(ts_b200_slabs *s, int tile, int32_t out[8]);
+
+/* `iterations` steps of every slab, ordered after the work queued on the
+ * tiles' streams, and the tiles' streams ordered after them (no host
+ * synchronisation).  Steps 0 .. iterations-2 exchange every message, the
+ * last leaves out the ones across the periodic wrap. */
+int ts_b200_slabs_evolve(ts_b200_slabs *s, int iterations);
+const char *ts_b200_slabs_last_error(const ts_b200_slabs *s);
+int ts_b200_slabs_destroy(ts_b200_slabs *s);
+
 /* Queue all work of this handle on `stream` (a cudaStream_t); NULL restores
  * the handle's own stream. */
 int ts_b200_set_stream(ts_b200_kernel *k, void *stream);

@@ -150,3 +150,106 @@ def test_layout_matches_the_reference_borders():
     # after the last step of a call the wrap (rank 2 -> 0) is skipped
     sends, recvs = SlabLayout(100, 4, True, 2, 3).messages(final=True)
     assert sends == [(4, 4, 1, 2)] and recvs == [(0, 4, 1, 1)]
+
+
+# ---- the library's slab plan (ts_b200_slab_messages / ts_b200_slab_windows):
+# host functions, no device needed
+
+LAYOUTS = [(ny, h, per, world) for ny in (40, 41, 100, 333) for h in (4, 8)
+           for per in (False, True) for world in (1, 2, 3, 5)]
+
+
+def _layouts():
+    from trottersuzuki_b200.slab import SlabLayout
+    for ny, h, per, world in LAYOUTS:
+        for rank in range(world):
+            try:
+                yield SlabLayout(ny, h, per, rank, world)
+            except ValueError:
+                continue
+
+
+def test_library_messages_match_the_layout():
+    """The messages the native engine posts are the layout's (the reference's
+    exchange, src/cpukernel.cpp:717-747), in the same order, final or not."""
+    from trottersuzuki_b200.slab import slab_messages
+    n = 0
+    for lay in _layouts():
+        for final in (False, True):
+            assert slab_messages(lay, final) == lay.messages(final), (lay.ny, lay.rank, final)
+            n += 1
+    assert n > 100
+
+
+def test_split_windows_cover_the_slab():
+    """Edge bands hold every row sent to a neighbour, the interior reads no
+    halo row (its walk reaches `reach` rows past its window), the windows
+    start on even rows and together cover the tile once."""
+    from trottersuzuki_b200.slab import split_windows
+    n_split = 0
+    for lay in _layouts():
+        a, b = lay.inner_rows()
+        for reach in (4, 6):
+            if reach > lay.halo:
+                continue
+            edge, inner, split = split_windows(lay.rows, a, b, lay.halo, reach,
+                                               lay.up is not None, lay.down is not None)
+            if not split:
+                continue
+            n_split += 1
+            wins = [w for w in edge if w[1] > w[0]] + [inner]
+            covered = sorted(r for w in wins for r in range(*w))
+            assert covered == list(range(lay.rows))
+            assert all(w[0] % 2 == 0 for w in wins)
+            sends, _ = lay.messages()
+            for row, cnt, _, _ in sends:
+                assert any(w[0] <= row and row + cnt <= w[1] for w in edge)
+            # halo rows exist on the sides with a neighbour
+            assert lay.up is None or inner[0] - reach >= a
+            assert lay.down is None or inner[1] + reach <= b
+    assert n_split > 50
+
+
+def _plan_rank(rank, world, port, out_dir):
+    import datetime
+    import sys
+
+    import torch.distributed as dist
+    sys.path.insert(0, os.path.join(REPO, "trotter-suzuki-mpi_b200"))
+    from trottersuzuki_b200.slab import SlabLayout, slab_messages
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
+                            world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        res = {}
+        for ny, per in ((100, True), (100, False), (41, True)):
+            lay = SlabLayout(ny, 4, per, rank, world)
+            plans = [None] * world
+            mine = {f: slab_messages(lay, f) for f in (False, True)}
+            dist.all_gather_object(plans, mine)
+            # every span sent to a peer meets a receive of that peer from this
+            # rank, in the same position of the per-peer order (NCCL matches
+            # sends and receives between two ranks in posting order)
+            ok = True
+            for f in (False, True):
+                for p in range(world):
+                    to_p = [(c, tag) for _, c, peer, tag in plans[rank][f][0] if peer == p]
+                    p_from_me = [(c, tag) for _, c, peer, tag in plans[p][f][1] if peer == rank]
+                    ok = ok and to_p == p_from_me
+            res[f"{ny}-{per}"] = ok
+        with open(os.path.join(out_dir, f"plan{rank}.json"), "w") as fh:
+            json.dump(res, fh)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_library_messages_pair_up_across_ranks(world, tmp_path):
+    """Over gloo ranks: each rank's sends to a peer and that peer's receives
+    from it agree in number, size, tag and order (so NCCL's in-order matching
+    pairs them), on every step and on the last step of a call."""
+    import torch.multiprocessing as mp
+    mp.start_processes(_plan_rank, args=(world, free_port(), str(tmp_path)), nprocs=world,
+                       join=True, start_method="spawn")
+    for r in range(world):
+        res = json.loads((tmp_path / f"plan{r}.json").read_text())
+        assert all(res.values()), (r, res)

@@ -92,4 +92,32 @@ int launch_step_buffers(ts_b200_kernel *k, const void *in, void *out);
 // the step, so a captured evolve graph is dropped when it changes).
 int set_norm0(ts_b200_kernel *k, double norm0);
 
+// One launch of the fused step over some of the tile's output rows: window
+// [a0, a1) and, if b1 > b0, window [b0, b1) (even starts; a1 = 0: the whole
+// tile), on `stream`, with its own block ticket and, in imaginary time, its
+// own block partials.  pair_norm / pair_ticket non-null: the step is split
+// over two such launches (pair_slot 0 and 1) that read the same input buffer
+// and write disjoint rows; the second to finish ends the step.  blocks > 0
+// caps the grid.
+struct StepPart {
+    int a0 = 0, a1 = 0, b0 = 0, b1 = 0;
+    cudaStream_t stream = nullptr;
+    double *partials = nullptr;
+    unsigned int *ticket = nullptr;
+    double *pair_norm = nullptr;
+    unsigned int *pair_ticket = nullptr;
+    int pair_slot = 0;
+    int blocks = 0;
+};
+
+// Resident grid and segment height of the tile's step (once per shape).
+int configure_step(ts_b200_kernel *k);
+// Grid of a part's launch (after configure_step).
+int part_blocks(const ts_b200_kernel *k, const StepPart &p);
+int launch_step_part(ts_b200_kernel *k, const void *in, void *out, const StepPart &p);
+// Rows a segment's walk reads beyond its output rows (the variant's HY).
+int step_reach_rows(const ts_b200_kernel *k);
+// Periodic halo of the current buffer (x only for a slab tile) on `stream`.
+int launch_halo_on(ts_b200_kernel *k, cudaStream_t stream);
+
 }  // namespace tsbh

@@ -95,7 +95,67 @@ struct StepArgs {
     // (a - 1 in delta form); the sign of the mirrored axis column
     const void *rad;
     T mirror_sign;
+    // Output rows of the launch.  win_n0 = 0: the whole tile, segment s the
+    // rows [s seg_h, (s + 1) seg_h) clipped to H.  Otherwise two windows of
+    // rows (even starts): segments 0 .. win_n0-1 cover [win_a0, win_a1),
+    // the rest [win_b0, win_b1).  A slab's step runs as two launches over
+    // disjoint windows (its edge bands, then its interior), which read the
+    // same input buffer.
+    int win_n0, win_a0, win_a1, win_b0, win_b1;
+    // The launch's block ticket (null: scal->ticket).  pair_norm non-null:
+    // the step is split over two launches, each writes its squared norm to
+    // pair_norm[pair_slot]; the last block of the second launch to finish
+    // (pair_ticket) sums them, slot 0 first, and ends the step (norm,
+    // renormalisation, coefficient schedule).
+    unsigned int *ticket;
+    double *pair_norm;
+    unsigned int *pair_ticket;
+    int pair_slot;
 };
+
+// Output rows [oy0, oy1) of segment `seg` of the launch.
+template <typename T>
+__device__ __forceinline__ void segment_rows(const StepArgs<T> &a, int seg, int &oy0, int &oy1) {
+    if (a.win_n0 == 0) {
+        oy0 = seg * a.seg_h;
+        oy1 = min(oy0 + a.seg_h, a.H);
+    } else if (seg < a.win_n0) {
+        oy0 = a.win_a0 + seg * a.seg_h;
+        oy1 = min(oy0 + a.seg_h, a.win_a1);
+    } else {
+        oy0 = a.win_b0 + (seg - a.win_n0) * a.seg_h;
+        oy1 = min(oy0 + a.seg_h, a.win_b1);
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ unsigned int *launch_ticket(const StepArgs<T> &a) {
+    return a.ticket ? a.ticket : &a.scal->ticket;
+}
+
+// Called by the last block of a launch (one thread): true when the step ends
+// with this launch (a single launch, or the second of a split step to finish).
+template <typename T>
+__device__ __forceinline__ bool step_ends_here(const StepArgs<T> &a) {
+    if (!a.pair_ticket) return true;
+    __threadfence();
+    if (atomicAdd(a.pair_ticket, 1u) != 1u) return false;
+    *a.pair_ticket = 0u;
+    __threadfence();
+    return true;
+}
+
+// Imaginary time, the last block of a launch with the launch's squared norm
+// in *tot: true when the step ends here, with the step's norm in *tot (for a
+// split step, the two launches' norms, slot 0 first).
+template <typename T>
+__device__ __forceinline__ bool split_norm_total(const StepArgs<T> &a, double *tot) {
+    if (!a.pair_norm) return true;
+    a.pair_norm[a.pair_slot] = *tot;
+    if (!step_ends_here(a)) return false;
+    *tot = __ldcg(&a.pair_norm[0]) + __ldcg(&a.pair_norm[1]);
+    return true;
+}
 
 // ---------------------------------------------------------------- PTX helpers
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -1082,8 +1142,7 @@ __device__ __forceinline__ void run_task(Walk<V> &w, const StepArgs<typename V::
     }
     const int ox0 = strip * WO, ox1 = min(ox0 + WO, a.W);
     const int c0 = ox0 - HX;
-    w.oy0 = seg * a.seg_h;
-    w.oy1 = min(w.oy0 + a.seg_h, a.H);
+    segment_rows(a, seg, w.oy0, w.oy1);
     w.ra = max(w.oy0 - HY, 0);
     w.rb = min(w.oy1 + HY, a.H);
     const int cs = max(c0, 0);
@@ -1214,9 +1273,10 @@ __global__ void __launch_bounds__(128, V::MIN_BLOCKS) step_kernel(StepArgs<typen
             __syncthreads();
             if (threadIdx.x == 0) {
                 __threadfence();
-                if (atomicAdd(&a.scal->ticket, 1u) == gridDim.x - 1) {
-                    a.scal->step += 1u;
-                    a.scal->ticket = 0u;
+                unsigned int *tk = launch_ticket(a);
+                if (atomicAdd(tk, 1u) == gridDim.x - 1) {
+                    *tk = 0u;
+                    if (step_ends_here(a)) a.scal->step += 1u;
                     __threadfence();
                 }
             }
@@ -1240,7 +1300,7 @@ __global__ void __launch_bounds__(128, V::MIN_BLOCKS) step_kernel(StepArgs<typen
             for (int i = 0; i < warps; ++i) b += s_warp[i];
             a.partials[blockIdx.x] = b;
             __threadfence();
-            const unsigned int t = atomicAdd(&a.scal->ticket, 1u);
+            const unsigned int t = atomicAdd(launch_ticket(a), 1u);
             s_last = (t == gridDim.x - 1) ? 1u : 0u;
         }
         __syncthreads();
@@ -1265,9 +1325,10 @@ __global__ void __launch_bounds__(128, V::MIN_BLOCKS) step_kernel(StepArgs<typen
                 __syncthreads();
             }
             if (threadIdx.x == 0) {
-                const double tot = red[0] * a.dxdy;
-                a.scal->last_norm = tot;
+                double tot = red[0] * a.dxdy;
+                *launch_ticket(a) = 0u;
                 if constexpr (V::PB) {
+                    a.scal->last_norm = tot;
                     // the other species' next step reads this step's input
                     // buffer with the factor that was pending on it
                     a.scal->prev_inv = a.scal->pending_inv;
@@ -1276,10 +1337,10 @@ __global__ void __launch_bounds__(128, V::MIN_BLOCKS) step_kernel(StepArgs<typen
                     // a share (src/cpukernel.cpp:551, norm[i] != 0)
                     const double n0 = a.scal->norm_target;
                     if (n0 != 0.0) a.scal->pending_inv = 1.0 / sqrt(tot / n0);
-                } else {
+                } else if (split_norm_total(a, &tot)) {
+                    a.scal->last_norm = tot;
                     if (a.scal->renorm) a.scal->pending_inv = 1.0 / sqrt(tot / a.norm0);
                 }
-                a.scal->ticket = 0u;
             }
         }
     }
@@ -1345,6 +1406,10 @@ __device__ __forceinline__ StepArgs<T> load_tile_args(const StepArgs<T> *p) {
     a.scal = bcast0_ptr(ldg_ptr(&p->scal));
     a.dxdy = bcast0(__ldg(&p->dxdy));
     a.norm0 = bcast0(__ldg(&p->norm0));
+    a.win_n0 = 0;
+    a.ticket = nullptr;
+    a.pair_norm = nullptr;
+    a.pair_ticket = nullptr;
     return a;
 }
 

@@ -645,15 +645,24 @@ void auto_segments(ts_b200_kernel *k) {
 // pad: the shared memory of a launch with programmatic dependent launch
 // (padded to the grid's share of blocks per SM); without it, the kernel's own
 // need (for the occupancy that chooses the shape).
+// part: the launch covers the part's row windows (no padding).
 void geometry(const ts_b200_kernel *k, int *strips, int *segs, int *blocks, size_t *smem,
-              bool pad = true) {
+              bool pad = true, const tsbh::StepPart *part = nullptr) {
     const int hx = (k->rot || k->cyl) ? 8 : 4;  // Variant::HX
     const int wo = 32 * k->C - 2 * hx;
     *strips = div_up(k->W, wo);
-    *segs = div_up(k->H, eff_seg(k));
+    const int sh = eff_seg(k);
+    if (part && part->a1 > 0) {
+        *segs = div_up(part->a1 - part->a0, sh) +
+                (part->b1 > part->b0 ? div_up(part->b1 - part->b0, sh) : 0);
+        pad = false;
+    } else {
+        *segs = div_up(k->H, sh);
+    }
     const int tasks = *strips * *segs;
     *blocks = div_up(tasks, k->warps);
     if (k->resident_blocks > 0) *blocks = std::min(*blocks, k->resident_blocks);
+    if (part && part->blocks > 0) *blocks = std::min(*blocks, part->blocks);
     if (use_walk2(k)) {
         // per warp: a ring of 6 rows, the vertical pair coefficients and one
         // mbarrier per ring slot (of 1 or 2 rows)
@@ -679,7 +688,8 @@ void geometry(const ts_b200_kernel *k, int *strips, int *segs, int *blocks, size
 }
 
 template <typename T>
-int launch_halo_t(ts_b200_kernel *k) {
+int launch_halo_t(ts_b200_kernel *k, cudaStream_t stream = nullptr) {
+    if (!stream) stream = k->stream;
     if (!(k->d.periodic_x || k->d.periodic_y)) return TS_B200_OK;
     const int hx = k->d.halo_x, hy = k->d.halo_y;
     const int nx = k->d.periodic_x ? 2 * hx * k->H : 0;
@@ -688,7 +698,7 @@ int launch_halo_t(ts_b200_kernel *k) {
     if (n <= 0) return TS_B200_OK;
     const int threads = 256;
     const int nb = std::min(div_up(n, threads), 4096);
-    halo_kernel<T><<<nb, threads, 0, k->stream>>>(reinterpret_cast<Cx<T> *>(k->psi[k->cur]), k->W,
+    halo_kernel<T><<<nb, threads, 0, stream>>>(reinterpret_cast<Cx<T> *>(k->psi[k->cur]), k->W,
                                                   k->H, k->P, hx, hy, k->d.periodic_x,
                                                   k->d.periodic_y, k->d.inner_y0);
     cudaError_t e = cudaGetLastError();
@@ -757,24 +767,33 @@ template void tsbh::fill_step_constants<float>(const ts_b200_kernel *, StepArgs<
 
 namespace {
 
+// Resident blocks of this variant and shape (the persistent grid size) and,
+// from them, the segment height.
+template <typename T>
+int configure_t(ts_b200_kernel *k) {
+    if (k->resident_blocks > 0) return TS_B200_OK;
+    int strips, segs, blocks;
+    size_t smem;
+    geometry(k, &strips, &segs, &blocks, &smem, false);
+    StepArgs<T> a0{};
+    int bps = 0;
+    cudaError_t e = dispatch_step<T>(k->C, k->imag, k->rot, k->phase, walk_rows(k), a0, k->warps,
+                                     smem, 0, k->stream, &bps);
+    if (e != cudaSuccess) return cuda_fail(k, e, "step kernel configuration");
+    if (bps < 1) return fail(k, TS_B200_UNSUPPORTED, "step kernel does not fit on an SM");
+    k->resident_blocks = bps * k->num_sms;
+    if (k->auto_seg) auto_segments(k);
+    return TS_B200_OK;
+}
+
 // One fused step from buffer `in` to buffer `out` (no buffer flip, no halo);
 // dry: configure and size the scratch only.
 template <typename T>
 int launch_step_buffers_t(ts_b200_kernel *k, const void *in, void *out, bool dry) {
     int strips, segs, blocks;
     size_t smem;
-    if (k->resident_blocks <= 0) {
-        // resident blocks of this variant and shape: the persistent grid size
-        geometry(k, &strips, &segs, &blocks, &smem, false);
-        StepArgs<T> a0{};
-        int bps = 0;
-        cudaError_t e = dispatch_step<T>(k->C, k->imag, k->rot, k->phase, walk_rows(k), a0,
-                                         k->warps, smem, 0, k->stream, &bps);
-        if (e != cudaSuccess) return cuda_fail(k, e, "step kernel configuration");
-        if (bps < 1) return fail(k, TS_B200_UNSUPPORTED, "step kernel does not fit on an SM");
-        k->resident_blocks = bps * k->num_sms;
-        if (k->auto_seg) auto_segments(k);
-    }
+    const int c = configure_t<T>(k);
+    if (c) return c;
     geometry(k, &strips, &segs, &blocks, &smem);
     const size_t nwarps = (size_t)std::max(blocks, 1) * k->warps;
     if (k->imag && nwarps > k->partials_cap) {
@@ -816,7 +835,67 @@ int launch_step(ts_b200_kernel *k, int exchange, bool dry = false) {
     return k->fp32 ? launch_step_t<float>(k, exchange, dry) : launch_step_t<double>(k, exchange, dry);
 }
 
+template <typename T>
+int launch_step_part_t(ts_b200_kernel *k, const void *in, void *out, const tsbh::StepPart &p) {
+    const int c = configure_t<T>(k);
+    if (c) return c;
+    if (p.a1 > 0 && (p.a0 < 0 || p.a1 <= p.a0 || p.a1 > k->H || (p.a0 & 1) ||
+                     (p.b1 > p.b0 && (p.b0 < 0 || p.b1 > k->H || (p.b0 & 1)))))
+        return fail(k, TS_B200_INVALID_ARGUMENT, "step part: row windows");
+    if (k->imag && !p.partials) return fail(k, TS_B200_INVALID_ARGUMENT, "step part: partials");
+    int strips, segs, blocks;
+    size_t smem;
+    geometry(k, &strips, &segs, &blocks, &smem, false, &p);
+    StepArgs<T> a{};
+    a.psi_in = in;
+    a.psi_out = out;
+    tsbh::fill_step_constants(k, a);
+    a.n_strips = strips;
+    a.n_segs = segs;
+    a.seg_h = eff_seg(k);
+    a.ring = use_walk2(k) ? 6 / walk_rows(k) : k->ring;
+    a.partials = p.partials;
+    if (p.a1 > 0) {
+        a.win_n0 = div_up(p.a1 - p.a0, a.seg_h);
+        a.win_a0 = p.a0;
+        a.win_a1 = p.a1;
+        a.win_b0 = p.b0;
+        a.win_b1 = p.b1 > p.b0 ? p.b1 : p.b0;
+    }
+    a.ticket = p.ticket;
+    a.pair_norm = p.pair_norm;
+    a.pair_ticket = p.pair_ticket;
+    a.pair_slot = p.pair_slot;
+    cudaError_t e = dispatch_step<T>(k->C, k->imag, k->rot, k->phase, walk_rows(k), a, k->warps,
+                                     smem, blocks, p.stream, nullptr, false);
+    if (e != cudaSuccess) return cuda_fail(k, e, "step part launch");
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    return TS_B200_OK;
+}
+
 }  // namespace
+
+int tsbh::configure_step(ts_b200_kernel *k) {
+    return k->fp32 ? configure_t<float>(k) : configure_t<double>(k);
+}
+
+int tsbh::part_blocks(const ts_b200_kernel *k, const tsbh::StepPart &p) {
+    int strips, segs, blocks;
+    size_t smem;
+    geometry(k, &strips, &segs, &blocks, &smem, false, &p);
+    return std::max(blocks, 1);
+}
+
+int tsbh::launch_step_part(ts_b200_kernel *k, const void *in, void *out, const tsbh::StepPart &p) {
+    return k->fp32 ? launch_step_part_t<float>(k, in, out, p)
+                   : launch_step_part_t<double>(k, in, out, p);
+}
+
+int tsbh::step_reach_rows(const ts_b200_kernel *k) { return k->rot ? 6 : 4; }  // Variant::HY
+
+int tsbh::launch_halo_on(ts_b200_kernel *k, cudaStream_t stream) {
+    return k->fp32 ? launch_halo_t<float>(k, stream) : launch_halo_t<double>(k, stream);
+}
 
 int tsbh::launch_step_tile(ts_b200_kernel *k, int exchange) { return launch_step(k, exchange); }
 

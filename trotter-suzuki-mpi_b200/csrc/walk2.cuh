@@ -358,7 +358,8 @@ __device__ __forceinline__ void w2_task(Walk2<V, R> &w, const StepArgs<typename 
     }
     const int ox0 = strip * S::WO, ox1 = min(ox0 + S::WO, a.W);
     const int c0 = ox0 - S::HX;
-    const int oy0 = seg * a.seg_h, oy1 = min(oy0 + a.seg_h, a.H);
+    int oy0, oy1;
+    segment_rows(a, seg, oy0, oy1);
     w.ra = oy0 - S::HY;
     w.nit = (oy1 - oy0) + 2 * S::HY;
     w.n_lo = a.iy0 - oy0 + 8;
@@ -479,9 +480,10 @@ __device__ __forceinline__ void w2_finish(const StepArgs<typename V::T> &a, doub
             __syncthreads();
             if (threadIdx.x == 0) {
                 __threadfence();
-                if (atomicAdd(&a.scal->ticket, 1u) == gridDim.x - 1) {
-                    a.scal->step += 1u;
-                    a.scal->ticket = 0u;
+                unsigned int *tk = launch_ticket(a);
+                if (atomicAdd(tk, 1u) == gridDim.x - 1) {
+                    *tk = 0u;
+                    if (step_ends_here(a)) a.scal->step += 1u;
                     __threadfence();
                 }
             }
@@ -500,7 +502,7 @@ __device__ __forceinline__ void w2_finish(const StepArgs<typename V::T> &a, doub
             for (int i = 0; i < warps; ++i) b += s_warp[i];
             a.partials[blockIdx.x] = b;
             __threadfence();
-            const unsigned int t = atomicAdd(&a.scal->ticket, 1u);
+            const unsigned int t = atomicAdd(launch_ticket(a), 1u);
             s_last = (t == gridDim.x - 1) ? 1u : 0u;
         }
         __syncthreads();
@@ -529,18 +531,19 @@ __device__ __forceinline__ void w2_finish(const StepArgs<typename V::T> &a, doub
             if (threadIdx.x == 0) {
                 double t = 0.0;
                 for (int i = 0; i < warps; ++i) t += red[i];
-                const double tot = t * a.dxdy;
-                a.scal->last_norm = tot;
-                if (a.scal->renorm) a.scal->pending_inv = 1.0 / sqrt(tot / a.norm0);
-                a.scal->ticket = 0u;
+                double tot = t * a.dxdy;
+                *launch_ticket(a) = 0u;
+                if (split_norm_total(a, &tot)) {
+                    a.scal->last_norm = tot;
+                    if (a.scal->renorm) a.scal->pending_inv = 1.0 / sqrt(tot / a.norm0);
+                }
             }
         }
     }
 }
 
-// Blocks of 4 or 8 warps (the block partial reduction assumes a power of two
-// threads, at most 256); each warp loops over the tasks
-// t = warp_global, warp_global + total_warps, ...
+// Blocks of 4 or 8 warps; each warp loops over the tasks t = warp_global,
+// warp_global + total_warps, ...
 // Register budget: 2 cells per lane fit 128 registers, so 16 warps of the
 // default 4-warp blocks stay resident per SM; 4 cells per lane take up to 255.
 template <class V, int R>

@@ -70,6 +70,11 @@ class LaunchShape(C.Structure):
     ]
 
 
+class SlabLink(C.Structure):
+    _fields_ = [("up", C.c_int32), ("down", C.c_int32),
+                ("up_wraps", C.c_int32), ("down_wraps", C.c_int32)]
+
+
 # name -> (restype, argtypes); every symbol declared in include/ts_b200.h
 _VP, _SZ, _DP, _I = C.c_void_p, C.c_size_t, C.c_void_p, C.c_int
 SIGNATURES = {
@@ -95,6 +100,17 @@ SIGNATURES = {
     "ts_b200_rows": (_I, [_VP, C.c_int, C.c_int, C.POINTER(_VP), C.POINTER(_SZ)]),
     "ts_b200_last_norm": (_I, [_VP, C.POINTER(_VP)]),
     "ts_b200_renormalize_from": (_I, [_VP, _VP]),
+    "ts_b200_slab_windows": (_I, [_I, _I, _I, _I, _I, _I, _I, C.POINTER(C.c_int32)]),
+    "ts_b200_slab_messages": (_I, [_I, _I, _I, C.POINTER(SlabLink), _I, C.POINTER(C.c_int32)]),
+    "ts_b200_nccl_unique_id": (_I, [_VP, _SZ]),
+    "ts_b200_slabs_create_local": (_I, [C.POINTER(_VP), C.POINTER(_VP), C.POINTER(SlabLink), _I]),
+    "ts_b200_slabs_create_nccl": (_I, [C.POINTER(_VP), _VP, C.POINTER(SlabLink), _VP, _SZ, _I,
+                                       _I]),
+    "ts_b200_slabs_set_split": (_I, [_VP, _I]),
+    "ts_b200_slabs_plan": (_I, [_VP, _I, C.POINTER(C.c_int32)]),
+    "ts_b200_slabs_evolve": (_I, [_VP, _I]),
+    "ts_b200_slabs_last_error": (C.c_char_p, [_VP]),
+    "ts_b200_slabs_destroy": (_I, [_VP]),
     "ts_b200_pair_create": (_I, [_VP, _VP, C.c_double, C.c_double, C.c_double, C.c_double,
                                  C.POINTER(_VP)]),
     "ts_b200_pair_rabi": (_I, [_VP, C.c_double]),
@@ -164,9 +180,11 @@ def lib():
     return _lib
 
 
-def check(status, handle=None, batch=None, adjoint=None, pair=None):
+def check(status, handle=None, batch=None, adjoint=None, pair=None, slabs=None):
     if status != OK:
-        if pair:
+        if slabs:
+            msg = lib().ts_b200_slabs_last_error(slabs).decode()
+        elif pair:
             msg = lib().ts_b200_pair_last_error(pair).decode()
         elif adjoint:
             msg = lib().ts_b200_adjoint_last_error(adjoint).decode()

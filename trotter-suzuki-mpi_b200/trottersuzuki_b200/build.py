@@ -21,6 +21,22 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + INCLUDE, "-I" + CSRC]
 
 
+def _nccl_include():
+    """nccl.h (types only: the library is loaded at run time): the NCCL
+    wheel's, else the system's."""
+    try:
+        import nvidia.nccl
+        d = os.path.join(list(nvidia.nccl.__path__)[0], "include")
+        if os.path.exists(os.path.join(d, "nccl.h")):
+            return d
+    except ImportError:
+        pass
+    return "/usr/include"
+
+
+FLAGS.append("-I" + _nccl_include())
+
+
 def _stale(obj, deps):
     if not os.path.exists(obj):
         return True
@@ -87,7 +103,7 @@ def build(verbose=True, extra=()):
         objs = list(ex.map(lambda s: _compile(s, list(extra)), srcs))
     out = os.path.join(HERE, "libtsb200.so")
     if _stale(out, objs):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", out + ".tmp"] + objs + ["-lcudart"]
+        cmd = [NVCC] + ARCH + ["-shared", "-o", out + ".tmp"] + objs + ["-lcudart", "-ldl"]
         subprocess.check_call(cmd)
         os.replace(out + ".tmp", out)
     if verbose:

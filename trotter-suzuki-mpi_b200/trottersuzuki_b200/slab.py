@@ -17,12 +17,18 @@ step(), rows(row0, nrows) (a writable 1D tensor view of those rows),
 last_norm() (a 1-element float64 tensor view) and renormalize_from(t).
 `KernelTile` is the GPU tile; the tests drive the same exchange over the
 oracle on the CPU.
+
+`NativeSlabs` runs the same layout inside the library (ts_b200_slabs_*):
+each step as the slab's edge bands and its interior on two streams, the
+halo rows over NCCL (one slab per rank) or by device copies (slabs of one
+process), the norm summed on the device, all issued on the streams without
+a host round trip per step and replayed from CUDA graphs.
 """
 import contextlib
 import ctypes as C
 import math
 
-from ._capi import check, lib
+from ._capi import SlabLink, check, lib
 
 
 def calculate_borders(coord, dims, length, halo, periodic, inner=None):
@@ -56,8 +62,8 @@ class SlabLayout:
     puts them, and an odd start shifts their checkerboard)."""
 
     def __init__(self, ny, halo_y, periodic_y, rank, world):
-        if world < 2:
-            raise ValueError("a slab layout needs at least two ranks")
+        if world < 1 or not 0 <= rank < world:
+            raise ValueError("rank outside the world")
         if halo_y % 2:
             raise ValueError("the halo must be even")
         self.ny, self.halo, self.periodic = ny, halo_y, bool(periodic_y)
@@ -74,6 +80,10 @@ class SlabLayout:
         # neighbours along y (MPI_Cart_shift(cartcomm, 0, 1, &UP, &DOWN))
         self.up = rank - 1 if rank > 0 else (world - 1 if periodic_y else None)
         self.down = rank + 1 if rank < world - 1 else (0 if periodic_y else None)
+        if self.down is not None and self.end - self.inner_end != halo_y:
+            # the borders reach the lattice's end before the last rank (too
+            # many ranks for the rows): the slabs would overlap
+            raise ValueError("too few rows for this many ranks")
 
     def inner_rows(self):
         """Tile-local [first, last) of the rows this rank owns."""
@@ -187,3 +197,118 @@ class KernelTile:
     def renormalize_from(self, t):
         check(lib().ts_b200_renormalize_from(self.k.handle, C.c_void_p(t.data_ptr())),
               self.k.handle)
+
+
+def slab_link(layout):
+    """The C-ABI link of a layout: its neighbours (-1: none) and the links that
+    cross the lattice's periodic wrap (rank 0 upwards, the last rank
+    downwards)."""
+    up = -1 if layout.up is None else int(layout.up)
+    down = -1 if layout.down is None else int(layout.down)
+    return SlabLink(up, down, int(up >= 0 and layout.periodic and layout.rank == 0),
+                    int(down >= 0 and layout.periodic and layout.rank == layout.world - 1))
+
+
+def split_windows(rows, inner_y0, inner_y1, halo, reach, has_up, has_down):
+    """Row windows of a slab's split step (ts_b200_slab_windows, host only):
+    (edge windows [(a0, a1), (b0, b1)], interior (i0, i1), split)."""
+    out = (C.c_int32 * 8)()
+    check(lib().ts_b200_slab_windows(int(rows), int(inner_y0), int(inner_y1), int(halo),
+                                     int(reach), int(bool(has_up)), int(bool(has_down)), out))
+    v = list(out)
+    return [(v[0], v[1]), (v[2], v[3])], (v[4], v[5]), bool(v[6])
+
+
+def slab_messages(layout, final=False):
+    """(sends, recvs) of the library's exchange for `layout`, in the form of
+    SlabLayout.messages (tile row, rows, peer, tag): ts_b200_slab_messages."""
+    a, b = layout.inner_rows()
+    out = (C.c_int32 * 16)()
+    link = slab_link(layout)
+    n = lib().ts_b200_slab_messages(a, b, layout.halo, C.byref(link), int(bool(final)), out)
+    if n < 0:
+        raise ValueError("invalid slab")
+    v = list(out)
+    sends, recvs = [], []
+    for i in range(n):
+        peer, row, tag, send = v[4 * i:4 * i + 4]
+        (sends if send else recvs).append((row, layout.halo, peer, tag))
+    return sends, recvs
+
+
+class NativeSlabs:
+    """Slabs of one lattice driven by the library.
+
+    local(kernels, layouts): every slab in this process, on one GPU; the
+    halo rows move by device copies.  nccl(kernel, layout, dist): one slab
+    per rank of `dist` (torch.distributed, initialised); the ranks build an
+    NCCL communicator of their own (the id travels over `dist`) and exchange
+    halo rows with ncclSend/ncclRecv on the slab's streams.  Each kernel is a
+    Kernel whose descriptor is its slab's tile (closed in y, inner rows of the
+    layout, the whole lattice's norm0 in imaginary time)."""
+
+    def __init__(self, ptr, keep):
+        self._ptr = ptr
+        self._keep = keep
+
+    @classmethod
+    def local(cls, kernels, layouts):
+        n = len(kernels)
+        handles = (C.c_void_p * n)(*[k.handle for k in kernels])
+        links = (SlabLink * n)(*[slab_link(lay) for lay in layouts])
+        ptr = C.c_void_p()
+        check(lib().ts_b200_slabs_create_local(C.byref(ptr), handles, links, n), kernels[0].handle)
+        return cls(ptr, list(kernels))
+
+    @classmethod
+    def nccl(cls, kernel, layout, dist=None, group=None):
+        """dist may be None for a one-rank layout (its own neighbour across
+        the periodic wrap)."""
+        buf = (C.c_ubyte * 128)()
+        if dist is None:
+            if layout.world != 1:
+                raise ValueError("several ranks need torch.distributed to share the NCCL id")
+            check(lib().ts_b200_nccl_unique_id(buf, 128))
+            uid = buf
+        else:
+            if dist.get_rank(group) == 0:
+                check(lib().ts_b200_nccl_unique_id(buf, 128))
+            obj = [bytes(buf)]
+            src = 0 if group is None else dist.get_global_rank(group, 0)
+            dist.broadcast_object_list(obj, src=src, group=group)
+            uid = (C.c_ubyte * 128).from_buffer_copy(obj[0])
+        link = slab_link(layout)
+        ptr = C.c_void_p()
+        check(lib().ts_b200_slabs_create_nccl(C.byref(ptr), kernel.handle, C.byref(link), uid, 128,
+                                              int(layout.world), int(layout.rank)), kernel.handle)
+        return cls(ptr, [kernel])
+
+    def set_split(self, on):
+        check(lib().ts_b200_slabs_set_split(self._ptr, int(bool(on))), slabs=self._ptr)
+
+    def plan(self, tile=0):
+        """(edge windows, interior window, split, kernel launches per step)."""
+        out = (C.c_int32 * 8)()
+        check(lib().ts_b200_slabs_plan(self._ptr, int(tile), out), slabs=self._ptr)
+        v = list(out)
+        return [(v[0], v[1]), (v[2], v[3])], (v[4], v[5]), bool(v[6]), v[7]
+
+    def evolve(self, iterations):
+        check(lib().ts_b200_slabs_evolve(self._ptr, int(iterations)), slabs=self._ptr)
+
+    def close(self):
+        if self._ptr:
+            lib().ts_b200_slabs_destroy(self._ptr)
+            self._ptr = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
