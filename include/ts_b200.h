@@ -238,6 +238,13 @@ typedef struct ts_b200_slabs ts_b200_slabs;
 typedef struct {
     int32_t up, down;
     int32_t up_wraps, down_wraps;
+    /* periodic x: the tile rows [xhalo_row0, xhalo_row1) whose x halo the
+     * slab refreshes after a step, the rows whose lattice row the whole
+     * tile refreshes (src/cpukernel.cpp:706-716: its rows [inner_y0,
+     * inner_y0 + dim_y - 2 halo_y); for a lattice periodic in y every row,
+     * its y-halo rows taking refreshed rows).  The received halo rows are
+     * refreshed by the receiver: a row's x halo comes from its own cells. */
+    int32_t xhalo_row0, xhalo_row1;
 } ts_b200_slab_link;
 
 /* Row windows of a slab's split step (host only, no device needed): out[0..3]

@@ -223,11 +223,15 @@ def test_native_slabs_fp32(imag):
         assert np.array_equal(got, want)
 
 
-def test_native_slabs_periodic_both_axes():
-    """Periodic in x too: each slab refreshes its own x halo after the
-    exchange (the interior then waits for the end of the previous step)."""
-    lat, psi0, V = _lattice(40, 64, True, True)
-    got, want, _ = _compare_native(lat, psi0, V, 2, (6, 19), g=1.5)
+@pytest.mark.parametrize("world", [2, 3])
+@pytest.mark.parametrize("py", [True, False], ids=["periodic_y", "closed_y"])
+def test_native_slabs_periodic_x(py, world):
+    """Periodic in x: each slab refreshes the x halo of the rows whose
+    lattice rows the whole tile refreshes, received halo rows included, after
+    the exchange (the interior then waits for the end of the previous step);
+    the whole tile's bits, halo columns included."""
+    lat, psi0, V = _lattice(40, 64, True, py)
+    got, want, _ = _compare_native(lat, psi0, V, world, (6, 19), g=1.5)
     assert np.array_equal(got, want)
 
 

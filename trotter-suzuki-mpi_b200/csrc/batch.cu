@@ -82,7 +82,7 @@ template <typename T>
 __global__ void batch_halo_kernel(const StepArgs<T> *inst, const TileHalo *th) {
     const TileHalo h = th[blockIdx.y];
     Cx<T> *psi = reinterpret_cast<Cx<T> *>(const_cast<void *>(inst[h.tile].psi_out));
-    tsb::halo_cells(psi, h.W, h.H, h.P, h.hx, h.hy, h.px, h.py, h.iy0,
+    tsb::halo_cells(psi, h.W, h.H, h.P, h.hx, h.hy, h.px, h.py, h.iy0, h.iy0 + h.H - 2 * h.hy,
                     blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 

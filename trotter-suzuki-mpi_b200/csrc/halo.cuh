@@ -1,6 +1,7 @@
 // Periodic halo refresh of one tile (src/cpukernel.cpp:706-716,738-746, one
-// process): x-halo columns of rows [iy0, iy0 + H - 2*hy) take the opposite
-// inner columns, then y-halo rows take the opposite inner rows (all columns).
+// process): x-halo columns of rows [xr0, xr1) take the opposite inner
+// columns (the reference: [iy0, iy0 + H - 2*hy)), then y-halo rows take the
+// opposite inner rows (all columns).
 // Each destination cell is written from the cell its value ends up coming
 // from; those source cells are never destinations, so one pass suffices.
 #pragma once
@@ -18,12 +19,11 @@ __host__ __device__ inline int halo_cell_count(int W, int H, int hx, int hy, int
 // Destination cells k0, k0 + stride, ... of the refresh.
 template <typename T>
 __device__ __forceinline__ void halo_cells(Cx<T> *psi, int W, int H, int P, int hx, int hy, int px,
-                                           int py, int iy0, int k0, int stride) {
+                                           int py, int xr0, int xr1, int k0, int stride) {
     const int nx_dest = px ? 2 * hx * H : 0;
     const int ncols_b = px ? W - 2 * hx : W;  // y-halo cells outside the x-halo columns
     const int n = halo_cell_count(W, H, hx, hy, px, py);
     const int Nx = W - 2 * hx, Ny = H - 2 * hy;
-    const int xr0 = iy0, xr1 = iy0 + H - 2 * hy;
     for (int k = k0; k < n; k += stride) {
         int x, y;
         if (k < nx_dest) {

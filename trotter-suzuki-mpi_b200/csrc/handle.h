@@ -117,7 +117,8 @@ int part_blocks(const ts_b200_kernel *k, const StepPart &p);
 int launch_step_part(ts_b200_kernel *k, const void *in, void *out, const StepPart &p);
 // Rows a segment's walk reads beyond its output rows (the variant's HY).
 int step_reach_rows(const ts_b200_kernel *k);
-// Periodic halo of the current buffer (x only for a slab tile) on `stream`.
-int launch_halo_on(ts_b200_kernel *k, cudaStream_t stream);
+// Periodic halo of the current buffer (x only for a slab tile) on `stream`;
+// xr1 > xr0: the x halo of rows [xr0, xr1) (default: the reference's rows).
+int launch_halo_on(ts_b200_kernel *k, cudaStream_t stream, int xr0 = 0, int xr1 = 0);
 
 }  // namespace tsbh

@@ -122,7 +122,7 @@ __global__ void slab_renorm_kernel(tsb::Scalars *scal, const double *total, doub
 // ------------------------------------------------------------------ group
 struct SlabTile {
     ts_b200_kernel *k = nullptr;
-    ts_b200_slab_link link{-1, -1, 0, 0};
+    ts_b200_slab_link link{-1, -1, 0, 0, 0, 0};
     int h = 0;                // halo rows
     bool split = false;       // edge bands and interior as two launches
     bool chained = false;     // the interior waits for the end of the previous step
@@ -400,10 +400,12 @@ int issue_step(ts_b200_slabs *s, bool final) {
         k->cur = 1 - k->cur;
     }
     TSS_OK(issue_exchange(s, final));
-    // what needs the whole step: the x halo and the norm
+    // what needs the whole step: the x halo (not after the last step of a
+    // call, as a single tile skips its halo copy there) and the norm
     for (SlabTile &x : s->t) {
         if (x.split && x.chained) TSS_CHECK(s, cudaStreamWaitEvent(x.se, x.ev_int, 0));
-        if (x.k->d.periodic_x) TSS_OK(tsbh::launch_halo_on(x.k, x.se));
+        if (x.k->d.periodic_x && !final && x.link.xhalo_row1 > x.link.xhalo_row0)
+            TSS_OK(tsbh::launch_halo_on(x.k, x.se, x.link.xhalo_row0, x.link.xhalo_row1));
     }
     if (s->imag) {
         if (s->use_nccl) {

@@ -289,8 +289,8 @@ __global__ void copy_tile_kernel(Cx<T> *dst, size_t dpitch, const Cx<T> *src, si
 // those source cells are never destinations, so one pass suffices.
 template <typename T>
 __global__ void halo_kernel(Cx<T> *psi, int W, int H, int P, int hx, int hy, int px, int py,
-                            int iy0) {
-    tsb::halo_cells(psi, W, H, P, hx, hy, px, py, iy0, blockIdx.x * blockDim.x + threadIdx.x,
+                            int xr0, int xr1) {
+    tsb::halo_cells(psi, W, H, P, hx, hy, px, py, xr0, xr1, blockIdx.x * blockDim.x + threadIdx.x,
                     gridDim.x * blockDim.x);
 }
 
@@ -687,9 +687,15 @@ void geometry(const ts_b200_kernel *k, int *strips, int *segs, int *blocks, size
              8 * k->ring);
 }
 
+// xr1 > xr0: the rows whose x halo is refreshed (default: the reference's
+// [inner_y0, inner_y0 + dim_y - 2 halo_y)).
 template <typename T>
-int launch_halo_t(ts_b200_kernel *k, cudaStream_t stream = nullptr) {
+int launch_halo_t(ts_b200_kernel *k, cudaStream_t stream = nullptr, int xr0 = 0, int xr1 = 0) {
     if (!stream) stream = k->stream;
+    if (xr1 <= xr0) {
+        xr0 = k->d.inner_y0;
+        xr1 = k->d.inner_y0 + k->H - 2 * k->d.halo_y;
+    }
     if (!(k->d.periodic_x || k->d.periodic_y)) return TS_B200_OK;
     const int hx = k->d.halo_x, hy = k->d.halo_y;
     const int nx = k->d.periodic_x ? 2 * hx * k->H : 0;
@@ -700,7 +706,7 @@ int launch_halo_t(ts_b200_kernel *k, cudaStream_t stream = nullptr) {
     const int nb = std::min(div_up(n, threads), 4096);
     halo_kernel<T><<<nb, threads, 0, stream>>>(reinterpret_cast<Cx<T> *>(k->psi[k->cur]), k->W,
                                                   k->H, k->P, hx, hy, k->d.periodic_x,
-                                                  k->d.periodic_y, k->d.inner_y0);
+                                                  k->d.periodic_y, xr0, xr1);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(k, e, "halo kernel launch");
     g_launches.fetch_add(1, std::memory_order_relaxed);
@@ -893,8 +899,9 @@ int tsbh::launch_step_part(ts_b200_kernel *k, const void *in, void *out, const t
 
 int tsbh::step_reach_rows(const ts_b200_kernel *k) { return k->rot ? 6 : 4; }  // Variant::HY
 
-int tsbh::launch_halo_on(ts_b200_kernel *k, cudaStream_t stream) {
-    return k->fp32 ? launch_halo_t<float>(k, stream) : launch_halo_t<double>(k, stream);
+int tsbh::launch_halo_on(ts_b200_kernel *k, cudaStream_t stream, int xr0, int xr1) {
+    return k->fp32 ? launch_halo_t<float>(k, stream, xr0, xr1)
+                   : launch_halo_t<double>(k, stream, xr0, xr1);
 }
 
 int tsbh::launch_step_tile(ts_b200_kernel *k, int exchange) { return launch_step(k, exchange); }

@@ -72,7 +72,8 @@ class LaunchShape(C.Structure):
 
 class SlabLink(C.Structure):
     _fields_ = [("up", C.c_int32), ("down", C.c_int32),
-                ("up_wraps", C.c_int32), ("down_wraps", C.c_int32)]
+                ("up_wraps", C.c_int32), ("down_wraps", C.c_int32),
+                ("xhalo_row0", C.c_int32), ("xhalo_row1", C.c_int32)]
 
 
 # name -> (restype, argtypes); every symbol declared in include/ts_b200.h

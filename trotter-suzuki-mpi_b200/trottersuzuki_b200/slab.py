@@ -199,14 +199,27 @@ class KernelTile:
               self.k.handle)
 
 
+def xhalo_rows(layout):
+    """Tile rows [r0, r1) of a slab whose periodic x halo is refreshed after
+    a step: those whose lattice row the whole tile refreshes.  The whole
+    tile refreshes its rows [inner_y0, inner_y0 + dim_y - 2 halo_y)
+    (src/cpukernel.cpp:706-716): for a lattice periodic in y every lattice
+    row (its y-halo rows then copy refreshed rows), for a closed one the
+    lattice rows below ny - 2 halo_y."""
+    if layout.periodic:
+        return 0, layout.rows
+    return 0, max(0, min(layout.rows, layout.ny - 2 * layout.halo - layout.start))
+
+
 def slab_link(layout):
-    """The C-ABI link of a layout: its neighbours (-1: none) and the links that
+    """The C-ABI link of a layout: its neighbours (-1: none), the links that
     cross the lattice's periodic wrap (rank 0 upwards, the last rank
-    downwards)."""
+    downwards) and the rows whose periodic x halo the slab refreshes."""
     up = -1 if layout.up is None else int(layout.up)
     down = -1 if layout.down is None else int(layout.down)
     return SlabLink(up, down, int(up >= 0 and layout.periodic and layout.rank == 0),
-                    int(down >= 0 and layout.periodic and layout.rank == layout.world - 1))
+                    int(down >= 0 and layout.periodic and layout.rank == layout.world - 1),
+                    *xhalo_rows(layout))
 
 
 def split_windows(rows, inner_y0, inner_y1, halo, reach, has_up, has_down):
