@@ -401,6 +401,9 @@ int ts_b200_adjoint_create(const ts_b200_desc *d, double delta_t, int steps, int
                            ts_b200_adjoint **out);
 void ts_b200_adjoint_destroy(ts_b200_adjoint *a);
 int ts_b200_adjoint_set_stream(ts_b200_adjoint *a, void *stream);
+/* Rows per segment task of the adjoint pass (even, >= 2) and of the forward
+ * and recomputation steps (ts_b200_set_launch); 0 keeps the choice. */
+int ts_b200_adjoint_set_segments(ts_b200_adjoint *a, int adjoint_rows, int forward_rows);
 /* psi_t may be NULL (the final state stays in the engine). */
 int ts_b200_adjoint_forward(ts_b200_adjoint *a, const double *potential, const void *psi0,
                             void *psi_t);

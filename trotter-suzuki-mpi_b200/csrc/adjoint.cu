@@ -40,7 +40,6 @@ struct ts_b200_adjoint {
     void *lam[2] = {nullptr, nullptr};
     double *gv = nullptr;
     void *ckpt = nullptr;  // n_ckpt states
-    void *seg = nullptr;   // every - 1 recomputed states
     int *error = nullptr;
     int seg_h = 32, warps = 2, ring = 4, blocks = 0;
     bool forward_done = false;
@@ -48,13 +47,22 @@ struct ts_b200_adjoint {
     // the projection coefficients mu (ping-pong), the running sum of the
     // inner products, block partials and ticket of the reductions; norm0
     bool imag = false;
-    double *ckpt_c = nullptr, *seg_c = nullptr, *mu = nullptr, *ksum = nullptr;
+    double *ckpt_c = nullptr, *mu = nullptr, *ksum = nullptr;
     double *partials = nullptr;
     unsigned int *ticket = nullptr;
     double norm0 = 0.0;
-    void *state0 = nullptr;           // a segment's first state (graph-fixed address)
+    // checkpointed reverse pass: up to two buffer sets, so that the states of
+    // one segment are recomputed (on rstream) while the adjoint passes of the
+    // next run (on the tile's stream); one set when memory is short
+    int nsets = 1;
+    void *seg[2] = {nullptr, nullptr};     // a segment's recomputed states
+    void *state0[2] = {nullptr, nullptr};  // its first state (graph-fixed address)
+    double *seg_c[2] = {nullptr, nullptr}; // imaginary time: their factors
+    cudaStream_t rstream = nullptr;
+    cudaEvent_t ev_start = nullptr, ev_ready[2] = {nullptr, nullptr}, ev_free[2] = {nullptr, nullptr};
     cudaGraphExec_t inv_graph = nullptr;  // kInvGraphSteps inverse adjoint steps
-    cudaGraphExec_t seg_graph = nullptr;  // one full checkpoint segment
+    cudaGraphExec_t rec_graph[2] = {nullptr, nullptr};   // recomputation of a full segment
+    cudaGraphExec_t pass_graph[2] = {nullptr, nullptr};  // the passes of a full segment
     std::string err;
 };
 
@@ -168,8 +176,17 @@ void *ckpt_at(ts_b200_adjoint *a, int j) {
     return static_cast<unsigned char *>(a->ckpt) + (size_t)j * state_bytes(a);
 }
 
-void *seg_at(ts_b200_adjoint *a, int j) {  // recomputed state j (1 .. every-1; .. every imag)
-    return static_cast<unsigned char *>(a->seg) + (size_t)(j - 1) * state_bytes(a);
+// recomputed state j (1 .. every-1; .. every in imaginary time) of buffer set b
+void *seg_at(ts_b200_adjoint *a, int b, int j) {
+    return static_cast<unsigned char *>(a->seg[b]) + (size_t)(j - 1) * state_bytes(a);
+}
+
+void drop_segment_graphs(ts_b200_adjoint *a) {
+    for (int b = 0; b < 2; ++b)
+        for (cudaGraphExec_t *g : {&a->rec_graph[b], &a->pass_graph[b]}) {
+            if (*g) cudaGraphExecDestroy(*g);
+            *g = nullptr;
+        }
 }
 
 size_t adj_smem(const ts_b200_adjoint *a) {
@@ -193,8 +210,19 @@ cudaError_t launch_adj_variant(ts_b200_adjoint *a, const AdjArgs &args, int bloc
         if (e != cudaSuccess) return e;
     }
     if (blocks == 0) return cudaSuccess;
-    fn<<<blocks, a->warps * kAdjThreadsPerWarp, smem, a->k->stream>>>(args);
-    return cudaGetLastError();
+    // programmatic dependent launch (the kernel waits for its predecessor
+    // before it reads anything)
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)blocks);
+    cfg.blockDim = dim3((unsigned)(a->warps * kAdjThreadsPerWarp));
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = a->k->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, fn, args);
 }
 
 cudaError_t launch_adj(ts_b200_adjoint *a, int mode, int phase, const AdjArgs &args, int blocks,
@@ -282,10 +310,9 @@ int tile_status(ts_b200_adjoint *a, int s) {
     return s;
 }
 
-// Capture the launches `body` queues on the tile's stream into *exec.
+// Capture the launches `body` queues on stream `st` into *exec.
 template <class F>
-int capture(ts_b200_adjoint *a, cudaGraphExec_t *exec, F body) {
-    cudaStream_t st = a->k->stream;
+int capture(ts_b200_adjoint *a, cudaStream_t st, cudaGraphExec_t *exec, F body) {
     cudaGraph_t g = nullptr;
     TSBA_CHECK(a, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     const uint64_t before = g_launches.load();
@@ -304,47 +331,110 @@ int capture(ts_b200_adjoint *a, cudaGraphExec_t *exec, F body) {
     return TS_B200_OK;
 }
 
-// Imaginary time: recompute states 1 .. len of the segment from a->state0
-// (factor seg_c[0]), each step's factor into seg_c[i], then len reverse steps
-// (lambda ping-pongs from lam[l], mu from mu[l]); `first` is the global index
-// of the segment's first step (the step 0 pass adds nothing to the sum).
-int segment_pass_imag(ts_b200_adjoint *a, int len, int l, int first) {
+// Recompute the states of a checkpoint segment of `len` steps from
+// state0[b] into buffer set b, on the recomputation stream: states 1 .. len-1
+// (real time) or 1 .. len with each step's renormalisation factor into
+// seg_c[b][i] (imaginary time, from the factor seg_c[b][0]; the step writes
+// it itself, so that the steps follow one another without a copy between).
+int recompute(ts_b200_adjoint *a, int b, int len) {
     ts_b200_kernel *k = a->k;
-    int s = TS_B200_OK;
-    cudaError_t e = cudaMemcpyAsync(&k->scal->pending_inv, &a->seg_c[0], sizeof(double),
-                                    cudaMemcpyDeviceToDevice, k->stream);
-    if (e != cudaSuccess) return acuda(a, e, "segment factor");
-    for (int i = 1; i <= len && s == TS_B200_OK; ++i) {
-        s = tile_status(a, tsbh::launch_step_buffers(k, i == 1 ? a->state0 : seg_at(a, i - 1),
-                                                     seg_at(a, i)));
-        if (s == TS_B200_OK) {
-            e = cudaMemcpyAsync(&a->seg_c[i], &k->scal->pending_inv, sizeof(double),
-                                cudaMemcpyDeviceToDevice, k->stream);
-            if (e != cudaSuccess) return acuda(a, e, "segment factor");
-        }
+    if (a->imag) {
+        cudaError_t e = cudaMemcpyAsync(&k->scal->pending_inv, &a->seg_c[b][0], sizeof(double),
+                                        cudaMemcpyDeviceToDevice, a->rstream);
+        if (e != cudaSuccess) return acuda(a, e, "segment factor");
     }
+    tsbh::StepPart part;
+    part.pdl = true;
+    part.stream = a->rstream;
+    const int n = a->imag ? len : len - 1;
+    int s = TS_B200_OK;
+    for (int i = 1; i <= n && s == TS_B200_OK; ++i) {
+        if (a->imag) part.inv_copy = &a->seg_c[b][i];
+        s = tile_status(a, tsbh::launch_step_part(k, i == 1 ? a->state0[b] : seg_at(a, b, i - 1),
+                                                  seg_at(a, b, i), part));
+    }
+    return s;
+}
+
+// The len reverse steps of a segment from its states in buffer set b
+// (lambda ping-pongs from lam[l]; in imaginary time mu from mu[l], `first`
+// the global index of the segment's first step: the step 0 pass adds nothing
+// to the sum), on the tile's stream.
+int passes(ts_b200_adjoint *a, int b, int len, int l, int first) {
+    int s = TS_B200_OK;
     for (int i = len - 1; i >= 0 && s == TS_B200_OK; --i) {
-        const void *psi_n = i == 0 ? a->state0 : seg_at(a, i);
-        s = adj_step_imag(a, psi_n, &a->seg_c[i], seg_at(a, i + 1), &a->seg_c[i + 1], a->lam[l],
-                          a->lam[l ^ 1], &a->mu[l], &a->mu[l ^ 1], first + i > 0);
+        const void *psi_n = i == 0 ? a->state0[b] : seg_at(a, b, i);
+        if (a->imag)
+            s = adj_step_imag(a, psi_n, &a->seg_c[b][i], seg_at(a, b, i + 1), &a->seg_c[b][i + 1],
+                              a->lam[l], a->lam[l ^ 1], &a->mu[l], &a->mu[l ^ 1], first + i > 0);
+        else
+            s = adj_step(a, 1, psi_n, nullptr, a->lam[l], a->lam[l ^ 1]);
         l ^= 1;
     }
     return s;
 }
 
-// Reverse pass of one checkpoint segment of `len` steps starting from the
-// state in a->state0: recompute states 1 .. len-1, then len adjoint steps
-// (lambda ping-pongs from lam[l]).
-int segment_pass(ts_b200_adjoint *a, int len, int l) {
+// The checkpointed reverse pass, segments from the last: segment j's states
+// are recomputed into buffer set j % nsets on the recomputation stream while
+// the passes of segment j + 1 run on the tile's stream (with two sets; one
+// set orders them one after the other).  Full segments of an even length
+// replay graphs (the recomputation of a set; its passes, which leave lambda
+// and mu in [0]); returns the final lambda index in *l_out.
+int checkpointed_reverse(ts_b200_adjoint *a, int *l_out) {
+    ts_b200_kernel *k = a->k;
+    cudaStream_t A = k->stream, B = a->rstream;
+    int l = 0;
     int s = TS_B200_OK;
-    for (int i = 1; i < len && s == TS_B200_OK; ++i)
-        s = tile_status(a, tsbh::launch_step_buffers(a->k, i == 1 ? a->state0 : seg_at(a, i - 1),
-                                                     seg_at(a, i)));
-    for (int i = len - 1; i >= 0 && s == TS_B200_OK; --i) {
-        const void *psi_n = i == 0 ? a->state0 : seg_at(a, i);
-        s = adj_step(a, 1, psi_n, nullptr, a->lam[l], a->lam[l ^ 1]);
-        l ^= 1;
+    TSBA_CHECK(a, cudaEventRecord(a->ev_start, A));
+    TSBA_CHECK(a, cudaStreamWaitEvent(B, a->ev_start, 0));
+    for (int b = 0; b < 2; ++b) TSBA_CHECK(a, cudaEventRecord(a->ev_free[b], A));
+    for (int j = a->n_ckpt - 1; j >= 0 && s == TS_B200_OK; --j) {
+        const int b = j % a->nsets;
+        const int len = std::min(a->every, a->steps - j * a->every);
+        const bool full = len == a->every && (len & 1) == 0;
+        // recompute segment j once set b is free
+        TSBA_CHECK(a, cudaStreamWaitEvent(B, a->ev_free[b], 0));
+        TSBA_CHECK(a, cudaMemcpyAsync(a->state0[b], ckpt_at(a, j), state_bytes(a),
+                                      cudaMemcpyDeviceToDevice, B));
+        if (a->imag)
+            TSBA_CHECK(a, cudaMemcpyAsync(&a->seg_c[b][0], &a->ckpt_c[j], sizeof(double),
+                                          cudaMemcpyDeviceToDevice, B));
+        if (full) {
+            if (!a->rec_graph[b]) {
+                s = capture(a, B, &a->rec_graph[b], [&] { return recompute(a, b, len); });
+                if (s) return s;
+            }
+            TSBA_CHECK(a, cudaGraphLaunch(a->rec_graph[b], B));
+            g_launches.fetch_add(a->imag ? len : len - 1, std::memory_order_relaxed);
+        } else {
+            s = recompute(a, b, len);
+            if (s) return s;
+        }
+        TSBA_CHECK(a, cudaEventRecord(a->ev_ready[b], B));
+        // its passes once its states are there
+        TSBA_CHECK(a, cudaStreamWaitEvent(A, a->ev_ready[b], 0));
+        if (full && (!a->imag || j > 0)) {
+            if (!a->pass_graph[b]) {
+                s = capture(a, A, &a->pass_graph[b], [&] { return passes(a, b, len, 0, 1); });
+                if (s) return s;
+            }
+            if (l != 0) {  // the graph starts from lam[0] (and mu[0])
+                TSBA_CHECK(a, cudaMemcpyAsync(a->lam[0], a->lam[1], state_bytes(a),
+                                              cudaMemcpyDeviceToDevice, A));
+                if (a->imag)
+                    TSBA_CHECK(a, cudaMemcpyAsync(&a->mu[0], &a->mu[1], sizeof(double),
+                                                  cudaMemcpyDeviceToDevice, A));
+                l = 0;
+            }
+            TSBA_CHECK(a, cudaGraphLaunch(a->pass_graph[b], A));
+            g_launches.fetch_add(len, std::memory_order_relaxed);
+        } else {
+            s = passes(a, b, len, l, j * a->every);
+            if (len & 1) l ^= 1;
+        }
+        TSBA_CHECK(a, cudaEventRecord(a->ev_free[b], A));
     }
+    *l_out = l;
     return s;
 }
 
@@ -391,14 +481,26 @@ int ts_b200_adjoint_create(const ts_b200_desc *d, double delta_t, int steps, int
     if (a->every > 0) {
         a->n_ckpt = (steps + a->every - 1) / a->every;  // states at 0, every, 2 every, ...
         alloc(&a->ckpt, sb * a->n_ckpt);
-        // imaginary time also recomputes the next segment's first state
+        // imaginary time also recomputes the next segment's first state; a
+        // second buffer set (recomputation overlapping the passes) when it
+        // takes under a quarter of the free device memory
         const int nseg = a->imag ? a->every : a->every - 1;
-        if (nseg > 0) alloc(&a->seg, sb * nseg);
-        alloc(&a->state0, sb);
+        size_t free_b = 0, total_b = 0;
+        if (e == cudaSuccess) e = cudaMemGetInfo(&free_b, &total_b);
+        a->nsets = (a->n_ckpt > 1 && sb * (nseg + 1) * 4 <= free_b) ? 2 : 1;
+        for (int b = 0; b < a->nsets; ++b) {
+            if (nseg > 0) alloc(&a->seg[b], sb * nseg);
+            alloc(&a->state0[b], sb);
+            if (a->imag)
+                alloc(reinterpret_cast<void **>(&a->seg_c[b]), sizeof(double) * (a->every + 1));
+        }
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&a->rstream, cudaStreamNonBlocking);
+        for (cudaEvent_t *ev : {&a->ev_start, &a->ev_ready[0], &a->ev_ready[1], &a->ev_free[0],
+                                &a->ev_free[1]})
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
     }
     if (a->imag) {
         alloc(reinterpret_cast<void **>(&a->ckpt_c), sizeof(double) * a->n_ckpt);
-        alloc(reinterpret_cast<void **>(&a->seg_c), sizeof(double) * (a->every + 1));
         alloc(reinterpret_cast<void **>(&a->mu), sizeof(double) * 2);
         alloc(reinterpret_cast<void **>(&a->ksum), sizeof(double));
         alloc(reinterpret_cast<void **>(&a->ticket), sizeof(unsigned int));
@@ -409,10 +511,14 @@ int ts_b200_adjoint_create(const ts_b200_desc *d, double delta_t, int steps, int
         e = launch_adj(a, a->imag ? 2 : (a->every > 0 ? 1 : 0), a->k->phase, x, 0, &bps);
         if (e == cudaSuccess && bps < 1) e = cudaErrorInvalidConfiguration;
         a->blocks = bps * a->k->num_sms;
-        // one round of tasks over the resident warps (the tile is often small)
+        // one round of tasks over the resident warps (the tile is often
+        // small), segments of at least 4 rows (6 in imaginary time): on
+        // 512^2 the pass took 63.6 / 128.3 / 162.8 ms (linear, checkpointed,
+        // imaginary time, 3000 steps) at 4 / 4 / 6 rows against 67.2 /
+        // 144.3 / 169.0 at 8 and 89 / 195 / 235 at 2
         const int strips = div_up(a->W, AdjVariant<0, 0>::WO);
         const int per_strip = std::max(1, a->blocks * a->warps / strips);
-        a->seg_h = std::max(8, div_up(a->H, per_strip));
+        a->seg_h = std::max(a->imag ? 6 : 4, div_up(a->H, per_strip));
         a->seg_h += a->seg_h & 1;
         // block partials of the reductions (adjoint steps and the dot kernel)
         if (a->imag) alloc(reinterpret_cast<void **>(&a->partials),
@@ -430,21 +536,27 @@ int ts_b200_adjoint_create(const ts_b200_desc *d, double delta_t, int steps, int
 void ts_b200_adjoint_destroy(ts_b200_adjoint *a) {
     if (!a) return;
     if (a->k) cudaStreamSynchronize(a->k->stream);
+    if (a->rstream) cudaStreamSynchronize(a->rstream);
     cudaFree(a->lam[0]);
     cudaFree(a->lam[1]);
     cudaFree(a->gv);
     cudaFree(a->ckpt);
-    cudaFree(a->seg);
+    for (int b = 0; b < 2; ++b) {
+        cudaFree(a->seg[b]);
+        cudaFree(a->state0[b]);
+        cudaFree(a->seg_c[b]);
+    }
     cudaFree(a->error);
-    cudaFree(a->state0);
     cudaFree(a->ckpt_c);
-    cudaFree(a->seg_c);
     cudaFree(a->mu);
     cudaFree(a->ksum);
     cudaFree(a->partials);
     cudaFree(a->ticket);
     if (a->inv_graph) cudaGraphExecDestroy(a->inv_graph);
-    if (a->seg_graph) cudaGraphExecDestroy(a->seg_graph);
+    drop_segment_graphs(a);
+    for (cudaEvent_t ev : {a->ev_start, a->ev_ready[0], a->ev_ready[1], a->ev_free[0], a->ev_free[1]})
+        if (ev) cudaEventDestroy(ev);
+    if (a->rstream) cudaStreamDestroy(a->rstream);
     ts_b200_destroy(a->k);
     delete a;
 }
@@ -452,6 +564,23 @@ void ts_b200_adjoint_destroy(ts_b200_adjoint *a) {
 int ts_b200_adjoint_set_stream(ts_b200_adjoint *a, void *stream) {
     if (!a) return TS_B200_INVALID_ARGUMENT;
     return tile_status(a, ts_b200_set_stream(a->k, stream));
+}
+
+int ts_b200_adjoint_set_segments(ts_b200_adjoint *a, int adjoint_rows, int forward_rows) {
+    if (!a || adjoint_rows < 0 || forward_rows < 0 || (adjoint_rows & 1) || adjoint_rows == 1)
+        return TS_B200_INVALID_ARGUMENT;
+    if (forward_rows > 0) {
+        const int s = tile_status(a, ts_b200_set_launch(a->k, 0, forward_rows, 0, 0));
+        if (s) return s;
+        drop_segment_graphs(a);
+    }
+    if (adjoint_rows > 0 && adjoint_rows != a->seg_h) {
+        a->seg_h = adjoint_rows;
+        if (a->inv_graph) cudaGraphExecDestroy(a->inv_graph);
+        a->inv_graph = nullptr;
+        drop_segment_graphs(a);
+    }
+    return TS_B200_OK;
 }
 
 int ts_b200_adjoint_forward(ts_b200_adjoint *a, const double *potential, const void *psi0,
@@ -481,10 +610,7 @@ int ts_b200_adjoint_forward(ts_b200_adjoint *a, const double *potential, const v
             a->norm0 = n0;
             s = tile_status(a, tsbh::set_norm0(k, n0));
             if (s) return s;
-            if (a->seg_graph) {
-                cudaGraphExecDestroy(a->seg_graph);
-                a->seg_graph = nullptr;
-            }
+            drop_segment_graphs(a);
         }
     }
     if (a->every > 0) {
@@ -529,32 +655,7 @@ int ts_b200_adjoint_backward(ts_b200_adjoint *a, const void *grad_psi_t, double 
             a->ksum);
         TSBA_CHECK(a, cudaGetLastError());
         g_launches.fetch_add(1, std::memory_order_relaxed);
-        for (int j = a->n_ckpt - 1; j >= 0 && s == TS_B200_OK; --j) {
-            const int len = std::min(a->every, a->steps - j * a->every);
-            TSBA_CHECK(a, cudaMemcpyAsync(a->state0, ckpt_at(a, j), state_bytes(a),
-                                          cudaMemcpyDeviceToDevice, k->stream));
-            TSBA_CHECK(a, cudaMemcpyAsync(&a->seg_c[0], &a->ckpt_c[j], sizeof(double),
-                                          cudaMemcpyDeviceToDevice, k->stream));
-            if (len == a->every && (len & 1) == 0 && j > 0) {
-                // full segments of an even length leave lambda and mu in [l]
-                if (!a->seg_graph) {
-                    s = capture(a, &a->seg_graph, [&] { return segment_pass_imag(a, len, 0, 1); });
-                    if (s) return s;
-                }
-                if (l != 0) {  // the graph starts from lam[0], mu[0]
-                    TSBA_CHECK(a, cudaMemcpyAsync(a->lam[0], a->lam[1], state_bytes(a),
-                                                  cudaMemcpyDeviceToDevice, k->stream));
-                    TSBA_CHECK(a, cudaMemcpyAsync(&a->mu[0], &a->mu[1], sizeof(double),
-                                                  cudaMemcpyDeviceToDevice, k->stream));
-                    l = 0;
-                }
-                TSBA_CHECK(a, cudaGraphLaunch(a->seg_graph, k->stream));
-                g_launches.fetch_add(2 * len, std::memory_order_relaxed);
-            } else {
-                s = segment_pass_imag(a, len, l, j * a->every);
-                if (len & 1) l ^= 1;
-            }
-        }
+        s = checkpointed_reverse(a, &l);
         if (s) return s;
         a->forward_done = false;
         if (grad_potential)
@@ -579,7 +680,7 @@ int ts_b200_adjoint_backward(ts_b200_adjoint *a, const void *grad_psi_t, double 
         int n = a->steps;
         if (n >= kInvGraphSteps && c == 0) {
             if (!a->inv_graph) {
-                s = capture(a, &a->inv_graph, [&] {
+                s = capture(a, k->stream, &a->inv_graph, [&] {
                     int st = TS_B200_OK, cc = 0, ll = 0;
                     for (int i = 0; i < kInvGraphSteps && st == TS_B200_OK; ++i) {
                         st = adj_step(a, 0, k->psi[cc], k->psi[cc ^ 1], a->lam[ll], a->lam[ll ^ 1]);
@@ -603,28 +704,7 @@ int ts_b200_adjoint_backward(ts_b200_adjoint *a, const void *grad_psi_t, double 
         }
         k->cur = c;  // the tile now holds the recomputed psi(0)
     } else {
-        for (int j = a->n_ckpt - 1; j >= 0 && s == TS_B200_OK; --j) {
-            const int len = std::min(a->every, a->steps - j * a->every);
-            TSBA_CHECK(a, cudaMemcpyAsync(a->state0, ckpt_at(a, j), state_bytes(a),
-                                          cudaMemcpyDeviceToDevice, k->stream));
-            if (len == a->every && (len & 1) == 0) {
-                // full segments of an even length leave lambda in lam[l]
-                if (!a->seg_graph) {
-                    s = capture(a, &a->seg_graph, [&] { return segment_pass(a, len, 0); });
-                    if (s) return s;
-                }
-                if (l != 0) {  // the graph starts from lam[0]
-                    TSBA_CHECK(a, cudaMemcpyAsync(a->lam[0], a->lam[1], state_bytes(a),
-                                                  cudaMemcpyDeviceToDevice, k->stream));
-                    l = 0;
-                }
-                TSBA_CHECK(a, cudaGraphLaunch(a->seg_graph, k->stream));
-                g_launches.fetch_add(2 * len - 1, std::memory_order_relaxed);
-            } else {
-                s = segment_pass(a, len, l);
-                if (len & 1) l ^= 1;
-            }
-        }
+        s = checkpointed_reverse(a, &l);
     }
     if (s) return s;
     a->forward_done = false;  // the reverse pass consumed the kept states

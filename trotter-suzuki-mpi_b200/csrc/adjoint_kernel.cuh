@@ -358,6 +358,10 @@ __device__ __forceinline__ void adj_rows(AdjWalk &w, const AdjArgs &a, int base,
 template <class A>
 __global__ void __launch_bounds__(64, 6) adjoint_kernel(AdjArgs a) {
     extern __shared__ __align__(128) unsigned char smem[];
+    // programmatic dependent launch: the next pass's blocks may be placed as
+    // this pass's blocks retire and set up their shared memory; they wait
+    // (griddepcontrol.wait below) for this pass to complete before reading
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     const int warps = blockDim.x >> 5;
     const int warp = __shfl_sync(0xffffffffu, (int)(threadIdx.x >> 5), 0);
     const int lane = threadIdx.x & 31;
@@ -376,11 +380,6 @@ __global__ void __launch_bounds__(64, 6) adjoint_kernel(AdjArgs a) {
     w.pitch16 = (size_t)a.P * 16;
     w.pitch8 = (size_t)a.P * 8;
     w.kacc = 0.0;
-    if constexpr (A::IMAG) {
-        w.cin = *a.c_in;
-        w.cnext = *a.c_next;
-        w.m2 = *a.mu_next * w.cnext;
-    }
     {
         uint4 *z = reinterpret_cast<uint4 *>(w.ring);
         const int n16 = D * A::SLOT / 16;
@@ -392,6 +391,14 @@ __global__ void __launch_bounds__(64, 6) adjoint_kernel(AdjArgs a) {
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
     __syncwarp();
+    // the previous kernel of the stream (recomputation or pass) has completed
+    // and its writes are visible from here on
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    if constexpr (A::IMAG) {
+        w.cin = *a.c_in;
+        w.cnext = *a.c_next;
+        w.m2 = *a.mu_next * w.cnext;
+    }
 
     for (int task = blockIdx.x * warps + warp; task < n_tasks && !w.failed;
          task += gridDim.x * warps) {

@@ -94,11 +94,11 @@ int set_norm0(ts_b200_kernel *k, double norm0);
 
 // One launch of the fused step over some of the tile's output rows: window
 // [a0, a1) and, if b1 > b0, window [b0, b1) (even starts; a1 = 0: the whole
-// tile), on `stream`, with its own block ticket and, in imaginary time, its
-// own block partials.  pair_norm / pair_ticket non-null: the step is split
-// over two such launches (pair_slot 0 and 1) that read the same input buffer
-// and write disjoint rows; the second to finish ends the step.  blocks > 0
-// caps the grid.
+// tile), on `stream` (null: the tile's), with its own block ticket and, in
+// imaginary time, its own block partials (null: the tile's).  pair_norm /
+// pair_ticket non-null: the step is split over two such launches (pair_slot
+// 0 and 1) that read the same input buffer and write disjoint rows; the
+// second to finish ends the step.  blocks > 0 caps the grid.
 struct StepPart {
     int a0 = 0, a1 = 0, b0 = 0, b1 = 0;
     cudaStream_t stream = nullptr;
@@ -108,6 +108,8 @@ struct StepPart {
     unsigned int *pair_ticket = nullptr;
     int pair_slot = 0;
     int blocks = 0;
+    double *inv_copy = nullptr;  // imaginary time: the step's factor also written here
+    bool pdl = false;            // programmatic dependent launch (whole-tile parts)
 };
 
 // Resident grid and segment height of the tile's step (once per shape).

@@ -111,6 +111,9 @@ struct StepArgs {
     double *pair_norm;
     unsigned int *pair_ticket;
     int pair_slot;
+    // imaginary time, non-null: the step's renormalisation factor is also
+    // written here (a recomputation keeping each step's factor)
+    double *inv_copy;
 };
 
 // Output rows [oy0, oy1) of segment `seg` of the launch.
@@ -1340,6 +1343,7 @@ __global__ void __launch_bounds__(128, V::MIN_BLOCKS) step_kernel(StepArgs<typen
                 } else if (split_norm_total(a, &tot)) {
                     a.scal->last_norm = tot;
                     if (a.scal->renorm) a.scal->pending_inv = 1.0 / sqrt(tot / a.norm0);
+                    if (a.inv_copy) *a.inv_copy = a.scal->pending_inv;
                 }
             }
         }
@@ -1410,6 +1414,7 @@ __device__ __forceinline__ StepArgs<T> load_tile_args(const StepArgs<T> *p) {
     a.ticket = nullptr;
     a.pair_norm = nullptr;
     a.pair_ticket = nullptr;
+    a.inv_copy = nullptr;
     return a;
 }
 

@@ -848,10 +848,22 @@ int launch_step_part_t(ts_b200_kernel *k, const void *in, void *out, const tsbh:
     if (p.a1 > 0 && (p.a0 < 0 || p.a1 <= p.a0 || p.a1 > k->H || (p.a0 & 1) ||
                      (p.b1 > p.b0 && (p.b0 < 0 || p.b1 > k->H || (p.b0 & 1)))))
         return fail(k, TS_B200_INVALID_ARGUMENT, "step part: row windows");
-    if (k->imag && !p.partials) return fail(k, TS_B200_INVALID_ARGUMENT, "step part: partials");
+    const bool pdl = p.pdl && p.a1 == 0 && k->overlap && use_walk2(k);
     int strips, segs, blocks;
     size_t smem;
-    geometry(k, &strips, &segs, &blocks, &smem, false, &p);
+    geometry(k, &strips, &segs, &blocks, &smem, pdl, &p);
+    double *partials = p.partials;
+    if (k->imag && !partials) {
+        const size_t nb = (size_t)std::max(blocks, 1);
+        if (nb * k->warps > k->partials_cap) {
+            if (k->partials) cudaFree(k->partials);
+            k->partials = nullptr;
+            k->partials_cap = 0;
+            TSB_CHECK(k, cudaMalloc(&k->partials, nb * k->warps * sizeof(double)));
+            k->partials_cap = nb * k->warps;
+        }
+        partials = k->partials;
+    }
     StepArgs<T> a{};
     a.psi_in = in;
     a.psi_out = out;
@@ -860,7 +872,8 @@ int launch_step_part_t(ts_b200_kernel *k, const void *in, void *out, const tsbh:
     a.n_segs = segs;
     a.seg_h = eff_seg(k);
     a.ring = use_walk2(k) ? 6 / walk_rows(k) : k->ring;
-    a.partials = p.partials;
+    a.partials = partials;
+    a.inv_copy = p.inv_copy;
     if (p.a1 > 0) {
         a.win_n0 = div_up(p.a1 - p.a0, a.seg_h);
         a.win_a0 = p.a0;
@@ -873,7 +886,7 @@ int launch_step_part_t(ts_b200_kernel *k, const void *in, void *out, const tsbh:
     a.pair_ticket = p.pair_ticket;
     a.pair_slot = p.pair_slot;
     cudaError_t e = dispatch_step<T>(k->C, k->imag, k->rot, k->phase, walk_rows(k), a, k->warps,
-                                     smem, blocks, p.stream, nullptr, false);
+                                     smem, blocks, p.stream ? p.stream : k->stream, nullptr, pdl);
     if (e != cudaSuccess) return cuda_fail(k, e, "step part launch");
     g_launches.fetch_add(1, std::memory_order_relaxed);
     return TS_B200_OK;

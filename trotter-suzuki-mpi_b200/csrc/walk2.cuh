@@ -536,6 +536,7 @@ __device__ __forceinline__ void w2_finish(const StepArgs<typename V::T> &a, doub
                 if (split_norm_total(a, &tot)) {
                     a.scal->last_norm = tot;
                     if (a.scal->renorm) a.scal->pending_inv = 1.0 / sqrt(tot / a.norm0);
+                    if (a.inv_copy) *a.inv_copy = a.scal->pending_inv;
                 }
             }
         }

@@ -141,6 +141,7 @@ SIGNATURES = {
     "ts_b200_adjoint_create": (_I, [C.POINTER(Desc), C.c_double, _I, _I, C.POINTER(_VP)]),
     "ts_b200_adjoint_destroy": (None, [_VP]),
     "ts_b200_adjoint_set_stream": (_I, [_VP, _VP]),
+    "ts_b200_adjoint_set_segments": (_I, [_VP, _I, _I]),
     "ts_b200_adjoint_forward": (_I, [_VP, _VP, _VP, _VP]),
     "ts_b200_adjoint_backward": (_I, [_VP, _VP, _VP, _VP]),
     "ts_b200_adjoint_synchronize": (_I, [_VP]),

@@ -48,6 +48,12 @@ class AdjointEngine:
     def set_stream(self, stream_ptr):
         self._check(lib().ts_b200_adjoint_set_stream(self._a, C.c_void_p(stream_ptr)))
 
+    def set_segments(self, adjoint_rows=0, forward_rows=0):
+        """Rows per segment task of the adjoint pass and of the forward steps
+        (0 keeps the current choice)."""
+        self._check(lib().ts_b200_adjoint_set_segments(self._a, int(adjoint_rows),
+                                                       int(forward_rows)))
+
     def forward_ptrs(self, v_ptr, psi0_ptr, psi_t_ptr):
         self._check(lib().ts_b200_adjoint_forward(self._a, C.c_void_p(v_ptr), C.c_void_p(psi0_ptr),
                                                   C.c_void_p(psi_t_ptr)))
