@@ -136,10 +136,71 @@ def test_look_ahead_walk_fp32(imag, cells, walk):
         assert np.array_equal(got, old)
 
 
-def test_rotating_frame_keeps_the_checked_walk():
-    from trottersuzuki_b200 import Kernel
-    lat, psi0, V = seeded_case(64, 10.0, None, (False, False), omega=0.7)
-    p = lat.params(1e-3, False, 1.0, 1.0, 0.0, 0.7)
-    with Kernel(desc_from_params(p)) as k:
-        k.set_walk(1)
-        assert k.launch_shape()["walk"] == 0
+# rotating frame: name, N, Ny, periodic, g, lhy, omega, imag, steps
+ROT_CASES = [
+    ("rot_real", 64, None, (False, False), 1.0, 0.0, 0.7, False, 20),
+    ("rot_imag", 64, None, (False, False), 5.0, 0.0, 0.7, True, 20),
+    ("rot_lhy_real", 72, 60, (False, False), 3.0, 0.2, 0.4, False, 15),
+    ("rot_periodic", 64, None, (True, True), 2.0, 0.0, 0.5, False, 12),
+    ("rot_periodic_imag", 80, 64, (True, True), 2.0, 0.0, 0.5, True, 12),
+    ("rot_ragged", 61, 47, (False, False), 1.0, 0.0, 0.9, False, 14),
+    ("rot_short", 50, 9, (False, False), 1.0, 0.0, 0.6, True, 7),
+]
+
+
+def _rot_oracle(case, split):
+    """The oracle over the same evolve() calls (a periodic tile skips its halo
+    refresh after the last step of each call)."""
+    _, N, Ny, per, g, lhy, omega, imag, steps = case
+    lat, psi0, V = seeded_case(N, 10.0, Ny, per, omega=omega)
+    n0 = O.expectations(lat, psi0)["norm2"] if imag else 0.0
+    p = lat.params(1e-3, imag, 1.0, g, lhy, omega, norm0=n0)
+    tr, ti = O.exp_table(V, 1e-3, imag)
+    ref = psi0
+    for n in split:
+        ref = O.evolve(p, ref, tr, ti, n)
+    return lat, psi0, p, tr, ti, ref
+
+
+@pytest.mark.parametrize("walk", [1, 2])
+@pytest.mark.parametrize("case", ROT_CASES, ids=[c[0] for c in ROT_CASES])
+def test_rotating_frame_look_ahead_walk(case, walk):
+    """The rotating frame's look-ahead walk (8-row window, row and column
+    rotation sweeps, their identity across the tile edges) against the oracle
+    and the checked walk."""
+    steps = case[-1]
+    imag = case[7]
+    split = [steps // 2, steps - steps // 2]
+    lat, psi0, p, tr, ti, ref = _rot_oracle(case, split)
+    got, shape = _gpu(p, psi0, tr, ti, steps, walk=walk, split=split)
+    assert shape["walk"] == walk and shape["ring_depth"] == 8
+    assert np.abs(got - ref).max() <= TOL_PSI * max(1.0, np.abs(ref).max())
+    old, shape0 = _gpu(p, psi0, tr, ti, steps, walk=0, split=split)
+    assert shape0["walk"] == 0
+    if imag:
+        assert np.abs(got - old).max() <= 1e-13 * np.abs(old).max()
+    else:
+        assert np.array_equal(got, old)
+
+
+@pytest.mark.parametrize("imag", [False, True], ids=["real", "imag"])
+@pytest.mark.parametrize("seg", [8, 14, 40])
+def test_rotating_frame_segments_and_fp32(imag, seg):
+    """Segment cuts of the rotating-frame walk (301 rows, ragged columns) in
+    both precisions: the checked walk's bits in real time."""
+    from trottersuzuki_b200 import _capi
+    lat, psi0, V = seeded_case(233, 12.0, 301, (False, False), omega=0.5)
+    n0 = O.expectations(lat, psi0)["norm2"] if imag else 0.0
+    p = lat.params(1e-3, imag, 1.0, 3.0, 0.0, 0.5, norm0=n0)
+    tr, ti = O.exp_table(V, 1e-3, imag)
+    ref = O.evolve(p, psi0, tr, ti, 7)
+    launch = dict(cells_per_lane=2, segment_rows=seg)
+    for prec, tol in ((_capi.FP64, TOL_PSI), (_capi.FP32, 2e-5)):
+        got, shape = _gpu(p, psi0, tr, ti, 7, walk=2, launch=launch, precision=prec, split=[3, 4])
+        assert shape["walk"] == 2
+        assert np.abs(got - ref).max() <= tol * np.abs(ref).max()
+        old, _ = _gpu(p, psi0, tr, ti, 7, walk=0, launch=launch, precision=prec, split=[3, 4])
+        if imag:
+            assert np.abs(got - old).max() <= (1e-13 if prec == _capi.FP64 else 1e-6) * np.abs(old).max()
+        else:
+            assert np.array_equal(got, old)

@@ -8,7 +8,7 @@
 
 namespace tsb {
 
-// The look-ahead walk (walk2.cuh): phases 0-2, no rotating frame, cartesian;
+// The look-ahead walk (walk2.cuh): phases 0-2, cartesian, one component;
 // R rows per iteration (1, or 2 with 2 cells per lane); pdl: programmatic
 // dependent launch after the stream's previous kernel.
 cudaError_t launch_step2_f64_real(int C, int R, int phase, const StepArgs<double> &a, int warps,
@@ -23,5 +23,19 @@ cudaError_t launch_step2_f32_real(int C, int R, int phase, const StepArgs<float>
 cudaError_t launch_step2_f32_imag(int C, int R, int phase, const StepArgs<float> &a, int warps,
                                   size_t smem, int blocks, cudaStream_t st, int *blocks_per_sm,
                                   bool pdl);
+
+// The same in a rotating frame (2 cells per lane; step2rot_f{64,32}_{real,imag}.cu).
+cudaError_t launch_step2rot_f64_real(int R, int phase, const StepArgs<double> &a, int warps,
+                                     size_t smem, int blocks, cudaStream_t st, int *blocks_per_sm,
+                                     bool pdl);
+cudaError_t launch_step2rot_f64_imag(int R, int phase, const StepArgs<double> &a, int warps,
+                                     size_t smem, int blocks, cudaStream_t st, int *blocks_per_sm,
+                                     bool pdl);
+cudaError_t launch_step2rot_f32_real(int R, int phase, const StepArgs<float> &a, int warps,
+                                     size_t smem, int blocks, cudaStream_t st, int *blocks_per_sm,
+                                     bool pdl);
+cudaError_t launch_step2rot_f32_imag(int R, int phase, const StepArgs<float> &a, int warps,
+                                     size_t smem, int blocks, cudaStream_t st, int *blocks_per_sm,
+                                     bool pdl);
 
 }  // namespace tsb

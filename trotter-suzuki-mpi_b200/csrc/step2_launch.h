@@ -60,4 +60,20 @@ cudaError_t launch_step2_t(int C, int R, int phase, const StepArgs<T> &a, int wa
     return cudaErrorInvalidValue;
 }
 
+// The rotating frame (2 cells per lane), R rows per iteration.
+template <typename T, bool IMAG>
+cudaError_t launch_step2rot_t(int R, int phase, const StepArgs<T> &a, int warps, size_t smem,
+                              int blocks, cudaStream_t st, int *bps, bool pdl) {
+    if (R == 2) {
+        if (phase == 0) return launch_step2_variant<Variant<T, 2, IMAG, true, 0>, 2>(a, warps, smem, blocks, st, bps, pdl);
+        if (phase == 1) return launch_step2_variant<Variant<T, 2, IMAG, true, 1>, 2>(a, warps, smem, blocks, st, bps, pdl);
+        if (phase == 2) return launch_step2_variant<Variant<T, 2, IMAG, true, 2>, 2>(a, warps, smem, blocks, st, bps, pdl);
+    } else if (R == 1) {
+        if (phase == 0) return launch_step2_variant<Variant<T, 2, IMAG, true, 0>>(a, warps, smem, blocks, st, bps, pdl);
+        if (phase == 1) return launch_step2_variant<Variant<T, 2, IMAG, true, 1>>(a, warps, smem, blocks, st, bps, pdl);
+        if (phase == 2) return launch_step2_variant<Variant<T, 2, IMAG, true, 2>>(a, warps, smem, blocks, st, bps, pdl);
+    }
+    return cudaErrorInvalidValue;
+}
+
 }  // namespace tsb

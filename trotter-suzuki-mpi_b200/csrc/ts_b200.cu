@@ -525,6 +525,9 @@ template <>
 cudaError_t dispatch_step<double>(int C, bool imag, bool rot, int phase, int w2,
                                   const StepArgs<double> &a, int warps, size_t smem, int blocks,
                                   cudaStream_t st, int *bps, bool pdl) {
+    if (w2 && rot)
+        return imag ? tsb::launch_step2rot_f64_imag(w2, phase, a, warps, smem, blocks, st, bps, pdl)
+                    : tsb::launch_step2rot_f64_real(w2, phase, a, warps, smem, blocks, st, bps, pdl);
     if (w2)
         return imag ? tsb::launch_step2_f64_imag(C, w2, phase, a, warps, smem, blocks, st, bps, pdl)
                     : tsb::launch_step2_f64_real(C, w2, phase, a, warps, smem, blocks, st, bps, pdl);
@@ -536,6 +539,9 @@ template <>
 cudaError_t dispatch_step<float>(int C, bool imag, bool rot, int phase, int w2,
                                  const StepArgs<float> &a, int warps, size_t smem, int blocks,
                                  cudaStream_t st, int *bps, bool pdl) {
+    if (w2 && rot)
+        return imag ? tsb::launch_step2rot_f32_imag(w2, phase, a, warps, smem, blocks, st, bps, pdl)
+                    : tsb::launch_step2rot_f32_real(w2, phase, a, warps, smem, blocks, st, bps, pdl);
     if (w2)
         return imag ? tsb::launch_step2_f32_imag(C, w2, phase, a, warps, smem, blocks, st, bps, pdl)
                     : tsb::launch_step2_f32_real(C, w2, phase, a, warps, smem, blocks, st, bps, pdl);
@@ -600,9 +606,16 @@ void choose_launch(ts_b200_kernel *k) {
 // three rows plus at least one in flight.
 int min_ring(const ts_b200_kernel *) { return 4; }
 
-// The look-ahead walk covers single-component cartesian tiles without a
-// rotating frame (phases 0-2); the other variants take the checked walk.
-bool use_walk2(const ts_b200_kernel *k) { return k->walk2 > 0 && !k->rot && !k->cyl && k->phase <= 2; }
+// The look-ahead walk covers single-component cartesian tiles (phases 0-2,
+// in a rotating frame with 2 cells per lane); the other variants take the
+// checked walk.
+bool use_walk2(const ts_b200_kernel *k) {
+    return k->walk2 > 0 && !k->cyl && k->phase <= 2 && (!k->rot || k->C == 2);
+}
+
+// Rows of the look-ahead walk's register window and ring (8 in a rotating
+// frame: its step has 6 vertical sweeps).
+int walk_window(const ts_b200_kernel *k) { return k->rot ? 8 : 6; }
 
 // Rows per iteration of the look-ahead walk in use (0: the checked walk);
 // two rows per iteration exist for 2 cells per lane.
@@ -666,9 +679,9 @@ void geometry(const ts_b200_kernel *k, int *strips, int *segs, int *blocks, size
     if (use_walk2(k)) {
         // per warp: a ring of 6 rows, the vertical pair coefficients and one
         // mbarrier per ring slot (of 1 or 2 rows)
-        *smem = (size_t)k->warps * (6 * slot_bytes(k->C, k->fp32, k->imag) +
-                                    tsb::w2_vlen(eff_seg(k)) * 2 * (k->fp32 ? 4 : 8) +
-                                    (6 / walk_rows(k)) * 8);
+        *smem = (size_t)k->warps * (walk_window(k) * slot_bytes(k->C, k->fp32, k->imag) +
+                                    tsb::w2_vlen(eff_seg(k), k->rot) * 2 * (k->fp32 ? 4 : 8) +
+                                    (walk_window(k) / walk_rows(k)) * 8);
         if (k->overlap && pad) {
             // with programmatic dependent launch the next step's blocks are
             // placed as soon as an SM has room: reserve enough shared memory
@@ -816,7 +829,7 @@ int launch_step_buffers_t(ts_b200_kernel *k, const void *in, void *out, bool dry
     a.n_strips = strips;
     a.n_segs = segs;
     a.seg_h = eff_seg(k);
-    a.ring = use_walk2(k) ? 6 / walk_rows(k) : k->ring;
+    a.ring = use_walk2(k) ? walk_window(k) / walk_rows(k) : k->ring;
     a.partials = k->partials;
     cudaError_t e = dispatch_step<T>(k->C, k->imag, k->rot, k->phase, walk_rows(k), a, k->warps,
                                      smem, blocks, k->stream, nullptr, k->overlap);
@@ -871,7 +884,7 @@ int launch_step_part_t(ts_b200_kernel *k, const void *in, void *out, const tsbh:
     a.n_strips = strips;
     a.n_segs = segs;
     a.seg_h = eff_seg(k);
-    a.ring = use_walk2(k) ? 6 / walk_rows(k) : k->ring;
+    a.ring = use_walk2(k) ? walk_window(k) / walk_rows(k) : k->ring;
     a.partials = partials;
     a.inv_copy = p.inv_copy;
     if (p.a1 > 0) {
@@ -1585,7 +1598,7 @@ int ts_b200_launch_info(const ts_b200_kernel *k, ts_b200_launch_shape *out) {
     out->cells_per_lane = k->C;
     out->segment_rows = eff_seg(k);
     out->warps_per_block = k->warps;
-    out->ring_depth = use_walk2(k) ? 6 : k->ring;
+    out->ring_depth = use_walk2(k) ? walk_window(k) : k->ring;
     out->walk = walk_rows(k);
     out->strips = strips;
     out->segments = segs;

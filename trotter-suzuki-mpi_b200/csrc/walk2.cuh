@@ -6,21 +6,22 @@
 // previous one), arranged so that the row body carries no row checks:
 //
 //   * The walk of a segment with output rows [oy0, oy1) visits the rows
-//     oy0 - 4 .. oy1 + 3 (the 4 vertical sweeps spoil one row per sweep at
-//     each end of the walk, so these halo rows absorb everything that happens
-//     beyond them).  Rows of the walk outside the tile are not copied: their
+//     oy0 - HY .. oy1 + HY - 1 (the HY vertical sweeps, 4, or 6 in a
+//     rotating frame, spoil one row per sweep at each end of the walk, so
+//     these halo rows absorb everything that happens beyond them).  Rows of the walk outside the tile are not copied: their
 //     ring slot keeps an older row (finite values), which only ever meets a
 //     tile row through a vertical pair across the tile edge, and those pairs
 //     carry the identity (1, 0) from a per-warp table of pair coefficients
 //     (src/cpucartesian.cpp:4-70 skips them: closed boundary).  Every other
 //     stage needs no check at all.
-//   * The walk stores row c - 4 in the iteration that loads row c; with the
-//     4 halo rows below the segment the last stored row is finished in the
-//     iteration of the last loaded row, so there is no drain.
+//   * The walk stores row c - HY in the iteration that loads row c; with
+//     the HY halo rows below the segment the last stored row is finished in
+//     the iteration of the last loaded row, so there is no drain.
 //   * Ring slots and window rows are compile-time indices: the body is
-//     unrolled over 6 rows, which is the ring depth and the window height
-//     (the window holds the row being loaded one iteration ahead plus rows
-//     c .. c-4), and even, so row parities are compile-time as well.  The
+//     unrolled over NW rows (6; 8 in a rotating frame), which is the ring
+//     depth and the window height (the window holds the row being loaded one
+//     iteration ahead plus rows c .. c-HY), and even, so row parities are
+//     compile-time as well.  The
 //     mbarriers are re-initialised for every task, so their phases are
 //     compile-time up to one bit per chunk.
 //   * Loads run one row ahead: the iteration of row c waits for row c + 1
@@ -31,10 +32,12 @@
 //     the second row's chain of stages runs one stage behind the first's
 //     (row c + 1's V0 needs only row c's V0), so the two chains overlap.
 //
-// Variants: single component, no rotating frame, cartesian (phases 0-2), 2 or
-// 4 cells per lane, both precisions and time modes.  The arithmetic of each
-// cell is that of step_kernel (the same pair forms, potential row and
-// reductions), so both give the same bits.
+// Variants: single component, cartesian (phases 0-2), 2 or 4 cells per lane
+// (2 in a rotating frame), both precisions and time modes.  The arithmetic of
+// each cell is that of step_kernel (the same pair forms, potential row,
+// rotation sweeps and reductions), so both give the same bits; the rotating
+// frame's row and column rotations across the tile's edges take the identity
+// as its vertical pairs do.
 #pragma once
 #include "step_kernel.cuh"
 #include "walk2_shape.h"
@@ -44,19 +47,27 @@ namespace tsb {
 template <class V, int R_ = 1>
 struct W2Shape {
     static constexpr int C = V::C;
-    static constexpr int R = R_;        // rows per iteration (and per ring slot)
-    static constexpr int NW = 6;        // window rows
-    static constexpr int D = 6 / R_;    // ring slots per warp
-    static constexpr int UNROLL = 6;    // rows per unrolled chunk
-    static constexpr int HX = 4, HY = 4;
+    static constexpr bool ROT = V::ROT;
+    static constexpr int R = R_;               // rows per iteration (and per ring slot)
+    // window rows: the row loaded ahead and rows c .. c-4 (c-6 in a rotating
+    // frame, whose step has 6 vertical sweeps)
+    static constexpr int NW = ROT ? 8 : 6;
+    static constexpr int D = NW / R_;          // ring slots per warp
+    static constexpr int UNROLL = NW;          // rows per unrolled chunk
+    static constexpr int HX = ROT ? 8 : 4, HY = ROT ? 6 : 4;
+    static constexpr int SO = 2 * HY;          // walk index of the first stored row
+    // slot indices in flight ahead of the current one: the slot of row c-2
+    // (whose table the current iteration reads) is refilled with row c-2+NW
+    static constexpr int AHEAD = D - 2 / R_;
     static constexpr int SW = 32 * C, WO = SW - 2 * HX;
     static constexpr int ROWB = V::PSI_BYTES + V::TAB_BYTES;  // one row of psi and table
     static constexpr int SLOT = R_ * ROWB;
     // vertical pair coefficients: entry j is the pair (u - 1, u) with
-    // u = ra + j - VPAD; the first stages of a walk read up to VPAD entries
-    // before the first row
-    static constexpr int VPAD = 4;
-    static_assert(!V::ROT && !V::PB && !V::CYL, "look-ahead walk: plain variants only");
+    // u = ra + j - VPAD; the first stages of a walk read up to VPAD - 1
+    // entries before the first row
+    static constexpr int VPAD = ROT ? 6 : 4;
+    static_assert(V::HX == HX && (!ROT || V::C == 2), "look-ahead walk geometry");
+    static_assert(!V::PB && !V::CYL, "look-ahead walk: one cartesian component");
     static_assert(R_ == 1 || R_ == 2, "one or two rows per iteration");
     static_assert(D * R == UNROLL && NW == UNROLL && UNROLL % 2 == 0,
                   "compile-time slots and parities");
@@ -80,6 +91,11 @@ struct Walk2 {
     Cx<T> win[S::NW][C];
     T hpa[C - 1], hpb[C - 1];  // this lane's horizontal pairs (i, i+1)
     T hal, hbl, har, hbr;      // and its pairs with the neighbour lanes
+    // rotating frame: this lane's column rotation coefficients, its pair
+    // masks for the row rotation sweeps, the per-row coefficients
+    Cx<T> colab[C];
+    LaneMask<C> m;
+    const Cx<T> *row_ab;
     bool out_col[C], norm_col[C], all_out;
     int ra, nit, lane;
     int n_lo, n_hi;  // iterations whose stored row is in the norm region
@@ -195,9 +211,35 @@ __device__ __forceinline__ void store_row_cells(Cx<T> *o, const Cx<T> (&v)[C], c
         if (in[i]) st_cx_global(o + i, v[i]);
 }
 
-// The stages of current row c = ra + t (t = base + K, base a multiple of 6):
-// V0 H0 V1 (H1 P H1) V1 H0 V0 one row behind each other, then the store of
-// the finished row c - 4.
+// Rotating frame: the row rotation coefficients of tile row u (rows of the
+// walk outside the tile take row 0's or row H-1's: their results never reach
+// a tile row).
+template <class V, int R>
+__device__ __forceinline__ Cx<typename V::T> w2_row_ab(const Walk2<V, R> &w, int u) {
+    u = u < 0 ? 0 : (u >= w.H ? w.H - 1 : u);
+    return w.row_ab[u];
+}
+
+// Rotating frame: the column rotation sweep on rows (u - 1, u), the identity
+// unless both rows are in the tile.
+template <class V, int R>
+__device__ __forceinline__ void w2_rcol(const Walk2<V, R> &w, Cx<typename V::T> (&up)[V::C],
+                                        Cx<typename V::T> (&lo)[V::C], int u) {
+    using T = typename V::T;
+    const bool ok = u >= 1 && u < w.H;
+    Cx<T> ab[V::C];
+#pragma unroll
+    for (int i = 0; i < V::C; ++i)
+        ab[i] = ok ? w.colab[i] : Cx<T>{DeltaForm<T>::value ? T(0) : T(1), T(0)};
+    rcol<V::IMAG, V::C>(up, lo, ab);
+}
+
+// The stages of current row c = ra + t (t = base + K, base a multiple of
+// UNROLL): V0 H0 V1 (H1 P H1) V1 H0 V0 one row behind each other, then the
+// store of the finished row c - 4; in a rotating frame V0 H0 V1 (H1 P R R)
+// Rc Rc (R R H1) V1 H0 V0 (R: a row rotation sweep of parity 0 then 1, Rc:
+// the column rotation sweeps on the pairs starting at even, then odd rows,
+// src/cpucartesian.cpp:139-177), the store of row c - 6.
 template <class V, int R, int K>
 __device__ __forceinline__ void w2_stages(Walk2<V, R> &w, int t) {
     using T = typename V::T;
@@ -205,53 +247,108 @@ __device__ __forceinline__ void w2_stages(Walk2<V, R> &w, int t) {
     using S = W2Shape<V, R>;
     constexpr int C = V::C;
     constexpr bool IMAG = V::IMAG, PHASE = V::PHASE;
-    // row c - j lives in win[(K - j) mod 6]
+    // row c - j lives in win[(K - j) mod NW]
 #define W2S(j) w.win[((K) - (j) + 2 * S::NW) % S::NW]
     const Cx<T> *vc = w.vco + t + S::VPAD;
-    // ---- S1: V0 on rows (c-1, c)
-    {
-        const Cx<T> cv = vc[0];
-        vsweep<IMAG, C, ((K + 1) & 1)>(W2S(1), W2S(0), cv.re, cv.im);
+    if constexpr (S::ROT) {
+        const int c = w.ra + t;
+        // ---- S1: V0 on rows (c-1, c)
+        {
+            const Cx<T> cv = vc[0];
+            vsweep<IMAG, C, ((K + 1) & 1)>(W2S(1), W2S(0), cv.re, cv.im);
+        }
+        // ---- S2: H0 on row c-1
+        hsweep_lanes<IMAG, ((K + 1) & 1), C>(W2S(1), w.hpa, w.hpb, w.hal, w.hbl, w.har, w.hbr);
+        // ---- S3: V1 on rows (c-2, c-1)
+        {
+            const Cx<T> cv = vc[-1];
+            vsweep<IMAG, C, ((K + 1) & 1)>(W2S(2), W2S(1), cv.re, cv.im);
+        }
+        // ---- S4: H1, P and the row rotations on row c-2
+        {
+            constexpr int RT = (K + S::UNROLL - 2) % S::UNROLL;
+            constexpr int q = RT / R, pos = RT % R;
+            hsweep_lanes<IMAG, ((K + 1) & 1), C>(W2S(2), w.hpa, w.hpb, w.hal, w.hbl, w.har, w.hbr);
+            alignas(16) TabT tv[C];
+            load_tab_cells<TabT, C>(w.ring + q * S::SLOT + pos * S::ROWB + V::PSI_BYTES +
+                                        C * (int)sizeof(TabT) * w.lane,
+                                    tv);
+            potential_row<IMAG, PHASE, V::LHY, false, C>(W2S(2), tv, w.ca, w.caa);
+            const Cx<T> ab = w2_row_ab(w, c - 2);
+            rrow<IMAG, C, 0, true>(W2S(2), ab.re, ab.im, w.m);
+            rrow<IMAG, C, 1, true>(W2S(2), ab.re, ab.im, w.m);
+        }
+        if constexpr ((K & 1) == 1) {
+            // ---- S5: column rotations on rows (c-3, c-2), c-3 even
+            w2_rcol(w, W2S(3), W2S(2), c - 2);
+            // ---- S6: column rotations on rows (c-4, c-3), c-4 odd
+            w2_rcol(w, W2S(4), W2S(3), c - 3);
+        }
+        // ---- S7: the row rotations again, then H1, on row c-4
+        {
+            const Cx<T> ab = w2_row_ab(w, c - 4);
+            rrow<IMAG, C, 0, true>(W2S(4), ab.re, ab.im, w.m);
+            rrow<IMAG, C, 1, true>(W2S(4), ab.re, ab.im, w.m);
+            hsweep_lanes<IMAG, ((K + 1) & 1), C>(W2S(4), w.hpa, w.hpb, w.hal, w.hbl, w.har, w.hbr);
+        }
+        // ---- S8: V1 on rows (c-5, c-4)
+        {
+            const Cx<T> cv = vc[-4];
+            vsweep<IMAG, C, ((K) & 1)>(W2S(5), W2S(4), cv.re, cv.im);
+        }
+        // ---- S9: H0 on row c-5
+        hsweep_lanes<IMAG, ((K + 1) & 1), C>(W2S(5), w.hpa, w.hpb, w.hal, w.hbl, w.har, w.hbr);
+        // ---- S10: V0 on rows (c-6, c-5)
+        {
+            const Cx<T> cv = vc[-5];
+            vsweep<IMAG, C, ((K) & 1)>(W2S(6), W2S(5), cv.re, cv.im);
+        }
+    } else {
+        // ---- S1: V0 on rows (c-1, c)
+        {
+            const Cx<T> cv = vc[0];
+            vsweep<IMAG, C, ((K + 1) & 1)>(W2S(1), W2S(0), cv.re, cv.im);
+        }
+        // ---- S2: H0 on row c-1
+        hsweep_lanes<IMAG, ((K + 1) & 1), C>(W2S(1), w.hpa, w.hpb, w.hal, w.hbl, w.har, w.hbr);
+        // ---- S3: V1 on rows (c-2, c-1)
+        {
+            const Cx<T> cv = vc[-1];
+            vsweep<IMAG, C, ((K + 1) & 1)>(W2S(2), W2S(1), cv.re, cv.im);
+        }
+        // ---- S4: H1, P, H1 on row c-2 (its table from its ring slot)
+        {
+            constexpr int RT = (K + S::UNROLL - 2) % S::UNROLL;  // row c-2 within the chunk
+            constexpr int q = RT / R, pos = RT % R;
+            hsweep_lanes<IMAG, ((K + 1) & 1), C>(W2S(2), w.hpa, w.hpb, w.hal, w.hbl, w.har, w.hbr);
+            alignas(16) TabT tv[C];
+            load_tab_cells<TabT, C>(w.ring + q * S::SLOT + pos * S::ROWB + V::PSI_BYTES +
+                                        C * (int)sizeof(TabT) * w.lane,
+                                    tv);
+            potential_row<IMAG, PHASE, V::LHY, false, C>(W2S(2), tv, w.ca, w.caa);
+            hsweep_lanes<IMAG, ((K + 1) & 1), C>(W2S(2), w.hpa, w.hpb, w.hal, w.hbl, w.har, w.hbr);
+        }
+        // ---- S5: V1 on rows (c-3, c-2)
+        {
+            const Cx<T> cv = vc[-2];
+            vsweep<IMAG, C, ((K) & 1)>(W2S(3), W2S(2), cv.re, cv.im);
+        }
+        // ---- S6: H0 on row c-3
+        hsweep_lanes<IMAG, ((K + 1) & 1), C>(W2S(3), w.hpa, w.hpb, w.hal, w.hbl, w.har, w.hbr);
+        // ---- S7: V0 on rows (c-4, c-3)
+        {
+            const Cx<T> cv = vc[-3];
+            vsweep<IMAG, C, ((K) & 1)>(W2S(4), W2S(3), cv.re, cv.im);
+        }
     }
-    // ---- S2: H0 on row c-1
-    hsweep_lanes<IMAG, ((K + 1) & 1), C>(W2S(1), w.hpa, w.hpb, w.hal, w.hbl, w.har, w.hbr);
-    // ---- S3: V1 on rows (c-2, c-1)
-    {
-        const Cx<T> cv = vc[-1];
-        vsweep<IMAG, C, ((K + 1) & 1)>(W2S(2), W2S(1), cv.re, cv.im);
-    }
-    // ---- S4: H1, P, H1 on row c-2 (its table from its ring slot)
-    {
-        constexpr int RT = (K + S::UNROLL - 2) % S::UNROLL;  // row c-2 within the chunk
-        constexpr int q = RT / R, pos = RT % R;
-        hsweep_lanes<IMAG, ((K + 1) & 1), C>(W2S(2), w.hpa, w.hpb, w.hal, w.hbl, w.har, w.hbr);
-        alignas(16) TabT tv[C];
-        load_tab_cells<TabT, C>(w.ring + q * S::SLOT + pos * S::ROWB + V::PSI_BYTES +
-                                    C * (int)sizeof(TabT) * w.lane,
-                                tv);
-        potential_row<IMAG, PHASE, V::LHY, false, C>(W2S(2), tv, w.ca, w.caa);
-        hsweep_lanes<IMAG, ((K + 1) & 1), C>(W2S(2), w.hpa, w.hpb, w.hal, w.hbl, w.har, w.hbr);
-    }
-    // ---- S5: V1 on rows (c-3, c-2)
-    {
-        const Cx<T> cv = vc[-2];
-        vsweep<IMAG, C, ((K) & 1)>(W2S(3), W2S(2), cv.re, cv.im);
-    }
-    // ---- S6: H0 on row c-3
-    hsweep_lanes<IMAG, ((K + 1) & 1), C>(W2S(3), w.hpa, w.hpb, w.hal, w.hbl, w.har, w.hbr);
-    // ---- S7: V0 on rows (c-4, c-3)
-    {
-        const Cx<T> cv = vc[-3];
-        vsweep<IMAG, C, ((K) & 1)>(W2S(4), W2S(3), cv.re, cv.im);
-    }
-    // ---- row c-4 is finished: store it (the first 8 rows of a walk are halo;
+    // ---- row c-HY is finished: store it (the first 2 HY rows of a walk are halo;
     // with two rows per iteration the second row can lie past the walk)
-    if (t >= 8 && (R == 1 || t < w.nit)) {
-        store_row_cells<T, C>(w.orow, W2S(4), w.out_col, w.all_out);
+    if (t >= S::SO && (R == 1 || t < w.nit)) {
+        store_row_cells<T, C>(w.orow, W2S(S::HY), w.out_col, w.all_out);
         if (IMAG && t >= w.n_lo && t < w.n_hi) {
 #pragma unroll
             for (int i = 0; i < C; ++i) {
-                const Cx<T> v = W2S(4)[i];
+                const Cx<T> v = W2S(S::HY)[i];
                 if (w.norm_col[i])
                     w.nacc += (double)v.re * (double)v.re + (double)v.im * (double)v.im;
             }
@@ -291,12 +388,12 @@ __device__ __forceinline__ void w2_iter(Walk2<V, R> &w, int t, uint32_t ph) {
         }
         w2_load(w, q, 0, W2S(-1));
         w2_stages<V, R, K>(w, t);
-        // the slot of row t-2 is free: copy row t + 4 into it
-        constexpr int qi = (K + S::D - 2) % S::D;
+        // the slot of row t-2 is free: copy row t-2+NW into it
+        constexpr int qi = (K + S::AHEAD) % S::D;
         __syncwarp();
         // the slot's generic-proxy reads happen-before the bulk copy refills it
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        w.issue(t + 4, qi);
+        w.issue(t + S::AHEAD, qi);
     } else {
         // rows t and t + 1 arrive together in slot K / 2
         constexpr int q = K / 2;
@@ -309,11 +406,11 @@ __device__ __forceinline__ void w2_iter(Walk2<V, R> &w, int t, uint32_t ph) {
         w2_load(w, q, 1, W2S(-1));
         w2_stages<V, R, K>(w, t);
         w2_stages<V, R, K + 1>(w, t + 1);
-        // the slot of rows t-2, t-1 is free: copy rows t + 4, t + 5 into it
-        constexpr int qi = (q + 2) % S::D;
+        // the slot of rows t-2, t-1 is free: copy rows t-2+NW, t-1+NW into it
+        constexpr int qi = (q + S::AHEAD) % S::D;
         __syncwarp();
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        w.issue(t / 2 + 2, qi);
+        w.issue(t / 2 + S::AHEAD, qi);
     }
 #undef W2S
 }
@@ -362,8 +459,8 @@ __device__ __forceinline__ void w2_task(Walk2<V, R> &w, const StepArgs<typename 
     segment_rows(a, seg, oy0, oy1);
     w.ra = oy0 - S::HY;
     w.nit = (oy1 - oy0) + 2 * S::HY;
-    w.n_lo = a.iy0 - oy0 + 8;
-    w.n_hi = a.iy1 - oy0 + 8;
+    w.n_lo = a.iy0 - oy0 + S::SO;
+    w.n_hi = a.iy1 - oy0 + S::SO;
     const int cs = max(c0, 0);
     const int ce = min(c0 + S::SW, a.P);
     w.psi_off = (uint32_t)(cs - c0) * sizeof(Cx<T>);
@@ -397,15 +494,27 @@ __device__ __forceinline__ void w2_task(Walk2<V, R> &w, const StepArgs<typename 
         w.hbl = pl ? w.bH : T(0);
         w.har = pr ? w.aH : one;
         w.hbr = pr ? w.bH : T(0);
+        if constexpr (S::ROT) {
+            // the row rotation sweeps' pair masks and this lane's column
+            // rotation coefficients
+#pragma unroll
+            for (int i = 0; i + 1 < C; ++i) w.m.pair_int[i] = present[i] && present[i + 1];
+            w.m.pair_int[C - 1] = false;
+            w.m.pair_left = pl;
+            w.m.pair_right = pr;
+#pragma unroll
+            for (int i = 0; i < C; ++i)
+                w.colab[i] = reinterpret_cast<const Cx<T> *>(a.col_ab)[present[i] ? xl + i : 0];
+        }
         // vertical pairs (u - 1, u): the identity unless both rows are in the tile
-        const int vl = w2_vlen(a.seg_h);
+        const int vl = w2_vlen(a.seg_h, S::ROT);
         for (int j = lane; j < vl; j += 32) {
             const int u = w.ra + j - S::VPAD;
             const bool ok = u >= 1 && u < a.H;
             w.vco[j] = ok ? Cx<T>{w.aV, w.bV} : Cx<T>{one, T(0)};
         }
     }
-    w.orow = reinterpret_cast<Cx<T> *>(a.psi_out) + (ptrdiff_t)(oy0 - 8) * a.P + xl;
+    w.orow = reinterpret_cast<Cx<T> *>(a.psi_out) + (ptrdiff_t)(oy0 - S::SO) * a.P + xl;
     __syncwarp();  // the previous task's reads of the ring are done
     if (c0 < 0 || c0 + S::SW > a.P) {
         // cells of the strip outside the tile read as 0 (copies do not cover them)
@@ -434,8 +543,8 @@ __device__ __forceinline__ void w2_task(Walk2<V, R> &w, const StepArgs<typename 
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
     __syncwarp();
-    // the first 4 rows of the walk (slots 0 .. 3, or row pairs 0 .. 1)
-    constexpr int PRE = 4 / R;
+    // the first rows of the walk (slots 0 .. AHEAD-1)
+    constexpr int PRE = S::AHEAD;
 #pragma unroll
     for (int q = 0; q < PRE; ++q) w.issue(q, q);
     bool ok = true;
@@ -460,9 +569,10 @@ __device__ __forceinline__ void w2_task(Walk2<V, R> &w, const StepArgs<typename 
         // let the copies still in flight land before the block can exit:
         // slots [0, PRE) were issued before the walk and one more by each
         // completed iteration (R = 1: iteration t waits for row t + 1 and
-        // issues row t + 4; R = 2: iteration k waits for pair k and issues
-        // pair k + 2); the wait for slot index fail_idx gave up
-        const int issued_to = R == 1 ? max(PRE, w.fail_idx + 3) : max(PRE, w.fail_idx + 2);
+        // issues row t + AHEAD; R = 2: iteration k waits for pair k and
+        // issues pair k + AHEAD); the wait for slot index fail_idx gave up
+        const int issued_to =
+            R == 1 ? max(PRE, w.fail_idx - 1 + S::AHEAD) : max(PRE, w.fail_idx + S::AHEAD);
         for (int j = w.fail_idx; j < issued_to; ++j)
             (void)mbar_wait_bounded(&w.bars[j % S::D], (uint32_t)(j / S::D) & 1u, 100000000ull);
     }
@@ -546,9 +656,11 @@ __device__ __forceinline__ void w2_finish(const StepArgs<typename V::T> &a, doub
 // Blocks of 4 or 8 warps; each warp loops over the tasks t = warp_global,
 // warp_global + total_warps, ...
 // Register budget: 2 cells per lane fit 128 registers, so 16 warps of the
-// default 4-warp blocks stay resident per SM; 4 cells per lane take up to 255.
+// default 4-warp blocks stay resident per SM; 4 cells per lane and the
+// rotating frame's 8-row window take up to 255.
 template <class V, int R>
-__global__ void __launch_bounds__(256, V::C == 2 ? 2 : 1) step2_kernel(StepArgs<typename V::T> a) {
+__global__ void __launch_bounds__(256, (V::C == 2 && !V::ROT) ? 2 : 1)
+    step2_kernel(StepArgs<typename V::T> a) {
     using T = typename V::T;
     using S = W2Shape<V, R>;
     extern __shared__ __align__(128) unsigned char smem[];
@@ -561,7 +673,7 @@ __global__ void __launch_bounds__(256, V::C == 2 ? 2 : 1) step2_kernel(StepArgs<
     const int warp = __shfl_sync(0xffffffffu, (int)(threadIdx.x >> 5), 0);
     const int lane = threadIdx.x & 31;
     const int n_tasks = a.n_strips * a.n_segs;
-    const int vl = w2_vlen(a.seg_h);
+    const int vl = w2_vlen(a.seg_h, S::ROT);
 
     Walk2<V, R> w;
     w.lane = lane;
@@ -611,6 +723,7 @@ __global__ void __launch_bounds__(256, V::C == 2 ? 2 : 1) step2_kernel(StepArgs<
     }
     w.ca = a.ca;
     w.caa = a.caa;
+    w.row_ab = reinterpret_cast<const Cx<T> *>(a.row_ab);
     w.opitch = (size_t)a.P;
     w.gpsi_pitch = (size_t)a.P * sizeof(Cx<T>);
     w.gtab_pitch = (size_t)a.P * sizeof(typename V::TabT);
