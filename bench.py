@@ -90,6 +90,15 @@ def committed_traffic(summary="step_kernel_gpe_imag_2048.md"):
         return None
 
 
+def rotating_frame_traffic():
+    """DRAM bytes per FP64 rotating-frame step launch at the current vortex
+    side: the committed capture on 4096^2 (the 8192^2 workload is too large
+    to capture within a few GB) scaled by the lattice sites (the traffic grows
+    with the cells: every strip and segment has the same shape)."""
+    t = committed_traffic("step_kernel_rotating_frame_4096.md")
+    return None if t is None else int(t * (VORTEX_N / 4096.0) ** 2)
+
+
 class Clocks:
     """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
     FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -994,7 +1003,7 @@ def pg_world(pg):
 
 
 def vortex_config(steps=VORTEX_STEPS):
-    return {"workload": "vortex8192_precision", "lattice": f"{VORTEX_N}x{VORTEX_N}",
+    return {"workload": f"vortex{VORTEX_N}_precision", "lattice": f"{VORTEX_N}x{VORTEX_N}",
             "length": VORTEX_LENGTH, "boundary": "periodic", "g": VORTEX_G,
             "omega_rot": VORTEX_OMEGA, "dt": VORTEX_DT, "trotter_steps": steps,
             "initial": "Thomas-Fermi x 8 windings (radius 10)", "seed": VORTEX_SEED}
@@ -1118,7 +1127,7 @@ def slab_leg(args, rank, world, local, pg, device, per_gpu=1, split=True, steps=
 
 
 def slab_config(steps=SLAB_STEPS):
-    return dict(vortex_config(steps), workload="vortex8192_slabs", precision="fp64",
+    return dict(vortex_config(steps), workload=f"vortex{VORTEX_N}_slabs", precision="fp64",
                 split="rows, one slab per rank")
 
 
@@ -1141,8 +1150,9 @@ def run_slab_workload(args, rank, world, local, pg):
         "slab": res,
         "roofline": {"bound": "hbm", "achieved": r["achieved"], "peak": r["peak"],
                      "unit": "GB/s", "frac": r["frac"], "peak_kind": r["peak_kind"],
-                     "traffic": None, "kernel": "tsb::step_kernel<double, C=2, real, rotating "
-                                                "frame, GPE>, edge bands + interior"},
+                     "traffic": None, "kernel": "tsb::step2_kernel<double, C=2, real, rotating "
+                                                "frame, GPE> (look-ahead walk), edge bands + "
+                                                "interior"},
         "clocks": clk,
         "gpu_launches": launches,
     }
@@ -1171,9 +1181,11 @@ def run_vortex_workload(args, rank, world, local, pg):
         "fp64_from_fp32_rounded_psi0_vs_fp64": res["errors_fp64_from_fp32_psi0"],
         "roofline": {"bound": "hbm", "achieved": r64["achieved"], "peak": r64["peak"],
                      "unit": "GB/s", "frac": r64["frac"], "peak_kind": r64["peak_kind"],
-                     "traffic": None,
+                     "traffic": rotating_frame_traffic(),
+                     "traffic_source": "ncu capture on 4096^2 scaled by the sites",
                      "algorithmic_bytes_per_launch": r64["algorithmic_bytes_per_launch"],
-                     "kernel": "tsb::step_kernel<double, C=2, real, rotating frame, GPE> + halo"},
+                     "kernel": "tsb::step2_kernel<double, C=2, real, rotating frame, GPE, 2 rows "
+                               "per iteration> (look-ahead walk) + halo"},
         "clocks": clk,
         "gpu_launches": launches,
     }
@@ -1536,6 +1548,9 @@ def main():
     ap.add_argument("--split", choices=["none", "slab"], default="none",
                     help="slab: the 8192^2 vortex lattice as one lattice in slabs of rows "
                          "over the ranks (strong scaling)")
+    ap.add_argument("--vortex-side", type=int, default=0,
+                    help="lattice side of the vortex / slab workloads (default 8192; smaller "
+                         "sides keep an ncu capture of their kernels within a few GB)")
     ap.add_argument("--slabs-per-gpu", type=int, default=1,
                     help="--split slab in one process: this many slabs on its GPU")
     ap.add_argument("--no-split", action="store_true",
@@ -1545,6 +1560,9 @@ def main():
                                            "two_component_2048", "cylindrical_vortex_2048"],
                     default="gpe_imaginary_time_2048")
     args = ap.parse_args()
+    if args.vortex_side:
+        global VORTEX_N
+        VORTEX_N = int(args.vortex_side)
     args.warmup = max(3, args.warmup)
     rank, world, local, pg = dist_setup(args)
     try:
