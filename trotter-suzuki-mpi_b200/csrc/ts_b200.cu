@@ -1618,6 +1618,8 @@ int ts_b200_set_launch(ts_b200_kernel *k, int C, int seg_h, int warps, int ring)
         return TS_B200_INVALID_ARGUMENT;
     if (warps == 8 && !use_walk2(k))
         return fail(k, TS_B200_UNSUPPORTED, "8 warps per block need the look-ahead walk");
+    if (warps == 8 && k->rot)
+        return fail(k, TS_B200_UNSUPPORTED, "rotating-frame kernels use blocks of at most 4 warps");
     if (ring != 0 && (ring < min_ring(k) || ring > 16))
         return fail(k, TS_B200_INVALID_ARGUMENT, "ring depth out of range for this variant");
     if (seg_h < 0) return TS_B200_INVALID_ARGUMENT;
@@ -1674,10 +1676,11 @@ int ts_b200_autotune(ts_b200_kernel *k, int trial_steps) {
     int best_seg = seg0, best_warps = warps0;
     bool best_overlap = overlap0;
     int st = TS_B200_OK;
-    // the look-ahead walk: blocks of 4 or 8 warps, with and without
-    // programmatic dependent launch; the checked walk: 4 or 2 warps
+    // the look-ahead walk: blocks of 4 or 8 warps (4 or 2 in a rotating
+    // frame), with and without programmatic dependent launch; the checked
+    // walk: 4 or 2 warps
     const bool w2 = use_walk2(k);
-    const int warp_opts[2] = {4, w2 ? 8 : 2};
+    const int warp_opts[2] = {4, (w2 && !k->rot) ? 8 : 2};
     for (int trial = 0; trial < (w2 ? 4 : 2) && st == TS_B200_OK; ++trial) {
         const int warps = warp_opts[trial & 1];
         k->overlap = w2 ? ((trial >> 1) ? !overlap0 : overlap0) : overlap0;

@@ -96,6 +96,12 @@ struct Walk2 {
     Cx<T> colab[C];
     LaneMask<C> m;
     const Cx<T> *row_ab;
+    // single precision: the row rotation coefficients of walk rows t-4 .. t-1
+    // (row j in rab[j % 4]), each loaded two rows ahead of its first use
+    // (measured 624 -> 600 us per 8192^2 step; in double the four registers
+    // cost more than the loads: 967 -> 991 us)
+    static constexpr bool AB_AHEAD = sizeof(T) == 4;
+    Cx<T> rab[4];
     bool out_col[C], norm_col[C], all_out;
     int ra, nit, lane;
     int n_lo, n_hi;  // iterations whose stored row is in the norm region
@@ -274,7 +280,7 @@ __device__ __forceinline__ void w2_stages(Walk2<V, R> &w, int t) {
                                         C * (int)sizeof(TabT) * w.lane,
                                     tv);
             potential_row<IMAG, PHASE, V::LHY, false, C>(W2S(2), tv, w.ca, w.caa);
-            const Cx<T> ab = w2_row_ab(w, c - 2);
+            const Cx<T> ab = Walk2<V, R>::AB_AHEAD ? w.rab[(K + 2) % 4] : w2_row_ab(w, c - 2);
             rrow<IMAG, C, 0, true>(W2S(2), ab.re, ab.im, w.m);
             rrow<IMAG, C, 1, true>(W2S(2), ab.re, ab.im, w.m);
         }
@@ -284,12 +290,15 @@ __device__ __forceinline__ void w2_stages(Walk2<V, R> &w, int t) {
             // ---- S6: column rotations on rows (c-4, c-3), c-4 odd
             w2_rcol(w, W2S(4), W2S(3), c - 3);
         }
-        // ---- S7: the row rotations again, then H1, on row c-4
+        // ---- S7: the row rotations again, then H1, on row c-4 (ahead: its
+        // coefficients' register takes row c's, used two and four rows on)
         {
-            const Cx<T> ab = w2_row_ab(w, c - 4);
+            constexpr bool AHEAD = Walk2<V, R>::AB_AHEAD;
+            const Cx<T> ab = AHEAD ? w.rab[K % 4] : w2_row_ab(w, c - 4);
             rrow<IMAG, C, 0, true>(W2S(4), ab.re, ab.im, w.m);
             rrow<IMAG, C, 1, true>(W2S(4), ab.re, ab.im, w.m);
             hsweep_lanes<IMAG, ((K + 1) & 1), C>(W2S(4), w.hpa, w.hpb, w.hal, w.hbl, w.har, w.hbr);
+            if constexpr (AHEAD) w.rab[K % 4] = w2_row_ab(w, c);
         }
         // ---- S8: V1 on rows (c-5, c-4)
         {
@@ -505,6 +514,11 @@ __device__ __forceinline__ void w2_task(Walk2<V, R> &w, const StepArgs<typename 
 #pragma unroll
             for (int i = 0; i < C; ++i)
                 w.colab[i] = reinterpret_cast<const Cx<T> *>(a.col_ab)[present[i] ? xl + i : 0];
+            // the row coefficients of the rows before the walk's first
+            if constexpr (Walk2<V, R>::AB_AHEAD) {
+#pragma unroll
+                for (int j = 0; j < 4; ++j) w.rab[j] = w2_row_ab(w, w.ra - 4 + j);
+            }
         }
         // vertical pairs (u - 1, u): the identity unless both rows are in the tile
         const int vl = w2_vlen(a.seg_h, S::ROT);
@@ -653,13 +667,24 @@ __device__ __forceinline__ void w2_finish(const StepArgs<typename V::T> &a, doub
     }
 }
 
-// Blocks of 4 or 8 warps; each warp loops over the tasks t = warp_global,
-// warp_global + total_warps, ...
+// Blocks of 4 or 8 warps (4 in a rotating frame); each warp loops over the
+// tasks t = warp_global, warp_global + total_warps, ...
 // Register budget: 2 cells per lane fit 128 registers, so 16 warps of the
-// default 4-warp blocks stay resident per SM; 4 cells per lane and the
-// rotating frame's 8-row window take up to 255.
+// default 4-warp blocks stay resident per SM; 4 cells per lane take up to
+// 255.  In a rotating frame (blocks of at most 4 warps) the 8-row window
+// takes ~150 registers in double, 3 blocks per SM as its 8-row ring allows
+// (capping the registers at 170 for 3 blocks made the compiler's schedule
+// slower: 967 -> 1012 us per 8192^2 step); in float a cap of 170 (4 blocks
+// per SM) ran 600 us against 621 at a cap of 128 (5 blocks).
+template <class V>
+struct W2Bounds {
+    static constexpr bool ROT32 = V::ROT && sizeof(typename V::T) == 4;
+    static constexpr int THREADS = ROT32 ? 128 : 256;
+    static constexpr int MIN_BLOCKS = ROT32 ? 3 : ((V::C == 2 && !V::ROT) ? 2 : 1);
+};
+
 template <class V, int R>
-__global__ void __launch_bounds__(256, (V::C == 2 && !V::ROT) ? 2 : 1)
+__global__ void __launch_bounds__(W2Bounds<V>::THREADS, W2Bounds<V>::MIN_BLOCKS)
     step2_kernel(StepArgs<typename V::T> a) {
     using T = typename V::T;
     using S = W2Shape<V, R>;
