@@ -509,12 +509,14 @@ __device__ __forceinline__ bool phase_tiny(float th) { return fabsf(th) < 0.0039
 __device__ __forceinline__ bool phase_small(double th) { return fabs(th) < 0.03125; }
 __device__ __forceinline__ bool phase_small(float th) { return fabsf(th) < 0.03125f; }
 
-template <typename T>
+// TIERS = false: the 1/32 tier and the library only (less code, for the
+// kernels whose row body is long enough for instruction fetch to limit them).
+template <typename T, bool TIERS = true>
 __device__ __forceinline__ void phase_sincos(T th, T *s, T *c) {
     constexpr bool F = std::is_same<T, float>::value;
     // warp-uniform choice: the shorter series if every lane allows it, the
     // library path only if some lane needs it
-    if (!__any_sync(0xffffffffu, !phase_tiny(th))) {
+    if (TIERS && !__any_sync(0xffffffffu, !phase_tiny(th))) {
         const T t = th * th;
         if (F) {
             const T pc = fma_t(T(4.1666666666666664e-02), t, T(-0.5));               // 1/4!, -1/2!
@@ -558,10 +560,10 @@ __device__ __forceinline__ void phase_sincos(T th, T *s, T *c) {
 }
 
 // exp(-th) for the imaginary-time nonlinear factor (same tiers).
-template <typename T>
+template <typename T, bool TIERS = true>
 __device__ __forceinline__ T phase_expneg(T th) {
     constexpr bool F = std::is_same<T, float>::value;
-    if (!__any_sync(0xffffffffu, !phase_tiny(th))) {
+    if (TIERS && !__any_sync(0xffffffffu, !phase_tiny(th))) {
         const T x = -th;
         if (F) {
             T p = fma_t(T(4.1666666666666664e-02), x, T(1.6666666666666666e-01));  // 1/4!, 1/3!
@@ -597,8 +599,9 @@ __device__ __forceinline__ T phase_expneg(T th) {
 
 // exp(-th0), exp(-th1) of two single-precision cells: the series of both in
 // one packed pair, each cell with the roundings of phase_expneg.
+template <bool TIERS = true>
 __device__ __forceinline__ float2 phase_expneg2(float th0, float th1) {
-    if (!__any_sync(0xffffffffu, !(phase_tiny(th0) && phase_tiny(th1)))) {
+    if (TIERS && !__any_sync(0xffffffffu, !(phase_tiny(th0) && phase_tiny(th1)))) {
         const float2 x = make_float2(-th0, -th1);
         constexpr double k[4] = {1.6666666666666666e-01, 0.5, 1.0, 1.0};
         float2 p = make_float2(float(4.1666666666666664e-02), float(4.1666666666666664e-02));
@@ -616,7 +619,7 @@ __device__ __forceinline__ float2 phase_expneg2(float th0, float th1) {
         for (int j = 0; j < 8; ++j) p = __ffma2_rn(p, x, make_float2(float(k[j]), float(k[j])));
         return p;
     }
-    return make_float2(phase_expneg(th0), phase_expneg(th1));
+    return make_float2(phase_expneg<float, TIERS>(th0), phase_expneg<float, TIERS>(th1));
 }
 
 template <typename T>
@@ -662,7 +665,8 @@ __device__ __forceinline__ Cx<T> rabi_cell(Cx<T> self, Cx<T> other, T cc, T sr, 
 // PB (two components): the phase adds g_ab dt |psi_b|^2, psi_b the other
 // species' cell at the start of this step (`ub`, already scaled)
 // (src/cpucartesian.cpp:73-92,113-126).
-template <bool IMAG, bool PHASE, bool LHY, bool PB, int C, typename T, typename TabT>
+template <bool IMAG, bool PHASE, bool LHY, bool PB, int C, bool TIERS = true, typename T,
+          typename TabT>
 __device__ __forceinline__ void potential_row(Cx<T> (&w)[C], const TabT *tab, T ca, T caa,
                                               const Cx<T> (*ub)[C] = nullptr, T cab = T(0)) {
     if constexpr (IMAG && PHASE && std::is_same<T, float>::value && C % 2 == 0) {
@@ -683,7 +687,7 @@ __device__ __forceinline__ void potential_row(Cx<T> (&w)[C], const TabT *tab, T 
         for (int i = 0; i < C; i += 2) {
             const float2 pr = make_float2(reinterpret_cast<const T *>(tab)[i],
                                           reinterpret_cast<const T *>(tab)[i + 1]);
-            const float2 f = __fmul2_rn(phase_expneg2(th[i], th[i + 1]), pr);
+            const float2 f = __fmul2_rn(phase_expneg2<TIERS>(th[i], th[i + 1]), pr);
             w[i] = scale_cx(w[i], f.x);
             w[i + 1] = scale_cx(w[i + 1], f.y);
         }
@@ -704,7 +708,7 @@ __device__ __forceinline__ void potential_row(Cx<T> (&w)[C], const TabT *tab, T 
                 T th = mul_t(ca, n2);
                 if (LHY) th = fma_t(caa, mul_t(n2, sqrt_t(n2)), th);
                 if (PB) th = th + thb;
-                v = scale_cx(v, mul_t(phase_expneg(th), pr));
+                v = scale_cx(v, mul_t(phase_expneg<T, TIERS>(th), pr));
             } else {
                 v = scale_cx(v, pr);
             }
@@ -716,7 +720,7 @@ __device__ __forceinline__ void potential_row(Cx<T> (&w)[C], const TabT *tab, T 
                 T th = mul_t(ca, n2);
                 if (LHY) th = fma_t(caa, mul_t(n2, sqrt_t(n2)), th);
                 if (PB) th = th + thb;
-                phase_sincos(th, &s, &c);
+                phase_sincos<T, TIERS>(th, &s, &c);
             }
             // the table holds (cos, sin) of -dt V; in delta form (cos - 1, sin):
             // v (cos + i sin), the kinetic pair's form with the cell as its own
@@ -938,9 +942,9 @@ __device__ __forceinline__ void walk_row(Walk<V> &w, const StepArgs<typename V::
                 }
                 ub[i] = u;
             }
-            potential_row<IMAG, PHASE, false, true, C>(WS(2), tp, w.ca, w.caa, &ub, w.cab);
+            potential_row<IMAG, PHASE, false, true, C, false>(WS(2), tp, w.ca, w.caa, &ub, w.cab);
         } else {
-            potential_row<IMAG, PHASE, V::LHY, false, C>(WS(2), tp, w.ca, w.caa);
+            potential_row<IMAG, PHASE, V::LHY, false, C, !V::CYL>(WS(2), tp, w.ca, w.caa);
         }
         if constexpr (ROT) {
             const Cx<T> ab = reinterpret_cast<const Cx<T> *>(a.row_ab)[u];
@@ -1267,7 +1271,7 @@ __global__ void __launch_bounds__(128, V::MIN_BLOCKS) step_kernel(StepArgs<typen
     bind_args(w, a);
     for (int task = blockIdx.x * warps + warp; task < n_tasks && !w.failed;
          task += gridDim.x * warps)
-        run_task<V, !IMAG>(w, a, task);
+        run_task<V, !IMAG && !V::PB>(w, a, task);
 
     if constexpr (!IMAG && DeltaForm<typename V::T>::value) {
         // the last block to finish advances the schedule's step (every block
