@@ -294,8 +294,16 @@ const char *ts_b200_slabs_last_error(const ts_b200_slabs *s);
 int ts_b200_slabs_destroy(ts_b200_slabs *s);
 
 /* Queue all work of this handle on `stream` (a cudaStream_t); NULL restores
- * the handle's own stream. */
+ * the handle's own stream.  Every call that reads or writes device memory the
+ * caller owns (the *_device calls) is ordered on the handle's stream only:
+ * the caller orders its own stream against it, with these two or with
+ * ts_b200_set_stream to its own stream.  ts_b200_stream_wait: the handle's
+ * stream waits for the work queued so far on `stream` (NULL: the legacy
+ * default stream); ts_b200_stream_signal: `stream` waits for the work queued
+ * so far on the handle's. */
 int ts_b200_set_stream(ts_b200_kernel *k, void *stream);
+int ts_b200_stream_wait(ts_b200_kernel *k, void *stream);
+int ts_b200_stream_signal(ts_b200_kernel *k, void *stream);
 int ts_b200_synchronize(ts_b200_kernel *k);
 
 /* Geometry of the fused step launch chosen for this tile (for reporting):
@@ -316,13 +324,14 @@ int ts_b200_set_launch(ts_b200_kernel *k, int cells_per_lane, int segment_rows, 
                        int ring_depth);
 
 /* Row walk of the fused step (no counterpart in the reference; every walk
- * performs the same operations per cell): 2 (default) the look-ahead walk,
- * which single-component cartesian tiles without a rotating frame use, with
- * even segments, a ring of 6 rows, 4 or 8 warps per block and two rows per
- * iteration (one mbarrier per row pair; with 4 cells per lane one row); 1 the
- * same walk with one row per iteration; 0 the checked walk of every variant.  Variants without a
- * look-ahead walk ignore the choice.  ts_b200_launch_info reports the rows per
- * iteration in use (0 for the checked walk). */
+ * performs the same operations per cell): 2 (default) the look-ahead walk of
+ * every variant, with even segments, a ring of 6 rows (8 in a rotating
+ * frame), 4 or 8 warps per block (4 in a rotating frame) and two rows per
+ * iteration (one mbarrier per row pair; with 4 cells per lane one row,
+ * except in a single-precision rotating frame); 1 the same walk with one row
+ * per iteration; 0 the checked walk (a rotating frame then takes 2 cells per
+ * lane).  ts_b200_launch_info reports the rows per iteration in use (0 for
+ * the checked walk). */
 int ts_b200_set_walk(ts_b200_kernel *k, int walk);
 
 /* The look-ahead walk launches each fused step with a programmatic

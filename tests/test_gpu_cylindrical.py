@@ -111,3 +111,42 @@ def test_drop_in_cylindrical_solver(name):
     assert np.abs(state.get_state() - z["psi"]).max() <= 1e-10
     got = solver._energies()
     assert np.allclose(got, z["energies"], rtol=1e-10, atol=1e-12), (got, z["energies"])
+
+
+@pytest.mark.parametrize("imag", [False, True], ids=["real", "imag"])
+@pytest.mark.parametrize("walk", [1, 2])
+@pytest.mark.parametrize("g,l", [(0.0, 0), (40.0, 1), (25.0, 2)])
+def test_cylindrical_look_ahead_walk_matches_checked_walk(imag, walk, g, l):
+    """The look-ahead walk on a cylindrical lattice (radial sweeps around the
+    potential stage, 8 halo columns, the mirrored axis column at the store):
+    the checked walk's bits in real time, its result to 1e-13 in imaginary
+    time, the oracle at the parity bar; a tall ragged tile in several
+    segments and strips, two evolve calls."""
+    from trottersuzuki_b200 import Kernel
+    lat = O.Lattice(150, 8.0, 133, 10.0, cylindrical=True)
+    X, Y = lat.coordinates()
+    rng = np.random.default_rng(7 + l)
+    psi0 = np.exp(-((X - 2.0) ** 2 + Y ** 2) / 3.0) * (1 + 0.05 * rng.uniform(-1, 1, lat.shape))
+    psi0 = psi0 * np.exp(0.3j * Y)
+    V = 0.5 * (X ** 2 + Y ** 2) + lat.azimuthal(l)
+    n0 = O.expectations(lat, psi0)["norm2"] if imag else 0.0
+    p = lat.params(1e-3, imag, 1.0, g, 0.0, 0.0, norm0=n0, angular_momentum=l)
+    tr, ti = O.exp_table(V, 1e-3, imag)
+    ref = O.evolve(p, O.evolve(p, psi0, tr, ti, 6), tr, ti, 5)
+    out = {}
+    for wk in (walk, 0):
+        with Kernel(desc_from_params(p)) as k:
+            k.set_walk(wk)
+            k.set_launch(segment_rows=24)
+            assert k.launch_shape()["walk"] == wk
+            k.set_state(psi0)
+            k.set_exp_potential(tr, ti)
+            k.evolve(6)
+            k.evolve(5)
+            out[wk] = k.get_state()
+    got, old = out[walk], out[0]
+    assert np.abs(got - ref).max() <= 1e-10 * np.abs(ref).max()
+    if imag:
+        assert np.abs(got - old).max() <= 1e-13 * np.abs(old).max()
+    else:
+        assert np.array_equal(got, old)

@@ -232,3 +232,29 @@ def test_fp32_storage_at_large_pair_angle(periodic, omega):
     assert abs(n32 - n64) / abs(n64) <= 1e-5
     assert abs(e32 - e64) / abs(e64) <= 1e-5
     assert np.linalg.norm(p32 - p64) / np.linalg.norm(p64) <= 1e-4
+
+
+def test_device_pointer_calls_follow_the_torch_stream():
+    """set_state_device / get_state_device on tensors that torch writes and
+    reads on its own (non-default) stream, without a synchronisation in
+    between: the handle's stream waits for torch's work before the copy in,
+    and torch's stream waits for the copy out."""
+    import torch
+    from trottersuzuki_b200 import Kernel
+    from helpers import desc_from_params, seeded_case
+    lat, psi0, V = seeded_case(96, 10.0, 80, (False, False))
+    p = lat.params(1e-3, False, 1.0, 1.0, 0.0, 0.0)
+    s = torch.cuda.Stream()
+    H, W = psi0.shape
+    with Kernel(desc_from_params(p)) as k, torch.cuda.stream(s):
+        src = torch.tensor(psi0, dtype=torch.complex128, device="cuda")
+        # a long chain of kernels on torch's stream ends in the state to upload
+        big = torch.rand(4096, 4096, dtype=torch.float64, device="cuda")
+        for _ in range(20):
+            big = big @ big * 1e-4
+        src = src + 0.0 * big[:H, :W]
+        k.set_state_device(src.data_ptr(), W)
+        out = torch.empty_like(src)
+        k.get_state_device(out.data_ptr(), W)
+        res = (out - src).abs().max()
+        assert float(res.item()) == 0.0

@@ -16,7 +16,7 @@ from test_oracle_two import load_two, oracle_two, two_names
 pytestmark = pytest.mark.gpu
 
 
-def run_pair(lat, meta, z, precision=0, segments=None):
+def run_pair(lat, meta, z, precision=0, segments=None, walk=None, seg_rows=0):
     from trottersuzuki_b200 import Kernel, Pair
     dt, imag = meta["dt"], meta["segments"][0][1]
     a0, b0 = z["psi0_a"], z["psi0_b"]
@@ -25,6 +25,11 @@ def run_pair(lat, meta, z, precision=0, segments=None):
     pa = lat.params(dt, imag, 1.0, meta["g"], 0.0, 0.0, norm0=na)
     pb = lat.params(dt, imag, meta["mass_b"], meta["g_b"], 0.0, 0.0, norm0=nb)
     ka, kb = Kernel(desc_from_params(pa, precision)), Kernel(desc_from_params(pb, precision))
+    for k in (ka, kb):
+        if walk is not None:
+            k.set_walk(walk)
+        if seg_rows:
+            k.set_launch(segment_rows=seg_rows)
     ka.set_state(a0)
     kb.set_state(b0)
     ka.set_exp_potential(*O.exp_table(z["Va"], dt, imag))
@@ -201,3 +206,30 @@ def test_pair_with_an_empty_species_matches_oracle(imag):
     assert np.abs(ka.get_state() - oa).max() <= 1e-10
     assert np.abs(kb.get_state() - ob).max() <= 1e-10
     pair.close()
+
+
+@pytest.mark.parametrize("walk", [1, 2])
+@pytest.mark.parametrize("name", ["two_real_rabi", "two_imag_rabi"])
+@pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "fp32"])
+def test_pair_look_ahead_walk_matches_checked_walk(name, walk, precision):
+    """Both species on the look-ahead walk (the other species' rows in the
+    ring, the Rabi rotation at load in real time, the joint normalisation in
+    the last block) against the checked walk: its bits in real time, its
+    result to rounding in imaginary time; short segments so that every tile
+    has several, odd step counts per call."""
+    lat, meta, z = load_two(name)
+    imag = meta["segments"][0][1]
+    segs = [(7, imag), (4, imag)]
+    out = {}
+    for wk in (walk, 0):
+        ka, kb, pair = run_pair(lat, meta, z, precision=precision, segments=segs, walk=wk,
+                                seg_rows=10)
+        assert ka.launch_shape()["walk"] == wk
+        out[wk] = (ka.get_state(), kb.get_state())
+        pair.close()
+    for got, old in zip(out[walk], out[0]):
+        if imag:
+            tol = 1e-13 if precision == 0 else 1e-6
+            assert np.abs(got - old).max() <= tol * np.abs(old).max()
+        else:
+            assert np.array_equal(got, old)

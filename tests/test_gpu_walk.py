@@ -194,12 +194,14 @@ def test_rotating_frame_segments_and_fp32(imag, seg):
     p = lat.params(1e-3, imag, 1.0, 3.0, 0.0, 0.5, norm0=n0)
     tr, ti = O.exp_table(V, 1e-3, imag)
     ref = O.evolve(p, psi0, tr, ti, 7)
-    launch = dict(cells_per_lane=2, segment_rows=seg)
-    for prec, tol in ((_capi.FP64, TOL_PSI), (_capi.FP32, 2e-5)):
+    for prec, cells, tol in ((_capi.FP64, 2, TOL_PSI), (_capi.FP32, 2, 2e-5), (_capi.FP32, 4, 2e-5)):
+        launch = dict(cells_per_lane=cells, segment_rows=seg)
         got, shape = _gpu(p, psi0, tr, ti, 7, walk=2, launch=launch, precision=prec, split=[3, 4])
-        assert shape["walk"] == 2
+        assert shape["walk"] == 2 and shape["cells_per_lane"] == cells
         assert np.abs(got - ref).max() <= tol * np.abs(ref).max()
-        old, _ = _gpu(p, psi0, tr, ti, 7, walk=0, launch=launch, precision=prec, split=[3, 4])
+        # the checked walk (2 cells per lane in a rotating frame)
+        old, _ = _gpu(p, psi0, tr, ti, 7, walk=0, launch=dict(cells_per_lane=2, segment_rows=seg),
+                      precision=prec, split=[3, 4])
         if imag:
             assert np.abs(got - old).max() <= (1e-13 if prec == _capi.FP64 else 1e-6) * np.abs(old).max()
         else:

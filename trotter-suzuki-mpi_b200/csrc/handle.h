@@ -32,6 +32,7 @@ struct ts_b200_kernel {
     double *red_out = nullptr;
     unsigned int *red_ticket = nullptr;
     cudaStream_t own_stream = nullptr, stream = nullptr;
+    cudaEvent_t ev_order = nullptr;  // ts_b200_stream_wait / _signal
     int C = 2, seg_h = 64, warps = 4, ring = 4;
     int resident_blocks = 0;  // blocks of the current launch shape resident on the GPU (0: unknown)
     bool auto_seg = true;     // pick the segment height from the resident grid

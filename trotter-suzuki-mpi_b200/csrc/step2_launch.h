@@ -60,10 +60,26 @@ cudaError_t launch_step2_t(int C, int R, int phase, const StepArgs<T> &a, int wa
     return cudaErrorInvalidValue;
 }
 
-// The rotating frame (2 cells per lane), R rows per iteration.
+// The rotating frame (2 cells per lane; 4 in single precision), R rows per
+// iteration.
 template <typename T, bool IMAG>
-cudaError_t launch_step2rot_t(int R, int phase, const StepArgs<T> &a, int warps, size_t smem,
+cudaError_t launch_step2rot_t(int C, int R, int phase, const StepArgs<T> &a, int warps, size_t smem,
                               int blocks, cudaStream_t st, int *bps, bool pdl) {
+    if constexpr (sizeof(T) == 4) {
+        if (C == 4 && R == 2) {
+            if (phase == 0) return launch_step2_variant<Variant<T, 4, IMAG, true, 0>, 2>(a, warps, smem, blocks, st, bps, pdl);
+            if (phase == 1) return launch_step2_variant<Variant<T, 4, IMAG, true, 1>, 2>(a, warps, smem, blocks, st, bps, pdl);
+            if (phase == 2) return launch_step2_variant<Variant<T, 4, IMAG, true, 2>, 2>(a, warps, smem, blocks, st, bps, pdl);
+            return cudaErrorInvalidValue;
+        }
+        if (C == 4 && R == 1) {
+            if (phase == 0) return launch_step2_variant<Variant<T, 4, IMAG, true, 0>>(a, warps, smem, blocks, st, bps, pdl);
+            if (phase == 1) return launch_step2_variant<Variant<T, 4, IMAG, true, 1>>(a, warps, smem, blocks, st, bps, pdl);
+            if (phase == 2) return launch_step2_variant<Variant<T, 4, IMAG, true, 2>>(a, warps, smem, blocks, st, bps, pdl);
+            return cudaErrorInvalidValue;
+        }
+    }
+    if (C != 2) return cudaErrorInvalidValue;
     if (R == 2) {
         if (phase == 0) return launch_step2_variant<Variant<T, 2, IMAG, true, 0>, 2>(a, warps, smem, blocks, st, bps, pdl);
         if (phase == 1) return launch_step2_variant<Variant<T, 2, IMAG, true, 1>, 2>(a, warps, smem, blocks, st, bps, pdl);
@@ -72,6 +88,39 @@ cudaError_t launch_step2rot_t(int R, int phase, const StepArgs<T> &a, int warps,
         if (phase == 0) return launch_step2_variant<Variant<T, 2, IMAG, true, 0>>(a, warps, smem, blocks, st, bps, pdl);
         if (phase == 1) return launch_step2_variant<Variant<T, 2, IMAG, true, 1>>(a, warps, smem, blocks, st, bps, pdl);
         if (phase == 2) return launch_step2_variant<Variant<T, 2, IMAG, true, 2>>(a, warps, smem, blocks, st, bps, pdl);
+    }
+    return cudaErrorInvalidValue;
+}
+
+// One species of a pair (2 cells per lane): phase 3, and 7 (the Rabi
+// rotation at load, Variant phase 11, real time), R rows per iteration.
+template <typename T, bool IMAG>
+cudaError_t launch_step2pair_t(int R, int phase, const StepArgs<T> &a, int warps, size_t smem,
+                               int blocks, cudaStream_t st, int *bps, bool pdl) {
+    if (R == 2) {
+        if (phase == 3) return launch_step2_variant<Variant<T, 2, IMAG, false, 3>, 2>(a, warps, smem, blocks, st, bps, pdl);
+        if constexpr (!IMAG)
+            if (phase == 7) return launch_step2_variant<Variant<T, 2, IMAG, false, 11>, 2>(a, warps, smem, blocks, st, bps, pdl);
+    } else if (R == 1) {
+        if (phase == 3) return launch_step2_variant<Variant<T, 2, IMAG, false, 3>>(a, warps, smem, blocks, st, bps, pdl);
+        if constexpr (!IMAG)
+            if (phase == 7) return launch_step2_variant<Variant<T, 2, IMAG, false, 11>>(a, warps, smem, blocks, st, bps, pdl);
+    }
+    return cudaErrorInvalidValue;
+}
+
+// Cylindrical lattices (2 cells per lane): phases 4-6, R rows per iteration.
+template <typename T, bool IMAG>
+cudaError_t launch_step2cyl_t(int R, int phase, const StepArgs<T> &a, int warps, size_t smem,
+                              int blocks, cudaStream_t st, int *bps, bool pdl) {
+    if (R == 2) {
+        if (phase == 4) return launch_step2_variant<Variant<T, 2, IMAG, false, 4>, 2>(a, warps, smem, blocks, st, bps, pdl);
+        if (phase == 5) return launch_step2_variant<Variant<T, 2, IMAG, false, 5>, 2>(a, warps, smem, blocks, st, bps, pdl);
+        if (phase == 6) return launch_step2_variant<Variant<T, 2, IMAG, false, 6>, 2>(a, warps, smem, blocks, st, bps, pdl);
+    } else if (R == 1) {
+        if (phase == 4) return launch_step2_variant<Variant<T, 2, IMAG, false, 4>>(a, warps, smem, blocks, st, bps, pdl);
+        if (phase == 5) return launch_step2_variant<Variant<T, 2, IMAG, false, 5>>(a, warps, smem, blocks, st, bps, pdl);
+        if (phase == 6) return launch_step2_variant<Variant<T, 2, IMAG, false, 6>>(a, warps, smem, blocks, st, bps, pdl);
     }
     return cudaErrorInvalidValue;
 }

@@ -1,0 +1,12 @@
+// Look-ahead walk variants on a cylindrical lattice: float, imaginary time.
+#include "step2_launch.h"
+
+namespace tsb {
+
+cudaError_t launch_step2cyl_f32_imag(int R, int phase, const StepArgs<float> &a,
+                                     int warps, size_t smem, int blocks, cudaStream_t st, int *bps,
+                                     bool pdl) {
+    return launch_step2cyl_t<float, true>(R, phase, a, warps, smem, blocks, st, bps, pdl);
+}
+
+}  // namespace tsb

@@ -3,10 +3,10 @@
 
 namespace tsb {
 
-cudaError_t launch_step2rot_f32_imag(int R, int phase, const StepArgs<float> &a, int warps,
-                                     size_t smem, int blocks, cudaStream_t st, int *bps,
+cudaError_t launch_step2rot_f32_imag(int C, int R, int phase, const StepArgs<float> &a,
+                                     int warps, size_t smem, int blocks, cudaStream_t st, int *bps,
                                      bool pdl) {
-    return launch_step2rot_t<float, true>(R, phase, a, warps, smem, blocks, st, bps, pdl);
+    return launch_step2rot_t<float, true>(C, R, phase, a, warps, smem, blocks, st, bps, pdl);
 }
 
 }  // namespace tsb

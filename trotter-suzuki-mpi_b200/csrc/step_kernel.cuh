@@ -944,7 +944,7 @@ __device__ __forceinline__ void walk_row(Walk<V> &w, const StepArgs<typename V::
             }
             potential_row<IMAG, PHASE, false, true, C, false>(WS(2), tp, w.ca, w.caa, &ub, w.cab);
         } else {
-            potential_row<IMAG, PHASE, V::LHY, false, C, !V::CYL>(WS(2), tp, w.ca, w.caa);
+            potential_row<IMAG, PHASE, V::LHY, false, C>(WS(2), tp, w.ca, w.caa);
         }
         if constexpr (ROT) {
             const Cx<T> ab = reinterpret_cast<const Cx<T> *>(a.row_ab)[u];

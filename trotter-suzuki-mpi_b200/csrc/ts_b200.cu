@@ -525,9 +525,15 @@ template <>
 cudaError_t dispatch_step<double>(int C, bool imag, bool rot, int phase, int w2,
                                   const StepArgs<double> &a, int warps, size_t smem, int blocks,
                                   cudaStream_t st, int *bps, bool pdl) {
+    if (w2 && (phase == 3 || phase == 7))
+        return imag ? tsb::launch_step2pair_f64_imag(w2, phase, a, warps, smem, blocks, st, bps, pdl)
+                    : tsb::launch_step2pair_f64_real(w2, phase, a, warps, smem, blocks, st, bps, pdl);
+    if (w2 && phase >= 4 && phase <= 6)
+        return imag ? tsb::launch_step2cyl_f64_imag(w2, phase, a, warps, smem, blocks, st, bps, pdl)
+                    : tsb::launch_step2cyl_f64_real(w2, phase, a, warps, smem, blocks, st, bps, pdl);
     if (w2 && rot)
-        return imag ? tsb::launch_step2rot_f64_imag(w2, phase, a, warps, smem, blocks, st, bps, pdl)
-                    : tsb::launch_step2rot_f64_real(w2, phase, a, warps, smem, blocks, st, bps, pdl);
+        return imag ? tsb::launch_step2rot_f64_imag(C, w2, phase, a, warps, smem, blocks, st, bps, pdl)
+                    : tsb::launch_step2rot_f64_real(C, w2, phase, a, warps, smem, blocks, st, bps, pdl);
     if (w2)
         return imag ? tsb::launch_step2_f64_imag(C, w2, phase, a, warps, smem, blocks, st, bps, pdl)
                     : tsb::launch_step2_f64_real(C, w2, phase, a, warps, smem, blocks, st, bps, pdl);
@@ -539,9 +545,15 @@ template <>
 cudaError_t dispatch_step<float>(int C, bool imag, bool rot, int phase, int w2,
                                  const StepArgs<float> &a, int warps, size_t smem, int blocks,
                                  cudaStream_t st, int *bps, bool pdl) {
+    if (w2 && (phase == 3 || phase == 7))
+        return imag ? tsb::launch_step2pair_f32_imag(w2, phase, a, warps, smem, blocks, st, bps, pdl)
+                    : tsb::launch_step2pair_f32_real(w2, phase, a, warps, smem, blocks, st, bps, pdl);
+    if (w2 && phase >= 4 && phase <= 6)
+        return imag ? tsb::launch_step2cyl_f32_imag(w2, phase, a, warps, smem, blocks, st, bps, pdl)
+                    : tsb::launch_step2cyl_f32_real(w2, phase, a, warps, smem, blocks, st, bps, pdl);
     if (w2 && rot)
-        return imag ? tsb::launch_step2rot_f32_imag(w2, phase, a, warps, smem, blocks, st, bps, pdl)
-                    : tsb::launch_step2rot_f32_real(w2, phase, a, warps, smem, blocks, st, bps, pdl);
+        return imag ? tsb::launch_step2rot_f32_imag(C, w2, phase, a, warps, smem, blocks, st, bps, pdl)
+                    : tsb::launch_step2rot_f32_real(C, w2, phase, a, warps, smem, blocks, st, bps, pdl);
     if (w2)
         return imag ? tsb::launch_step2_f32_imag(C, w2, phase, a, warps, smem, blocks, st, bps, pdl)
                     : tsb::launch_step2_f32_real(C, w2, phase, a, warps, smem, blocks, st, bps, pdl);
@@ -600,17 +612,24 @@ void choose_launch(ts_b200_kernel *k) {
     // in imaginary time (FP64 39.9 -> 38.6 us, FP32 29.2 -> 28.4 us) and FP32
     // real time (30.1 -> 29.0 us), slower in FP64 real time (47.3 -> 48.3 us)
     k->overlap = !(k->imag == false && k->fp32 == false);
+    // single precision in a rotating frame: 4 cells per lane (strips of 128
+    // columns carry 112 output columns instead of 48 of 64: 8192^2 vortex
+    // step 610 -> 569 us)
+    if (k->rot && k->fp32 && k->walk2 > 0 && !k->cyl && k->phase <= 2) k->C = 4;
 }
 
 // A row's table is read two rows after its psi: the ring must hold those
 // three rows plus at least one in flight.
 int min_ring(const ts_b200_kernel *) { return 4; }
 
-// The look-ahead walk covers single-component cartesian tiles (phases 0-2,
-// in a rotating frame with 2 cells per lane); the other variants take the
-// checked walk.
+// The look-ahead walk covers every variant: phases 0-2 cartesian (in a
+// rotating frame with 2 cells per lane, or 4 in single precision), one
+// species of a pair (phases 3 and 7) and cylindrical lattices (phases 4-6)
+// with 2 cells per lane.
 bool use_walk2(const ts_b200_kernel *k) {
-    return k->walk2 > 0 && !k->cyl && k->phase <= 2 && (!k->rot || k->C == 2);
+    if (k->walk2 <= 0) return false;
+    if (k->cyl || (k->phase & 3) == 3) return k->C == 2 && !k->rot;
+    return !k->rot || k->C == 2 || k->fp32;
 }
 
 // Rows of the look-ahead walk's register window and ring (8 in a rotating
@@ -618,10 +637,11 @@ bool use_walk2(const ts_b200_kernel *k) {
 int walk_window(const ts_b200_kernel *k) { return k->rot ? 8 : 6; }
 
 // Rows per iteration of the look-ahead walk in use (0: the checked walk);
-// two rows per iteration exist for 2 cells per lane.
+// two rows per iteration exist for 2 cells per lane, and for 4 in a
+// single-precision rotating frame.
 int walk_rows(const ts_b200_kernel *k) {
     if (!use_walk2(k)) return 0;
-    return (k->walk2 == 2 && k->C == 2) ? 2 : 1;
+    return (k->walk2 == 2 && (k->C == 2 || (k->rot && k->fp32))) ? 2 : 1;
 }
 
 // Rows per segment as launched: the look-ahead walk needs even segments
@@ -679,7 +699,8 @@ void geometry(const ts_b200_kernel *k, int *strips, int *segs, int *blocks, size
     if (use_walk2(k)) {
         // per warp: a ring of 6 rows, the vertical pair coefficients and one
         // mbarrier per ring slot (of 1 or 2 rows)
-        *smem = (size_t)k->warps * (walk_window(k) * slot_bytes(k->C, k->fp32, k->imag) +
+        *smem = (size_t)k->warps * (walk_window(k) * slot_bytes(k->C, k->fp32, k->imag,
+                                                                (k->phase & 3) == 3) +
                                     tsb::w2_vlen(eff_seg(k), k->rot) * 2 * (k->fp32 ? 4 : 8) +
                                     (walk_window(k) / walk_rows(k)) * 8);
         if (k->overlap && pad) {
@@ -1256,6 +1277,7 @@ int ts_b200_destroy(ts_b200_kernel *k) {
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (k->own_stream) cudaStreamDestroy(k->own_stream);
+    if (k->ev_order) cudaEventDestroy(k->ev_order);
     delete k;
     return TS_B200_OK;
 }
@@ -1265,6 +1287,26 @@ int ts_b200_set_stream(ts_b200_kernel *k, void *stream) {
     drop_graph(k);
     k->stream = stream ? reinterpret_cast<cudaStream_t>(stream) : k->own_stream;
     return TS_B200_OK;
+}
+
+namespace {
+int order_streams(ts_b200_kernel *k, cudaStream_t first, cudaStream_t then) {
+    if (first == then) return TS_B200_OK;
+    if (!k->ev_order) TSB_CHECK(k, cudaEventCreateWithFlags(&k->ev_order, cudaEventDisableTiming));
+    TSB_CHECK(k, cudaEventRecord(k->ev_order, first));
+    TSB_CHECK(k, cudaStreamWaitEvent(then, k->ev_order, 0));
+    return TS_B200_OK;
+}
+}  // namespace
+
+int ts_b200_stream_wait(ts_b200_kernel *k, void *stream) {
+    if (!k) return TS_B200_INVALID_ARGUMENT;
+    return order_streams(k, reinterpret_cast<cudaStream_t>(stream), k->stream);
+}
+
+int ts_b200_stream_signal(ts_b200_kernel *k, void *stream) {
+    if (!k) return TS_B200_INVALID_ARGUMENT;
+    return order_streams(k, k->stream, reinterpret_cast<cudaStream_t>(stream));
 }
 
 int ts_b200_synchronize(ts_b200_kernel *k) {
@@ -1611,7 +1653,9 @@ int ts_b200_launch_info(const ts_b200_kernel *k, ts_b200_launch_shape *out) {
 int ts_b200_set_launch(ts_b200_kernel *k, int C, int seg_h, int warps, int ring) {
     if (!k) return TS_B200_INVALID_ARGUMENT;
     if (C != 0 && C != 2 && C != 4) return TS_B200_INVALID_ARGUMENT;
-    if (C == 4 && k->rot) return fail(k, TS_B200_UNSUPPORTED, "rotation kernels use 2 cells per lane");
+    if (C == 4 && k->rot && !(k->fp32 && k->walk2 > 0))
+        return fail(k, TS_B200_UNSUPPORTED,
+                    "rotation kernels use 2 cells per lane (4: single precision, look-ahead walk)");
     if (C == 4 && k->pair_mode) return fail(k, TS_B200_UNSUPPORTED, "pair kernels use 2 cells per lane");
     if (C == 4 && k->cyl) return fail(k, TS_B200_UNSUPPORTED, "cylindrical kernels use 2 cells per lane");
     if (warps != 0 && warps != 1 && warps != 2 && warps != 4 && warps != 8)
@@ -1644,6 +1688,8 @@ int ts_b200_set_walk(ts_b200_kernel *k, int walk) {
     if (k->walk2 == walk) return TS_B200_OK;
     k->walk2 = walk;
     if (!use_walk2(k) && k->warps > 4) k->warps = 4;
+    // the checked walk's rotating frame has 2 cells per lane
+    if (walk == 0 && k->rot && k->C == 4) k->C = 2;
     k->resident_blocks = 0;
     drop_graph(k);
     return TS_B200_OK;

@@ -32,8 +32,11 @@
 //     the second row's chain of stages runs one stage behind the first's
 //     (row c + 1's V0 needs only row c's V0), so the two chains overlap.
 //
-// Variants: single component, cartesian (phases 0-2), 2 or 4 cells per lane
-// (2 in a rotating frame), both precisions and time modes.  The arithmetic of
+// Variants: every one of step_kernel: cartesian (phases 0-2; 2 or 4 cells per
+// lane, 2 in a double-precision rotating frame), one species of a pair
+// (phases 3 and 7: the other species' rows ride in the ring, the Rabi
+// rotation at load) and cylindrical lattices (phases 4-6: radial sweeps,
+// the mirrored axis column at the store), both precisions and time modes.  The arithmetic of
 // each cell is that of step_kernel (the same pair forms, potential row,
 // rotation sweeps and reductions), so both give the same bits; the rotating
 // frame's row and column rotations across the tile's edges take the identity
@@ -54,20 +57,28 @@ struct W2Shape {
     static constexpr int NW = ROT ? 8 : 6;
     static constexpr int D = NW / R_;          // ring slots per warp
     static constexpr int UNROLL = NW;          // rows per unrolled chunk
-    static constexpr int HX = ROT ? 8 : 4, HY = ROT ? 6 : 4;
+    static constexpr bool CYL = V::CYL;
+    // halo columns: one per horizontal sweep (4 kinetic, 4 more rotation row
+    // or radial sweeps); halo rows: one per vertical sweep
+    static constexpr int HX = (ROT || CYL) ? 8 : 4, HY = ROT ? 6 : 4;
     static constexpr int SO = 2 * HY;          // walk index of the first stored row
     // slot indices in flight ahead of the current one: the slot of row c-2
     // (whose table the current iteration reads) is refilled with row c-2+NW
     static constexpr int AHEAD = D - 2 / R_;
     static constexpr int SW = 32 * C, WO = SW - 2 * HX;
-    static constexpr int ROWB = V::PSI_BYTES + V::TAB_BYTES;  // one row of psi and table
+    // one row of psi and of the table (and, for one species of a pair, of
+    // the other species' psi)
+    static constexpr int ROWB = V::PSI_BYTES + V::TAB_BYTES + (V::PB ? V::PSI_BYTES : 0);
+    static constexpr int PB_OFF = V::PSI_BYTES + V::TAB_BYTES;
     static constexpr int SLOT = R_ * ROWB;
     // vertical pair coefficients: entry j is the pair (u - 1, u) with
     // u = ra + j - VPAD; the first stages of a walk read up to VPAD - 1
     // entries before the first row
     static constexpr int VPAD = ROT ? 6 : 4;
-    static_assert(V::HX == HX && (!ROT || V::C == 2), "look-ahead walk geometry");
-    static_assert(!V::PB && !V::CYL, "look-ahead walk: one cartesian component");
+    static_assert(V::HX == HX && (!ROT || V::C == 2 || sizeof(typename V::T) == 4),
+                  "look-ahead walk geometry (4 cells per lane in a rotating frame: float)");
+    static_assert((!CYL && !V::PB) || (V::C == 2 && !ROT && !(CYL && V::PB)),
+                  "look-ahead walk: cylinder or pair with 2 cells per lane, no rotating frame");
     static_assert(R_ == 1 || R_ == 2, "one or two rows per iteration");
     static_assert(D * R == UNROLL && NW == UNROLL && UNROLL % 2 == 0,
                   "compile-time slots and parities");
@@ -102,10 +113,20 @@ struct Walk2 {
     // cost more than the loads: 967 -> 991 us)
     static constexpr bool AB_AHEAD = sizeof(T) == 4;
     Cx<T> rab[4];
+    // cylindrical: radial (a, b) of cell [i] for the sweep of parity [p]; the
+    // mirror sign on the lane of column 0 (imaginary time), else 0
+    T rca[2][2], rcb[2][2];
+    T msign;
     bool out_col[C], norm_col[C], all_out;
     int ra, nit, lane;
     int n_lo, n_hi;  // iterations whose stored row is in the norm region
     const unsigned char *gpsi, *gtab;  // row 0 of the strip's first copied column
+    const unsigned char *gpb;          // pair: the other species' row 0, same column
+    // pair: the other species' pending factor, g_ab dt; with the Rabi
+    // rotation at load (real time) its coefficients for the own and the
+    // other species' cell
+    T pbs, cab;
+    T rcc, rsr, rsi, ror, roi;
     size_t gpsi_pitch, gtab_pitch;
     uint32_t psi_off, psi_bytes, tab_off, tab_bytes;
     int H;
@@ -128,9 +149,9 @@ struct Walk2 {
     __device__ __forceinline__ void issue(int si, int q) {
         const uint32_t sb = smem_u32(ring + q * S::SLOT);
         const uint32_t bar = smem_u32(&bars[q]);
-        const uint32_t rowbytes = psi_bytes + tab_bytes;
+        const uint32_t rowbytes = psi_bytes + tab_bytes + (V::PB ? psi_bytes : 0u);
         uint32_t p[2], n = 0;
-        const unsigned char *src_psi[2], *src_tab[2];
+        const unsigned char *src_psi[2], *src_tab[2], *src_pb[2];
 #pragma unroll
         for (int k = 0; k < R; ++k) {
             const int tp = R * si + k, row = ra + tp;
@@ -140,6 +161,7 @@ struct Walk2 {
             const int rr = real ? row : 0;
             src_psi[k] = gpsi + (size_t)rr * gpsi_pitch;
             src_tab[k] = gtab + (size_t)rr * gtab_pitch;
+            if constexpr (V::PB) src_pb[k] = gpb + (size_t)rr * gpsi_pitch;
         }
         const uint32_t pc = (lane == 0 && n > 0) ? 1u : 0u;
         const uint32_t pa = (lane == 0 && n == 0) ? 1u : 0u;
@@ -162,6 +184,14 @@ struct Walk2 {
                 "r"(rb + psi_off), "l"(src_psi[k]), "r"(psi_bytes), "r"(bar),
                 "r"(rb + (uint32_t)V::PSI_BYTES + tab_off), "l"(src_tab[k]), "r"(tab_bytes)
                 : "memory");
+            if constexpr (V::PB)
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.u32 p, %0, 0;\n\t"
+                    "@p cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%1], [%2], %3, [%4];\n\t}" ::"r"(p[k]),
+                    "r"(rb + (uint32_t)S::PB_OFF + psi_off), "l"(src_pb[k]), "r"(psi_bytes),
+                    "r"(bar)
+                    : "memory");
         }
     }
 };
@@ -325,16 +355,43 @@ __device__ __forceinline__ void w2_stages(Walk2<V, R> &w, int t) {
             const Cx<T> cv = vc[-1];
             vsweep<IMAG, C, ((K + 1) & 1)>(W2S(2), W2S(1), cv.re, cv.im);
         }
-        // ---- S4: H1, P, H1 on row c-2 (its table from its ring slot)
+        // ---- S4: H1, P, H1 on row c-2 (its table from its ring slot); in a
+        // cylinder the radial sweeps of both parities around P
+        // (src/cpukernel.cpp:22-92 with src/cpucylindrical.cpp:4-81)
         {
             constexpr int RT = (K + S::UNROLL - 2) % S::UNROLL;  // row c-2 within the chunk
             constexpr int q = RT / R, pos = RT % R;
             hsweep_lanes<IMAG, ((K + 1) & 1), C>(W2S(2), w.hpa, w.hpb, w.hal, w.hbl, w.har, w.hbr);
+            if constexpr (S::CYL) {
+                rsweep_lane<IMAG, 0>(W2S(2), w.rca[0][0], w.rcb[0][0], w.rca[0][1], w.rcb[0][1]);
+                rsweep_lane<IMAG, 1>(W2S(2), w.rca[1][0], w.rcb[1][0], w.rca[1][1], w.rcb[1][1]);
+            }
+            const unsigned char *row = w.ring + q * S::SLOT + pos * S::ROWB;
             alignas(16) TabT tv[C];
-            load_tab_cells<TabT, C>(w.ring + q * S::SLOT + pos * S::ROWB + V::PSI_BYTES +
-                                        C * (int)sizeof(TabT) * w.lane,
-                                    tv);
-            potential_row<IMAG, PHASE, V::LHY, false, C>(W2S(2), tv, w.ca, w.caa);
+            load_tab_cells<TabT, C>(row + V::PSI_BYTES + C * (int)sizeof(TabT) * w.lane, tv);
+            if constexpr (V::PB) {
+                // the other species' cells, scaled (and, with the Rabi
+                // rotation at load, rotated with the cells this row started
+                // from); the short phase tier left out as in step_kernel,
+                // whose bits this walk keeps
+                Cx<T> ub[C];
+                load_row_cells<T, C>(row + S::PB_OFF + C * (int)sizeof(Cx<T>) * w.lane, ub);
+                Cx<T> own[C];
+                if constexpr (V::RABI) load_row_cells<T, C>(row + C * (int)sizeof(Cx<T>) * w.lane, own);
+#pragma unroll
+                for (int i = 0; i < C; ++i) {
+                    ub[i] = scale_cx(ub[i], w.pbs);
+                    if constexpr (V::RABI) ub[i] = rabi_cell(ub[i], own[i], w.rcc, w.ror, w.roi);
+                }
+                potential_row<IMAG, PHASE, false, true, C, false>(W2S(2), tv, w.ca, w.caa, &ub,
+                                                                  w.cab);
+            } else {
+                potential_row<IMAG, PHASE, V::LHY, false, C>(W2S(2), tv, w.ca, w.caa);
+            }
+            if constexpr (S::CYL) {
+                rsweep_lane<IMAG, 1>(W2S(2), w.rca[1][0], w.rcb[1][0], w.rca[1][1], w.rcb[1][1]);
+                rsweep_lane<IMAG, 0>(W2S(2), w.rca[0][0], w.rcb[0][0], w.rca[0][1], w.rcb[0][1]);
+            }
             hsweep_lanes<IMAG, ((K + 1) & 1), C>(W2S(2), w.hpa, w.hpb, w.hal, w.hbl, w.har, w.hbr);
         }
         // ---- S5: V1 on rows (c-3, c-2)
@@ -353,6 +410,14 @@ __device__ __forceinline__ void w2_stages(Walk2<V, R> &w, int t) {
     // ---- row c-HY is finished: store it (the first 2 HY rows of a walk are halo;
     // with two rows per iteration the second row can lie past the walk)
     if (t >= S::SO && (R == 1 || t < w.nit)) {
+        if constexpr (S::CYL && IMAG) {
+            // column 0 mirrors column 1 (src/cpukernel.cpp:669-689); msign
+            // is 0 on every other lane
+            if (w.msign != T(0)) {
+                W2S(S::HY)[0].re = w.msign * W2S(S::HY)[1].re;
+                W2S(S::HY)[0].im = w.msign * W2S(S::HY)[1].im;
+            }
+        }
         store_row_cells<T, C>(w.orow, W2S(S::HY), w.out_col, w.all_out);
         if (IMAG && t >= w.n_lo && t < w.n_hi) {
 #pragma unroll
@@ -374,8 +439,17 @@ __device__ __forceinline__ void w2_load(Walk2<V, R> &w, int q, int pos,
     using T = typename V::T;
     using S = W2Shape<V, R>;
     constexpr int C = V::C;
+    const unsigned char *row = w.ring + q * S::SLOT + pos * S::ROWB;
     Cx<T> v[C];
-    load_row_cells<T, C>(w.ring + q * S::SLOT + pos * S::ROWB + C * (int)sizeof(Cx<T>) * w.lane, v);
+    load_row_cells<T, C>(row + C * (int)sizeof(Cx<T>) * w.lane, v);
+    if constexpr (V::RABI) {
+        // one species of a pair, real time: the Rabi rotation of the previous
+        // step with the other species' cell of the same row
+        Cx<T> u[C];
+        load_row_cells<T, C>(row + S::PB_OFF + C * (int)sizeof(Cx<T>) * w.lane, u);
+#pragma unroll
+        for (int i = 0; i < C; ++i) v[i] = rabi_cell(v[i], scale_cx(u[i], w.pbs), w.rcc, w.rsr, w.rsi);
+    }
 #pragma unroll
     for (int i = 0; i < C; ++i) dst[i] = V::IMAG ? scale_cx(v[i], w.inv) : v[i];
 }
@@ -478,6 +552,7 @@ __device__ __forceinline__ void w2_task(Walk2<V, R> &w, const StepArgs<typename 
     w.tab_bytes = (uint32_t)(ce - cs) * sizeof(TabT);
     w.gpsi = reinterpret_cast<const unsigned char *>(a.psi_in) + (size_t)cs * sizeof(Cx<T>);
     w.gtab = reinterpret_cast<const unsigned char *>(a.pot) + (size_t)cs * sizeof(TabT);
+    if constexpr (V::PB) w.gpb = reinterpret_cast<const unsigned char *>(a.pb) + (size_t)cs * sizeof(Cx<T>);
     const int xl = c0 + C * lane;
     bool present[C];
     w.all_out = true;
@@ -503,6 +578,26 @@ __device__ __forceinline__ void w2_task(Walk2<V, R> &w, const StepArgs<typename 
         w.hbl = pl ? w.bH : T(0);
         w.har = pr ? w.aH : one;
         w.hbr = pr ? w.bH : T(0);
+        if constexpr (S::CYL) {
+            // radial pairs (x, x+1), valid when x >= 0 and x + 1 < W; the
+            // table holds (a, b), (c, 0) per column x
+            const Cx<T> *rad = reinterpret_cast<const Cx<T> *>(a.rad);
+            auto pair_ok = [&](int x) { return x >= 0 && x + 1 < a.W; };
+            // parity 0: cells 0, 1 pair with each other (pair at xl)
+            const bool p0 = pair_ok(xl);
+            w.rca[0][0] = p0 ? rad[2 * xl].re : one;
+            w.rcb[0][0] = p0 ? rad[2 * xl].im : T(0);
+            w.rca[0][1] = w.rca[0][0];
+            w.rcb[0][1] = p0 ? rad[2 * xl + 1].re : T(0);
+            // parity 1: cell 0 is the second cell of the pair at xl - 1,
+            // cell 1 the first of the pair at xl + 1
+            const bool q0 = pair_ok(xl - 1), q1 = pair_ok(xl + 1);
+            w.rca[1][0] = q0 ? rad[2 * (xl - 1)].re : one;
+            w.rcb[1][0] = q0 ? rad[2 * (xl - 1) + 1].re : T(0);
+            w.rca[1][1] = q1 ? rad[2 * (xl + 1)].re : one;
+            w.rcb[1][1] = q1 ? rad[2 * (xl + 1)].im : T(0);
+            w.msign = (V::IMAG && xl == 0) ? a.mirror_sign : T(0);
+        }
         if constexpr (S::ROT) {
             // the row rotation sweeps' pair masks and this lane's column
             // rotation coefficients
@@ -538,9 +633,12 @@ __device__ __forceinline__ void w2_task(Walk2<V, R> &w, const StepArgs<typename 
             bool copied;
             if (off < (uint32_t)V::PSI_BYTES) {
                 copied = off >= w.psi_off && off < w.psi_off + w.psi_bytes;
-            } else {
+            } else if (off < (uint32_t)S::PB_OFF) {
                 const uint32_t tt = off - (uint32_t)V::PSI_BYTES;
                 copied = tt >= w.tab_off && tt < w.tab_off + w.tab_bytes;
+            } else {
+                const uint32_t tt = off - (uint32_t)S::PB_OFF;
+                copied = tt >= w.psi_off && tt < w.psi_off + w.psi_bytes;
             }
             if (!copied) ring32[i] = 0u;
         }
@@ -657,7 +755,16 @@ __device__ __forceinline__ void w2_finish(const StepArgs<typename V::T> &a, doub
                 for (int i = 0; i < warps; ++i) t += red[i];
                 double tot = t * a.dxdy;
                 *launch_ticket(a) = 0u;
-                if (split_norm_total(a, &tot)) {
+                if constexpr (V::PB) {
+                    // one species of a pair (as step_kernel): the other
+                    // species' next step reads this step's input buffer with
+                    // the factor that was pending on it; the kept norm moves
+                    // with the joint normalisation (src/cpukernel.cpp:551)
+                    a.scal->last_norm = tot;
+                    a.scal->prev_inv = a.scal->pending_inv;
+                    const double n0 = a.scal->norm_target;
+                    if (n0 != 0.0) a.scal->pending_inv = 1.0 / sqrt(tot / n0);
+                } else if (split_norm_total(a, &tot)) {
                     a.scal->last_norm = tot;
                     if (a.scal->renorm) a.scal->pending_inv = 1.0 / sqrt(tot / a.norm0);
                     if (a.inv_copy) *a.inv_copy = a.scal->pending_inv;
@@ -749,6 +856,17 @@ __global__ void __launch_bounds__(W2Bounds<V>::THREADS, W2Bounds<V>::MIN_BLOCKS)
     w.ca = a.ca;
     w.caa = a.caa;
     w.row_ab = reinterpret_cast<const Cx<T> *>(a.row_ab);
+    if constexpr (V::PB) {
+        w.pbs = (T)__ldcg(a.pb_scale);
+        w.cab = a.cab;
+    }
+    if constexpr (V::RABI) {
+        w.rcc = a.rabi_cc;
+        w.rsr = a.rabi_sr;
+        w.rsi = a.rabi_si;
+        w.ror = a.rabi_or;
+        w.roi = a.rabi_oi;
+    }
     w.opitch = (size_t)a.P;
     w.gpsi_pitch = (size_t)a.P * sizeof(Cx<T>);
     w.gtab_pitch = (size_t)a.P * sizeof(typename V::TabT);

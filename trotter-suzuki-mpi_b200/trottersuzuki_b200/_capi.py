@@ -98,6 +98,8 @@ SIGNATURES = {
     "ts_b200_set_potential_device": (_I, [_VP, _VP, _SZ, C.c_double]),
     "ts_b200_evolve_potentials": (_I, [_VP, _VP, _SZ, _SZ, C.c_int, C.c_double, C.c_int]),
     "ts_b200_set_stream": (_I, [_VP, _VP]),
+    "ts_b200_stream_wait": (_I, [_VP, _VP]),
+    "ts_b200_stream_signal": (_I, [_VP, _VP]),
     "ts_b200_rows": (_I, [_VP, C.c_int, C.c_int, C.POINTER(_VP), C.POINTER(_SZ)]),
     "ts_b200_last_norm": (_I, [_VP, C.POINTER(_VP)]),
     "ts_b200_renormalize_from": (_I, [_VP, _VP]),

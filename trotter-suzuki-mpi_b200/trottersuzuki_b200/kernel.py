@@ -21,6 +21,16 @@ def _soa(psi):
     return re, im
 
 
+def _torch_stream():
+    """torch's current CUDA stream (a cudaStream_t address) when torch is in
+    use with CUDA initialised, else None."""
+    import sys
+    torch = sys.modules.get("torch")
+    if torch is None or not torch.cuda.is_initialized():
+        return None
+    return torch.cuda.current_stream().cuda_stream
+
+
 class Kernel:
     """A tile resident on the GPU plus its exponential table.
 
@@ -84,18 +94,36 @@ class Kernel:
                                              re.ctypes.data, im.ctypes.data))
         return re + 1j * im
 
+    # The *_device calls read or write memory the caller produced or consumes
+    # on torch's current stream: they are ordered after it (the handle's
+    # stream waits for it) and, for reads back, before what torch queues next.
+    def _after_torch(self):
+        s = _torch_stream()
+        if s is not None:
+            self._check(lib().ts_b200_stream_wait(self._h, C.c_void_p(s)))
+
+    def _before_torch(self):
+        s = _torch_stream()
+        if s is not None:
+            self._check(lib().ts_b200_stream_signal(self._h, C.c_void_p(s)))
+
     def set_state_device(self, ptr, pitch):
+        self._after_torch()
         self._check(lib().ts_b200_set_state_device(self._h, C.c_void_p(ptr), pitch))
 
     def get_state_device(self, ptr, pitch):
+        self._after_torch()
         self._check(lib().ts_b200_get_state_device(self._h, C.c_void_p(ptr), pitch))
+        self._before_torch()
 
     def set_exp_potential_device(self, ptr, pitch):
+        self._after_torch()
         self._check(lib().ts_b200_set_exp_potential_device(self._h, C.c_void_p(ptr), pitch))
 
     def set_potential_device(self, ptr, pitch, delta_t):
         """The table exp(-i dt V) (exp(-dt V) in imaginary time) built on the
         device from V: dim_y rows of float64 at `ptr`, row pitch `pitch`."""
+        self._after_torch()
         self._check(lib().ts_b200_set_potential_device(self._h, C.c_void_p(ptr), pitch,
                                                        float(delta_t)))
 
