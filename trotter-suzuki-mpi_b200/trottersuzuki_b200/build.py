@@ -65,12 +65,17 @@ def _includes(path, seen=None):
 
 def _compile(src, extra):
     obj = os.path.join(BUILD, os.path.basename(src) + ".o")
-    if _stale(obj, [src] + sorted(_includes(src))):
+    deps = [src] + sorted(_includes(src))
+    if _stale(obj, deps):
+        # the object carries the sources' time at the start of the compile,
+        # so that an edit made while it compiles leaves it stale
+        stamp = max(os.path.getmtime(d) for d in deps)
         cmd = [NVCC] + ARCH + FLAGS + extra + ["-c", src, "-o", obj + ".tmp"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"nvcc failed for {src}:\n{r.stdout}\n{r.stderr}")
         os.replace(obj + ".tmp", obj)
+        os.utime(obj, (stamp, stamp))
     return obj
 
 
