@@ -1412,8 +1412,9 @@ def run_two_component_workload(args, rank, world, local, pg):
                      "frac": achieved / peak, "peak_kind": peak_kind,
                      "traffic": committed_traffic("step_kernel_two_component_2048.md"),
                      "algorithmic_bytes_per_species_site_step": two_bytes,
-                     "kernel": "tsb::step_kernel<double, C=2, real, two components, "
-                               "Rabi rotation at load> x 2 per Trotter step"},
+                     "kernel": "tsb::step2_kernel<double, C=2, real, two components, "
+                               "Rabi rotation at load, 2 rows per iteration> "
+                               "x 2 per Trotter step"},
         "energy_drift_rel": abs(e_end - e_start) / abs(e_start),
         "norm_after": n_end,
         "cpu_baseline": cpu,
@@ -1523,7 +1524,8 @@ def run_cylindrical_workload(args, rank, world, local, pg):
                      "frac": achieved / peak, "peak_kind": peak_kind,
                      "traffic": committed_traffic("step_kernel_cylindrical_2048.md"),
                      "algorithmic_bytes_per_site_step": BYTES_PER_SITE_STEP["fp64"],
-                     "kernel": "tsb::step_kernel<double, C=2, imaginary, cylindrical, GPE>"},
+                     "kernel": "tsb::step2_kernel<double, C=2, imaginary, cylindrical, GPE, "
+                               "2 rows per iteration>"},
         "energy_after": energy,
         "clocks": clocks.summary(),
         "gpu_launches": launches,
