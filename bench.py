@@ -697,7 +697,8 @@ def run_batch_workload(args, rank, world, local, pg):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
                      "algorithmic_bytes_per_launch": bytes_step,
-                     "kernel": "tsb::batch_step_kernel<double, C=2, real, no rotation, GPE>"},
+                     "kernel": "tsb::batch2_kernel<double, C=2, real, no rotation, GPE, "
+                               "2 rows per iteration> (look-ahead walk)"},
         "e2e": e2e,
         "cpu_baseline": cpu,
         "clocks": clk,

@@ -354,7 +354,10 @@ int ts_b200_set_overlap(ts_b200_kernel *k, int on);
  * norms through the tiles' own calls.  All tiles must share precision, time
  * mode and device and have no rotating frame (TS_B200_UNSUPPORTED); a tile
  * appears once.  The batch orders itself after work queued on the tiles'
- * streams and the tiles' streams after the batch's work. */
+ * streams and the tiles' streams after the batch's work.  The batched step
+ * runs the row walk its tiles are set to at creation (ts_b200_set_walk): the
+ * look-ahead walk with two rows per iteration, or the checked walk if any
+ * tile is set to it; ts_b200_batch_launch_info reports it. */
 typedef struct ts_b200_batch ts_b200_batch;
 
 int ts_b200_batch_create(ts_b200_kernel *const *kernels, int n, ts_b200_batch **out);

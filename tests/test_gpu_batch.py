@@ -146,6 +146,35 @@ def test_batch_shape_does_not_change_result(seg, warps):
     close_all(tiles)
 
 
+@pytest.mark.parametrize("imag", [False, True], ids=["real", "imag"])
+@pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "fp32"])
+def test_batch_walks_agree(precision, imag):
+    """The batch runs its tiles' row walk: the look-ahead walk by default, the
+    checked walk when the tiles are set to it; both give the same bits in real
+    time and agree to rounding in imaginary time."""
+    from trottersuzuki_b200 import Batch
+    got = {}
+    for walk in (2, 0):
+        tiles = make_tiles(imag, precision)
+        for t in tiles:
+            t["k"].set_walk(walk)
+        with Batch([t["k"] for t in tiles]) as b:
+            b.set_launch(segment_rows=24, warps_per_block=2)
+            assert b.launch_shape()["walk"] == walk
+            for n in (33, 5):
+                b.evolve(n)
+            b.synchronize()
+            got[walk] = [t["k"].get_state() for t in tiles]
+        close_all(tiles)
+    for t, x, y in zip(make_tiles(imag, precision), got[2], got[0]):
+        if imag:
+            tol = 1e-12 if precision == 0 else 1e-6
+            assert np.abs(x - y).max() <= tol * np.abs(y).max(), t["name"]
+        else:
+            assert np.array_equal(x, y), f"{t['name']}: max|d| = {np.abs(x - y).max():.3e}"
+        t["k"].close()
+
+
 def test_batch_rejects_mixed_or_unsupported_tiles():
     from trottersuzuki_b200 import B200Error, Batch, Kernel
     t64 = make_tiles(False, 0, tiles=TILES[:1])

@@ -3,7 +3,8 @@
 //
 // A batch borrows the device buffers of existing tile handles
 // (ts_b200_kernel): their state, exponential tables and scalars.  Per step it
-// launches the batched step kernel over the task list of all tiles, then (in
+// launches the batched step kernel (batch2_kernel on the look-ahead walk,
+// batch_step_kernel on the checked walk) over the task list of all tiles, then (in
 // imaginary time) one reduction block per tile that turns the task partials
 // into the tile's squared norm and renormalisation factor, then (for tiles
 // with periodic boundaries, except on the last step of an evolve) one
@@ -26,6 +27,7 @@
 #include "halo.cuh"
 #include "handle.h"
 #include "ts_b200.h"
+#include "walk2_shape.h"
 
 using tsb::BatchArgs;
 using tsb::Cx;
@@ -102,6 +104,9 @@ struct ts_b200_batch {
     int phase = 0;
     int device = 0, num_sms = 148;
     Shape shape{128, 4};
+    // row walk: 2 the look-ahead walk (two rows per iteration, a ring of 6
+    // rows), 0 the checked walk (a ring of `ring` rows)
+    int walk = 0;
     int ring = 4;
     int resident_blocks = 0;  // of the current shape (0: unknown)
     int n_tasks = 0;
@@ -150,7 +155,21 @@ int tile_seg_rows(const ts_b200_kernel *t, int seg_rows) {
     return std::max(2, std::min(even_up(t->H), even_up(seg_rows)));
 }
 
+// Look-ahead walk: vertical pair table entries per warp, for the tallest
+// segment of the batch.
+int batch_vlen(const ts_b200_batch *b) {
+    int seg = 2;
+    for (const ts_b200_kernel *t : b->k) seg = std::max(seg, tile_seg_rows(t, b->shape.seg_rows));
+    return tsb::w2_vlen(seg, false);
+}
+
 size_t batch_smem(const ts_b200_batch *b, int warps) {
+    if (b->walk) {
+        // per warp: the ring, the vertical pair table and one mbarrier per
+        // ring slot of two rows
+        return (size_t)warps * (b->ring * tsbh::slot_bytes(2, b->fp32, b->imag) +
+                                (size_t)batch_vlen(b) * (b->fp32 ? 8 : 16) + (b->ring / 2) * 8);
+    }
     return (size_t)warps * (b->ring * tsbh::slot_bytes(2, b->fp32, b->imag) + 8 * b->ring);
 }
 
@@ -167,14 +186,24 @@ cudaError_t launch_batch_kernel(ts_b200_batch *b, const BatchArgs<T> &a, int blo
 template <>
 cudaError_t launch_batch_kernel<double>(ts_b200_batch *b, const BatchArgs<double> &a, int blocks,
                                         int *bps) {
-    return tsb::launch_batch_f64(b->imag, b->phase, a, b->shape.warps, batch_smem(b, b->shape.warps),
-                                 blocks, b->stream, bps);
+    const size_t smem = batch_smem(b, b->shape.warps);
+    if (b->walk)
+        return b->imag ? tsb::launch_batch2_f64_imag(b->phase, a, b->shape.warps, smem, blocks,
+                                                     b->stream, bps)
+                       : tsb::launch_batch2_f64_real(b->phase, a, b->shape.warps, smem, blocks,
+                                                     b->stream, bps);
+    return tsb::launch_batch_f64(b->imag, b->phase, a, b->shape.warps, smem, blocks, b->stream, bps);
 }
 template <>
 cudaError_t launch_batch_kernel<float>(ts_b200_batch *b, const BatchArgs<float> &a, int blocks,
                                        int *bps) {
-    return tsb::launch_batch_f32(b->imag, b->phase, a, b->shape.warps, batch_smem(b, b->shape.warps),
-                                 blocks, b->stream, bps);
+    const size_t smem = batch_smem(b, b->shape.warps);
+    if (b->walk)
+        return b->imag ? tsb::launch_batch2_f32_imag(b->phase, a, b->shape.warps, smem, blocks,
+                                                     b->stream, bps)
+                       : tsb::launch_batch2_f32_real(b->phase, a, b->shape.warps, smem, blocks,
+                                                     b->stream, bps);
+    return tsb::launch_batch_f32(b->imag, b->phase, a, b->shape.warps, smem, blocks, b->stream, bps);
 }
 
 // Task list, per-tile reduction table and halo table for the current shape.
@@ -281,6 +310,7 @@ int launch_batch_step(ts_b200_batch *b, int p, bool exchange, bool renorm_pass =
     a.error = b->d_error;
     a.n_tasks = b->n_tasks;
     a.ring = b->ring;
+    a.vlen = b->walk ? batch_vlen(b) : 0;
     const int blocks = std::max(1, std::min(b->resident_blocks, div_up(b->n_tasks, b->shape.warps)));
     cudaError_t e = launch_batch_kernel<T>(b, a, blocks, nullptr);
     if (e != cudaSuccess) return bcuda(b, e, "batch step launch");
@@ -476,6 +506,7 @@ int ts_b200_batch_create(ts_b200_kernel *const *kernels, int n, ts_b200_batch **
     const ts_b200_kernel *k0 = kernels[0];
     if (!k0) return TS_B200_INVALID_ARGUMENT;
     int phase = 0;
+    bool walk2 = true;
     for (int i = 0; i < n; ++i) {
         const ts_b200_kernel *t = kernels[i];
         if (!t) return TS_B200_INVALID_ARGUMENT;
@@ -486,6 +517,7 @@ int ts_b200_batch_create(ts_b200_kernel *const *kernels, int n, ts_b200_batch **
         // batched strips carry no rotating frame, second species or radial term
         if (t->rot || t->pair_mode || t->cyl) return TS_B200_UNSUPPORTED;
         phase = std::max(phase, t->phase);
+        walk2 = walk2 && t->walk2 > 0;
     }
     ts_b200_batch *b = new (std::nothrow) ts_b200_batch();
     if (!b) return TS_B200_OUT_OF_MEMORY;
@@ -493,6 +525,8 @@ int ts_b200_batch_create(ts_b200_kernel *const *kernels, int n, ts_b200_batch **
     b->fp32 = k0->fp32;
     b->imag = k0->imag;
     b->phase = phase;
+    b->walk = walk2 ? 2 : 0;
+    b->ring = walk2 ? 6 : 4;
     b->device = k0->device;
     b->num_sms = k0->num_sms;
     b->args_bytes = b->fp32 ? sizeof(StepArgs<float>) : sizeof(StepArgs<double>);
@@ -584,7 +618,7 @@ int ts_b200_batch_launch_info(ts_b200_batch *b, ts_b200_launch_shape *out) {
     out->blocks = std::max(1, std::min(b->resident_blocks, div_up(b->n_tasks, b->shape.warps)));
     out->threads = 32 * b->shape.warps;
     out->smem_bytes = (int64_t)batch_smem(b, b->shape.warps);
-    out->walk = 0;
+    out->walk = b->walk;
     out->reserved = 0;
     return TS_B200_OK;
 }

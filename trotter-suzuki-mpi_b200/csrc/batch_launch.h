@@ -14,6 +14,17 @@ cudaError_t launch_batch_f64(bool imag, int phase, const BatchArgs<double> &b, i
 cudaError_t launch_batch_f32(bool imag, int phase, const BatchArgs<float> &b, int warps,
                              size_t smem, int blocks, cudaStream_t st, int *blocks_per_sm);
 
+// The batched step on the look-ahead walk (walk2.cuh, two rows per
+// iteration; batch2_f{64,32}_{real,imag}.cu), same arguments.
+cudaError_t launch_batch2_f64_real(int phase, const BatchArgs<double> &b, int warps, size_t smem,
+                                   int blocks, cudaStream_t st, int *blocks_per_sm);
+cudaError_t launch_batch2_f64_imag(int phase, const BatchArgs<double> &b, int warps, size_t smem,
+                                   int blocks, cudaStream_t st, int *blocks_per_sm);
+cudaError_t launch_batch2_f32_real(int phase, const BatchArgs<float> &b, int warps, size_t smem,
+                                   int blocks, cudaStream_t st, int *blocks_per_sm);
+cudaError_t launch_batch2_f32_imag(int phase, const BatchArgs<float> &b, int warps, size_t smem,
+                                   int blocks, cudaStream_t st, int *blocks_per_sm);
+
 template <class V>
 cudaError_t launch_batch_variant(const BatchArgs<typename V::T> &b, int warps, size_t smem,
                                  int blocks, cudaStream_t st, int *blocks_per_sm) {

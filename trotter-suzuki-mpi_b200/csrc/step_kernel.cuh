@@ -1365,7 +1365,8 @@ struct BatchArgs {
     double *task_norm;        // imaginary time: squared norm of each task's inner cells
     int *error;               // set when a bounded wait gives up
     int n_tasks;
-    int ring;
+    int ring;  // ring slots per warp (checked walk)
+    int vlen;  // vertical pair table entries per warp (look-ahead walk)
 };
 
 template <typename X>

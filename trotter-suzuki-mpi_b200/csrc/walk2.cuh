@@ -790,28 +790,16 @@ struct W2Bounds {
     static constexpr int MIN_BLOCKS = ROT32 ? 3 : ((V::C == 2 && !V::ROT) ? 2 : 1);
 };
 
+// Per-warp set-up: this warp's ring (D slots), its vertical pair table of
+// `vl` entries and its mbarriers, the ring zeroed and the window finite.
 template <class V, int R>
-__global__ void __launch_bounds__(W2Bounds<V>::THREADS, W2Bounds<V>::MIN_BLOCKS)
-    step2_kernel(StepArgs<typename V::T> a) {
+__device__ __forceinline__ void w2_warp_setup(Walk2<V, R> &w, unsigned char *smem, int warps,
+                                              int warp, int lane, int vl) {
     using T = typename V::T;
     using S = W2Shape<V, R>;
-    extern __shared__ __align__(128) unsigned char smem[];
-    // the next step's blocks may be scheduled as this step's blocks retire
-    // (programmatic dependent launch): their set-up below overlaps this
-    // step's tail, and they wait for this step's completion before reading
-    // its output
-    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-    const int warps = blockDim.x >> 5;
-    const int warp = __shfl_sync(0xffffffffu, (int)(threadIdx.x >> 5), 0);
-    const int lane = threadIdx.x & 31;
-    const int n_tasks = a.n_strips * a.n_segs;
-    const int vl = w2_vlen(a.seg_h, S::ROT);
-
-    Walk2<V, R> w;
     w.lane = lane;
     w.nacc = 0.0;
     w.failed = false;
-    w.H = a.H;
     w.ring = smem + (size_t)warp * S::D * S::SLOT;
     w.vco = reinterpret_cast<Cx<T> *>(smem + (size_t)warps * S::D * S::SLOT) + (size_t)warp * vl;
     w.bars = reinterpret_cast<uint64_t *>(smem + (size_t)warps * S::D * S::SLOT +
@@ -833,11 +821,15 @@ __global__ void __launch_bounds__(W2Bounds<V>::THREADS, W2Bounds<V>::MIN_BLOCKS)
     for (int j = 0; j < S::NW; ++j)
 #pragma unroll
         for (int i = 0; i < V::C; ++i) w.win[j][i] = Cx<T>{T(0), T(0)};
-    // everything below reads what the previous step wrote (the tile, the
-    // renormalisation factor, the schedule's step): wait for its completion
-    // (immediate without a programmatic dependency)
-    asm volatile("griddepcontrol.wait;" ::: "memory");
-    // step constants
+}
+
+// The step constants of one tile (read after the previous step completed:
+// the renormalisation factor and, in FP32 real time, the step of the
+// kinetic coefficient schedule).
+template <class V, int R>
+__device__ __forceinline__ void w2_bind(Walk2<V, R> &w, const StepArgs<typename V::T> &a) {
+    using T = typename V::T;
+    w.H = a.H;
     w.inv = V::IMAG ? (T)a.scal->pending_inv : T(1);
     w.aH = a.aH;
     w.bH = a.bH;
@@ -870,12 +862,69 @@ __global__ void __launch_bounds__(W2Bounds<V>::THREADS, W2Bounds<V>::MIN_BLOCKS)
     w.opitch = (size_t)a.P;
     w.gpsi_pitch = (size_t)a.P * sizeof(Cx<T>);
     w.gtab_pitch = (size_t)a.P * sizeof(typename V::TabT);
+}
+
+template <class V, int R>
+__global__ void __launch_bounds__(W2Bounds<V>::THREADS, W2Bounds<V>::MIN_BLOCKS)
+    step2_kernel(StepArgs<typename V::T> a) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    // the next step's blocks may be scheduled as this step's blocks retire
+    // (programmatic dependent launch): their set-up below overlaps this
+    // step's tail, and they wait for this step's completion before reading
+    // its output
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    const int warps = blockDim.x >> 5;
+    const int warp = __shfl_sync(0xffffffffu, (int)(threadIdx.x >> 5), 0);
+    const int lane = threadIdx.x & 31;
+    const int n_tasks = a.n_strips * a.n_segs;
+
+    Walk2<V, R> w;
+    w2_warp_setup(w, smem, warps, warp, lane, w2_vlen(a.seg_h, W2Shape<V, R>::ROT));
+    // everything below reads what the previous step wrote (the tile, the
+    // renormalisation factor, the schedule's step): wait for its completion
+    // (immediate without a programmatic dependency)
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    w2_bind(w, a);
 
     for (int task = blockIdx.x * warps + warp; task < n_tasks && !w.failed;
          task += gridDim.x * warps)
         w2_task(w, a, task);
 
     w2_finish<V>(a, w.nacc, warps, warp, lane);
+}
+
+// Many tiles of one precision and time mode in one persistent launch (the
+// batched step on the look-ahead walk): the task list of all tiles is
+// walked as by batch_step_kernel, each task binding its tile's buffers and
+// constants; in imaginary time each task's squared norm goes to
+// task_norm[task], which a per-tile pass sums into the tile's
+// renormalisation factor.  b.vlen: vertical pair table entries per warp (for
+// the tallest segment of the batch).
+template <class V, int R>
+__global__ void __launch_bounds__(128, 4) batch2_kernel(BatchArgs<typename V::T> b) {
+    using T = typename V::T;
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int warps = blockDim.x >> 5;
+    const int warp = __shfl_sync(0xffffffffu, (int)(threadIdx.x >> 5), 0);
+    const int lane = threadIdx.x & 31;
+
+    Walk2<V, R> w;
+    w2_warp_setup(w, smem, warps, warp, lane, b.vlen);
+    for (int t = blockIdx.x * warps + warp; t < b.n_tasks && !w.failed; t += gridDim.x * warps) {
+        const int2 it = __ldg(&b.tasks[t]);
+        const int tile = bcast0(it.x), task = bcast0(it.y);
+        const StepArgs<T> a = load_tile_args(b.inst + tile);
+        w2_bind(w, a);
+        w.nacc = 0.0;
+        w2_task(w, a, task);
+        if constexpr (V::IMAG) {
+            double n = w.nacc;
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) n += __shfl_xor_sync(0xffffffffu, n, off);
+            if (lane == 0) b.task_norm[t] = n;
+        }
+    }
+    if (w.failed && lane == 0) atomicExch(b.error, 1);
 }
 
 }  // namespace tsb
