@@ -117,11 +117,16 @@ struct Walk2 {
     // mirror sign on the lane of column 0 (imaginary time), else 0
     T rca[2][2], rcb[2][2];
     T msign;
-    bool out_col[C], norm_col[C], all_out;
+    bool out_col[C], norm_col[C];
     int ra, nit, lane;
     int n_lo, n_hi;  // iterations whose stored row is in the norm region
     const unsigned char *gpsi, *gtab;  // row 0 of the strip's first copied column
     const unsigned char *gpb;          // pair: the other species' row 0, same column
+    // the first row of the next slot to issue (slot indices advance by one
+    // per issue); the walk indices [t_lo, t_lo + t_span) of copied rows (in
+    // the tile and in the walk); row_tx: the bytes of one copied row
+    const unsigned char *cpsi, *ctab, *cpb;
+    uint32_t t_lo, t_span, row_tx;
     // pair: the other species' pending factor, g_ab dt; with the Rabi
     // rotation at load (real time) its coefficients for the own and the
     // other species' cell
@@ -145,23 +150,18 @@ struct Walk2 {
     // into ring slot q; rows outside the tile or past the walk are not
     // copied, and a slot without any row completes its phase by a plain
     // arrive.  Lane 0 issues, through predicates (no divergent branch in the
-    // row body).
+    // row body).  Slot indices are issued in order, one more per call, so
+    // the copy addresses advance from the walk's first row; a walk index tp
+    // is a copied row when t_lo <= tp < t_lo + t_span.
     __device__ __forceinline__ void issue(int si, int q) {
         const uint32_t sb = smem_u32(ring + q * S::SLOT);
         const uint32_t bar = smem_u32(&bars[q]);
-        const uint32_t rowbytes = psi_bytes + tab_bytes + (V::PB ? psi_bytes : 0u);
-        uint32_t p[2], n = 0;
-        const unsigned char *src_psi[2], *src_tab[2], *src_pb[2];
+        uint32_t p[R], n = 0;
 #pragma unroll
         for (int k = 0; k < R; ++k) {
-            const int tp = R * si + k, row = ra + tp;
-            const bool real = tp < nit && row >= 0 && row < H;
+            const bool real = (uint32_t)(R * si + k - t_lo) < t_span;
             p[k] = (lane == 0 && real) ? 1u : 0u;
             n += real ? 1u : 0u;
-            const int rr = real ? row : 0;
-            src_psi[k] = gpsi + (size_t)rr * gpsi_pitch;
-            src_tab[k] = gtab + (size_t)rr * gtab_pitch;
-            if constexpr (V::PB) src_pb[k] = gpb + (size_t)rr * gpsi_pitch;
         }
         const uint32_t pc = (lane == 0 && n > 0) ? 1u : 0u;
         const uint32_t pa = (lane == 0 && n == 0) ? 1u : 0u;
@@ -171,7 +171,7 @@ struct Walk2 {
             "setp.ne.u32 pa, %1, 0;\n\t"
             "@pc mbarrier.arrive.expect_tx.shared::cta.b64 _, [%2], %3;\n\t"
             "@pa mbarrier.arrive.shared::cta.b64 _, [%2];\n\t}" ::"r"(pc),
-            "r"(pa), "r"(bar), "r"(n * rowbytes)
+            "r"(pa), "r"(bar), "r"(n * row_tx)
             : "memory");
 #pragma unroll
         for (int k = 0; k < R; ++k) {
@@ -181,18 +181,21 @@ struct Walk2 {
                 "setp.ne.u32 p, %0, 0;\n\t"
                 "@p cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%1], [%2], %3, [%4];\n\t"
                 "@p cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%5], [%6], %7, [%4];\n\t}" ::"r"(p[k]),
-                "r"(rb + psi_off), "l"(src_psi[k]), "r"(psi_bytes), "r"(bar),
-                "r"(rb + (uint32_t)V::PSI_BYTES + tab_off), "l"(src_tab[k]), "r"(tab_bytes)
+                "r"(rb + psi_off), "l"(cpsi + k * gpsi_pitch), "r"(psi_bytes), "r"(bar),
+                "r"(rb + (uint32_t)V::PSI_BYTES + tab_off), "l"(ctab + k * gtab_pitch), "r"(tab_bytes)
                 : "memory");
             if constexpr (V::PB)
                 asm volatile(
                     "{\n\t.reg .pred p;\n\t"
                     "setp.ne.u32 p, %0, 0;\n\t"
                     "@p cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%1], [%2], %3, [%4];\n\t}" ::"r"(p[k]),
-                    "r"(rb + (uint32_t)S::PB_OFF + psi_off), "l"(src_pb[k]), "r"(psi_bytes),
+                    "r"(rb + (uint32_t)S::PB_OFF + psi_off), "l"(cpb + k * gpsi_pitch), "r"(psi_bytes),
                     "r"(bar)
                     : "memory");
         }
+        cpsi += R * gpsi_pitch;
+        ctab += R * gtab_pitch;
+        if constexpr (V::PB) cpb += R * gpsi_pitch;
     }
 };
 
@@ -231,16 +234,21 @@ __device__ __forceinline__ void load_tab_cells(const unsigned char *p, TabT (&v)
 }
 
 template <typename T, int C>
-__device__ __forceinline__ void store_row_cells(Cx<T> *o, const Cx<T> (&v)[C], const bool (&in)[C],
-                                                bool all) {
+__device__ __forceinline__ void store_row_cells(Cx<T> *o, const Cx<T> (&v)[C],
+                                                const bool (&in)[C]) {
     if constexpr (sizeof(T) == 4 && C % 2 == 0) {
-        if (all) {
+        // a pair of cells in one 16-byte store where both are output cells
+        // (predicated stores: no divergent branch at the strip's halo lanes)
 #pragma unroll
-            for (int i = 0; i < C; i += 2)
+        for (int i = 0; i < C; i += 2) {
+            const bool both = in[i] && in[i + 1];
+            if (both)
                 reinterpret_cast<float4 *>(o)[i / 2] =
                     make_float4(v[i].re, v[i].im, v[i + 1].re, v[i + 1].im);
-            return;
+            if (in[i] && !both) st_cx_global(o + i, v[i]);
+            if (in[i + 1] && !both) st_cx_global(o + i + 1, v[i + 1]);
         }
+        return;
     }
 #pragma unroll
     for (int i = 0; i < C; ++i)
@@ -418,7 +426,7 @@ __device__ __forceinline__ void w2_stages(Walk2<V, R> &w, int t) {
                 W2S(S::HY)[0].im = w.msign * W2S(S::HY)[1].im;
             }
         }
-        store_row_cells<T, C>(w.orow, W2S(S::HY), w.out_col, w.all_out);
+        store_row_cells<T, C>(w.orow, W2S(S::HY), w.out_col);
         if (IMAG && t >= w.n_lo && t < w.n_hi) {
 #pragma unroll
             for (int i = 0; i < C; ++i) {
@@ -553,16 +561,26 @@ __device__ __forceinline__ void w2_task(Walk2<V, R> &w, const StepArgs<typename 
     w.gpsi = reinterpret_cast<const unsigned char *>(a.psi_in) + (size_t)cs * sizeof(Cx<T>);
     w.gtab = reinterpret_cast<const unsigned char *>(a.pot) + (size_t)cs * sizeof(TabT);
     if constexpr (V::PB) w.gpb = reinterpret_cast<const unsigned char *>(a.pb) + (size_t)cs * sizeof(Cx<T>);
+    // running copy addresses from the walk's first row (which may lie above
+    // the tile: only rows inside it are ever read through them)
+    w.cpsi = w.gpsi + (ptrdiff_t)w.ra * (ptrdiff_t)w.gpsi_pitch;
+    w.ctab = w.gtab + (ptrdiff_t)w.ra * (ptrdiff_t)w.gtab_pitch;
+    if constexpr (V::PB) w.cpb = w.gpb + (ptrdiff_t)w.ra * (ptrdiff_t)w.gpsi_pitch;
+    {
+        const int lo = max(0, -w.ra);               // the first walk row inside the tile
+        const int hi = min(a.H - w.ra, w.nit);      // past the tile's last row and the walk's
+        w.t_lo = (uint32_t)lo;
+        w.t_span = (uint32_t)max(0, hi - lo);
+    }
+    w.row_tx = w.psi_bytes + w.tab_bytes + (V::PB ? w.psi_bytes : 0u);
     const int xl = c0 + C * lane;
     bool present[C];
-    w.all_out = true;
 #pragma unroll
     for (int i = 0; i < C; ++i) {
         const int x = xl + i;
         present[i] = x >= 0 && x < a.W;
         w.out_col[i] = x >= ox0 && x < ox1;
         w.norm_col[i] = w.out_col[i] && x >= a.ix0 && x < a.ix1;
-        w.all_out = w.all_out && w.out_col[i];
     }
     {
         const T one = DeltaForm<T>::value ? T(0) : T(1);
