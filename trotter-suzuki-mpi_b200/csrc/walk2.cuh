@@ -152,16 +152,28 @@ struct Walk2 {
     // arrive.  Lane 0 issues, through predicates (no divergent branch in the
     // row body).  Slot indices are issued in order, one more per call, so
     // the copy addresses advance from the walk's first row; a walk index tp
-    // is a copied row when t_lo <= tp < t_lo + t_span.
+    // is a copied row when t_lo <= tp < t_lo + t_span.  In a rotating frame
+    // the addresses are computed from the row instead: loop-carried pointers
+    // took the double kernel from 158 to 174 registers, 2 blocks per SM
+    // instead of 3 (1182 against 1039 us per 8192^2 step).
     __device__ __forceinline__ void issue(int si, int q) {
         const uint32_t sb = smem_u32(ring + q * S::SLOT);
         const uint32_t bar = smem_u32(&bars[q]);
         uint32_t p[R], n = 0;
+        const unsigned char *src_psi[R], *src_tab[R];
 #pragma unroll
         for (int k = 0; k < R; ++k) {
             const bool real = (uint32_t)(R * si + k - t_lo) < t_span;
             p[k] = (lane == 0 && real) ? 1u : 0u;
             n += real ? 1u : 0u;
+            if constexpr (S::ROT) {
+                const int rr = real ? ra + R * si + k : 0;
+                src_psi[k] = gpsi + (size_t)rr * gpsi_pitch;
+                src_tab[k] = gtab + (size_t)rr * gtab_pitch;
+            } else {
+                src_psi[k] = cpsi + k * gpsi_pitch;
+                src_tab[k] = ctab + k * gtab_pitch;
+            }
         }
         const uint32_t pc = (lane == 0 && n > 0) ? 1u : 0u;
         const uint32_t pa = (lane == 0 && n == 0) ? 1u : 0u;
@@ -181,8 +193,8 @@ struct Walk2 {
                 "setp.ne.u32 p, %0, 0;\n\t"
                 "@p cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%1], [%2], %3, [%4];\n\t"
                 "@p cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%5], [%6], %7, [%4];\n\t}" ::"r"(p[k]),
-                "r"(rb + psi_off), "l"(cpsi + k * gpsi_pitch), "r"(psi_bytes), "r"(bar),
-                "r"(rb + (uint32_t)V::PSI_BYTES + tab_off), "l"(ctab + k * gtab_pitch), "r"(tab_bytes)
+                "r"(rb + psi_off), "l"(src_psi[k]), "r"(psi_bytes), "r"(bar),
+                "r"(rb + (uint32_t)V::PSI_BYTES + tab_off), "l"(src_tab[k]), "r"(tab_bytes)
                 : "memory");
             if constexpr (V::PB)
                 asm volatile(
@@ -193,9 +205,11 @@ struct Walk2 {
                     "r"(bar)
                     : "memory");
         }
-        cpsi += R * gpsi_pitch;
-        ctab += R * gtab_pitch;
-        if constexpr (V::PB) cpb += R * gpsi_pitch;
+        if constexpr (!S::ROT) {
+            cpsi += R * gpsi_pitch;
+            ctab += R * gtab_pitch;
+            if constexpr (V::PB) cpb += R * gpsi_pitch;
+        }
     }
 };
 
@@ -797,10 +811,11 @@ __device__ __forceinline__ void w2_finish(const StepArgs<typename V::T> &a, doub
 // Register budget: 2 cells per lane fit 128 registers, so 16 warps of the
 // default 4-warp blocks stay resident per SM; 4 cells per lane take up to
 // 255.  In a rotating frame (blocks of at most 4 warps) the 8-row window
-// takes ~150 registers in double, 3 blocks per SM as its 8-row ring allows
+// takes ~160 registers in double, 3 blocks per SM as its 8-row ring allows
 // (capping the registers at 170 for 3 blocks made the compiler's schedule
-// slower: 967 -> 1012 us per 8192^2 step); in float a cap of 170 (4 blocks
-// per SM) ran 600 us against 621 at a cap of 128 (5 blocks).
+// slower: 1039 -> 1072 us per 8192^2 step; with more live state, 174
+// registers, 2 blocks per SM, it took 1182 us); in float a cap of 170 (3
+// blocks per SM) ran 600 us against 621 at a cap of 128 (5 blocks).
 template <class V>
 struct W2Bounds {
     static constexpr bool ROT32 = V::ROT && sizeof(typename V::T) == 4;
