@@ -411,6 +411,13 @@ def run_b200_arm(args, rank, world, local, pg):
                 "max_abs_psi_err_vs_fp64": float(np.abs(d).max()),
                 "trotter_steps_compared": (args.warmup + args.steps) * TROTTER_PER_STEP + 1,
                 "bytes_per_site_step": BYTES_PER_SITE_STEP["fp32"]}
+        peak32, peak32_kind = measured_peak()
+        ach32 = BYTES_PER_SITE_STEP["fp32"] * v32 / world / 1e9
+        fp32["roofline"] = {"bound": "hbm", "achieved": ach32, "peak": peak32, "unit": "GB/s",
+                            "frac": ach32 / peak32, "peak_kind": peak32_kind,
+                            "traffic": committed_traffic("step_kernel_gpe_imag_2048_fp32.md"),
+                            "kernel": "tsb::step2_kernel<float, C=2, imaginary, GPE, 2 rows per "
+                                      "iteration> (look-ahead walk)"}
         del solver32
 
     # ---- the metric's other two parts, on their own configurations: FP64
