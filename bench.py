@@ -90,6 +90,22 @@ def committed_traffic(summary="step_kernel_gpe_imag_2048.md"):
         return None
 
 
+def committed_traffic_per_site(summary, sites):
+    """DRAM bytes per launch scaled to `sites` from a committed capture of a
+    smaller case of the same kernel (lines `dram_bytes_per_launch: <int>` and
+    `sites_per_launch: <int>`), if any."""
+    import re
+    t = committed_traffic(summary)
+    try:
+        with open(os.path.join(REPO, "profiles", summary)) as f:
+            m = re.search(r"^sites_per_launch:\s*(\d+)", f.read(), re.M)
+    except OSError:
+        return None
+    if t is None or not m:
+        return None
+    return int(t * sites / int(m.group(1)))
+
+
 def rotating_frame_traffic():
     """DRAM bytes per FP64 rotating-frame step launch at the current vortex
     side: the committed capture on 4096^2 (the 8192^2 workload is too large
@@ -585,7 +601,7 @@ def run_batch_workload(args, rank, world, local, pg):
     import trottersuzuki_b200 as ts
     from trottersuzuki_b200 import _capi, launch_count
     L = _capi.lib()
-    cfgs = batch_config()
+    cfgs = batch_config(args.batch_instances)
     total_sites = float(sum(c["side"] ** 2 for c in cfgs))
     T = BATCH_TROTTER_PER_STEP
     stream = torch.cuda.Stream(device=device)
@@ -688,7 +704,7 @@ def run_batch_workload(args, rank, world, local, pg):
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": res["fp64"]["ms_per_step"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "batch512_real_time", "instances": BATCH_N,
+        "config": {"workload": "batch512_real_time", "instances": len(cfgs),
                    "sides": list(BATCH_SIDES), "total_sites": total_sites, "length": BATCH_LENGTH,
                    "dt": BATCH_DT, "trotter_steps_per_step": T, "boundary": "closed",
                    "imag_time": False, "seed": BATCH_SEED, "parallelism": f"replicas{world}",
@@ -702,7 +718,8 @@ def run_batch_workload(args, rank, world, local, pg):
                        "loop_value": res["fp32"]["loop_value"],
                        "speedup_batch_vs_loop": res["fp32"]["speedup_vs_loop"]},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                     "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": committed_traffic_per_site("batch_step_batch512.md", total_sites),
                      "algorithmic_bytes_per_launch": bytes_step,
                      "kernel": "tsb::batch2_kernel<double, C=2, real, no rotation, GPE, "
                                "2 rows per iteration> (look-ahead walk)"},
@@ -1558,6 +1575,9 @@ def main():
     ap.add_argument("--split", choices=["none", "slab"], default="none",
                     help="slab: the 8192^2 vortex lattice as one lattice in slabs of rows "
                          "over the ranks (strong scaling)")
+    ap.add_argument("--batch-instances", type=int, default=BATCH_N,
+                    help="instances of the batch workload (the first of its seeded list; "
+                         "fewer for an ncu capture)")
     ap.add_argument("--vortex-side", type=int, default=0,
                     help="lattice side of the vortex / slab workloads (default 8192; smaller "
                          "sides keep an ncu capture of their kernels within a few GB)")

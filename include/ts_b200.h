@@ -381,7 +381,8 @@ int ts_b200_batch_set_stream(ts_b200_batch *b, void *stream);
 int ts_b200_batch_set_launch(ts_b200_batch *b, int segment_rows, int warps_per_block);
 
 /* Autotuner: times `trial_steps` batched steps for each candidate shape (rows
- * per segment 16..256, 2 or 4 warps per block) and keeps the fastest.  The
+ * per segment 16..256, 2 or 4 warps per block), twice over the candidate list,
+ * and keeps the shape with the fastest of its two times.  The
  * trials read the tiles' current state and write only the scratch buffer, so
  * the state is unchanged.  With use_cache != 0 a shape tuned earlier in this
  * process for the same precision, time mode and tile sizes is reused
