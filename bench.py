@@ -495,6 +495,10 @@ def run_b200_arm(args, rank, world, local, pg):
         rate, cores, kind, sample, _ = cpu_reference_rate(psi0, budget_s=args.ref_budget)
         cpu = {"value": rate, "unit": "site-steps/s", "cores": cores, "kind": kind,
                "sample": sample}
+        if cores > 1:
+            # the same reference path on one thread (a bounded ~4 s sample)
+            r1, _, _, s1, _ = cpu_reference_rate(psi0, budget_s=4.0, threads=1)
+            cpu["single_thread"] = {"value": r1, "unit": "site-steps/s", "sample": s1}
 
     clk = clocks.summary()
     line = {
