@@ -199,7 +199,12 @@ int ts_b200_set_potential_device(ts_b200_kernel *k, const double *potential, siz
  * table built as by ts_b200_set_potential_device before the step.  Every
  * step refreshes the halo when `exchange` is nonzero, none does otherwise
  * (a run of the reference's per-step Python loop, classes_extension.py:
- * 393-403, where each step is an evolve call of its own). */
+ * 393-403, where each step is an evolve call of its own).  With count >= 2
+ * in FP64 real time on cartesian one-component tiles (no rotating frame, the
+ * default row walk) with an even dim_x, even `pitch` and `slab` and 16-byte
+ * aligned planes, each step forms the table's entries from V_i itself (the
+ * same values) instead of a table pass; the table of the last potential is
+ * then built once, so later steps see the same table either way. */
 int ts_b200_evolve_potentials(ts_b200_kernel *k, const double *potentials, size_t pitch,
                               size_t slab, int count, double delta_t, int exchange);
 

@@ -142,13 +142,22 @@ def test_c_abi_table_from_device_potential(imag, precision):
     assert np.abs(out[0] - out[1]).max() <= tol * np.abs(out[0]).max()
 
 
+# (N, Ny, periodic, lhy): even tile widths take the step that forms the
+# table's entries from the potential rows itself, the odd one the table pass
+SEQUENCE_CASES = [(64, 48, (True, False), 0.0), (64, 64, (False, False), 0.3),
+                  (61, 47, (False, False), 0.3)]
+
+
+@pytest.mark.parametrize("case", SEQUENCE_CASES, ids=["periodic_x", "lhy", "odd_width"])
 @pytest.mark.parametrize("exchange", [False, True])
-def test_c_abi_potential_sequence_is_the_per_step_loop(exchange):
-    """ts_b200_evolve_potentials == per step: set_potential_device, step."""
+def test_c_abi_potential_sequence_is_the_per_step_loop(exchange, case):
+    """ts_b200_evolve_potentials == per step: set_potential_device, step,
+    bit for bit (the fused path forms the same table entries)."""
     import torch
     from trottersuzuki_b200 import Kernel
-    lat, psi0, V = seeded_case(64, 8.0, 48, (True, False), 0.0, seed=8)
-    p = lat.params(DT, False, 1.0, G, 0.0, 0.0)
+    N, Ny, periodic, lhy = case
+    lat, psi0, V = seeded_case(N, 8.0, Ny, periodic, 0.0, seed=8)
+    p = lat.params(DT, False, 1.0, G, lhy, 0.0)
     X, Y = lat.coordinates()
     n = 6
     Vs = torch.from_numpy(np.stack([moving_trap(X, Y, i * DT) for i in range(n)])).cuda()
@@ -165,7 +174,11 @@ def test_c_abi_potential_sequence_is_the_per_step_loop(exchange):
             else:
                 k.evolve_potentials(Vs.data_ptr(), Vs.shape[2], slab, n, DT, exchange)
             out.append(k.get_state())
-    assert np.array_equal(out[0], out[1])
+            # the table left for later steps is the last potential's either way
+            k.step(False)
+            out.append(k.get_state())
+    assert np.array_equal(out[0], out[2])
+    assert np.array_equal(out[1], out[3])
 
 
 def test_c_abi_rejects_bad_potential_arguments():

@@ -33,6 +33,11 @@ struct ts_b200_kernel {
     unsigned int *red_ticket = nullptr;
     cudaStream_t own_stream = nullptr, stream = nullptr;
     cudaEvent_t ev_order = nullptr;  // ts_b200_stream_wait / _signal
+    // ts_b200_evolve_potentials in progress with the table made inside the
+    // step: the potential the next step reads (row pitch in bytes) and dt
+    const double *vpot = nullptr;
+    size_t vpot_pitch = 0;
+    double vpot_dt = 0.0;
     int C = 2, seg_h = 64, warps = 4, ring = 4;
     int resident_blocks = 0;  // blocks of the current launch shape resident on the GPU (0: unknown)
     bool auto_seg = true;     // pick the segment height from the resident grid

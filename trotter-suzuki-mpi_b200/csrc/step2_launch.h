@@ -41,6 +41,14 @@ cudaError_t launch_step2_variant(const StepArgs<typename V::T> &a, int warps, si
 template <typename T, bool IMAG>
 cudaError_t launch_step2_t(int C, int R, int phase, const StepArgs<T> &a, int warps, size_t smem,
                            int blocks, cudaStream_t st, int *bps, bool pdl) {
+    if constexpr (std::is_same<T, double>::value && !IMAG) {
+        // the table's entries from potential rows (phase bit 16)
+        if (C == 2 && R == 2 && phase >= 16) {
+            if (phase == 16) return launch_step2_variant<Variant<T, 2, false, false, 16>, 2>(a, warps, smem, blocks, st, bps, pdl);
+            if (phase == 17) return launch_step2_variant<Variant<T, 2, false, false, 17>, 2>(a, warps, smem, blocks, st, bps, pdl);
+            if (phase == 18) return launch_step2_variant<Variant<T, 2, false, false, 18>, 2>(a, warps, smem, blocks, st, bps, pdl);
+        }
+    }
     if (C == 2 && R == 2) {
         if (phase == 0) return launch_step2_variant<Variant<T, 2, IMAG, false, 0>, 2>(a, warps, smem, blocks, st, bps, pdl);
         if (phase == 1) return launch_step2_variant<Variant<T, 2, IMAG, false, 1>, 2>(a, warps, smem, blocks, st, bps, pdl);

@@ -114,6 +114,10 @@ struct StepArgs {
     // imaginary time, non-null: the step's renormalisation factor is also
     // written here (a recomputation keeping each step's factor)
     double *inv_copy;
+    // pot's row pitch in bytes (0: P cells of the table type) and, for the
+    // variants that read V instead of the table (phase bit 16), dt
+    size_t pot_pitch;
+    double pot_dt;
 };
 
 // Output rows [oy0, oy1) of segment `seg` of the launch.
@@ -622,6 +626,42 @@ __device__ __forceinline__ float2 phase_expneg2(float th0, float th1) {
     return make_float2(phase_expneg<float, TIERS>(th0), phase_expneg<float, TIERS>(th1));
 }
 
+// sin(a) and cos(a) - 1 for |a| <= 1/16 from their Maclaurin series (Horner's
+// rule in a^2).  With the last terms a^9/9! and a^10/10! the truncation error
+// is below 2^-64 relative, and a, -a^2/2 carry the leading bits exactly, so
+// both are within about half an ulp of the true values: no range reduction
+// and a few FMAs instead of a full sincos.
+constexpr double kSmallAngle = 0.0625;
+__device__ inline void small_angle_sincos(double a, double *s, double *cm1) {
+    const double a2 = a * a;
+    double ps = 1.0 / 362880.0;  // 1/9!
+    ps = fma(ps, a2, -1.0 / 5040.0);
+    ps = fma(ps, a2, 1.0 / 120.0);
+    ps = fma(ps, a2, -1.0 / 6.0);
+    *s = fma(a * a2, ps, a);
+    double pc = -1.0 / 3628800.0;  // -1/10!
+    pc = fma(pc, a2, 1.0 / 40320.0);
+    pc = fma(pc, a2, -1.0 / 720.0);
+    pc = fma(pc, a2, 1.0 / 24.0);
+    pc = fma(pc, a2, -0.5);
+    *cm1 = a2 * pc;
+}
+
+// The FP64 real-time table entry exp(-i ang), ang = dt V: (cos, -sin), the
+// series for small angles (src/solver.cpp:74-109 tabulates the same with
+// std::exp(complex)).
+__device__ inline Cx<double> vpot_table_entry(double ang) {
+    double s;
+    if (fabs(ang) <= kSmallAngle) {
+        double cm1;
+        small_angle_sincos(ang, &s, &cm1);
+        return Cx<double>{1.0 + cm1, -s};
+    }
+    double c;
+    sincos(ang, &s, &c);
+    return Cx<double>{c, -s};
+}
+
 template <typename T>
 struct Vec2T;
 template <>
@@ -751,6 +791,14 @@ struct Variant {
     static constexpr bool CYL = (PHASE_ & 4) != 0;
     static constexpr bool RABI = (PHASE_ & 8) != 0;
     static_assert(!RABI || (PB && !IMAG_ && !CYL), "Rabi loads: two components, real time");
+    // PHASE & 16: the table's entries made in the step from a potential V
+    // (FP64, real time, cartesian, one component): the ring carries rows of
+    // V, one double per cell, and the potential stage forms exp(-i dt V)
+    // as the table kernel does
+    static constexpr bool VPOT = (PHASE_ & 16) != 0;
+    static_assert(!VPOT || (!IMAG_ && !ROT_ && (PHASE_ & 12) == 0 && (PHASE_ & 3) != 3 &&
+                            std::is_same<T_, double>::value),
+                  "potential rows: double, real time, cartesian, one component");
     // recomputed halo columns: one per horizontal pair sweep of the step
     // (4 kinetic; 4 more rotation row sweeps or radial sweeps)
     static constexpr int HX = (ROT_ || (PHASE_ & 4)) ? 8 : 4;
@@ -776,7 +824,7 @@ struct Variant {
     // The batched kernel runs many tasks per warp: more resident warps (6
     // blocks in double, 8 in float: 80 / 64 registers) hide more latency.
     static constexpr int BATCH_MIN_BLOCKS = LANE_COEF ? (sizeof(T_) == 4 ? 8 : 6) : 4;  // C = 2
-    using TabT = typename std::conditional<IMAG_, T_, Cx<T_>>::type;
+    using TabT = typename std::conditional<IMAG_ || VPOT, T_, Cx<T_>>::type;
     static constexpr int PSI_BYTES = SW * (int)sizeof(Cx<T_>);
     static constexpr int TAB_BYTES = SW * (int)sizeof(TabT);
     // a slot: one row of psi, of the table and (PB) of the other species
@@ -1420,6 +1468,8 @@ __device__ __forceinline__ StepArgs<T> load_tile_args(const StepArgs<T> *p) {
     a.pair_norm = nullptr;
     a.pair_ticket = nullptr;
     a.inv_copy = nullptr;
+    a.pot_pitch = 0;
+    a.pot_dt = 0.0;
     return a;
 }
 

@@ -173,26 +173,8 @@ __global__ void pack_table_kernel(void *dst, int imag, int W, int H, int P, cons
     }
 }
 
-// sin(a) and cos(a) - 1 for |a| <= 1/16 from their Maclaurin series (Horner's
-// rule in a^2).  With the last terms a^9/9! and a^10/10! the truncation error
-// is below 2^-64 relative, and a, -a^2/2 carry the leading bits exactly, so
-// both are within about half an ulp of the true values: no range reduction
-// and a few FMAs instead of a full sincos.
-constexpr double kSmallAngle = 0.0625;
-__device__ inline void small_angle_sincos(double a, double *s, double *cm1) {
-    const double a2 = a * a;
-    double ps = 1.0 / 362880.0;  // 1/9!
-    ps = fma(ps, a2, -1.0 / 5040.0);
-    ps = fma(ps, a2, 1.0 / 120.0);
-    ps = fma(ps, a2, -1.0 / 6.0);
-    *s = fma(a * a2, ps, a);
-    double pc = -1.0 / 3628800.0;  // -1/10!
-    pc = fma(pc, a2, 1.0 / 40320.0);
-    pc = fma(pc, a2, -1.0 / 720.0);
-    pc = fma(pc, a2, 1.0 / 24.0);
-    pc = fma(pc, a2, -0.5);
-    *cm1 = a2 * pc;
-}
+using tsb::kSmallAngle;
+using tsb::small_angle_sincos;
 
 // The table from a potential on the device: exp(-i dt V) in real time
 // ((cos - 1, -sin) in float: delta form, pair chosen by the fast search),
@@ -852,7 +834,15 @@ int launch_step_buffers_t(ts_b200_kernel *k, const void *in, void *out, bool dry
     a.seg_h = eff_seg(k);
     a.ring = use_walk2(k) ? walk_window(k) / walk_rows(k) : k->ring;
     a.partials = k->partials;
-    cudaError_t e = dispatch_step<T>(k->C, k->imag, k->rot, k->phase, walk_rows(k), a, k->warps,
+    int phase = k->phase;
+    if (k->vpot) {
+        // the table made in the step from the potential rows
+        a.pot = k->vpot;
+        a.pot_pitch = k->vpot_pitch;
+        a.pot_dt = k->vpot_dt;
+        phase |= 16;
+    }
+    cudaError_t e = dispatch_step<T>(k->C, k->imag, k->rot, phase, walk_rows(k), a, k->warps,
                                      smem, blocks, k->stream, nullptr, k->overlap);
     if (e != cudaSuccess) return cuda_fail(k, e, "step kernel launch");
     if (!dry) g_launches.fetch_add(1, std::memory_order_relaxed);
@@ -1409,12 +1399,46 @@ int ts_b200_set_potential_device(ts_b200_kernel *k, const double *potential, siz
     return TS_B200_OK;
 }
 
+namespace {
+// The step can read the potential rows directly: FP64 real time, one
+// component, cartesian, no rotating frame, the look-ahead walk with two rows
+// per iteration; and the rows' copies aligned to 16 bytes (even width and
+// pitch, aligned planes).
+bool fused_potential_ok(const ts_b200_kernel *k, const double *V, size_t pitch, size_t slab) {
+    return !k->fp32 && !k->imag && !k->rot && !k->cyl && !k->pair_mode && k->phase <= 2 &&
+           use_walk2(k) && walk_rows(k) == 2 && k->C == 2 && (k->W % 2) == 0 &&
+           (pitch % 2) == 0 && (slab % 2) == 0 && (reinterpret_cast<uintptr_t>(V) % 16) == 0;
+}
+}  // namespace
+
 int ts_b200_evolve_potentials(ts_b200_kernel *k, const double *potentials, size_t pitch,
                               size_t slab, int count, double delta_t, int exchange) {
     if (!k || !potentials || count < 0 || pitch < (size_t)k->W || slab < pitch * k->H ||
         !(delta_t > 0.0))
         return TS_B200_INVALID_ARGUMENT;
     if (k->pair_mode) return reject_pair_mode(k);
+    // FP64 real-time cartesian steps on the look-ahead walk read the
+    // potential rows and form the table's entries themselves (no table pass:
+    // 8 B instead of 16 B per cell read, the table's 24 B per cell not moved);
+    // the table of the last potential is then built once, for later steps
+    // (so a single step keeps the table pass: the same traffic either way)
+    if (count >= 2 && fused_potential_ok(k, potentials, pitch, slab)) {
+        int s = TS_B200_OK;
+        for (int i = 0; i < count && s == TS_B200_OK; ++i) {
+            k->vpot = potentials + (size_t)i * slab;
+            k->vpot_pitch = pitch * sizeof(double);
+            k->vpot_dt = delta_t;
+            s = launch_step(k, exchange);
+        }
+        k->vpot = nullptr;
+        if (s) return s;
+        if (count > 0) {
+            launch_table_from_potential(k, potentials + (size_t)(count - 1) * slab, pitch, delta_t);
+            TSB_CHECK(k, cudaGetLastError());
+            g_launches.fetch_add(1, std::memory_order_relaxed);
+        }
+        return TS_B200_OK;
+    }
     for (int i = 0; i < count; ++i) {
         launch_table_from_potential(k, potentials + (size_t)i * slab, pitch, delta_t);
         TSB_CHECK(k, cudaGetLastError());

@@ -145,6 +145,7 @@ struct Walk2 {
     int fail_idx;  // ring slot index (rows R * fail_idx ..) whose wait gave up
     T inv;
     T aH, bH, aV, bV, ca, caa;
+    T vdt;  // potential rows (phase bit 16): dt
 
     // copy the rows of slot index `si` of the walk (rows R si .. R si + R - 1)
     // into ring slot q; rows outside the tile or past the walk are not
@@ -407,6 +408,13 @@ __device__ __forceinline__ void w2_stages(Walk2<V, R> &w, int t) {
                 }
                 potential_row<IMAG, PHASE, false, true, C, false>(W2S(2), tv, w.ca, w.caa, &ub,
                                                                   w.cab);
+            } else if constexpr (V::VPOT) {
+                // the table's entries from the potential row, as the table
+                // kernel forms them
+                Cx<T> te[C];
+#pragma unroll
+                for (int i = 0; i < C; ++i) te[i] = vpot_table_entry(w.vdt * tv[i]);
+                potential_row<IMAG, PHASE, V::LHY, false, C>(W2S(2), te, w.ca, w.caa);
             } else {
                 potential_row<IMAG, PHASE, V::LHY, false, C>(W2S(2), tv, w.ca, w.caa);
             }
@@ -571,7 +579,8 @@ __device__ __forceinline__ void w2_task(Walk2<V, R> &w, const StepArgs<typename 
     w.psi_off = (uint32_t)(cs - c0) * sizeof(Cx<T>);
     w.psi_bytes = (uint32_t)(ce - cs) * sizeof(Cx<T>);
     w.tab_off = (uint32_t)(cs - c0) * sizeof(TabT);
-    w.tab_bytes = (uint32_t)(ce - cs) * sizeof(TabT);
+    // a potential's rows hold the tile's W columns only
+    w.tab_bytes = (uint32_t)((V::VPOT ? min(ce, a.W) : ce) - cs) * sizeof(TabT);
     w.gpsi = reinterpret_cast<const unsigned char *>(a.psi_in) + (size_t)cs * sizeof(Cx<T>);
     w.gtab = reinterpret_cast<const unsigned char *>(a.pot) + (size_t)cs * sizeof(TabT);
     if constexpr (V::PB) w.gpb = reinterpret_cast<const unsigned char *>(a.pb) + (size_t)cs * sizeof(Cx<T>);
@@ -894,7 +903,8 @@ __device__ __forceinline__ void w2_bind(Walk2<V, R> &w, const StepArgs<typename 
     }
     w.opitch = (size_t)a.P;
     w.gpsi_pitch = (size_t)a.P * sizeof(Cx<T>);
-    w.gtab_pitch = (size_t)a.P * sizeof(typename V::TabT);
+    w.gtab_pitch = a.pot_pitch ? a.pot_pitch : (size_t)a.P * sizeof(typename V::TabT);
+    if constexpr (V::VPOT) w.vdt = (T)a.pot_dt;
 }
 
 template <class V, int R>
