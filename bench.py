@@ -720,7 +720,14 @@ def run_batch_workload(args, rank, world, local, pg):
         "fp32_store": {"value": res["fp32"]["value"], "unit": "site-steps/s",
                        "speedup_vs_fp64": res["fp32"]["value"] / res["fp64"]["value"],
                        "loop_value": res["fp32"]["loop_value"],
-                       "speedup_batch_vs_loop": res["fp32"]["speedup_vs_loop"]},
+                       "speedup_batch_vs_loop": res["fp32"]["speedup_vs_loop"],
+                       "roofline": {"bound": "hbm", "unit": "GB/s", "peak": peak,
+                                    "achieved": BATCH_BYTES["fp32"] * res["fp32"]["value"]
+                                    / world / 1e9,
+                                    "frac": BATCH_BYTES["fp32"] * res["fp32"]["value"]
+                                    / world / 1e9 / peak,
+                                    "peak_kind": peak_kind,
+                                    "bytes_per_site_step": BATCH_BYTES["fp32"]}},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,
                      "traffic": committed_traffic_per_site("batch_step_batch512.md", total_sites),
