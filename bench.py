@@ -1242,6 +1242,8 @@ MT_HOST_STEPS = 4
 
 
 MT_TIME_BATCH = 16
+# per site-step of the step that reads the potential rows: psi in + out, V
+MT_BYTES = 40
 
 
 def moving_trap(x, y, t):
@@ -1328,6 +1330,7 @@ def run_moving_trap_workload(args, rank, world, local, pg):
     v_host = world * sites * MT_HOST_STEPS / (ms_host * 1e-3)
     v_e2e = world * sites * MT_STEPS * e2e_calls / (ms_e2e * 1e-3)
     v_dps = world * sites * MT_STEPS * args.steps / (ms_dps * 1e-3)
+    peak, peak_kind = measured_peak()
     line = {
         "metric": "site-steps/s", "value": v_dev, "unit": "site-steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,
@@ -1346,6 +1349,15 @@ def run_moving_trap_workload(args, rank, world, local, pg):
                         "state copied into the State after each call)"},
         "static_potential_same_kernel": {"value": v_static, "unit": "site-steps/s"},
         "device_potential_per_step_call": {"value": v_dps, "unit": "site-steps/s"},
+        "roofline": {"bound": "hbm", "unit": "GB/s", "peak": peak, "peak_kind": peak_kind,
+                     "achieved": MT_BYTES * v_dev / world / 1e9,
+                     "frac": MT_BYTES * v_dev / world / 1e9 / peak,
+                     "traffic": committed_traffic("step_kernel_moving_trap_2048.md"),
+                     "algorithmic_bytes_per_site_step": MT_BYTES,
+                     "note": "over the whole Trotter step, the user's torch evaluation of V "
+                             "included",
+                     "kernel": "tsb::step2_kernel<double, C=2, real, GPE, potential rows, "
+                               "2 rows per iteration>"},
         "host_potential_path": {"value": v_host, "unit": "site-steps/s",
                                 "sample": f"{MT_HOST_STEPS} Trotter steps",
                                 "speedup_of_device_path": v_dev / v_host},
