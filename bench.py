@@ -77,6 +77,18 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
+_PINNED = []
+
+
+def pinned_array(shape):
+    """A float64 numpy array in page-locked host memory (the host buffers of
+    the end-to-end legs); the tensor that owns it is kept for the process."""
+    import torch
+    t = torch.empty(shape, dtype=torch.float64, pin_memory=True)
+    _PINNED.append(t)
+    return t.numpy()
+
+
 def committed_traffic(summary="step_kernel_gpe_imag_2048.md"):
     """DRAM bytes (read + write) per step-kernel launch on a workload, from
     its committed ncu summary (a line `dram_bytes_per_launch: <int>`), if any."""
@@ -670,8 +682,12 @@ def run_batch_workload(args, rank, world, local, pg):
                 X, Y = np.meshgrid(x, x)
                 w = 1.0 / c["width"] ** 2
                 g0 = np.sqrt(w / math.pi) * np.exp(-0.5 * w * ((X - c["cx"]) ** 2 + (Y - c["cy"]) ** 2))
-                init.append((np.ascontiguousarray(g0), np.zeros_like(g0)))
-            outs = [(np.empty_like(a), np.empty_like(a)) for a, _ in init]
+                re0 = pinned_array(g0.shape)
+                re0[...] = g0
+                im0 = pinned_array(g0.shape)
+                im0[...] = 0.0
+                init.append((re0, im0))
+            outs = [(pinned_array(a.shape), pinned_array(a.shape)) for a, _ in init]
             h2d = sum(a.nbytes + b.nbytes for a, b in init)
 
             def e2e_step():
@@ -693,7 +709,8 @@ def run_batch_workload(args, rank, world, local, pg):
             e2e_ms = max_over_ranks(e0.elapsed_time(e1), pg, device)
             e2e = {"value": world * total_sites * T * args.steps / (e2e_ms * 1e-3),
                    "unit": "site-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d,
-                   "path": "ts_b200_set_state x512, ts_b200_batch_evolve, ts_b200_get_sample x512"}
+                   "path": "ts_b200_set_state x512, ts_b200_batch_evolve, ts_b200_get_sample x512, "
+                           "pinned host buffers"}
         sb.close()
         del solvers, sb
         torch.cuda.synchronize()
