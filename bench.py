@@ -1212,6 +1212,39 @@ def run_slab_workload(args, rank, world, local, pg):
     print(json.dumps(line), flush=True)
 
 
+def vortex_cpu_rate(budget_s=10.0):
+    """The reference's CPUBlock (oracle/_ref) on the precision configuration's
+    lattice, trap, coupling and rotating frame, on all host cores, over a
+    bounded number of steps.  The reference refuses periodic boundaries with
+    a rotating frame (src/model.cpp:936-940), so this runs with closed ones;
+    psi0 is the normalised Gaussian of width 3 (the rate does not depend on
+    the state)."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import tsref
+    flavour = "fast" if tsref.available("fast") else ("parity" if tsref.available() else None)
+    if flavour is None:
+        return None
+    threads = os.cpu_count() or 1
+
+    def run(steps):
+        cfg = tsref.make_config(VORTEX_N, VORTEX_LENGTH, gaussian=(1 / 9.0, 1 / 9.0, 0.0, 0.0, 1.0, 0.0),
+                                harmonic=(1.0, 1.0, 1.0, 0.0, 0.0), coupling=VORTEX_G,
+                                angular_velocity=VORTEX_OMEGA, delta_t=VORTEX_DT,
+                                segments=((1, False), (steps, False)), omp_threads=threads)
+        _, res = tsref.run(cfg, None, None, flavour=flavour)
+        return res.seg_seconds[1]
+
+    t = run(1)
+    steps = int(max(1, min(50, budget_s / max(t, 1e-6))))
+    secs = run(steps)
+    return {"value": VORTEX_N * VORTEX_N * steps / secs, "unit": "site-steps/s", "cores": threads,
+            "kind": "reference",
+            "sample": f"{VORTEX_N}x{VORTEX_N}, closed boundaries (the reference refuses periodic "
+                      f"ones with a rotating frame), Omega = {VORTEX_OMEGA}, g = {VORTEX_G}, "
+                      f"{steps} real-time Trotter steps after 1 warm-up step, reference CPUBlock "
+                      f"({'-Ofast' if flavour == 'fast' else '-O2'} build), {threads} OpenMP threads"}
+
+
 def run_vortex_workload(args, rank, world, local, pg):
     import torch
     torch.cuda.set_device(local)
@@ -1220,6 +1253,7 @@ def run_vortex_workload(args, rank, world, local, pg):
     res, clk, launches = vortex_leg(args, local, pg, device, stream, conditioning=True)
     if rank != 0:
         return
+    cpu = None if args.no_cpu_baseline else vortex_cpu_rate(budget_s=args.ref_budget)
     r64 = res["fp64"]["roofline"]
     line = {
         "metric": "site-steps/s", "value": res["fp64"]["value"], "unit": "site-steps/s",
@@ -1239,6 +1273,7 @@ def run_vortex_workload(args, rank, world, local, pg):
                      "algorithmic_bytes_per_launch": r64["algorithmic_bytes_per_launch"],
                      "kernel": "tsb::step2_kernel<double, C=2, real, rotating frame, GPE, 2 rows "
                                "per iteration> (look-ahead walk) + halo"},
+        "cpu_baseline": cpu,
         "clocks": clk,
         "gpu_launches": launches,
     }
