@@ -1031,7 +1031,8 @@ def vortex_leg(args, local, pg, device, stream, conditioning=True, steps=VORTEX_
                      "roofline": {"achieved": ach, "peak": peak, "unit": "GB/s",
                                   "frac": ach / peak, "peak_kind": peak_kind,
                                   "algorithmic_bytes_per_launch": bpl},
-                     "launch": {k: getattr(shape, k) for k, _ in _capi.LaunchShape._fields_}}
+                     "launch": {k: getattr(shape, k) for k, _ in _capi.LaunchShape._fields_},
+                     "clocks": clocks.summary()}
         if prec == "fp64":
             psi64 = psi
             inner = (slice(grid.inner_start_y - grid.start_y, grid.inner_end_y - grid.start_y),
