@@ -21,6 +21,7 @@ CAPTURES = {
     "step_kernel_gpe_imag_2048.md": (2048 * 2048, 40),
     "step_kernel_gpe_imag_2048_fp32.md": (2048 * 2048, 20),
     "step_kernel_rotating_frame_4096.md": (4112 * 4112, 48),
+    "step_kernel_rotating_frame_4096_fp32.md": (4112 * 4112, 24),
     "step_kernel_two_component_2048.md": (2048 * 2048, 64),
     "step_kernel_cylindrical_2048.md": (2049 * 2048, 40),
     "step_kernel_moving_trap_2048.md": (2048 * 2048, 40),
